@@ -1,0 +1,194 @@
+/*
+ * slsf_gpu.h -- C ABI of the B200 (sm_100a) update-and-measure library for
+ * the 3D layered-disorder XY model of SLSF-rs.
+ *
+ * The reference is a Rust crate whose hot path sits behind the carlo-mc
+ * `MonteCarlo` trait implemented by `ThetaModel` (src/model.rs:308-477) and
+ * behind the re-exported lower-level functions of src/lib.rs:21-29.  It has no
+ * FFI of its own; every entry point below is the `extern "C"` function a Rust
+ * `GpuThetaModel` would bind in place of one of those calls, and its comment
+ * cites the reference item it replaces.
+ *
+ * Conventions
+ *   - Every function returns an int status: SLSF_OK (0) or an SLSF_ERR_*
+ *     code.  slsf_last_error() copies the calling thread's last message; for
+ *     argument errors that message is the reference's string, character for
+ *     character (src/types.rs:120-129, :373-385, src/updates.rs:430-438,
+ *     src/model.rs:318-348).
+ *   - Handles are single-owner: one host thread issues all calls on a context
+ *     and its tasks, as carlo-mc's Runner does (src/results.rs:200-202).
+ *   - Angles cross the boundary as FP32 (the device state).  J arrays cross
+ *     as FP64, as in ThetaTask (src/model.rs:45-46), and are stored as FP32.
+ *   - Randoms are Philox4x32-10 keyed by (seed, sweep counter, purpose,
+ *     site); a task's trajectory depends only on its seed, counters and state,
+ *     never on what else runs on the device.
+ *   - There is no CPU fallback: without a usable CUDA device every compute
+ *     entry point fails with SLSF_ERR_CUDA.
+ */
+#ifndef SLSF_GPU_H
+#define SLSF_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SLSF_OK 0
+#define SLSF_ERR_INVALID 1 /* argument rejected; message is the reference's string */
+#define SLSF_ERR_CUDA 2    /* CUDA runtime or device error, or no device */
+#define SLSF_ERR_BUDGET 3  /* allocation would exceed the context's HBM budget */
+#define SLSF_ERR_TIMEOUT 4 /* a bounded device loop hit its iteration limit */
+#define SLSF_ERR_STATE 5   /* call not valid in the handle's current state */
+
+typedef struct slsf_ctx slsf_ctx;
+typedef struct slsf_task slsf_task;
+
+/* Task parameters: the fields of ThetaTask (src/model.rs:20-47) that the
+ * update-and-measure step reads.  j_xy / j_z are the explicit per-layer
+ * arrays (ThetaTask::j_xy_array / j_z_array); the two-point disorder
+ * generator stays on the host. */
+typedef struct slsf_task_desc {
+    uint32_t lx, ly, lz;
+    double temperature;
+    double proposal_width;
+    uint32_t wolff_steps;
+    uint64_t seed;
+    const double* j_xy;
+    size_t n_j_xy;
+    const double* j_z;
+    size_t n_j_z;
+    /* Measurement plan of the batched engine: sweeps before the first
+     * measurement, measurements per bin, and the number of bins to keep. */
+    uint32_t thermalization;
+    uint32_t binsize;
+    uint32_t n_bins;
+} slsf_task_desc;
+
+/* ThetaObservables (src/types.rs:253-263). */
+typedef struct slsf_observables {
+    double energy;
+    double magnetization_squared;
+    double cos_x, cos_y, cos_z;
+    double sin_x, sin_y, sin_z;
+} slsf_observables;
+
+/* Counters accumulated over the sweeps of one call. */
+typedef struct slsf_sweep_stats {
+    uint64_t sweeps;
+    uint64_t accepted;            /* Metropolis acceptances (sum over sweeps) */
+    uint64_t wolff_clusters;      /* Wolff steps performed */
+    uint64_t wolff_cluster_sites; /* sum of cluster sizes */
+} slsf_sweep_stats;
+
+/* Columns of one measurement in the per-task bin accumulators: the
+ * observable stream of ThetaModel::measure (src/model.rs:406-409) and
+ * measure_theta_helicity (src/model.rs:890-904). */
+#define SLSF_BIN_COLS 12 /* Energy, EnergySquared, MagnetizationSquared,
+                            cos_x, cos_y, cos_z, sin_x, sin_y, sin_z,
+                            sin2_x, sin2_y, sin2_z */
+
+/* ---------------------------------------------------------------- library */
+
+/* Copies the calling thread's last error message (NUL-terminated, truncated
+ * to len) and returns its full length. */
+size_t slsf_last_error(char* buf, size_t len);
+
+/* Library version string. */
+const char* slsf_version(void);
+
+/* Creates a context on CUDA device `device` that may allocate up to
+ * `budget_bytes` of device memory (0 = 90% of the device's free memory).
+ * No reference counterpart: carlo-mc owns no device. */
+int slsf_ctx_create(int device, uint64_t budget_bytes, uint32_t flags, slsf_ctx** out);
+int slsf_ctx_destroy(slsf_ctx* ctx);
+/* Device bytes in use by the context's tasks, and its budget. */
+int slsf_ctx_memory(const slsf_ctx* ctx, uint64_t* used, uint64_t* budget);
+/* Device bytes a task of these dimensions and measurement plan would take. */
+uint64_t slsf_task_bytes(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t n_bins);
+
+/* ---------------------------------------------------------------- one task */
+
+/* Replaces ThetaModel::new (src/model.rs:314-371): validates the lattice
+ * dimensions (src/types.rs:120-129), the J array lengths and signs
+ * (src/model.rs:318-348), allocates the device state and uploads J.  Like the
+ * reference, T and proposal_width are checked when a sweep runs. */
+int slsf_task_create(slsf_ctx* ctx, const slsf_task_desc* desc, slsf_task** out);
+int slsf_task_destroy(slsf_task* task);
+
+/* Replaces ThetaModel::init (src/model.rs:373-377): theta_i = 2 pi u_i with
+ * u_i from the task's Philox stream (purpose INIT). */
+int slsf_task_init_random(slsf_task* task);
+/* InitMode::Cold (src/initialization.rs:58): all angles 0. */
+int slsf_task_init_cold(slsf_task* task);
+/* ThetaLattice::theta as FP32, index x + Lx (y + Ly z) (src/types.rs:146-149). */
+int slsf_task_set_angles(slsf_task* task, const float* theta, size_t n);
+int slsf_task_get_angles(slsf_task* task, float* theta, size_t n);
+
+/* Checkpoint counters: Metropolis sweeps and Wolff steps done so far.  With
+ * the angles they are the whole random state (the serde FastRng position of
+ * src/types.rs:9-37 has no other counterpart). */
+int slsf_task_get_counters(const slsf_task* task, uint64_t* metro_sweeps, uint64_t* wolff_steps);
+int slsf_task_set_counters(slsf_task* task, uint64_t metro_sweeps, uint64_t wolff_steps);
+
+/* Replaces ThetaModel::sweep (src/model.rs:379-400) n_sweeps times: one
+ * checkerboard Metropolis sweep then wolff_steps Wolff updates per sweep.
+ * stats may be NULL. */
+int slsf_task_sweep(slsf_task* task, uint32_t n_sweeps, slsf_sweep_stats* stats);
+
+/* Replaces metropolis_sweep_with_scratch (src/updates.rs:440-486): returns
+ * accepted / V. */
+int slsf_task_metropolis_sweep(slsf_task* task, double* acceptance);
+
+/* One colour of the checkerboard sweep (the parity loop body of
+ * src/updates.rs:455-483) without advancing the sweep counter.  When
+ * accept_mask is not NULL it receives one byte per site: 1 if the site was
+ * updated and accepted, 0 otherwise.  accepted may be NULL. */
+int slsf_task_metropolis_color(slsf_task* task, uint32_t color, uint8_t* accept_mask,
+                               uint64_t* accepted);
+
+/* Replaces wolff_cluster_step_with_theta_scratch (src/updates.rs:551-620):
+ * bond activation, cluster labelling from the seed site, reflection.
+ * cluster_size may be NULL. */
+int slsf_task_wolff_step(slsf_task* task, uint64_t* cluster_size);
+
+/* A Wolff step that also exports, per site, the active-bond bits (bit 0/1/2
+ * = bond to +x/+y/+z) and the cluster membership, plus the reflection axis
+ * and seed site it used.  Any output pointer may be NULL. */
+int slsf_task_wolff_step_debug(slsf_task* task, uint8_t* bonds, uint8_t* cluster, float* phi,
+                               uint32_t seed_site[3], uint64_t* cluster_size);
+
+/* Replaces measure_theta_observables_with_scratch (src/observables.rs:80-154):
+ * one fused pass; per-site terms in FP32, sums in FP64. */
+int slsf_task_measure(slsf_task* task, slsf_observables* out);
+
+/* Replaces measure_theta_correlations_with_scratch (src/observables.rs:166-265)
+ * for explicit rmax values (clamped to L/2 as at :177-181).  Outputs (any may
+ * be NULL): corr_x, corr_y, corr_xy [rmax_xy], corr_xy_by_z [lz][rmax_xy],
+ * corr_z [rmax_z]. */
+int slsf_task_correlations(slsf_task* task, uint32_t rmax_xy, uint32_t rmax_z, double* corr_x,
+                           double* corr_y, double* corr_xy, double* corr_xy_by_z,
+                           double* corr_z);
+
+/* Per-task bin accumulators of the batched engine: n_bins rows of
+ * SLSF_BIN_COLS bin means, and the number of measurements taken so far. */
+int slsf_task_get_bins(const slsf_task* task, double* bins, size_t n_rows, uint64_t* measurements);
+int slsf_task_reset_bins(slsf_task* task);
+
+/* ---------------------------------------------------------------- batches */
+
+/* Runs n_sweeps sweeps of every task in `tasks` in one persistent launch
+ * (the carlo-mc Runner's per-task loop of src/results.rs:200-202, batched):
+ * each sweep is ThetaModel::sweep followed, once the task's thermalization
+ * is done, by ThetaModel::measure accumulated into the task's bins.  Tasks
+ * may have different sizes.  stats (one per task) may be NULL.  Blocks until
+ * the work is done. */
+int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n_tasks, uint32_t n_sweeps,
+                   slsf_sweep_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SLSF_GPU_H */

@@ -1,0 +1,305 @@
+"""Python binding of the slsf-b200 C ABI (include/slsf_gpu.h).
+
+The CUDA library `libslsf_b200.so` is built in-tree by `build()` (nvcc,
+sm_100a).  This module only marshals arguments; every computation runs in the
+library on the GPU.  There is no CPU fallback: loading fails loudly when the
+library is missing, and context creation fails when there is no CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libslsf_b200.so")
+HEADER = os.path.join(ROOT, "include", "slsf_gpu.h")
+
+OK, ERR_INVALID, ERR_CUDA, ERR_BUDGET, ERR_TIMEOUT, ERR_STATE = range(6)
+OBS_FIELDS = ("energy", "magnetization_squared", "cos_x", "cos_y", "cos_z", "sin_x", "sin_y", "sin_z")
+BIN_COLS = 12
+BIN_NAMES = ("Energy", "EnergySquared", "MagnetizationSquared", "_helicity_cos_x", "_helicity_cos_y",
+             "_helicity_cos_z", "_helicity_sin_x", "_helicity_sin_y", "_helicity_sin_z", "_helicity_sin2_x",
+             "_helicity_sin2_y", "_helicity_sin2_z")
+
+
+class SlsfError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(message)
+        self.code = code
+
+
+class TaskDesc(C.Structure):
+    _fields_ = [
+        ("lx", C.c_uint32), ("ly", C.c_uint32), ("lz", C.c_uint32),
+        ("temperature", C.c_double), ("proposal_width", C.c_double),
+        ("wolff_steps", C.c_uint32), ("seed", C.c_uint64),
+        ("j_xy", C.POINTER(C.c_double)), ("n_j_xy", C.c_size_t),
+        ("j_z", C.POINTER(C.c_double)), ("n_j_z", C.c_size_t),
+        ("thermalization", C.c_uint32), ("binsize", C.c_uint32), ("n_bins", C.c_uint32),
+    ]
+
+
+class Observables(C.Structure):
+    _fields_ = [(n, C.c_double) for n in OBS_FIELDS]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n in OBS_FIELDS}
+
+
+class SweepStats(C.Structure):
+    _fields_ = [("sweeps", C.c_uint64), ("accepted", C.c_uint64), ("wolff_clusters", C.c_uint64),
+                ("wolff_cluster_sites", C.c_uint64)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+def build(force: bool = False) -> str:
+    """Compile the library with nvcc for sm_100a (works without a GPU)."""
+    if force:
+        subprocess.run(["make", "-s", "-C", HERE, "clean"], check=True)
+    subprocess.run(["make", "-s", "-j8", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_P = C.c_void_p
+_U8P = C.POINTER(C.c_uint8)
+_F32P = C.POINTER(C.c_float)
+_F64P = C.POINTER(C.c_double)
+_U32P = C.POINTER(C.c_uint32)
+_U64P = C.POINTER(C.c_uint64)
+
+SIGNATURES = {
+    "slsf_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "slsf_version": (C.c_char_p, []),
+    "slsf_ctx_create": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, C.POINTER(_P)]),
+    "slsf_ctx_destroy": (C.c_int, [_P]),
+    "slsf_ctx_memory": (C.c_int, [_P, _U64P, _U64P]),
+    "slsf_task_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]),
+    "slsf_task_create": (C.c_int, [_P, C.POINTER(TaskDesc), C.POINTER(_P)]),
+    "slsf_task_destroy": (C.c_int, [_P]),
+    "slsf_task_init_random": (C.c_int, [_P]),
+    "slsf_task_init_cold": (C.c_int, [_P]),
+    "slsf_task_set_angles": (C.c_int, [_P, _F32P, C.c_size_t]),
+    "slsf_task_get_angles": (C.c_int, [_P, _F32P, C.c_size_t]),
+    "slsf_task_get_counters": (C.c_int, [_P, _U64P, _U64P]),
+    "slsf_task_set_counters": (C.c_int, [_P, C.c_uint64, C.c_uint64]),
+    "slsf_task_sweep": (C.c_int, [_P, C.c_uint32, C.POINTER(SweepStats)]),
+    "slsf_task_metropolis_sweep": (C.c_int, [_P, _F64P]),
+    "slsf_task_metropolis_color": (C.c_int, [_P, C.c_uint32, _U8P, _U64P]),
+    "slsf_task_wolff_step": (C.c_int, [_P, _U64P]),
+    "slsf_task_wolff_step_debug": (C.c_int, [_P, _U8P, _U8P, _F32P, _U32P, _U64P]),
+    "slsf_task_measure": (C.c_int, [_P, C.POINTER(Observables)]),
+    "slsf_task_correlations": (C.c_int, [_P, C.c_uint32, C.c_uint32, _F64P, _F64P, _F64P, _F64P, _F64P]),
+    "slsf_task_get_bins": (C.c_int, [_P, _F64P, C.c_size_t, _U64P]),
+    "slsf_task_reset_bins": (C.c_int, [_P]),
+    "slsf_batch_run": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_uint32, C.POINTER(SweepStats)]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the in-tree library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run build() (nvcc, sm_100a) first")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    load().slsf_last_error(buf, len(buf))
+    return buf.value.decode("utf-8")
+
+
+def check(code):
+    if code != OK:
+        raise SlsfError(code, last_error())
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class Context:
+    """A device context (slsf_ctx_create)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0):
+        import weakref
+
+        h = _P()
+        check(load().slsf_ctx_create(device, budget_bytes, 0, C.byref(h)))
+        self.h = h
+        self._tasks = weakref.WeakSet()
+
+    def close(self):
+        """Destroy every live task of this context, then the context."""
+        if getattr(self, "h", None):
+            for t in list(self._tasks):
+                t.close()
+            check(load().slsf_ctx_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def memory(self):
+        used, budget = C.c_uint64(), C.c_uint64()
+        check(load().slsf_ctx_memory(self.h, C.byref(used), C.byref(budget)))
+        return used.value, budget.value
+
+    def batch_run(self, tasks, n_sweeps):
+        arr = (_P * len(tasks))(*[t.h for t in tasks])
+        stats = (SweepStats * len(tasks))()
+        check(load().slsf_batch_run(self.h, arr, len(tasks), n_sweeps, stats))
+        return [s.as_dict() for s in stats]
+
+
+class Task:
+    """One task (slsf_task_create): the device state of a ThetaModel."""
+
+    def __init__(self, ctx: Context, dims, j_xy, j_z, temperature, proposal_width=np.pi, wolff_steps=1, seed=0,
+                 thermalization=0, binsize=1, n_bins=0):
+        lx, ly, lz = dims
+        self.dims = (lx, ly, lz)
+        self.volume = lx * ly * lz
+        self._jxy = np.ascontiguousarray(j_xy, dtype=np.float64)
+        self._jz = np.ascontiguousarray(j_z, dtype=np.float64)
+        d = TaskDesc(lx=lx, ly=ly, lz=lz, temperature=temperature, proposal_width=proposal_width,
+                     wolff_steps=wolff_steps, seed=seed, j_xy=_ptr(self._jxy, C.c_double), n_j_xy=self._jxy.size,
+                     j_z=_ptr(self._jz, C.c_double), n_j_z=self._jz.size, thermalization=thermalization,
+                     binsize=binsize, n_bins=n_bins)
+        if not getattr(ctx, "h", None):
+            raise SlsfError(ERR_STATE, "context is closed")
+        h = _P()
+        check(load().slsf_task_create(ctx.h, C.byref(d), C.byref(h)))
+        self.h = h
+        self.ctx = ctx
+        self.n_bins = n_bins
+        ctx._tasks.add(self)
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().slsf_task_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init_random(self):
+        check(load().slsf_task_init_random(self.h))
+
+    def init_cold(self):
+        check(load().slsf_task_init_cold(self.h))
+
+    @property
+    def theta(self):
+        out = np.empty(self.volume, dtype=np.float32)
+        check(load().slsf_task_get_angles(self.h, _ptr(out, C.c_float), out.size))
+        return out
+
+    @theta.setter
+    def theta(self, values):
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        check(load().slsf_task_set_angles(self.h, _ptr(v, C.c_float), v.size))
+
+    @property
+    def counters(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        check(load().slsf_task_get_counters(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    @counters.setter
+    def counters(self, value):
+        check(load().slsf_task_set_counters(self.h, value[0], value[1]))
+
+    def sweep(self, n=1):
+        st = SweepStats()
+        check(load().slsf_task_sweep(self.h, n, C.byref(st)))
+        return st.as_dict()
+
+    def metropolis_sweep(self):
+        acc = C.c_double()
+        check(load().slsf_task_metropolis_sweep(self.h, C.byref(acc)))
+        return acc.value
+
+    def metropolis_color(self, colour, record=True):
+        acc = C.c_uint64()
+        mask = np.zeros(self.volume, dtype=np.uint8) if record else None
+        check(load().slsf_task_metropolis_color(self.h, colour, _ptr(mask, C.c_uint8) if record else None,
+                                                C.byref(acc)))
+        return acc.value, mask
+
+    def wolff_step(self):
+        n = C.c_uint64()
+        check(load().slsf_task_wolff_step(self.h, C.byref(n)))
+        return n.value
+
+    def wolff_step_debug(self):
+        bonds = np.zeros(self.volume, dtype=np.uint8)
+        cluster = np.zeros(self.volume, dtype=np.uint8)
+        phi = C.c_float()
+        site = (C.c_uint32 * 3)()
+        n = C.c_uint64()
+        check(load().slsf_task_wolff_step_debug(self.h, _ptr(bonds, C.c_uint8), _ptr(cluster, C.c_uint8),
+                                                C.byref(phi), site, C.byref(n)))
+        return {"bonds": bonds, "cluster": cluster, "phi": phi.value, "seed_site": tuple(site), "size": n.value}
+
+    def measure(self):
+        o = Observables()
+        check(load().slsf_task_measure(self.h, C.byref(o)))
+        return o.as_dict()
+
+    def correlations(self, rmax_xy, rmax_z):
+        lx, ly, lz = self.dims
+        rxy = min(rmax_xy, lx // 2, ly // 2)
+        rz = min(rmax_z, lz // 2)
+        cx, cy, cxy = np.zeros(max(rxy, 1)), np.zeros(max(rxy, 1)), np.zeros(max(rxy, 1))
+        cbz, cz = np.zeros(max(lz * rxy, 1)), np.zeros(max(rz, 1))
+        f = lambda a: _ptr(a, C.c_double)
+        check(load().slsf_task_correlations(self.h, rmax_xy, rmax_z, f(cx), f(cy), f(cxy), f(cbz), f(cz)))
+        return {"corr_x": cx[:rxy], "corr_y": cy[:rxy], "corr_xy": cxy[:rxy],
+                "corr_xy_by_z": cbz[: lz * rxy].reshape(lz, rxy), "corr_z": cz[:rz]}
+
+    def bins(self):
+        out = np.zeros((max(self.n_bins, 1), BIN_COLS))
+        m = C.c_uint64()
+        check(load().slsf_task_get_bins(self.h, _ptr(out, C.c_double), self.n_bins, C.byref(m)))
+        return out[: self.n_bins], m.value
+
+    def reset_bins(self):
+        check(load().slsf_task_reset_bins(self.h))
+
+
+def exported_symbols():
+    """Function names declared in include/slsf_gpu.h."""
+    import re
+
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(slsf_[a-z_0-9]+)\s*\(", text)))

@@ -1,0 +1,77 @@
+/*
+ * Internal interface between the C ABI (capi.cu) and the kernel files.
+ * Nothing here is exported from the shared library.
+ */
+#ifndef SLSF_ENGINE_H
+#define SLSF_ENGINE_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace slsf {
+
+/* Device-side counters of one task. */
+enum StatSlot : int {
+    kStatAccepted = 0,     /* Metropolis acceptances */
+    kStatClusterSites = 1, /* sum of Wolff cluster sizes */
+    kStatClusters = 2,     /* Wolff steps */
+    kStatError = 3,        /* nonzero: a bounded device loop gave up */
+    kStatSlots = 4
+};
+
+/* Error bits written to stats[kStatError]. */
+constexpr unsigned long long kErrUnionFindLimit = 1ull;
+constexpr unsigned long long kErrQueueLimit = 2ull;
+
+constexpr int kBinCols = 12;
+
+/* Everything a kernel needs to know about one task. */
+struct TaskView {
+    float* theta;
+    const float* jxy;
+    const float* jz;
+    uint32_t lx, ly, lz;
+    float beta;
+    float width;
+    uint32_t wolff_steps;
+    uint64_t seed;
+    uint64_t metro_sweeps; /* Metropolis sweeps done before this launch */
+    uint64_t wolff_done;   /* Wolff steps done before this launch */
+    double* bins;          /* [n_bins][kBinCols] sums */
+    uint32_t thermalization, binsize, n_bins;
+    unsigned long long* stats;
+};
+
+/* ---- single-task kernels (kernels_plain.cu) ---- */
+void launch_init_random(float* theta, uint32_t volume, uint64_t seed, cudaStream_t s);
+void launch_metro_colour(const TaskView& t, uint64_t sweep, uint32_t colour, uint8_t* record,
+                         cudaStream_t s);
+void launch_wolff(const TaskView& t, uint64_t wolff_counter, uint8_t* bonds, uint32_t* parent,
+                  uint8_t* cluster_out, cudaStream_t s, float* phi_out, uint32_t seed_site[3]);
+/* Fused observables: writes 8 FP64 sums (mx, my, cos xyz, sin xyz) to result. */
+void launch_measure(const TaskView& t, double* partials, unsigned int* done, double* result,
+                    cudaStream_t s);
+int measure_partial_blocks(uint32_t volume);
+/* Correlation sums: sx[lz][rmax_xy], sy[lz][rmax_xy], sz[rmax_z] (FP64). */
+void launch_correlations(const TaskView& t, uint32_t rmax_xy, uint32_t rmax_z, double* work,
+                         size_t work_doubles, double* sx, double* sy, double* sz,
+                         cudaStream_t s);
+size_t correlation_work_doubles(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rmax_xy,
+                                uint32_t rmax_z);
+
+/* ---- batched persistent engine (kernel_batched.cu) ---- */
+struct BatchLimits {
+    uint32_t max_volume; /* largest replica the shared-memory kernel holds */
+};
+BatchLimits batched_limits(int device);
+bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);
+/* Runs n_sweeps sweeps of every task view in `views` (device array of n)
+ * with a persistent grid; `queue` is a device counter the kernel consumes.
+ * max_* are the largest volume, row count (Ly Lz) and Lz over the views. */
+cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps,
+                           unsigned int* queue, int device, cudaStream_t s, uint32_t max_volume,
+                           uint32_t max_rows, uint32_t max_lz);
+
+}  // namespace slsf
+
+#endif /* SLSF_ENGINE_H */

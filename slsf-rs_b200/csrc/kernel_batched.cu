@@ -1,0 +1,508 @@
+/*
+ * Batched persistent kernel: many replicas of uneven size, one CTA per
+ * replica at a time, each replica resident in shared memory for all of its
+ * sweeps.  Replaces the carlo-mc Runner's task-by-task loop over
+ * ThetaModel::sweep + ThetaModel::measure (src/model.rs:379-442,
+ * src/results.rs:200-202) for every task of a batch at once.
+ *
+ * Per replica the CTA
+ *   1. copies theta from HBM into a colour-split shared layout
+ *      (colour c site with index idx at c * (V/2 + 16) + idx/2): every warp
+ *      access to one colour is to consecutive words, and the 16-word pad puts
+ *      the two colours of neighbouring sites in different banks;
+ *   2. per sweep: two colour half-sweeps (the same decision code as the
+ *      single-task kernel, xy_device.cuh), `wolff_steps` Wolff updates, and,
+ *      after thermalization, the fused measurement added to the task's bins;
+ *   3. copies theta back.
+ * HBM traffic is 8 bytes per site per launch, independent of the sweep count.
+ *
+ * Wolff labelling is bit-parallel: the active +x/+y/+z bonds of a row of
+ * L_x <= 32 sites are three 32-bit words, and the cluster grows from the seed
+ * by OR-ing neighbour rows through the bond words and closing each row along
+ * x, until a whole pass changes nothing.  The result is the seed's connected
+ * component over the active bonds, which is the set the reference's DFS
+ * (src/updates.rs:577-597) collects when fed the same per-bond randoms.
+ * Growth is monotone, so the pass count is bounded by V.
+ */
+#include <algorithm>
+
+#include "engine.h"
+#include "fastdiv.h"
+#include "xy_device.cuh"
+
+namespace slsf {
+
+namespace {
+
+constexpr int kBThreads = 1024;
+constexpr uint32_t kPad = 16;
+constexpr uint32_t kMaxRowBits = 32;
+
+struct Geo {
+    uint32_t lx, ly, lz, volume, half, rows, plane;
+    uint32_t stride1; /* offset of the colour-1 array */
+    uint32_t xmask;
+    bool lx_divides_warp;
+    slsf_fastdiv div_hx, div_ly, div_lx;
+};
+
+__device__ __forceinline__ Geo make_geo(const TaskView& t) {
+    Geo g;
+    g.lx = t.lx;
+    g.ly = t.ly;
+    g.lz = t.lz;
+    g.plane = t.lx * t.ly;
+    g.volume = g.plane * t.lz;
+    g.half = g.volume >> 1;
+    g.rows = t.ly * t.lz;
+    g.stride1 = g.half + kPad;
+    g.xmask = t.lx >= 32 ? 0xffffffffu : ((1u << t.lx) - 1u);
+    g.lx_divides_warp = (32u % t.lx) == 0;
+    g.div_hx = slsf_fastdiv_make(t.lx >> 1);
+    g.div_ly = slsf_fastdiv_make(t.ly);
+    g.div_lx = slsf_fastdiv_make(t.lx);
+    return g;
+}
+
+/* Shared-memory slot of natural site index idx with colour c. */
+__device__ __forceinline__ uint32_t slot(const Geo& g, uint32_t idx, uint32_t colour) {
+    return colour * g.stride1 + (idx >> 1);
+}
+
+struct Coords {
+    uint32_t x, y, z, row;
+};
+
+__device__ __forceinline__ Coords coords_of(const Geo& g, uint32_t idx) {
+    Coords c;
+    c.row = slsf_fastdiv_div(idx, g.div_lx);
+    c.x = idx - c.row * g.lx;
+    c.z = slsf_fastdiv_div(c.row, g.div_ly);
+    c.y = c.row - c.z * g.ly;
+    return c;
+}
+
+/* Forward neighbours of a site (+x, +y, +z) as natural indices. */
+__device__ __forceinline__ void forward_neighbours(const Geo& g, uint32_t idx, const Coords& c,
+                                                   uint32_t& xp, uint32_t& yp, uint32_t& zp) {
+    xp = (c.x + 1 == g.lx) ? idx + 1 - g.lx : idx + 1;
+    yp = (c.y + 1 == g.ly) ? idx + g.lx - g.plane : idx + g.lx;
+    zp = (c.z + 1 == g.lz) ? idx + g.plane - g.volume : idx + g.plane;
+}
+
+/* Lane holding the +x neighbour when rows of lx sites tile the warp. */
+__device__ __forceinline__ uint32_t xp_lane(uint32_t lane, uint32_t lx) {
+    return (lane & ~(lx - 1u)) | ((lane + 1u) & (lx - 1u));
+}
+
+__device__ __forceinline__ uint32_t rotl_row(uint32_t w, uint32_t lx, uint32_t mask) {
+    return lx >= 32 ? __funnelshift_l(w, w, 1) : (((w << 1) | (w >> (lx - 1u))) & mask);
+}
+
+__device__ __forceinline__ uint32_t rotr_row(uint32_t w, uint32_t lx, uint32_t mask) {
+    return lx >= 32 ? __funnelshift_r(w, w, 1) : (((w >> 1) | (w << (lx - 1u))) & mask);
+}
+
+/* Closure of a row's cluster bits along x through the +x bond bits. */
+__device__ __forceinline__ uint32_t close_row(uint32_t c, uint32_t bx, uint32_t lx, uint32_t mask) {
+    for (uint32_t it = 0; it < lx; ++it) {
+        const uint32_t n = c | rotl_row(c & bx, lx, mask) | (rotr_row(c, lx, mask) & bx);
+        if (n == c) break;
+        c = n;
+    }
+    return c;
+}
+
+struct Smem {
+    float* th;  /* two colour arrays */
+    uint32_t* bx;
+    uint32_t* by;
+    uint32_t* bz;
+    uint32_t* cl;
+    float* jxy;
+    float* jz;
+};
+
+__device__ __forceinline__ Smem carve(unsigned char* base, const Geo& g, uint32_t max_volume,
+                                      uint32_t max_rows, uint32_t max_lz) {
+    Smem s;
+    s.th = reinterpret_cast<float*>(base);
+    uint32_t* w = reinterpret_cast<uint32_t*>(base + 4ull * (max_volume + 2 * kPad));
+    s.bx = w;
+    s.by = w + max_rows;
+    s.bz = w + 2 * max_rows;
+    s.cl = w + 3 * max_rows;
+    s.jxy = reinterpret_cast<float*>(w + 4 * max_rows);
+    s.jz = s.jxy + max_lz;
+    (void)g;
+    return s;
+}
+
+/* ---- phases ---- */
+
+__device__ __forceinline__ void load_state(const TaskView& t, const Geo& g, Smem& s) {
+    const float4* src = reinterpret_cast<const float4*>(t.theta);
+    for (uint32_t q = threadIdx.x; q < g.volume / 4; q += blockDim.x) {
+        const float4 v = src[q];
+        const uint32_t idx = 4 * q;
+        const Coords c = coords_of(g, idx);
+        const uint32_t p = (c.y + c.z) & 1u; /* colour of the even-x site */
+        const uint32_t h = 2 * q;
+        s.th[p * g.stride1 + h] = v.x;
+        s.th[(p ^ 1u) * g.stride1 + h] = v.y;
+        s.th[p * g.stride1 + h + 1] = v.z;
+        s.th[(p ^ 1u) * g.stride1 + h + 1] = v.w;
+    }
+    for (uint32_t z = threadIdx.x; z < g.lz; z += blockDim.x) {
+        s.jxy[z] = t.jxy[z];
+        s.jz[z] = t.jz[z];
+    }
+}
+
+__device__ __forceinline__ void store_state(const TaskView& t, const Geo& g, const Smem& s) {
+    float4* dst = reinterpret_cast<float4*>(t.theta);
+    for (uint32_t q = threadIdx.x; q < g.volume / 4; q += blockDim.x) {
+        const uint32_t idx = 4 * q;
+        const Coords c = coords_of(g, idx);
+        const uint32_t p = (c.y + c.z) & 1u;
+        const uint32_t h = 2 * q;
+        float4 v;
+        v.x = s.th[p * g.stride1 + h];
+        v.y = s.th[(p ^ 1u) * g.stride1 + h];
+        v.z = s.th[p * g.stride1 + h + 1];
+        v.w = s.th[(p ^ 1u) * g.stride1 + h + 1];
+        dst[q] = v;
+    }
+}
+
+/* One colour half-sweep.  A warp owns 32 consecutive Philox blocks (64
+ * sites); lanes exchange words so that lane j updates colour-compact sites
+ * 2*base + j and 2*base + 32 + j, i.e. consecutive shared words. */
+__device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, Smem& s,
+                                               uint64_t sweep, uint32_t colour) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t nwarps = blockDim.x >> 5;
+    const uint32_t npairs = (g.half + 1) >> 1;
+    const uint32_t own = colour * g.stride1, other = (colour ^ 1u) * g.stride1;
+    uint32_t accepted = 0;
+    for (uint32_t base = warp * 32; base < npairs; base += nwarps * 32) {
+        const uint32_t p = base + lane;
+        slsf_u32x4 blk = {0, 0, 0, 0};
+        if (p < npairs) blk = slsf_stream(t.seed, sweep, SLSF_PURPOSE_METRO, colour, p);
+#pragma unroll
+        for (uint32_t r = 0; r < 2; ++r) {
+            const uint32_t src = 16 * r + (lane >> 1);
+            const uint32_t wx = __shfl_sync(0xffffffffu, blk.x, src);
+            const uint32_t wy = __shfl_sync(0xffffffffu, blk.y, src);
+            const uint32_t wz = __shfl_sync(0xffffffffu, blk.z, src);
+            const uint32_t ww = __shfl_sync(0xffffffffu, blk.w, src);
+            const uint32_t h = 2 * base + 32 * r + lane;
+            if (h >= g.half) continue;
+            const float u_prop = slsf_u24f((lane & 1u) ? wz : wx);
+            const float u_acc = slsf_u24f((lane & 1u) ? ww : wy);
+            /* decode the colour-compact index */
+            const uint32_t row = slsf_fastdiv_div(h, g.div_hx);
+            const uint32_t k = h - row * (g.lx >> 1);
+            const uint32_t z = slsf_fastdiv_div(row, g.div_ly);
+            const uint32_t y = row - z * g.ly;
+            SiteXYZ st;
+            st.x = 2u * k + ((colour + y + z) & 1u);
+            st.y = y;
+            st.z = z;
+            st.idx = st.x + g.lx * row;
+            uint32_t nb[6];
+            neighbour_indices(st, g.lx, g.ly, g.lz, nb);
+            float ns[6], nc[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) __sincosf(s.th[other + (nb[q] >> 1)], &ns[q], &nc[q]);
+            const float jx = s.jxy[z], jzp = s.jz[z], jzm = s.jz[z == 0 ? g.lz - 1 : z - 1];
+            const float hx = field_component(jx, jzp, jzm, nc[0], nc[1], nc[2], nc[3], nc[4], nc[5]);
+            const float hy = field_component(jx, jzp, jzm, ns[0], ns[1], ns[2], ns[3], ns[4], ns[5]);
+            const float th = s.th[own + h];
+            float si, ci;
+            __sincosf(th, &si, &ci);
+            float tn, sn, cn;
+            if (metro_decide(th, ci, si, hx, hy, t.beta, t.width, u_prop, u_acc, &tn, &sn, &cn)) {
+                s.th[own + h] = tn;
+                ++accepted;
+            }
+        }
+    }
+    return accepted;
+}
+
+__device__ __forceinline__ float site_theta(const Geo& g, const Smem& s, uint32_t idx, const Coords& c) {
+    return s.th[slot(g, idx, (c.x + c.y + c.z) & 1u)];
+}
+
+/* One Wolff update; returns the cluster size (valid in every thread). */
+__device__ __forceinline__ uint32_t wolff_update(const TaskView& t, const Geo& g, Smem& s,
+                                                 uint64_t counter, uint32_t* s_count) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const slsf_u32x4 pick = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_PICK, 0, 0);
+    const float phi = slsf_angle_from_word(pick.x);
+    const uint32_t x0 = slsf_range(pick.y, g.lx), y0 = slsf_range(pick.z, g.ly), z0 = slsf_range(pick.w, g.lz);
+    const float m2b = __fmul_rn(-2.0f, t.beta);
+
+    if (!g.lx_divides_warp) {
+        for (uint32_t r = threadIdx.x; r < g.rows; r += blockDim.x) {
+            s.bx[r] = 0;
+            s.by[r] = 0;
+            s.bz[r] = 0;
+        }
+        __syncthreads();
+    }
+    /* Bond activation, one thread per site, warp-aligned site ranges. */
+    for (uint32_t i0 = (threadIdx.x & ~31u); i0 < g.volume; i0 += blockDim.x) {
+        const uint32_t idx = i0 + lane;
+        const bool valid = idx < g.volume;
+        const uint32_t ii = valid ? idx : 0;
+        const Coords c = coords_of(g, ii);
+        uint32_t xp, yp, zp;
+        forward_neighbours(g, ii, c, xp, yp, zp);
+        const float ri = wolff_projection(site_theta(g, s, ii, c), phi);
+        float rxp;
+        if (g.lx_divides_warp) {
+            rxp = __shfl_sync(0xffffffffu, ri, xp_lane(lane, g.lx));
+        } else {
+            const Coords cx = {c.x + 1 == g.lx ? 0 : c.x + 1, c.y, c.z, c.row};
+            rxp = wolff_projection(site_theta(g, s, xp, cx), phi);
+        }
+        const Coords cy = {c.x, c.y + 1 == g.ly ? 0 : c.y + 1, c.z, 0};
+        const Coords cz = {c.x, c.y, c.z + 1 == g.lz ? 0 : c.z + 1, 0};
+        const float ryp = wolff_projection(site_theta(g, s, yp, cy), phi);
+        const float rzp = wolff_projection(site_theta(g, s, zp, cz), phi);
+        const slsf_u32x4 b = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, ii);
+        const float jx = s.jxy[c.z], jzz = s.jz[c.z];
+        const bool ax = valid && wolff_bond_active(jx, ri, rxp, m2b, b.x);
+        const bool ay = valid && wolff_bond_active(jx, ri, ryp, m2b, b.y);
+        const bool az = valid && wolff_bond_active(jzz, ri, rzp, m2b, b.z);
+        if (g.lx_divides_warp) {
+            const uint32_t bal_x = __ballot_sync(0xffffffffu, ax);
+            const uint32_t bal_y = __ballot_sync(0xffffffffu, ay);
+            const uint32_t bal_z = __ballot_sync(0xffffffffu, az);
+            if (valid && c.x == 0) {
+                const uint32_t sh = lane; /* lane of x == 0 is the row's first bit */
+                s.bx[c.row] = (bal_x >> sh) & g.xmask;
+                s.by[c.row] = (bal_y >> sh) & g.xmask;
+                s.bz[c.row] = (bal_z >> sh) & g.xmask;
+            }
+        } else if (valid) {
+            if (ax) atomicOr(&s.bx[c.row], 1u << c.x);
+            if (ay) atomicOr(&s.by[c.row], 1u << c.x);
+            if (az) atomicOr(&s.bz[c.row], 1u << c.x);
+        }
+    }
+    const uint32_t seed_row = y0 + g.ly * z0;
+    for (uint32_t r = threadIdx.x; r < g.rows; r += blockDim.x) s.cl[r] = (r == seed_row) ? (1u << x0) : 0u;
+    __syncthreads();
+
+    /* Grow the seed's component; bounded by V passes (monotone growth). */
+    for (uint32_t pass = 0; pass <= g.volume; ++pass) {
+        int changed = 0;
+        for (uint32_t r = threadIdx.x; r < g.rows; r += blockDim.x) {
+            const uint32_t old = s.cl[r];
+            const uint32_t z = slsf_fastdiv_div(r, g.div_ly);
+            const uint32_t y = r - z * g.ly;
+            const uint32_t r_yp = (y + 1 == g.ly) ? r + 1 - g.ly : r + 1;
+            const uint32_t r_ym = (y == 0) ? r + g.ly - 1 : r - 1;
+            const uint32_t r_zp = (z + 1 == g.lz) ? r + g.ly - g.rows : r + g.ly;
+            const uint32_t r_zm = (z == 0) ? r + g.rows - g.ly : r - g.ly;
+            uint32_t c = old;
+            c |= s.cl[r_ym] & s.by[r_ym];
+            c |= s.cl[r_yp] & s.by[r];
+            c |= s.cl[r_zm] & s.bz[r_zm];
+            c |= s.cl[r_zp] & s.bz[r];
+            if (c) c = close_row(c, s.bx[r], g.lx, g.xmask);
+            if (c != old) {
+                s.cl[r] = c;
+                changed = 1;
+            }
+        }
+        if (!__syncthreads_or(changed)) break;
+    }
+
+    /* Reflect the cluster (src/updates.rs:602-617) and count it. */
+    uint32_t members = 0;
+    for (uint32_t r = threadIdx.x; r < g.rows; r += blockDim.x) members += __popc(s.cl[r]);
+    for (uint32_t idx = threadIdx.x; idx < g.volume; idx += blockDim.x) {
+        const Coords c = coords_of(g, idx);
+        if ((s.cl[c.row] >> c.x) & 1u) {
+            const uint32_t sl = slot(g, idx, (c.x + c.y + c.z) & 1u);
+            s.th[sl] = slsf_reflect(s.th[sl], phi);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) members += __shfl_down_sync(0xffffffffu, members, off);
+    if (lane == 0 && members) atomicAdd(s_count, members);
+    __syncthreads();
+    return 0;
+}
+
+/* Fused observables of the resident state (src/observables.rs:99-141):
+ * mx, my, cos xyz, sin xyz, FP64 per thread and across the block. */
+__device__ __forceinline__ void measure(const Geo& g, const Smem& s, double (&acc)[8], double* red) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+    for (uint32_t i0 = (threadIdx.x & ~31u); i0 < g.volume; i0 += blockDim.x) {
+        const uint32_t idx = i0 + lane;
+        const bool valid = idx < g.volume;
+        const uint32_t ii = valid ? idx : 0;
+        const Coords c = coords_of(g, ii);
+        uint32_t xp, yp, zp;
+        forward_neighbours(g, ii, c, xp, yp, zp);
+        float si, ci, sx, cx, sy, cy, sz, cz;
+        __sincosf(site_theta(g, s, ii, c), &si, &ci);
+        if (g.lx_divides_warp) {
+            const uint32_t src = xp_lane(lane, g.lx);
+            sx = __shfl_sync(0xffffffffu, si, src);
+            cx = __shfl_sync(0xffffffffu, ci, src);
+        } else {
+            const Coords cxp = {c.x + 1 == g.lx ? 0 : c.x + 1, c.y, c.z, c.row};
+            __sincosf(site_theta(g, s, xp, cxp), &sx, &cx);
+        }
+        const Coords cyp = {c.x, c.y + 1 == g.ly ? 0 : c.y + 1, c.z, 0};
+        const Coords czp = {c.x, c.y, c.z + 1 == g.lz ? 0 : c.z + 1, 0};
+        __sincosf(site_theta(g, s, yp, cyp), &sy, &cy);
+        __sincosf(site_theta(g, s, zp, czp), &sz, &cz);
+        if (!valid) continue;
+        const float jx = s.jxy[c.z], jzz = s.jz[c.z];
+        acc[0] += ci;
+        acc[1] += si;
+        acc[2] += jx * (ci * cx + si * sx);
+        acc[3] += jx * (ci * cy + si * sy);
+        acc[4] += jzz * (ci * cz + si * sz);
+        acc[5] += jx * (si * cx - ci * sx);
+        acc[6] += jx * (si * cy - ci * sy);
+        acc[7] += jzz * (si * cz - ci * sz);
+    }
+    block_sum<8>(acc, red);
+}
+
+__global__ void __launch_bounds__(kBThreads, 1)
+    k_batched(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps,
+              unsigned int* __restrict__ queue, uint32_t max_volume, uint32_t max_rows,
+              uint32_t max_lz) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[8 * 32];
+    __shared__ double bin_acc[kBinCols];
+    __shared__ uint32_t s_item;
+    __shared__ uint32_t s_cluster;
+    __shared__ uint32_t s_accepted;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(queue, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= n) return;
+        const TaskView t = views[item];
+        const Geo g = make_geo(t);
+        Smem s = carve(smem_raw, g, max_volume, max_rows, max_lz);
+        if (threadIdx.x == 0) {
+            s_cluster = 0;
+            s_accepted = 0;
+        }
+        load_state(t, g, s);
+        __syncthreads();
+        uint32_t accepted = 0;
+        int64_t bin_cur = -1;
+        for (uint32_t sw = 0; sw < n_sweeps; ++sw) {
+            const uint64_t sweep = t.metro_sweeps + sw;
+            accepted += half_sweep(t, g, s, sweep, 0);
+            __syncthreads();
+            accepted += half_sweep(t, g, s, sweep, 1);
+            __syncthreads();
+            for (uint32_t k = 0; k < t.wolff_steps; ++k)
+                wolff_update(t, g, s, t.wolff_done + (uint64_t)sw * t.wolff_steps + k, &s_cluster);
+            /* ThetaModel::measure after the sweep, once thermalized. */
+            const uint64_t done = sweep + 1;
+            if (done > t.thermalization && t.n_bins > 0) {
+                const uint64_t m = done - t.thermalization - 1;
+                const int64_t b = (int64_t)(m / t.binsize);
+                double acc[8];
+                measure(g, s, acc, red);
+                if (threadIdx.x == 0) {
+                    if (b != bin_cur) {
+                        if (bin_cur >= 0 && bin_cur < (int64_t)t.n_bins)
+                            for (int q = 0; q < kBinCols; ++q) t.bins[bin_cur * kBinCols + q] += bin_acc[q];
+                        for (int q = 0; q < kBinCols; ++q) bin_acc[q] = 0.0;
+                        bin_cur = b;
+                    }
+                    const double v = (double)g.volume;
+                    const double e = -(acc[2] + acc[3] + acc[4]) / v;
+                    const double vals[kBinCols] = {e,
+                                                   e * e,
+                                                   (acc[0] * acc[0] + acc[1] * acc[1]) / (v * v),
+                                                   acc[2],
+                                                   acc[3],
+                                                   acc[4],
+                                                   acc[5],
+                                                   acc[6],
+                                                   acc[7],
+                                                   acc[5] * acc[5],
+                                                   acc[6] * acc[6],
+                                                   acc[7] * acc[7]};
+                    for (int q = 0; q < kBinCols; ++q) bin_acc[q] += vals[q];
+                }
+            }
+        }
+        if (threadIdx.x == 0 && bin_cur >= 0 && bin_cur < (int64_t)t.n_bins)
+            for (int q = 0; q < kBinCols; ++q) t.bins[bin_cur * kBinCols + q] += bin_acc[q];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) accepted += __shfl_down_sync(0xffffffffu, accepted, off);
+        if ((threadIdx.x & 31u) == 0 && accepted) atomicAdd(&s_accepted, accepted);
+        __syncthreads();
+        store_state(t, g, s);
+        if (threadIdx.x == 0) {
+            atomicAdd(&t.stats[kStatAccepted], (unsigned long long)s_accepted);
+            atomicAdd(&t.stats[kStatClusterSites], (unsigned long long)s_cluster);
+            atomicAdd(&t.stats[kStatClusters], (unsigned long long)n_sweeps * t.wolff_steps);
+        }
+    }
+}
+
+size_t smem_bytes(uint32_t max_volume, uint32_t max_rows, uint32_t max_lz) {
+    return 4ull * (max_volume + 2 * kPad) + 16ull * max_rows + 8ull * max_lz;
+}
+
+int max_dynamic_smem(int device) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    /* leave room for the kernel's static shared arrays */
+    return v - 4096;
+}
+
+}  // namespace
+
+BatchLimits batched_limits(int device) {
+    BatchLimits l;
+    l.max_volume = (uint32_t)(max_dynamic_smem(device) / 4.5);
+    return l;
+}
+
+bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
+    /* Row words hold L_x <= 32 bits; the float4 colour-split copy needs
+     * L_x % 4 == 0 so that four consecutive sites never span two rows. */
+    if (lx > kMaxRowBits || lx < 4 || lx % 4) return false;
+    const uint64_t v = (uint64_t)lx * ly * lz;
+    return smem_bytes((uint32_t)v, ly * lz, lz) <= (size_t)max_dynamic_smem(device);
+}
+
+cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps,
+                           unsigned int* queue, int device, cudaStream_t s, uint32_t max_volume,
+                           uint32_t max_rows, uint32_t max_lz) {
+    const size_t smem = smem_bytes(max_volume, max_rows, max_lz);
+    cudaError_t e = cudaFuncSetAttribute(k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int sms = 0, per_sm = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batched, kBThreads, smem);
+    if (e != cudaSuccess) return e;
+    const uint32_t grid = std::min<uint32_t>(n, (uint32_t)(sms * std::max(1, per_sm)));
+    k_batched<<<grid, kBThreads, smem, s>>>(views_dev, n, n_sweeps, queue, max_volume, max_rows, max_lz);
+    return cudaGetLastError();
+}
+
+}  // namespace slsf

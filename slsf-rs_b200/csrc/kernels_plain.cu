@@ -1,0 +1,423 @@
+/*
+ * Single-task kernels: the plain GPU path behind slsf_task_*.
+ *
+ *   k_init_random        ThetaModel::init (src/model.rs:373-377)
+ *   k_metro_colour       one colour of metropolis_sweep_with_scratch
+ *                        (src/updates.rs:440-486), one thread per Philox block
+ *                        (two same-colour sites)
+ *   k_wolff_bonds        per-site +x/+y/+z bond activation of
+ *   k_wolff_union        wolff_cluster_step_with_theta_scratch
+ *   k_wolff_flip         (src/updates.rs:551-620): lock-free union-find over
+ *                        the active bonds, then reflect the seed's component
+ *   k_measure            measure_theta_observables_with_scratch
+ *                        (src/observables.rs:80-154), FP64 block sums, fixed
+ *                        summation order (last block reduces the partials)
+ *   k_corr_*             measure_theta_correlations_with_scratch
+ *                        (src/observables.rs:166-265)
+ */
+#include <algorithm>
+
+#include "engine.h"
+#include "xy_device.cuh"
+
+namespace slsf {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__global__ void __launch_bounds__(kThreads) k_init_random(float* __restrict__ theta, uint32_t volume,
+                                                          uint64_t seed) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (4ull * q >= volume) return;
+    const slsf_u32x4 b = slsf_stream(seed, 0, SLSF_PURPOSE_INIT, 0, q);
+    const uint32_t w[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t i = 4 * q + k;
+        if (i < volume) theta[i] = slsf_angle_from_word(w[k]);
+    }
+}
+
+template <bool kRecord>
+__global__ void __launch_bounds__(kThreads)
+    k_metro_colour(float* __restrict__ theta, const float* __restrict__ jxy,
+                   const float* __restrict__ jz, uint32_t lx, uint32_t ly, uint32_t lz, float beta,
+                   float width, uint64_t seed, uint64_t sweep, uint32_t colour,
+                   unsigned long long* __restrict__ stats, uint8_t* __restrict__ record) {
+    const uint32_t volume = lx * ly * lz;
+    const uint32_t half = volume >> 1;
+    const uint32_t npairs = (half + 1) >> 1;
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t accepted = 0;
+    if (p < npairs) {
+        const slsf_u32x4 blk = slsf_stream(seed, sweep, SLSF_PURPOSE_METRO, colour, p);
+#pragma unroll
+        for (uint32_t lane = 0; lane < 2; ++lane) {
+            const uint32_t h = 2 * p + lane;
+            if (h >= half) break;
+            const SiteXYZ s = decode_colour_site(h, colour, lx, ly);
+            uint32_t nb[6];
+            neighbour_indices(s, lx, ly, lz, nb);
+            float ns[6], nc[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) __sincosf(theta[nb[k]], &ns[k], &nc[k]);
+            const float jx = jxy[s.z], jzp = jz[s.z], jzm = jz[s.z == 0 ? lz - 1 : s.z - 1];
+            const float hx = field_component(jx, jzp, jzm, nc[0], nc[1], nc[2], nc[3], nc[4], nc[5]);
+            const float hy = field_component(jx, jzp, jzm, ns[0], ns[1], ns[2], ns[3], ns[4], ns[5]);
+            const float th = theta[s.idx];
+            float si, ci;
+            __sincosf(th, &si, &ci);
+            float u_prop, u_acc;
+            slsf_metro_uniforms(blk, lane, &u_prop, &u_acc);
+            float tn, sn, cn;
+            const bool acc = metro_decide(th, ci, si, hx, hy, beta, width, u_prop, u_acc, &tn, &sn, &cn);
+            if (acc) {
+                theta[s.idx] = tn;
+                ++accepted;
+            }
+            if (kRecord) record[s.idx] = acc ? 1 : 0;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) accepted += __shfl_down_sync(0xffffffffu, accepted, off);
+    if ((threadIdx.x & 31) == 0 && accepted) atomicAdd(&stats[kStatAccepted], (unsigned long long)accepted);
+}
+
+/* ---- Wolff: union-find with links from larger to smaller roots ---- */
+
+/* Root of x with path splitting.  parent[i] <= i always holds, so every path
+ * is strictly decreasing and at most `volume` long; the loop is bounded by it. */
+__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x, uint32_t volume,
+                                            bool* ok) {
+    volatile uint32_t* par = parent;
+    for (uint32_t it = 0; it <= volume; ++it) {
+        const uint32_t p = par[x];
+        if (p == x) return x;
+        const uint32_t gp = par[p];
+        if (gp != p) par[x] = gp;
+        x = p;
+    }
+    *ok = false;
+    return x;
+}
+
+/* Lock-free union: hook the larger root under the smaller with a CAS.  A
+ * failed CAS means another thread linked that root; every retry follows some
+ * other thread's progress, and the retry count is bounded. */
+__device__ __forceinline__ bool uf_union(uint32_t* parent, uint32_t a, uint32_t b, uint32_t volume) {
+    bool ok = true;
+    for (uint32_t it = 0; it < (1u << 22); ++it) {
+        a = uf_find(parent, a, volume, &ok);
+        b = uf_find(parent, b, volume, &ok);
+        if (!ok) return false;
+        if (a == b) return true;
+        if (a > b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        const uint32_t old = atomicCAS(&parent[b], b, a);
+        if (old == b) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_wolff_bonds(const float* __restrict__ theta, const float* __restrict__ jxy,
+                  const float* __restrict__ jz, uint32_t lx, uint32_t ly, uint32_t lz,
+                  float minus_two_beta, float phi, uint64_t seed, uint64_t counter,
+                  uint8_t* __restrict__ bonds, uint32_t* __restrict__ parent) {
+    const uint32_t volume = lx * ly * lz;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= volume) return;
+    const uint32_t x = i % lx, row = i / lx, y = row % ly, z = row / ly;
+    const uint32_t plane = lx * ly;
+    const uint32_t xp = (x + 1 == lx) ? i + 1 - lx : i + 1;
+    const uint32_t yp = (y + 1 == ly) ? i + lx - plane : i + lx;
+    const uint32_t zp = (z + 1 == lz) ? i + plane - volume : i + plane;
+    const float ri = wolff_projection(theta[i], phi);
+    const slsf_u32x4 b = slsf_stream(seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, i);
+    uint32_t bits = 0;
+    if (wolff_bond_active(jxy[z], ri, wolff_projection(theta[xp], phi), minus_two_beta, b.x)) bits |= 1u;
+    if (wolff_bond_active(jxy[z], ri, wolff_projection(theta[yp], phi), minus_two_beta, b.y)) bits |= 2u;
+    if (wolff_bond_active(jz[z], ri, wolff_projection(theta[zp], phi), minus_two_beta, b.z)) bits |= 4u;
+    bonds[i] = (uint8_t)bits;
+    parent[i] = i;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_wolff_union(const uint8_t* __restrict__ bonds, uint32_t lx, uint32_t ly, uint32_t lz,
+                  uint32_t* parent, unsigned long long* stats) {
+    const uint32_t volume = lx * ly * lz;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= volume) return;
+    const uint32_t bits = bonds[i];
+    if (!bits) return;
+    const uint32_t x = i % lx, row = i / lx, y = row % ly, z = row / ly;
+    const uint32_t plane = lx * ly;
+    bool ok = true;
+    if (bits & 1u) ok &= uf_union(parent, i, (x + 1 == lx) ? i + 1 - lx : i + 1, volume);
+    if (bits & 2u) ok &= uf_union(parent, i, (y + 1 == ly) ? i + lx - plane : i + lx, volume);
+    if (bits & 4u) ok &= uf_union(parent, i, (z + 1 == lz) ? i + plane - volume : i + plane, volume);
+    if (!ok) atomicOr(&stats[kStatError], kErrUnionFindLimit);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_wolff_flip(float* __restrict__ theta, uint32_t volume, uint32_t* parent, uint32_t seed_idx,
+                 float phi, unsigned long long* stats, uint8_t* __restrict__ cluster_out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool ok = true;
+    uint32_t in = 0;
+    if (i < volume) {
+        const uint32_t root = uf_find(parent, seed_idx, volume, &ok);
+        in = (uf_find(parent, i, volume, &ok) == root) ? 1u : 0u;
+        if (in) theta[i] = slsf_reflect(theta[i], phi);
+        if (cluster_out) cluster_out[i] = (uint8_t)in;
+    }
+    if (!ok) atomicOr(&stats[kStatError], kErrUnionFindLimit);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) in += __shfl_down_sync(0xffffffffu, in, off);
+    if ((threadIdx.x & 31) == 0 && in) atomicAdd(&stats[kStatClusterSites], (unsigned long long)in);
+}
+
+/* ---- fused observables ---- */
+constexpr int kMeasureThreads = 256;
+
+__global__ void __launch_bounds__(kMeasureThreads)
+    k_measure(const float* __restrict__ theta, const float* __restrict__ jxy,
+              const float* __restrict__ jz, uint32_t lx, uint32_t ly, uint32_t lz,
+              double* __restrict__ partials, unsigned int* __restrict__ done,
+              double* __restrict__ result) {
+    __shared__ double scratch[8 * 32];
+    __shared__ bool last;
+    const uint32_t volume = lx * ly * lz, plane = lx * ly;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < volume; i += stride) {
+        const uint32_t x = i % lx, row = i / lx, y = row % ly, z = row / ly;
+        const uint32_t ix = (x + 1 == lx) ? i + 1 - lx : i + 1;
+        const uint32_t iy = (y + 1 == ly) ? i + lx - plane : i + lx;
+        const uint32_t iz = (z + 1 == lz) ? i + plane - volume : i + plane;
+        float si, ci, sx, cx, sy, cy, sz, cz;
+        __sincosf(theta[i], &si, &ci);
+        __sincosf(theta[ix], &sx, &cx);
+        __sincosf(theta[iy], &sy, &cy);
+        __sincosf(theta[iz], &sz, &cz);
+        const float jx = jxy[z], jzz = jz[z];
+        /* diff_cos_sin (src/observables.rs:9-11): cos(a-b), sin(a-b) from trig. */
+        acc[0] += ci;
+        acc[1] += si;
+        acc[2] += jx * (ci * cx + si * sx);
+        acc[3] += jx * (ci * cy + si * sy);
+        acc[4] += jzz * (ci * cz + si * sz);
+        acc[5] += jx * (si * cx - ci * sx);
+        acc[6] += jx * (si * cy - ci * sy);
+        acc[7] += jzz * (si * cz - ci * sz);
+    }
+    block_sum<8>(acc, scratch);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 8; ++k) partials[blockIdx.x * 8 + k] = acc[k];
+        __threadfence();
+        last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    /* Last block: sum the per-block partials in block order. */
+    __threadfence();
+    double tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+        for (int k = 0; k < 8; ++k) tot[k] += ((volatile double*)partials)[b * 8 + k];
+    block_sum<8>(tot, scratch);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 8; ++k) result[k] = tot[k];
+        *done = 0;
+    }
+}
+
+/* ---- correlations ----
+ * A "line" is a periodic 1-D array of n sites with a fixed stride; the
+ * circular correlation of a line at lag r is sum_k s_k . s_{(k+r) mod n}
+ * (src/observables.rs:196-220 for x and y rows, :230-244 for z columns).
+ * Lines along y and z are taken 32 consecutive x at a time so that the tile
+ * loads are coalesced; lines along x are whole rows. */
+constexpr int kCorrThreads = 256;
+constexpr int kCorrCols = 32;
+
+/* Lines along an axis with stride `stride` (lx for y, lx*ly for z), n sites
+ * each; a block takes kCorrCols consecutive x at one (other-axis) offset.
+ * out[block][r] = sum over its columns of the lag-r sums. */
+__global__ void __launch_bounds__(kCorrThreads)
+    k_corr_strided(const float* __restrict__ theta, uint32_t lx, uint32_t n, uint32_t stride,
+                   uint32_t outer_count, uint32_t outer_stride, uint32_t rmax,
+                   double* __restrict__ out) {
+    extern __shared__ float tile[]; /* [n][kCorrCols][2] (cos, sin) */
+    const uint32_t col_blocks = (lx + kCorrCols - 1) / kCorrCols;
+    const uint32_t outer = blockIdx.x / col_blocks;
+    const uint32_t x0 = (blockIdx.x % col_blocks) * kCorrCols;
+    const uint32_t cols = min((uint32_t)kCorrCols, lx - x0);
+    const uint32_t base = outer * outer_stride + x0;
+    for (uint32_t e = threadIdx.x; e < n * kCorrCols; e += blockDim.x) {
+        const uint32_t k = e / kCorrCols, c = e % kCorrCols;
+        float s = 0.0f, co = 0.0f;
+        if (c < cols) __sincosf(theta[base + k * stride + c], &s, &co);
+        tile[2 * e] = co;
+        tile[2 * e + 1] = s;
+    }
+    __syncthreads();
+    __shared__ double red[kCorrThreads];
+    for (uint32_t r = 1; r <= rmax; ++r) {
+        double acc = 0.0;
+        for (uint32_t e = threadIdx.x; e < n * kCorrCols; e += blockDim.x) {
+            const uint32_t k = e / kCorrCols, c = e % kCorrCols;
+            const uint32_t k2 = (k + r) % n;
+            const uint32_t f = k2 * kCorrCols + c;
+            acc += (double)(tile[2 * e] * tile[2 * f] + tile[2 * e + 1] * tile[2 * f + 1]);
+        }
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[(size_t)blockIdx.x * rmax + (r - 1)] = red[0];
+        __syncthreads();
+    }
+    (void)outer_count;
+}
+
+/* Rows along x: a block takes one row (y, z); out[row][r]. */
+__global__ void __launch_bounds__(kCorrThreads)
+    k_corr_rows(const float* __restrict__ theta, uint32_t lx, uint32_t rmax, double* __restrict__ out) {
+    extern __shared__ float row[]; /* [lx][2] */
+    const uint32_t base = blockIdx.x * lx;
+    for (uint32_t k = threadIdx.x; k < lx; k += blockDim.x) {
+        float s, c;
+        __sincosf(theta[base + k], &s, &c);
+        row[2 * k] = c;
+        row[2 * k + 1] = s;
+    }
+    __syncthreads();
+    __shared__ double red[kCorrThreads];
+    for (uint32_t r = 1; r <= rmax; ++r) {
+        double acc = 0.0;
+        for (uint32_t k = threadIdx.x; k < lx; k += blockDim.x) {
+            const uint32_t k2 = (k + r) % lx;
+            acc += (double)(row[2 * k] * row[2 * k2] + row[2 * k + 1] * row[2 * k2 + 1]);
+        }
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[(size_t)blockIdx.x * rmax + (r - 1)] = red[0];
+        __syncthreads();
+    }
+}
+
+/* out[g][r] = sum_{j < per_group} in[(g * per_group + j)][r], fixed order. */
+__global__ void k_sum_groups(const double* __restrict__ in, uint32_t groups, uint32_t per_group,
+                             uint32_t rmax, double* __restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= groups * rmax) return;
+    const uint32_t g = t / rmax, r = t % rmax;
+    double acc = 0.0;
+    for (uint32_t j = 0; j < per_group; ++j) acc += in[((size_t)g * per_group + j) * rmax + r];
+    out[t] = acc;
+}
+
+inline uint32_t blocks_for(uint64_t n, int threads) { return (uint32_t)((n + threads - 1) / threads); }
+
+}  // namespace
+
+void launch_init_random(float* theta, uint32_t volume, uint64_t seed, cudaStream_t s) {
+    const uint32_t quads = (volume + 3) / 4;
+    k_init_random<<<blocks_for(quads, kThreads), kThreads, 0, s>>>(theta, volume, seed);
+}
+
+void launch_metro_colour(const TaskView& t, uint64_t sweep, uint32_t colour, uint8_t* record,
+                         cudaStream_t s) {
+    const uint32_t volume = t.lx * t.ly * t.lz;
+    const uint32_t npairs = ((volume >> 1) + 1) >> 1;
+    const uint32_t grid = blocks_for(npairs, kThreads);
+    if (record)
+        k_metro_colour<true><<<grid, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, t.beta,
+                                                       t.width, t.seed, sweep, colour, t.stats, record);
+    else
+        k_metro_colour<false><<<grid, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, t.beta,
+                                                        t.width, t.seed, sweep, colour, t.stats, nullptr);
+}
+
+void launch_wolff(const TaskView& t, uint64_t counter, uint8_t* bonds, uint32_t* parent,
+                  uint8_t* cluster_out, cudaStream_t s, float* phi_out, uint32_t seed_site[3]) {
+    /* The reflection axis and seed site (src/updates.rs:564-568) come from
+     * the WOLFF_PICK block, computed here on the host from the same header. */
+    const slsf_u32x4 pick = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_PICK, 0, 0);
+    const float phi = slsf_angle_from_word(pick.x);
+    const uint32_t x0 = slsf_range(pick.y, t.lx), y0 = slsf_range(pick.z, t.ly), z0 = slsf_range(pick.w, t.lz);
+    const uint32_t volume = t.lx * t.ly * t.lz;
+    const uint32_t seed_idx = x0 + t.lx * (y0 + t.ly * z0);
+    const uint32_t grid = blocks_for(volume, kThreads);
+    k_wolff_bonds<<<grid, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, -2.0f * t.beta, phi,
+                                            t.seed, counter, bonds, parent);
+    k_wolff_union<<<grid, kThreads, 0, s>>>(bonds, t.lx, t.ly, t.lz, parent, t.stats);
+    k_wolff_flip<<<grid, kThreads, 0, s>>>(t.theta, volume, parent, seed_idx, phi, t.stats, cluster_out);
+    if (phi_out) *phi_out = phi;
+    if (seed_site) {
+        seed_site[0] = x0;
+        seed_site[1] = y0;
+        seed_site[2] = z0;
+    }
+}
+
+int measure_partial_blocks(uint32_t volume) {
+    return (int)std::max<uint32_t>(1, std::min<uint32_t>(blocks_for(volume, kMeasureThreads), 148 * 8));
+}
+
+void launch_measure(const TaskView& t, double* partials, unsigned int* done, double* result,
+                    cudaStream_t s) {
+    const uint32_t volume = t.lx * t.ly * t.lz;
+    k_measure<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly,
+                                                                         t.lz, partials, done, result);
+}
+
+size_t correlation_work_doubles(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rmax_xy,
+                                uint32_t rmax_z) {
+    const size_t col_blocks = (lx + kCorrCols - 1) / kCorrCols;
+    const size_t rows = (size_t)ly * lz * rmax_xy;          /* x lines */
+    const size_t ycols = col_blocks * lz * rmax_xy;         /* y lines */
+    const size_t zcols = col_blocks * (size_t)ly * rmax_z;  /* z lines */
+    return std::max(std::max(rows, ycols), zcols);
+}
+
+void launch_correlations(const TaskView& t, uint32_t rmax_xy, uint32_t rmax_z, double* work,
+                         size_t work_doubles, double* sx, double* sy, double* sz,
+                         cudaStream_t s) {
+    (void)work_doubles;
+    const uint32_t col_blocks = (t.lx + kCorrCols - 1) / kCorrCols;
+    const size_t smem_max = (size_t)2 * std::max(t.ly, t.lz) * kCorrCols * sizeof(float);
+    if (smem_max > 48 * 1024)
+        cudaFuncSetAttribute(k_corr_strided, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
+    if ((size_t)2 * t.lx * sizeof(float) > 48 * 1024)
+        cudaFuncSetAttribute(k_corr_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * t.lx * sizeof(float)));
+    if (rmax_xy > 0) {
+        /* x: one block per row, then sum the ly rows of each layer. */
+        k_corr_rows<<<t.ly * t.lz, kCorrThreads, 2 * t.lx * sizeof(float), s>>>(t.theta, t.lx, rmax_xy, work);
+        k_sum_groups<<<blocks_for((uint64_t)t.lz * rmax_xy, 128), 128, 0, s>>>(work, t.lz, t.ly, rmax_xy, sx);
+        /* y: lines of ly sites with stride lx; one block per (z, x-chunk). */
+        const size_t smem_y = (size_t)2 * t.ly * kCorrCols * sizeof(float);
+        k_corr_strided<<<t.lz * col_blocks, kCorrThreads, smem_y, s>>>(t.theta, t.lx, t.ly, t.lx, t.lz,
+                                                                        t.lx * t.ly, rmax_xy, work);
+        k_sum_groups<<<blocks_for((uint64_t)t.lz * rmax_xy, 128), 128, 0, s>>>(work, t.lz, col_blocks, rmax_xy, sy);
+    }
+    if (rmax_z > 0) {
+        /* z: lines of lz sites with stride lx*ly; one block per (y, x-chunk). */
+        const size_t smem_z = (size_t)2 * t.lz * kCorrCols * sizeof(float);
+        k_corr_strided<<<t.ly * col_blocks, kCorrThreads, smem_z, s>>>(t.theta, t.lx, t.lz, t.lx * t.ly, t.ly,
+                                                                        t.lx, rmax_z, work);
+        k_sum_groups<<<blocks_for(rmax_z, 128), 128, 0, s>>>(work, 1, t.ly * col_blocks, rmax_z, sz);
+    }
+}
+
+}  // namespace slsf

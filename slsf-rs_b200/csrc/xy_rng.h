@@ -59,7 +59,9 @@ typedef struct {
 } slsf_u32x4;
 
 SLSF_HD slsf_u32x4 slsf_philox4x32_10(slsf_u32x4 c, uint32_t k0, uint32_t k1) {
+#if defined(__CUDA_ARCH__)
 #pragma unroll
+#endif
     for (int round = 0; round < 10; ++round) {
 #if defined(__CUDA_ARCH__)
         const uint32_t hi0 = __umulhi(SLSF_PHILOX_M0, c.x);
