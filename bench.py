@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 update-and-measure path of the 3D layered-disorder XY model.
+
+Metric: site-updates/s (one site-update = one Metropolis proposal at one site;
+Wolff and measurement time are included).  Workload (per GPU): 256 disorder
+realisations x 16 temperatures uniformly spaced in [1.1, 1.5], L = 32 cubes,
+J_xy = 1.2, J_z(z) ~ U[0.5, 1.5] per realisation from its disorder seed, one
+Wolff update per sweep, every sweep after thermalization measured into 32
+bins (FP64 reductions).  A step is one persistent launch of S sweeps over all
+4096 replicas; the default W + K = 3 + 17 steps of S = 100 sweeps is the
+whole 2000-sweep job.  The state (512 MiB FP32) is larger than L2.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank runs its own 4096 replicas (weak scaling,
+no data-path collective); the time is the max over ranks of the CUDA-event
+time.  `--impl reference` times the CPU restatement of the reference path on
+the host cores instead (rank 0 only).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BASE_SEED = 20260710  # the reference's benchmark base_seed (examples/theta_l64_s1000_benchmark.toml:11)
+BYTES_PER_UPDATE = 12  # FP32 theta: read twice and half written per sweep
+
+
+def parse():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=17)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--sweeps-per-step", type=int, default=100)
+    p.add_argument("--samples", type=int, default=256, help="disorder realisations per GPU")
+    p.add_argument("--temperatures", type=int, default=16)
+    p.add_argument("--L", type=int, default=32)
+    p.add_argument("--no-plain", action="store_true", help="skip the single-task L=64 comparison")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
+    return p.parse_args()
+
+
+def load_pkg():
+    import importlib.util
+
+    pkg_dir = os.path.join(ROOT, "slsf-rs_b200")
+    if "slsf_rs_b200" in sys.modules:
+        return sys.modules["slsf_rs_b200"]
+    spec = importlib.util.spec_from_file_location("slsf_rs_b200", os.path.join(pkg_dir, "__init__.py"),
+                                                  submodule_search_locations=[pkg_dir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["slsf_rs_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload(pkg, samples, n_temps, L, rank):
+    """(disorder seed, T, run seed, J_xy, J_z) per replica; samples are offset by rank."""
+    temps = np.linspace(1.1, 1.5, n_temps)
+    out = []
+    for s in range(1, samples + 1):
+        sample = s + rank * samples
+        dseed = BASE_SEED + sample - 1  # src/model.rs:741
+        jz = pkg.uniform_layer_disorder(L, 0.5, 1.5, dseed)
+        jxy = np.full(L, 1.2)
+        for T in temps:
+            out.append((dseed, float(T), pkg.task_seed(BASE_SEED, L, sample, float(T)), jxy, jz))
+    return out
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_site():
+    """DRAM bytes per replica site per launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "k_batched_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["dram_bytes_per_site_per_launch"])
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], None, set()
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if r[3 + k].lower() == "active":
+                    reasons.add(name)
+        loaded = [v for v in sm if mx and v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(L, temps, sweeps_hint, seconds, threads=None):
+    """Time the oracle's reference-order CPU path on all host threads on a
+    bounded sample of the workload: one L^3 replica per thread (rank-per-task,
+    src/model.rs:680-685), sized to run about `seconds`."""
+    import oracle
+
+    threads = threads or os.cpu_count() or 1
+    jxy = np.full(L, 1.2)
+    jz = oracle.uniform_disorder(L, 0.5, 1.5, BASE_SEED)
+    # calibrate with one replica x 2 sweeps on one thread
+    t1, _ = oracle.bench_tasks((L, L, L), jxy, jz, [temps[0]], math.pi, 1, [1], 2, 1)
+    per_sweep = t1 / 2
+    sweeps = max(2, min(sweeps_hint, int(seconds / max(per_sweep, 1e-9))))
+    n = threads
+    tt = [temps[i % len(temps)] for i in range(n)]
+    sec, chk = oracle.bench_tasks((L, L, L), np.tile(jxy, n), np.tile(jz, n), tt, math.pi, 1,
+                                  [BASE_SEED + i for i in range(n)], sweeps, threads)
+    updates = n * sweeps * L ** 3
+    return {"value": updates / sec, "unit": "site-updates/s", "cores": threads, "kind": "port",
+            "sample": f"{n} replicas of L={L} x {sweeps} sweeps (Metropolis + 1 Wolff + measure each), "
+                      f"{threads} threads, FP64 C++ restatement of SLSF-rs (not the Rust binary)",
+            "seconds": sec}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    L = args.L
+    temps = list(np.linspace(1.1, 1.5, args.temperatures))
+    threads = os.cpu_count() or 1
+    step_seconds = max(1.0, min(10.0, 150.0 / max(1, args.steps + args.warmup)))
+    times, updates = [], []
+    for k in range(args.warmup + args.steps):
+        r = cpu_baseline(L, temps, args.sweeps_per_step, step_seconds, threads)
+        if k >= args.warmup:
+            times.append(r["seconds"])
+            updates.append(r["value"] * r["seconds"])
+    value = sum(updates) / sum(times)
+    line = {
+        "impl": "reference", "metric": "site-updates/s", "value": value, "unit": "site-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"c2 batched replicas: L={L}, J_xy=1.2, J_z~U[0.5,1.5], T in [1.1,1.5], "
+                               "Metropolis + 1 Wolff + measure per sweep", "L": L},
+        "cpu_baseline": {"value": value, "unit": "site-updates/s", "cores": threads, "kind": "port",
+                         "sample": r["sample"]},
+        "e2e": {"value": value, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def plain_rate(pkg, ctx, L=64, T=1.3, sweeps=1000):
+    """Single-task GPU path, as ThetaModel is driven (src/model.rs:379-442): per
+    sweep one slsf_task_sweep + one slsf_task_measure, each returning to the host."""
+    jz = pkg.uniform_layer_disorder(L, 0.5, 1.5, BASE_SEED)
+    t = pkg.Task(ctx, (L, L, L), np.full(L, 1.2), jz, T, wolff_steps=1, seed=pkg.task_seed(BASE_SEED, L, 1, T))
+    t.init_random()
+    for _ in range(20):
+        t.sweep(1)
+        t.measure()
+    t0 = time.perf_counter()
+    for _ in range(sweeps):
+        t.sweep(1)
+        t.measure()
+    dt = time.perf_counter() - t0
+    t.close()
+    return {"value": sweeps * L ** 3 / dt, "unit": "site-updates/s",
+            "config": f"c1 single replica L={L}, T={T}, {sweeps} sweeps, Metropolis + 1 Wolff + measure per sweep"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+
+    pkg = load_pkg()
+    pkg.load()
+    ctx = pkg.Context(local_rank)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+
+    L, S = args.L, args.sweeps_per_step
+    wl = workload(pkg, args.samples, args.temperatures, L, rank)
+    n = len(wl)
+    total_sweeps = (args.warmup + args.steps) * S
+    therm = args.warmup * S
+    n_bins = 32
+    binsize = max(1, (args.steps * S + n_bins - 1) // n_bins)
+    tasks = []
+    for dseed, T, seed, jxy, jz in wl:
+        t = pkg.Task(ctx, (L, L, L), jxy, jz, T, proposal_width=math.pi, wolff_steps=1, seed=seed,
+                     thermalization=therm, binsize=binsize, n_bins=n_bins)
+        t.init_random()
+        tasks.append(t)
+    handles = ctx.handle_array(tasks)
+
+    # warm-up steps = thermalization sweeps
+    for _ in range(args.warmup):
+        ctx.batch_run(tasks, S, handles=handles)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = ctx.launches
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for k in range(args.steps):
+            ctx.batch_run(tasks, S, handles=handles)
+            ev[k + 1].record(stream)
+    torch.cuda.synchronize(dev)
+    launches = ctx.launches - launches0
+    clk = clocks.stop()
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    elapsed = sum(step_ms) / 1e3
+    if dist:
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    updates_rank = n * S * args.steps * L ** 3
+    value = updates_rank * world / elapsed
+
+    # end-to-end through the public API: every step uploads its task table
+    # (pinned) and reads back every task's counters and bins
+    e2e_steps = max(1, min(args.steps, 5))
+    bins_out = np.zeros((n, n_bins, pkg.BIN_COLS))
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.batch_run(tasks, S, handles=handles)
+        ctx.batch_bins(tasks, n_bins, out=bins_out, handles=handles)
+    e2e_dt = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_dt], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_dt = float(t.item())
+    e2e_value = n * S * e2e_steps * L ** 3 * world / e2e_dt
+    view_bytes = 104  # sizeof(slsf::TaskView) uploaded per task per batch launch
+    h2d = n * view_bytes + 8 * n  # task table + handle table of the gather
+    d2h = n * 32 + n * n_bins * pkg.BIN_COLS * 8  # per-task counters + bins
+
+    peak, peak_kind = peaks()
+    avg_launch_s = elapsed / args.steps
+    alg_bytes = BYTES_PER_UPDATE * n * S * L ** 3
+    achieved = alg_bytes / avg_launch_s / 1e9
+    tps = traffic_per_site()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (tps * n * L ** 3) if tps is not None else None,
+                "peak_kind": peak_kind,
+                "kernel": "k_batched (one launch = S sweeps of every replica, state resident in shared memory)",
+                "algorithmic_bytes_per_launch": alg_bytes}
+
+    extra = {}
+    if rank == 0 and world == 1:
+        if not args.no_plain:
+            extra["plain"] = plain_rate(pkg, ctx)
+            extra["plain"]["batched_over_plain"] = value / extra["plain"]["value"]
+        if not args.no_cpu:
+            extra["cpu_baseline"] = cpu_baseline(L, list(np.linspace(1.1, 1.5, args.temperatures)), 2000,
+                                                 args.cpu_seconds)
+            extra["cpu_baseline"]["gpu_over_cpu"] = value / extra["cpu_baseline"]["value"]
+
+    if rank == 0:
+        line = {
+            "metric": "site-updates/s", "value": value, "unit": "site-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"c2 batched replicas per GPU: {args.samples} disorder x {args.temperatures} T "
+                                   f"in [1.1,1.5], L={L}, J_xy=1.2, J_z~U[0.5,1.5], Metropolis (width pi) + 1 Wolff "
+                                   f"+ measure per sweep, {total_sweeps} sweeps total, {S} sweeps per step",
+                       "replicas_per_gpu": n, "L": L, "sweeps_per_step": S, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (state 512 MiB per GPU)", "reductions": "fp64"},
+            "clocks": clk, "gpu_launches": launches,
+            "e2e": {"value": e2e_value, "unit": "site-updates/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "roofline": roofline,
+            "step_ms": step_ms,
+        }
+        line.update(extra)
+        print(json.dumps(line))
+    for t in tasks:
+        t.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -107,6 +107,12 @@ int slsf_ctx_destroy(slsf_ctx* ctx);
 int slsf_ctx_memory(const slsf_ctx* ctx, uint64_t* used, uint64_t* budget);
 /* Device bytes a task of these dimensions and measurement plan would take. */
 uint64_t slsf_task_bytes(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t n_bins);
+/* Runs the context's work on `stream` (a cudaStream_t; NULL restores the
+ * context's own stream), so a host framework can order and time it with its
+ * own events.  No reference counterpart. */
+int slsf_ctx_set_stream(slsf_ctx* ctx, void* stream);
+/* Number of kernels the library has launched on this context. */
+int slsf_ctx_launch_count(const slsf_ctx* ctx, uint64_t* launches);
 
 /* ---------------------------------------------------------------- one task */
 
@@ -186,6 +192,13 @@ int slsf_task_reset_bins(slsf_task* task);
  * the work is done. */
 int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n_tasks, uint32_t n_sweeps,
                    slsf_sweep_stats* stats);
+
+/* Bin means of many tasks in one device gather and one copy: out is
+ * [n_tasks][n_rows][SLSF_BIN_COLS]; measurements (may be NULL) receives each
+ * task's measurement count.  The batched form of slsf_task_get_bins, feeding
+ * carlo-mc's binned estimates (src/model.rs:906-934). */
+int slsf_batch_get_bins(slsf_ctx* ctx, slsf_task* const* tasks, size_t n_tasks, size_t n_rows,
+                        double* out, uint64_t* measurements);
 
 #ifdef __cplusplus
 }

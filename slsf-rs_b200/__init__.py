@@ -98,6 +98,9 @@ SIGNATURES = {
     "slsf_task_get_bins": (C.c_int, [_P, _F64P, C.c_size_t, _U64P]),
     "slsf_task_reset_bins": (C.c_int, [_P]),
     "slsf_batch_run": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_uint32, C.POINTER(SweepStats)]),
+    "slsf_batch_get_bins": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_size_t, _F64P, _U64P]),
+    "slsf_ctx_set_stream": (C.c_int, [_P, _P]),
+    "slsf_ctx_launch_count": (C.c_int, [_P, _U64P]),
 }
 
 _lib = None
@@ -170,11 +173,39 @@ class Context:
         check(load().slsf_ctx_memory(self.h, C.byref(used), C.byref(budget)))
         return used.value, budget.value
 
-    def batch_run(self, tasks, n_sweeps):
-        arr = (_P * len(tasks))(*[t.h for t in tasks])
+    def batch_run(self, tasks, n_sweeps, handles=None):
+        """Run n_sweeps sweeps of every task in one persistent launch.
+
+        `handles` may be a prepared ctypes array of the task handles (see
+        `handle_array`) to avoid rebuilding it on every call."""
+        arr = handles if handles is not None else self.handle_array(tasks)
         stats = (SweepStats * len(tasks))()
         check(load().slsf_batch_run(self.h, arr, len(tasks), n_sweeps, stats))
         return [s.as_dict() for s in stats]
+
+    @staticmethod
+    def handle_array(tasks):
+        return (_P * len(tasks))(*[t.h for t in tasks])
+
+    def batch_bins(self, tasks, n_rows, out=None, handles=None):
+        """Bin means of every task: array [n_tasks, n_rows, 12] (one gather, one copy)."""
+        arr = handles if handles is not None else self.handle_array(tasks)
+        if out is None:
+            out = np.zeros((len(tasks), n_rows, BIN_COLS))
+        meas = np.zeros(len(tasks), dtype=np.uint64)
+        check(load().slsf_batch_get_bins(self.h, arr, len(tasks), n_rows, _ptr(out, C.c_double),
+                                         _ptr(meas, C.c_uint64)))
+        return out, meas
+
+    def set_stream(self, stream_handle):
+        """Run the context's work on a cudaStream_t (an int handle; 0 = own stream)."""
+        check(load().slsf_ctx_set_stream(self.h, C.c_void_p(stream_handle or None)))
+
+    @property
+    def launches(self):
+        n = C.c_uint64()
+        check(load().slsf_ctx_launch_count(self.h, C.byref(n)))
+        return n.value
 
 
 class Task:
@@ -294,6 +325,44 @@ class Task:
 
     def reset_bins(self):
         check(load().slsf_task_reset_bins(self.h))
+
+
+_MASK64 = (1 << 64) - 1
+
+
+def splitmix64_uniforms(seed: int, n: int):
+    """n uniforms in [0, 1) from FastRng(seed) (src/types.rs:18-24): SplitMix64
+    words, top 53 bits times 2^-53 (rand's f64 sampling)."""
+    out = []
+    state = seed & _MASK64
+    for _ in range(n):
+        state = (state + 0x9E3779B97F4A7C15) & _MASK64
+        z = state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _MASK64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _MASK64
+        z ^= z >> 31
+        out.append((z >> 11) * (1.0 / 9007199254740992.0))
+    return np.array(out)
+
+
+def uniform_layer_disorder(lz: int, lo: float, hi: float, seed: int):
+    """Per-layer couplings lo + (hi - lo) u_z, u_z from FastRng(seed) in layer
+    order: the "J_z(z) uniform [0.5, 1.5] per layer from seed" workloads."""
+    return lo + (hi - lo) * splitmix64_uniforms(seed, lz)
+
+
+def _round_half_away(x: float) -> int:
+    """f64::round: halves round away from zero."""
+    import math
+
+    return int(math.copysign(math.floor(abs(x) + 0.5), x))
+
+
+def task_seed(base_seed: int, l_z: int, sample: int, temperature: float, delta_j_xy: float = 0.0,
+              delta_j_z: float = 0.0) -> int:
+    """Run seed of a task (ThetaJobConfig::make_theta_tasks, src/model.rs:741-747)."""
+    return (base_seed + 100_000 * l_z + 1_000 * sample + _round_half_away(100.0 * temperature)
+            + _round_half_away(1_000.0 * delta_j_xy) * 10_000 + _round_half_away(1_000.0 * delta_j_z)) & _MASK64
 
 
 def exported_symbols():

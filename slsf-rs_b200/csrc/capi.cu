@@ -2,15 +2,17 @@
  * C ABI of the library (include/slsf_gpu.h): contexts, tasks, validation with
  * the reference's error strings, and the host side of every launch.
  *
- * Device memory of one task (V = Lx Ly Lz sites):
+ * Device memory of one task (V = Lx Ly Lz sites) is one block from the
+ * context's pool (pool.h), carved into 256-byte aligned arrays:
  *   theta    FP32 [V]          the state, x fastest (src/types.rs:146-149)
  *   jxy, jz  FP32 [Lz]         layer couplings
  *   bonds    u8   [V]          Wolff active-bond bits (+x, +y, +z)
  *   parent   u32  [V]          Wolff union-find forest
  *   partials FP64 [blocks][8]  measurement block sums
  *   result   FP64 [8]          measurement sums
+ *   done     u32               last-block counter of the measurement
  *   stats    u64  [4]          accepted, cluster sites, clusters, error bits
- *   bins     FP64 [n_bins][12] batched-engine measurement bins
+ *   bins     FP64 [n_bins][12] batched-engine measurement bin sums
  */
 #include <cuda_runtime.h>
 
@@ -23,6 +25,7 @@
 
 #include "../../include/slsf_gpu.h"
 #include "engine.h"
+#include "pool.h"
 #include "xy_fp32.h"
 
 using slsf::TaskView;
@@ -40,9 +43,9 @@ int cuda_error(cudaError_t e, const char* what) {
     return set_error(SLSF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-#define SLSF_CUDA(call)                                   \
-    do {                                                  \
-        cudaError_t e_ = (call);                          \
+#define SLSF_CUDA(call)                                      \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
         if (e_ != cudaSuccess) return cuda_error(e_, #call); \
     } while (0)
 
@@ -53,19 +56,66 @@ const char* kErrEven = "red-black Metropolis sweep requires even lattice dimensi
 bool temperature_ok(double t) { return t > 0.0 && std::isfinite(t); }
 bool width_ok(double w) { return w >= 0.0 && std::isfinite(w); }
 
+uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
+
+/* Offsets of the arrays inside a task's block. */
+struct TaskLayout {
+    uint64_t theta, jxy, jz, bonds, parent, partials, result, done, stats, bins, total;
+};
+
+TaskLayout layout_of(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t n_bins) {
+    const uint64_t v = (uint64_t)lx * ly * lz;
+    TaskLayout L;
+    uint64_t o = 0;
+    L.theta = o;
+    o += align256(4 * v);
+    L.jxy = o;
+    o += align256(4ull * lz);
+    L.jz = o;
+    o += align256(4ull * lz);
+    L.bonds = o;
+    o += align256(v);
+    L.parent = o;
+    o += align256(4 * v);
+    L.partials = o;
+    o += align256(8ull * 8 * slsf::measure_partial_blocks((uint32_t)v));
+    L.result = o;
+    o += align256(8 * 8);
+    L.done = o;
+    o += align256(4);
+    L.stats = o;
+    o += align256(8 * slsf::kStatSlots);
+    L.bins = o;
+    o += align256(8ull * slsf::kBinCols * n_bins);
+    L.total = o;
+    return L;
+}
+
 }  // namespace
 
 struct slsf_ctx {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr; /* own_stream or the caller's */
     uint64_t budget = 0;
     uint64_t used = 0;
     uint64_t live_tasks = 0;
+    uint64_t launches = 0;
     int sm_count = 0;
+    slsf::DevicePool pool;
     /* batched engine scratch */
     TaskView* d_views = nullptr;
+    TaskView* h_views = nullptr; /* pinned */
+    unsigned long long* d_batch_stats = nullptr;
+    unsigned long long* h_batch_stats = nullptr; /* pinned */
     uint32_t views_cap = 0;
     unsigned int* d_queue = nullptr;
+    /* bins gather scratch */
+    const double** d_bin_src = nullptr;
+    const double** h_bin_src = nullptr; /* pinned */
+    double* d_bin_out = nullptr;
+    double* h_bin_out = nullptr; /* pinned */
+    size_t gather_tasks_cap = 0, gather_doubles_cap = 0;
 };
 
 struct slsf_task {
@@ -79,7 +129,7 @@ struct slsf_task {
     uint64_t metro_sweeps = 0, wolff_done = 0;
     uint64_t measurements = 0;
     uint64_t bytes = 0;
-    bool counted = false; /* registered in ctx->used / live_tasks */
+    void* block = nullptr;
     float* theta = nullptr;
     float* jxy = nullptr;
     float* jz = nullptr;
@@ -116,15 +166,6 @@ struct slsf_task {
 
 namespace {
 
-uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
-
-uint64_t task_bytes(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t n_bins) {
-    const uint64_t v = (uint64_t)lx * ly * lz;
-    return align256(4 * v) + 2 * align256(4ull * lz) + align256(v) + align256(4 * v) +
-           align256(8ull * 8 * slsf::measure_partial_blocks((uint32_t)v)) + align256(8 * 8) + align256(4) +
-           align256(8 * slsf::kStatSlots) + align256(8ull * slsf::kBinCols * n_bins);
-}
-
 /* Checks the state a sweep needs, with the reference's messages
  * (src/updates.rs:447-450). */
 int check_sweepable(const slsf_task* t) {
@@ -153,6 +194,62 @@ int bind_device(const slsf_ctx* ctx) {
     return SLSF_OK;
 }
 
+/* Grows the batched-engine scratch to hold n views. */
+int ensure_batch_capacity(slsf_ctx* ctx, size_t n) {
+    if (ctx->views_cap >= n) return SLSF_OK;
+    if (ctx->d_views) cudaFree(ctx->d_views);
+    if (ctx->h_views) cudaFreeHost(ctx->h_views);
+    if (ctx->d_batch_stats) cudaFree(ctx->d_batch_stats);
+    if (ctx->h_batch_stats) cudaFreeHost(ctx->h_batch_stats);
+    ctx->d_views = nullptr;
+    ctx->h_views = nullptr;
+    ctx->d_batch_stats = nullptr;
+    ctx->h_batch_stats = nullptr;
+    ctx->views_cap = 0;
+    const size_t cap = std::max<size_t>(n, 64);
+    SLSF_CUDA(cudaMalloc(&ctx->d_views, sizeof(TaskView) * cap));
+    SLSF_CUDA(cudaHostAlloc(&ctx->h_views, sizeof(TaskView) * cap, cudaHostAllocDefault));
+    SLSF_CUDA(cudaMalloc(&ctx->d_batch_stats, 8 * slsf::kStatSlots * cap));
+    SLSF_CUDA(cudaHostAlloc(&ctx->h_batch_stats, 8 * slsf::kStatSlots * cap, cudaHostAllocDefault));
+    ctx->views_cap = (uint32_t)cap;
+    return SLSF_OK;
+}
+
+int ensure_gather_capacity(slsf_ctx* ctx, size_t n, size_t doubles) {
+    if (ctx->gather_tasks_cap < n) {
+        if (ctx->d_bin_src) cudaFree(ctx->d_bin_src);
+        if (ctx->h_bin_src) cudaFreeHost(ctx->h_bin_src);
+        ctx->d_bin_src = nullptr;
+        ctx->h_bin_src = nullptr;
+        ctx->gather_tasks_cap = 0;
+        SLSF_CUDA(cudaMalloc(&ctx->d_bin_src, sizeof(double*) * n));
+        SLSF_CUDA(cudaHostAlloc(&ctx->h_bin_src, sizeof(double*) * n, cudaHostAllocDefault));
+        ctx->gather_tasks_cap = n;
+    }
+    if (ctx->gather_doubles_cap < doubles) {
+        if (ctx->d_bin_out) cudaFree(ctx->d_bin_out);
+        if (ctx->h_bin_out) cudaFreeHost(ctx->h_bin_out);
+        ctx->d_bin_out = nullptr;
+        ctx->h_bin_out = nullptr;
+        ctx->gather_doubles_cap = 0;
+        SLSF_CUDA(cudaMalloc(&ctx->d_bin_out, 8 * doubles));
+        SLSF_CUDA(cudaHostAlloc(&ctx->h_bin_out, 8 * doubles, cudaHostAllocDefault));
+        ctx->gather_doubles_cap = doubles;
+    }
+    return SLSF_OK;
+}
+
+/* Bin sums -> means: full bins hold binsize measurements, the last fewer. */
+void bin_means(const slsf_task* t, const double* sums, double* out, size_t n_rows) {
+    for (size_t b = 0; b < n_rows; ++b) {
+        const uint64_t first = (uint64_t)b * t->binsize;
+        const uint64_t count =
+            t->measurements > first ? std::min<uint64_t>(t->binsize, t->measurements - first) : 0;
+        for (int c = 0; c < slsf::kBinCols; ++c)
+            out[b * slsf::kBinCols + c] = count ? sums[b * slsf::kBinCols + c] / (double)count : 0.0;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -169,7 +266,7 @@ size_t slsf_last_error(char* buf, size_t len) {
 const char* slsf_version(void) { return "slsf-b200 0.1.0 (sm_100a)"; }
 
 uint64_t slsf_task_bytes(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t n_bins) {
-    return task_bytes(lx, ly, lz, n_bins);
+    return layout_of(lx, ly, lz, n_bins).total;
 }
 
 int slsf_ctx_create(int device, uint64_t budget_bytes, uint32_t flags, slsf_ctx** out) {
@@ -185,36 +282,38 @@ int slsf_ctx_create(int device, uint64_t budget_bytes, uint32_t flags, slsf_ctx*
     cudaDeviceProp prop;
     SLSF_CUDA(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10) return set_error(SLSF_ERR_CUDA, "this library is built for sm_100a (B200)");
+    size_t free_b = 0, total_b = 0;
+    SLSF_CUDA(cudaMemGetInfo(&free_b, &total_b));
     slsf_ctx* ctx = new slsf_ctx;
     ctx->device = device;
     ctx->sm_count = prop.multiProcessorCount;
-    size_t free_b = 0, total_b = 0;
-    e = cudaMemGetInfo(&free_b, &total_b);
-    if (e != cudaSuccess) {
-        delete ctx;
-        return cuda_error(e, "cudaMemGetInfo");
-    }
     ctx->budget = budget_bytes ? budget_bytes : (uint64_t)(0.9 * (double)free_b);
-    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_queue, sizeof(unsigned int));
     if (e != cudaSuccess) {
-        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
         delete ctx;
         return cuda_error(e, "context set-up");
     }
+    ctx->stream = ctx->own_stream;
     *out = ctx;
     return SLSF_OK;
 }
 
 int slsf_ctx_destroy(slsf_ctx* ctx) {
     if (!ctx) return SLSF_OK;
-    if (ctx->live_tasks)
-        return set_error(SLSF_ERR_STATE, "context still owns tasks; destroy them first");
+    if (ctx->live_tasks) return set_error(SLSF_ERR_STATE, "context still owns tasks; destroy them first");
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    if (ctx->d_views) cudaFree(ctx->d_views);
-    if (ctx->d_queue) cudaFree(ctx->d_queue);
-    cudaStreamDestroy(ctx->stream);
+    cudaStreamSynchronize(ctx->own_stream);
+    void* dev[] = {ctx->d_views, ctx->d_batch_stats, ctx->d_queue, (void*)ctx->d_bin_src, ctx->d_bin_out};
+    for (void* p : dev)
+        if (p) cudaFree(p);
+    void* host[] = {ctx->h_views, ctx->h_batch_stats, (void*)ctx->h_bin_src, ctx->h_bin_out};
+    for (void* p : host)
+        if (p) cudaFreeHost(p);
+    ctx->pool.release();
+    cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return SLSF_OK;
 }
@@ -223,6 +322,20 @@ int slsf_ctx_memory(const slsf_ctx* ctx, uint64_t* used, uint64_t* budget) {
     if (!ctx) return set_error(SLSF_ERR_INVALID, "context is NULL");
     if (used) *used = ctx->used;
     if (budget) *budget = ctx->budget;
+    return SLSF_OK;
+}
+
+int slsf_ctx_set_stream(slsf_ctx* ctx, void* stream) {
+    if (!ctx) return set_error(SLSF_ERR_INVALID, "context is NULL");
+    if (int rc = bind_device(ctx)) return rc;
+    SLSF_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return SLSF_OK;
+}
+
+int slsf_ctx_launch_count(const slsf_ctx* ctx, uint64_t* launches) {
+    if (!ctx || !launches) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    *launches = ctx->launches;
     return SLSF_OK;
 }
 
@@ -242,11 +355,14 @@ int slsf_task_create(slsf_ctx* ctx, const slsf_task_desc* d, slsf_task** out) {
         if (d->j_xy[i] < 0.0 || d->j_z[i] < 0.0)
             return set_error(SLSF_ERR_INVALID, "theta simulation requires nonnegative layer couplings");
     if (d->n_bins > 0 && d->binsize == 0) return set_error(SLSF_ERR_INVALID, "binsize must be positive");
-    const uint64_t bytes = task_bytes(d->lx, d->ly, d->lz, d->n_bins);
-    if (ctx->used + bytes > ctx->budget)
+    const TaskLayout L = layout_of(d->lx, d->ly, d->lz, d->n_bins);
+    if (ctx->used + L.total > ctx->budget)
         return set_error(SLSF_ERR_BUDGET, "task does not fit in the context's device memory budget");
     if (int rc = bind_device(ctx)) return rc;
 
+    void* block = nullptr;
+    cudaError_t e = ctx->pool.allocate(L.total, &block);
+    if (e != cudaSuccess) return cuda_error(e, "device pool allocation");
     slsf_task* t = new slsf_task;
     t->ctx = ctx;
     t->lx = d->lx;
@@ -260,58 +376,50 @@ int slsf_task_create(slsf_ctx* ctx, const slsf_task_desc* d, slsf_task** out) {
     t->thermalization = d->thermalization;
     t->binsize = d->binsize ? d->binsize : 1;
     t->n_bins = d->n_bins;
-    t->bytes = bytes;
-    cudaError_t e = cudaSuccess;
-    auto alloc = [&](void** p, size_t n) {
-        if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(n, 1));
-    };
-    alloc((void**)&t->theta, 4ull * volume);
-    alloc((void**)&t->jxy, 4ull * d->lz);
-    alloc((void**)&t->jz, 4ull * d->lz);
-    alloc((void**)&t->bonds, volume);
-    alloc((void**)&t->parent, 4ull * volume);
-    alloc((void**)&t->partials, 8ull * 8 * slsf::measure_partial_blocks(t->volume));
-    alloc((void**)&t->result, 8 * 8);
-    alloc((void**)&t->done, 4);
-    alloc((void**)&t->stats, 8 * slsf::kStatSlots);
-    alloc((void**)&t->bins, 8ull * slsf::kBinCols * d->n_bins);
-    std::vector<float> jx(d->lz), jzv(d->lz);
+    t->bytes = L.total;
+    t->block = block;
+    char* b = static_cast<char*>(block);
+    t->theta = reinterpret_cast<float*>(b + L.theta);
+    t->jxy = reinterpret_cast<float*>(b + L.jxy);
+    t->jz = reinterpret_cast<float*>(b + L.jz);
+    t->bonds = reinterpret_cast<uint8_t*>(b + L.bonds);
+    t->parent = reinterpret_cast<uint32_t*>(b + L.parent);
+    t->partials = reinterpret_cast<double*>(b + L.partials);
+    t->result = reinterpret_cast<double*>(b + L.result);
+    t->done = reinterpret_cast<unsigned int*>(b + L.done);
+    t->stats = reinterpret_cast<unsigned long long*>(b + L.stats);
+    t->bins = reinterpret_cast<double*>(b + L.bins);
+    std::vector<float> jv(2 * (size_t)d->lz);
     for (uint32_t i = 0; i < d->lz; ++i) {
-        jx[i] = (float)d->j_xy[i];
-        jzv[i] = (float)d->j_z[i];
+        jv[i] = (float)d->j_xy[i];
+        jv[d->lz + i] = (float)d->j_z[i];
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(t->jxy, jx.data(), 4ull * d->lz, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(t->jz, jzv.data(), 4ull * d->lz, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(t->theta, 0, 4ull * volume, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(t->done, 0, 4, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(t->stats, 0, 8 * slsf::kStatSlots, ctx->stream);
-    if (e == cudaSuccess && d->n_bins)
-        e = cudaMemsetAsync(t->bins, 0, 8ull * slsf::kBinCols * d->n_bins, ctx->stream);
+    /* theta, jxy and jz are separate 256-byte aligned arrays; zero the whole
+     * block, then copy J.  The copy is synchronous: jv is pageable. */
+    e = cudaMemsetAsync(block, 0, L.total, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(t->jxy, jv.data(), 4ull * d->lz, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(t->jz, jv.data() + d->lz, 4ull * d->lz, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
-        slsf_task_destroy(t);
-        return cuda_error(e, "task allocation");
+        ctx->pool.free(block, L.total);
+        delete t;
+        return cuda_error(e, "task set-up");
     }
-    ctx->used += bytes;
+    ctx->used += L.total;
     ctx->live_tasks += 1;
-    t->counted = true;
     *out = t;
     return SLSF_OK;
 }
 
 int slsf_task_destroy(slsf_task* t) {
     if (!t) return SLSF_OK;
-    if (t->ctx) {
-        cudaSetDevice(t->ctx->device);
-        cudaStreamSynchronize(t->ctx->stream);
-    }
-    void* ptrs[] = {t->theta, t->jxy, t->jz, t->bonds, t->parent, t->partials, t->result, t->done, t->stats, t->bins};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
-    if (t->ctx && t->counted) {
-        t->ctx->used -= t->bytes;
-        t->ctx->live_tasks -= 1;
-    }
+    slsf_ctx* ctx = t->ctx;
+    cudaSetDevice(ctx->device);
+    /* Work queued on the stream may still use the block. */
+    cudaStreamSynchronize(ctx->stream);
+    ctx->pool.free(t->block, t->bytes);
+    ctx->used -= t->bytes;
+    ctx->live_tasks -= 1;
     delete t;
     return SLSF_OK;
 }
@@ -320,6 +428,7 @@ int slsf_task_init_random(slsf_task* t) {
     if (!t) return set_error(SLSF_ERR_INVALID, "task is NULL");
     if (int rc = bind_device(t->ctx)) return rc;
     slsf::launch_init_random(t->theta, t->volume, t->seed, t->ctx->stream);
+    t->ctx->launches += 1;
     SLSF_CUDA(cudaGetLastError());
     SLSF_CUDA(cudaStreamSynchronize(t->ctx->stream));
     return SLSF_OK;
@@ -372,16 +481,16 @@ int slsf_task_metropolis_color(slsf_task* t, uint32_t colour, uint8_t* accept_ma
     if (int rc = bind_device(t->ctx)) return rc;
     uint8_t* d_mask = nullptr;
     if (accept_mask) {
-        SLSF_CUDA(cudaMallocAsync((void**)&d_mask, t->volume, t->ctx->stream));
+        /* the bonds array doubles as the mask buffer: one byte per site */
+        d_mask = t->bonds;
         SLSF_CUDA(cudaMemsetAsync(d_mask, 0, t->volume, t->ctx->stream));
     }
     if (int rc = zero_stats(t)) return rc;
     slsf::launch_metro_colour(t->view(), t->metro_sweeps, colour, d_mask, t->ctx->stream);
+    t->ctx->launches += 1;
     SLSF_CUDA(cudaGetLastError());
-    if (accept_mask) {
+    if (accept_mask)
         SLSF_CUDA(cudaMemcpyAsync(accept_mask, d_mask, t->volume, cudaMemcpyDeviceToHost, t->ctx->stream));
-        SLSF_CUDA(cudaFreeAsync(d_mask, t->ctx->stream));
-    }
     unsigned long long st[slsf::kStatSlots];
     if (int rc = read_stats(t, st)) return rc;
     if (accepted) *accepted = st[slsf::kStatAccepted];
@@ -396,6 +505,7 @@ int slsf_task_metropolis_sweep(slsf_task* t, double* acceptance) {
     const TaskView v = t->view();
     slsf::launch_metro_colour(v, t->metro_sweeps, 0, nullptr, t->ctx->stream);
     slsf::launch_metro_colour(v, t->metro_sweeps, 1, nullptr, t->ctx->stream);
+    t->ctx->launches += 2;
     SLSF_CUDA(cudaGetLastError());
     unsigned long long st[slsf::kStatSlots];
     if (int rc = read_stats(t, st)) return rc;
@@ -411,17 +521,26 @@ int slsf_task_wolff_step_debug(slsf_task* t, uint8_t* bonds, uint8_t* cluster, f
     if (!temperature_ok(t->temperature)) return set_error(SLSF_ERR_INVALID, kErrTemperature);
     if (int rc = bind_device(t->ctx)) return rc;
     if (int rc = zero_stats(t)) return rc;
-    uint8_t* d_cluster = nullptr;
-    if (cluster) SLSF_CUDA(cudaMallocAsync((void**)&d_cluster, t->volume, t->ctx->stream));
+    /* The exported cluster mask needs a byte per site of its own; it comes
+     * from the pool and goes back after the copy. */
+    void* d_cluster = nullptr;
+    if (cluster) {
+        cudaError_t e = t->ctx->pool.allocate(align256(t->volume), &d_cluster);
+        if (e != cudaSuccess) return cuda_error(e, "debug buffer");
+    }
     float phi_h = 0;
     uint32_t site[3] = {0, 0, 0};
-    slsf::launch_wolff(t->view(), t->wolff_done, t->bonds, t->parent, d_cluster, t->ctx->stream, &phi_h, site);
-    SLSF_CUDA(cudaGetLastError());
-    if (bonds) SLSF_CUDA(cudaMemcpyAsync(bonds, t->bonds, t->volume, cudaMemcpyDeviceToHost, t->ctx->stream));
-    if (cluster) {
-        SLSF_CUDA(cudaMemcpyAsync(cluster, d_cluster, t->volume, cudaMemcpyDeviceToHost, t->ctx->stream));
-        SLSF_CUDA(cudaFreeAsync(d_cluster, t->ctx->stream));
-    }
+    slsf::launch_wolff(t->view(), t->wolff_done, t->bonds, t->parent, (uint8_t*)d_cluster, t->ctx->stream, &phi_h,
+                       site);
+    t->ctx->launches += 3;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && bonds)
+        e = cudaMemcpyAsync(bonds, t->bonds, t->volume, cudaMemcpyDeviceToHost, t->ctx->stream);
+    if (e == cudaSuccess && cluster)
+        e = cudaMemcpyAsync(cluster, d_cluster, t->volume, cudaMemcpyDeviceToHost, t->ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t->ctx->stream);
+    if (d_cluster) t->ctx->pool.free(d_cluster, align256(t->volume));
+    if (e != cudaSuccess) return cuda_error(e, "wolff step");
     unsigned long long st[slsf::kStatSlots];
     if (int rc = read_stats(t, st)) return rc;
     t->wolff_done += 1;
@@ -445,9 +564,11 @@ int slsf_task_sweep(slsf_task* t, uint32_t n_sweeps, slsf_sweep_stats* stats) {
         slsf::launch_metro_colour(v, t->metro_sweeps, 0, nullptr, t->ctx->stream);
         slsf::launch_metro_colour(v, t->metro_sweeps, 1, nullptr, t->ctx->stream);
         t->metro_sweeps += 1;
+        t->ctx->launches += 2;
         for (uint32_t k = 0; k < t->wolff_steps; ++k) {
             slsf::launch_wolff(v, t->wolff_done, t->bonds, t->parent, nullptr, t->ctx->stream, nullptr, nullptr);
             t->wolff_done += 1;
+            t->ctx->launches += 3;
         }
     }
     SLSF_CUDA(cudaGetLastError());
@@ -466,6 +587,7 @@ int slsf_task_measure(slsf_task* t, slsf_observables* out) {
     if (!t || !out) return set_error(SLSF_ERR_INVALID, "NULL argument");
     if (int rc = bind_device(t->ctx)) return rc;
     slsf::launch_measure(t->view(), t->partials, t->done, t->result, t->ctx->stream);
+    t->ctx->launches += 1;
     SLSF_CUDA(cudaGetLastError());
     double r[8];
     SLSF_CUDA(cudaMemcpyAsync(r, t->result, sizeof(r), cudaMemcpyDeviceToHost, t->ctx->stream));
@@ -495,18 +617,22 @@ int slsf_task_correlations(slsf_task* t, uint32_t rmax_xy, uint32_t rmax_z, doub
     if (int rc = bind_device(t->ctx)) return rc;
     const size_t work_n = slsf::correlation_work_doubles(t->lx, t->ly, t->lz, rmax_xy, rmax_z);
     const size_t nsx = (size_t)t->lz * rmax_xy, nsz = rmax_z;
-    double* d = nullptr;
-    SLSF_CUDA(cudaMallocAsync((void**)&d, 8 * (work_n + 2 * nsx + nsz + 1), t->ctx->stream));
+    const size_t bytes = align256(8 * (work_n + 2 * nsx + nsz + 1));
+    void* dv = nullptr;
+    cudaError_t e = t->ctx->pool.allocate(bytes, &dv);
+    if (e != cudaSuccess) return cuda_error(e, "correlation scratch");
+    double* d = static_cast<double*>(dv);
     double* sx = d + work_n;
     double* sy = sx + nsx;
     double* sz = sy + nsx;
     slsf::launch_correlations(t->view(), rmax_xy, rmax_z, d, work_n, sx, sy, sz, t->ctx->stream);
-    cudaError_t e = cudaGetLastError();
+    t->ctx->launches += (rmax_xy ? 4 : 0) + (rmax_z ? 2 : 0);
+    e = cudaGetLastError();
     std::vector<double> h(2 * nsx + nsz);
     if (e == cudaSuccess && !h.empty())
         e = cudaMemcpyAsync(h.data(), sx, 8 * h.size(), cudaMemcpyDeviceToHost, t->ctx->stream);
-    cudaFreeAsync(d, t->ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(t->ctx->stream);
+    t->ctx->pool.free(dv, bytes);
     if (e != cudaSuccess) return cuda_error(e, "correlations");
     const double volume = (double)t->volume, area = (double)t->lx * t->ly;
     for (uint32_t r = 0; r < rmax_xy; ++r) {
@@ -532,15 +658,10 @@ int slsf_task_get_bins(const slsf_task* t, double* bins, size_t n_rows, uint64_t
     if (!bins || n_rows == 0) return SLSF_OK;
     if (n_rows > t->n_bins) return set_error(SLSF_ERR_INVALID, "more bin rows requested than the task keeps");
     if (int rc = bind_device(t->ctx)) return rc;
-    SLSF_CUDA(cudaMemcpyAsync(bins, t->bins, 8ull * slsf::kBinCols * n_rows, cudaMemcpyDeviceToHost, t->ctx->stream));
+    std::vector<double> sums(n_rows * slsf::kBinCols);
+    SLSF_CUDA(cudaMemcpyAsync(sums.data(), t->bins, 8 * sums.size(), cudaMemcpyDeviceToHost, t->ctx->stream));
     SLSF_CUDA(cudaStreamSynchronize(t->ctx->stream));
-    /* Sums -> means: full bins hold binsize measurements, the last one fewer. */
-    for (size_t b = 0; b < n_rows; ++b) {
-        const uint64_t first = (uint64_t)b * t->binsize;
-        const uint64_t count = t->measurements > first ? std::min<uint64_t>(t->binsize, t->measurements - first) : 0;
-        for (int c = 0; c < slsf::kBinCols; ++c)
-            bins[b * slsf::kBinCols + c] = count ? bins[b * slsf::kBinCols + c] / (double)count : 0.0;
-    }
+    bin_means(t, sums.data(), bins, n_rows);
     return SLSF_OK;
 }
 
@@ -559,7 +680,6 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_
     if (!ctx || (!tasks && n)) return set_error(SLSF_ERR_INVALID, "NULL argument");
     if (n == 0 || n_sweeps == 0) return SLSF_OK;
     if (int rc = bind_device(ctx)) return rc;
-    std::vector<TaskView> views(n);
     uint32_t max_volume = 0, max_rows = 0, max_lz = 0;
     for (size_t i = 0; i < n; ++i) {
         slsf_task* t = tasks[i];
@@ -569,34 +689,30 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_
             return set_error(SLSF_ERR_INVALID,
                              "lattice not supported by the shared-memory batched kernel (needs L_x <= 32, "
                              "L_x % 4 == 0 and the replica in shared memory)");
-        views[i] = t->view();
         max_volume = std::max(max_volume, t->volume);
         max_rows = std::max(max_rows, t->ly * t->lz);
         max_lz = std::max(max_lz, t->lz);
-        SLSF_CUDA(cudaMemsetAsync(t->stats, 0, 8 * slsf::kStatSlots, ctx->stream));
     }
-    /* Largest replicas first, so the persistent grid ends evenly. */
+    if (int rc = ensure_batch_capacity(ctx, n)) return rc;
+    /* Largest replicas first, so the persistent grid ends evenly; each view
+     * accumulates its counters into its own slot of the batch stats array. */
     std::vector<size_t> order(n);
     for (size_t i = 0; i < n; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(),
                      [&](size_t a, size_t b) { return tasks[a]->volume > tasks[b]->volume; });
-    std::vector<TaskView> sorted(n);
-    for (size_t i = 0; i < n; ++i) sorted[i] = views[order[i]];
-    views.swap(sorted);
-    if (ctx->views_cap < n) {
-        if (ctx->d_views) SLSF_CUDA(cudaFree(ctx->d_views));
-        ctx->d_views = nullptr;
-        SLSF_CUDA(cudaMalloc(&ctx->d_views, sizeof(TaskView) * n));
-        ctx->views_cap = (uint32_t)n;
+    for (size_t k = 0; k < n; ++k) {
+        TaskView v = tasks[order[k]]->view();
+        v.stats = ctx->d_batch_stats + slsf::kStatSlots * order[k];
+        ctx->h_views[k] = v;
     }
-    SLSF_CUDA(cudaMemcpyAsync(ctx->d_views, views.data(), sizeof(TaskView) * n, cudaMemcpyHostToDevice, ctx->stream));
+    SLSF_CUDA(cudaMemcpyAsync(ctx->d_views, ctx->h_views, sizeof(TaskView) * n, cudaMemcpyHostToDevice, ctx->stream));
+    SLSF_CUDA(cudaMemsetAsync(ctx->d_batch_stats, 0, 8 * slsf::kStatSlots * n, ctx->stream));
     SLSF_CUDA(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int), ctx->stream));
     SLSF_CUDA(slsf::launch_batched(ctx->d_views, (uint32_t)n, n_sweeps, ctx->d_queue, ctx->device, ctx->stream,
                                    max_volume, max_rows, max_lz));
-    std::vector<unsigned long long> st(n * slsf::kStatSlots);
-    for (size_t i = 0; i < n; ++i)
-        SLSF_CUDA(cudaMemcpyAsync(&st[i * slsf::kStatSlots], tasks[i]->stats, 8 * slsf::kStatSlots,
-                                  cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->launches += 1;
+    SLSF_CUDA(cudaMemcpyAsync(ctx->h_batch_stats, ctx->d_batch_stats, 8 * slsf::kStatSlots * n,
+                              cudaMemcpyDeviceToHost, ctx->stream));
     SLSF_CUDA(cudaStreamSynchronize(ctx->stream));
     int rc = SLSF_OK;
     for (size_t i = 0; i < n; ++i) {
@@ -606,8 +722,8 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_
         t->wolff_done += (uint64_t)n_sweeps * t->wolff_steps;
         /* Measurements happen after sweeps past the thermalization count. */
         const uint64_t lo = std::max<uint64_t>(before, t->thermalization);
-        if (t->metro_sweeps > lo) t->measurements += t->metro_sweeps - lo;
-        const unsigned long long* s = &st[i * slsf::kStatSlots];
+        if (t->metro_sweeps > lo && t->n_bins) t->measurements += t->metro_sweeps - lo;
+        const unsigned long long* s = &ctx->h_batch_stats[i * slsf::kStatSlots];
         if (s[slsf::kStatError]) rc = set_error(SLSF_ERR_TIMEOUT, "a bounded device loop hit its iteration limit");
         if (stats) {
             stats[i].sweeps = n_sweeps;
@@ -617,6 +733,30 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_
         }
     }
     return rc;
+}
+
+int slsf_batch_get_bins(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, size_t n_rows, double* out,
+                        uint64_t* measurements) {
+    if (!ctx || (!tasks && n)) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    if (n == 0) return SLSF_OK;
+    for (size_t i = 0; i < n; ++i) {
+        if (!tasks[i] || tasks[i]->ctx != ctx) return set_error(SLSF_ERR_INVALID, "task does not belong to this context");
+        if (n_rows > tasks[i]->n_bins) return set_error(SLSF_ERR_INVALID, "more bin rows requested than the task keeps");
+        if (measurements) measurements[i] = tasks[i]->measurements;
+    }
+    if (!out || n_rows == 0) return SLSF_OK;
+    if (int rc = bind_device(ctx)) return rc;
+    const size_t per = n_rows * slsf::kBinCols;
+    if (int rc = ensure_gather_capacity(ctx, n, n * per)) return rc;
+    for (size_t i = 0; i < n; ++i) ctx->h_bin_src[i] = tasks[i]->bins;
+    SLSF_CUDA(cudaMemcpyAsync(ctx->d_bin_src, ctx->h_bin_src, sizeof(double*) * n, cudaMemcpyHostToDevice, ctx->stream));
+    slsf::launch_gather(ctx->d_bin_src, (uint32_t)n, (uint32_t)per, ctx->d_bin_out, ctx->stream);
+    ctx->launches += 1;
+    SLSF_CUDA(cudaGetLastError());
+    SLSF_CUDA(cudaMemcpyAsync(ctx->h_bin_out, ctx->d_bin_out, 8 * n * per, cudaMemcpyDeviceToHost, ctx->stream));
+    SLSF_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < n; ++i) bin_means(tasks[i], ctx->h_bin_out + i * per, out + i * per, n_rows);
+    return SLSF_OK;
 }
 
 }  // extern "C"

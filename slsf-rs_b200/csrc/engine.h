@@ -58,6 +58,8 @@ void launch_correlations(const TaskView& t, uint32_t rmax_xy, uint32_t rmax_z, d
                          cudaStream_t s);
 size_t correlation_work_doubles(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rmax_xy,
                                 uint32_t rmax_z);
+/* dst[i * per + k] = src[i][k] for i < n, k < per. */
+void launch_gather(const double* const* src, uint32_t n, uint32_t per, double* dst, cudaStream_t s);
 
 /* ---- batched persistent engine (kernel_batched.cu) ---- */
 struct BatchLimits {

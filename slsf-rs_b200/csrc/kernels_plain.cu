@@ -329,7 +329,18 @@ __global__ void k_sum_groups(const double* __restrict__ in, uint32_t groups, uin
 
 inline uint32_t blocks_for(uint64_t n, int threads) { return (uint32_t)((n + threads - 1) / threads); }
 
+/* One block per source array; coalesced copy into the contiguous output. */
+__global__ void k_gather(const double* const* __restrict__ src, uint32_t per, double* __restrict__ dst) {
+    const double* s = src[blockIdx.x];
+    double* d = dst + (size_t)blockIdx.x * per;
+    for (uint32_t k = threadIdx.x; k < per; k += blockDim.x) d[k] = s[k];
+}
+
 }  // namespace
+
+void launch_gather(const double* const* src, uint32_t n, uint32_t per, double* dst, cudaStream_t s) {
+    k_gather<<<n, 128, 0, s>>>(src, per, dst);
+}
 
 void launch_init_random(float* theta, uint32_t volume, uint64_t seed, cudaStream_t s) {
     const uint32_t quads = (volume + 3) / 4;
