@@ -58,6 +58,10 @@ bool width_ok(double w) { return w >= 0.0 && std::isfinite(w); }
 
 uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
 
+/* One work-queue counter per kernel group of a batch: the one-CTA kernel and
+ * the cluster kernel at sizes 1, 2, 4, 8. */
+constexpr int kQueues = 5;
+
 /* Offsets of the arrays inside a task's block. */
 struct TaskLayout {
     uint64_t theta, jxy, jz, bonds, parent, partials, result, done, stats, bins, total;
@@ -289,7 +293,7 @@ int slsf_ctx_create(int device, uint64_t budget_bytes, uint32_t flags, slsf_ctx*
     ctx->sm_count = prop.multiProcessorCount;
     ctx->budget = budget_bytes ? budget_bytes : (uint64_t)(0.9 * (double)free_b);
     e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_queue, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_queue, sizeof(unsigned int) * kQueues);
     if (e != cudaSuccess) {
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
         delete ctx;
@@ -680,26 +684,34 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_
     if (!ctx || (!tasks && n)) return set_error(SLSF_ERR_INVALID, "NULL argument");
     if (n == 0 || n_sweeps == 0) return SLSF_OK;
     if (int rc = bind_device(ctx)) return rc;
-    uint32_t max_volume = 0, max_rows = 0, max_lz = 0;
+    std::vector<uint32_t> csize(n);
     for (size_t i = 0; i < n; ++i) {
         slsf_task* t = tasks[i];
         if (!t || t->ctx != ctx) return set_error(SLSF_ERR_INVALID, "task does not belong to this context");
         if (int rc = check_sweepable(t)) return rc;
-        if (!slsf::batched_supports(t->lx, t->ly, t->lz, ctx->device))
-            return set_error(SLSF_ERR_INVALID,
-                             "lattice not supported by the shared-memory batched kernel (needs L_x <= 32, "
-                             "L_x % 4 == 0 and the replica in shared memory)");
-        max_volume = std::max(max_volume, t->volume);
-        max_rows = std::max(max_rows, t->ly * t->lz);
-        max_lz = std::max(max_lz, t->lz);
+        /* 0: one CTA holds the replica (kernel_resident.cu); else the
+         * cluster size of kernel_cluster.cu. */
+        if (slsf::resident_supports(t->lx, t->ly, t->lz, ctx->device)) {
+            csize[i] = 0;
+        } else {
+            csize[i] = slsf::batched_cluster_size(t->lx, t->ly, t->lz, ctx->device);
+            if (!csize[i])
+                return set_error(SLSF_ERR_INVALID,
+                                 "lattice not supported by the shared-memory batched kernels (needs L_x <= 32, "
+                                 "L_x % 4 == 0, even L_y and L_z, and a slab of at most 8 CTAs in shared memory)");
+        }
     }
     if (int rc = ensure_batch_capacity(ctx, n)) return rc;
-    /* Largest replicas first, so the persistent grid ends evenly; each view
-     * accumulates its counters into its own slot of the batch stats array. */
+    /* Grouped by kernel (one persistent launch each, cluster groups first),
+     * largest replicas first within a group so the grid ends evenly; each
+     * view accumulates its counters into its own slot of the batch stats
+     * array. */
     std::vector<size_t> order(n);
     for (size_t i = 0; i < n; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](size_t a, size_t b) { return tasks[a]->volume > tasks[b]->volume; });
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        if (csize[a] != csize[b]) return csize[a] > csize[b];
+        return tasks[a]->volume > tasks[b]->volume;
+    });
     for (size_t k = 0; k < n; ++k) {
         TaskView v = tasks[order[k]]->view();
         v.stats = ctx->d_batch_stats + slsf::kStatSlots * order[k];
@@ -707,10 +719,29 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_
     }
     SLSF_CUDA(cudaMemcpyAsync(ctx->d_views, ctx->h_views, sizeof(TaskView) * n, cudaMemcpyHostToDevice, ctx->stream));
     SLSF_CUDA(cudaMemsetAsync(ctx->d_batch_stats, 0, 8 * slsf::kStatSlots * n, ctx->stream));
-    SLSF_CUDA(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int), ctx->stream));
-    SLSF_CUDA(slsf::launch_batched(ctx->d_views, (uint32_t)n, n_sweeps, ctx->d_queue, ctx->device, ctx->stream,
-                                   max_volume, max_rows, max_lz));
-    ctx->launches += 1;
+    SLSF_CUDA(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int) * kQueues, ctx->stream));
+    for (size_t lo = 0, q = 0; lo < n; ++q) {
+        const uint32_t c = csize[order[lo]];
+        size_t hi = lo;
+        const uint32_t parts = c ? c : 1;
+        uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0;
+        while (hi < n && csize[order[hi]] == c) {
+            const slsf_task* t = tasks[order[hi]];
+            max_vs = std::max(max_vs, t->volume / parts);
+            max_rows = std::max(max_rows, t->ly * (t->lz / parts));
+            max_lz = std::max(max_lz, t->lz);
+            max_plane = std::max(max_plane, t->lx * t->ly);
+            ++hi;
+        }
+        if (c == 0)
+            SLSF_CUDA(slsf::launch_resident(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
+                                            ctx->device, ctx->stream, max_vs, max_rows, max_lz));
+        else
+            SLSF_CUDA(slsf::launch_batched(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
+                                           ctx->device, ctx->stream, c, max_vs, max_rows, max_lz, max_plane));
+        ctx->launches += 1;
+        lo = hi;
+    }
     SLSF_CUDA(cudaMemcpyAsync(ctx->h_batch_stats, ctx->d_batch_stats, 8 * slsf::kStatSlots * n,
                               cudaMemcpyDeviceToHost, ctx->stream));
     SLSF_CUDA(cudaStreamSynchronize(ctx->stream));

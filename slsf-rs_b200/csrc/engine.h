@@ -61,18 +61,26 @@ size_t correlation_work_doubles(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t 
 /* dst[i * per + k] = src[i][k] for i < n, k < per. */
 void launch_gather(const double* const* src, uint32_t n, uint32_t per, double* dst, cudaStream_t s);
 
-/* ---- batched persistent engine (kernel_batched.cu) ---- */
-struct BatchLimits {
-    uint32_t max_volume; /* largest replica the shared-memory kernel holds */
-};
-BatchLimits batched_limits(int device);
+/* ---- batched persistent engine, one CTA per replica (kernel_resident.cu) ---- */
+bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);
+/* Runs n_sweeps sweeps of every view in `views_dev` (device array of n);
+ * `queue` is a zeroed device counter.  max_* are the largest volume, row
+ * count (Ly Lz) and Lz over the views. */
+cudaError_t launch_resident(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+                            int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz);
+
+/* ---- batched persistent engine, one cluster per replica (kernel_cluster.cu) ---- */
+/* Thread-block cluster size that holds one replica of these dimensions in
+ * shared memory (1, 2, 4 or 8 CTAs), or 0 if the kernel cannot hold it. */
+uint32_t batched_cluster_size(uint32_t lx, uint32_t ly, uint32_t lz, int device);
 bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);
-/* Runs n_sweeps sweeps of every task view in `views` (device array of n)
- * with a persistent grid; `queue` is a device counter the kernel consumes.
- * max_* are the largest volume, row count (Ly Lz) and Lz over the views. */
-cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps,
-                           unsigned int* queue, int device, cudaStream_t s, uint32_t max_volume,
-                           uint32_t max_rows, uint32_t max_lz);
+/* Runs n_sweeps sweeps of every task view in `views_dev` (device array of
+ * n, all needing the same cluster size) with a persistent grid of clusters;
+ * `queue` is a zeroed device counter the kernel consumes.  max_* are the
+ * largest per-CTA slab volume, slab row count, Lz and Lx Ly over the views. */
+cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+                           int device, cudaStream_t s, uint32_t cluster, uint32_t max_vs, uint32_t max_rows,
+                           uint32_t max_lz, uint32_t max_plane);
 
 }  // namespace slsf
 

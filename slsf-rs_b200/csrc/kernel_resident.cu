@@ -1,28 +1,31 @@
 /*
- * Batched persistent kernel: many replicas of uneven size, one CTA per
- * replica at a time, each replica resident in shared memory for all of its
- * sweeps.  Replaces the carlo-mc Runner's task-by-task loop over
- * ThetaModel::sweep + ThetaModel::measure (src/model.rs:379-442,
- * src/results.rs:200-202) for every task of a batch at once.
+ * Batched persistent kernel for replicas that fit in one CTA's shared
+ * memory: many replicas of uneven size, one CTA per replica at a time, each
+ * replica resident for all of its sweeps.  Replaces the carlo-mc Runner's
+ * task-by-task loop over ThetaModel::sweep + ThetaModel::measure
+ * (src/model.rs:379-442, src/results.rs:200-202) for every task of a batch.
  *
  * Per replica the CTA
- *   1. copies theta from HBM into a colour-split shared layout
- *      (colour c site with index idx at c * (V/2 + 16) + idx/2): every warp
- *      access to one colour is to consecutive words, and the 16-word pad puts
- *      the two colours of neighbouring sites in different banks;
+ *   1. copies theta from HBM into a colour-split shared layout: the colour-c
+ *      site with index idx sits at c * (V/2 + 16) + idx/2, so a warp reading
+ *      one colour reads consecutive words, and the 64-byte pad puts the two
+ *      colours of neighbouring sites in different bank halves;
  *   2. per sweep: two colour half-sweeps (the same decision code as the
  *      single-task kernel, xy_device.cuh), `wolff_steps` Wolff updates, and,
  *      after thermalization, the fused measurement added to the task's bins;
  *   3. copies theta back.
- * HBM traffic is 8 bytes per site per launch, independent of the sweep count.
+ * HBM traffic is 8 bytes per site per launch, independent of the sweep
+ * count.  Trig values are recomputed with __sincosf where needed (a 32^3
+ * replica leaves no room for a cos/sin cache next to theta; the cluster
+ * kernel, kernel_cluster.cu, holds larger replicas with one).
  *
  * Wolff labelling is bit-parallel: the active +x/+y/+z bonds of a row of
- * L_x <= 32 sites are three 32-bit words, and the cluster grows from the seed
- * by OR-ing neighbour rows through the bond words and closing each row along
- * x, until a whole pass changes nothing.  The result is the seed's connected
- * component over the active bonds, which is the set the reference's DFS
- * (src/updates.rs:577-597) collects when fed the same per-bond randoms.
- * Growth is monotone, so the pass count is bounded by V.
+ * L_x <= 32 sites are three 32-bit words; the cluster grows from the seed by
+ * OR-ing neighbour rows through the bond words and closing every row that
+ * gained bits along x, until a pass changes nothing.  The result is the
+ * seed's connected component over the active bonds -- the set the
+ * reference's DFS (src/updates.rs:577-597) collects when fed the same
+ * per-bond randoms.  Growth is monotone, so the pass count is bounded by V.
  */
 #include <algorithm>
 
@@ -35,14 +38,43 @@ namespace slsf {
 namespace {
 
 constexpr int kBThreads = 1024;
-constexpr uint32_t kPad = 16;
+constexpr uint32_t kPad = 16; /* floats: 64 bytes */
 constexpr uint32_t kMaxRowBits = 32;
+
+/* Optional per-phase cycle accounting (build with -DSLSF_PHASE_TIMING):
+ * thread 0 of every CTA adds the clock64 cycles of each phase, measured
+ * between block barriers, to g_phase_cycles; slot 6 counts cluster-growth
+ * passes and slot 7 Wolff updates. */
+#ifdef SLSF_PHASE_TIMING
+__device__ unsigned long long g_res_phase_cycles[8];
+__shared__ long long s_phase_mark;
+#define SLSF_PHASE(k)                                                                     \
+    do {                                                                                  \
+        __syncthreads();                                                                  \
+        if (threadIdx.x == 0) {                                                           \
+            const long long now_ = clock64();                                             \
+            atomicAdd(&g_res_phase_cycles[k], (unsigned long long)(now_ - s_phase_mark)); \
+            s_phase_mark = now_;                                                          \
+        }                                                                                 \
+    } while (0)
+#define SLSF_PHASE_COUNT(k, n)                                                              \
+    do {                                                                                    \
+        if (threadIdx.x == 0) atomicAdd(&g_res_phase_cycles[k], (unsigned long long)(n)); \
+    } while (0)
+#else
+#define SLSF_PHASE(k) \
+    do {              \
+    } while (0)
+#define SLSF_PHASE_COUNT(k, n) \
+    do {                       \
+    } while (0)
+#endif
 
 struct Geo {
     uint32_t lx, ly, lz, volume, half, rows, plane;
     uint32_t stride1; /* offset of the colour-1 array */
     uint32_t xmask;
-    bool lx_divides_warp;
+    bool lx_tiles_warp;
     slsf_fastdiv div_hx, div_ly, div_lx;
 };
 
@@ -57,7 +89,7 @@ __device__ __forceinline__ Geo make_geo(const TaskView& t) {
     g.rows = t.ly * t.lz;
     g.stride1 = g.half + kPad;
     g.xmask = t.lx >= 32 ? 0xffffffffu : ((1u << t.lx) - 1u);
-    g.lx_divides_warp = (32u % t.lx) == 0;
+    g.lx_tiles_warp = (32u % t.lx) == 0;
     g.div_hx = slsf_fastdiv_make(t.lx >> 1);
     g.div_ly = slsf_fastdiv_make(t.ly);
     g.div_lx = slsf_fastdiv_make(t.lx);
@@ -83,8 +115,8 @@ __device__ __forceinline__ Coords coords_of(const Geo& g, uint32_t idx) {
 }
 
 /* Forward neighbours of a site (+x, +y, +z) as natural indices. */
-__device__ __forceinline__ void forward_neighbours(const Geo& g, uint32_t idx, const Coords& c,
-                                                   uint32_t& xp, uint32_t& yp, uint32_t& zp) {
+__device__ __forceinline__ void forward_neighbours(const Geo& g, uint32_t idx, const Coords& c, uint32_t& xp,
+                                                   uint32_t& yp, uint32_t& zp) {
     xp = (c.x + 1 == g.lx) ? idx + 1 - g.lx : idx + 1;
     yp = (c.y + 1 == g.ly) ? idx + g.lx - g.plane : idx + g.lx;
     zp = (c.z + 1 == g.lz) ? idx + g.plane - g.volume : idx + g.plane;
@@ -95,26 +127,34 @@ __device__ __forceinline__ uint32_t xp_lane(uint32_t lane, uint32_t lx) {
     return (lane & ~(lx - 1u)) | ((lane + 1u) & (lx - 1u));
 }
 
-__device__ __forceinline__ uint32_t rotl_row(uint32_t w, uint32_t lx, uint32_t mask) {
-    return lx >= 32 ? __funnelshift_l(w, w, 1) : (((w << 1) | (w >> (lx - 1u))) & mask);
+__device__ __forceinline__ uint32_t rotl_row(uint32_t w, uint32_t s, uint32_t lx, uint32_t mask) {
+    return lx == 32 ? __funnelshift_l(w, w, s) : (((w << s) | (w >> (lx - s))) & mask);
 }
 
-__device__ __forceinline__ uint32_t rotr_row(uint32_t w, uint32_t lx, uint32_t mask) {
-    return lx >= 32 ? __funnelshift_r(w, w, 1) : (((w >> 1) | (w << (lx - 1u))) & mask);
+__device__ __forceinline__ uint32_t rotr_row(uint32_t w, uint32_t s, uint32_t lx, uint32_t mask) {
+    return lx == 32 ? __funnelshift_r(w, w, s) : (((w >> s) | (w << (lx - s))) & mask);
 }
 
-/* Closure of a row's cluster bits along x through the +x bond bits. */
-__device__ __forceinline__ uint32_t close_row(uint32_t c, uint32_t bx, uint32_t lx, uint32_t mask) {
-    for (uint32_t it = 0; it < lx; ++it) {
-        const uint32_t n = c | rotl_row(c & bx, lx, mask) | (rotr_row(c, lx, mask) & bx);
-        if (n == c) break;
-        c = n;
+/* Closure of a periodic row's cluster bits c along x through the bond bits b
+ * (bit x: bond x -- x+1).  Kogge-Stone doubling in both directions: after the
+ * step with shift s, every site within 2s - 1 bond steps of a seed is set;
+ * shifts 1..16 cover any row of L_x <= 32 sites. */
+__device__ __forceinline__ uint32_t close_row(uint32_t c, uint32_t b, uint32_t lx, uint32_t mask) {
+    uint32_t gr = c, pr = b;                        /* rightward: bond p -> p+1 */
+    uint32_t gl = c, pl = rotl_row(b, 1, lx, mask); /* leftward: bond p-1 -> p */
+#pragma unroll
+    for (uint32_t s = 1; s < 32; s <<= 1) {
+        if (s >= lx) break;
+        gr |= rotl_row(gr & pr, s, lx, mask);
+        pr &= rotr_row(pr, s, lx, mask);
+        gl |= rotr_row(gl & pl, s, lx, mask);
+        pl &= rotl_row(pl, s, lx, mask);
     }
-    return c;
+    return gr | gl;
 }
 
 struct Smem {
-    float* th;  /* two colour arrays */
+    float* th; /* two colour arrays */
     uint32_t* bx;
     uint32_t* by;
     uint32_t* bz;
@@ -123,8 +163,7 @@ struct Smem {
     float* jz;
 };
 
-__device__ __forceinline__ Smem carve(unsigned char* base, const Geo& g, uint32_t max_volume,
-                                      uint32_t max_rows, uint32_t max_lz) {
+__device__ __forceinline__ Smem carve(unsigned char* base, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz) {
     Smem s;
     s.th = reinterpret_cast<float*>(base);
     uint32_t* w = reinterpret_cast<uint32_t*>(base + 4ull * (max_volume + 2 * kPad));
@@ -134,7 +173,6 @@ __device__ __forceinline__ Smem carve(unsigned char* base, const Geo& g, uint32_
     s.cl = w + 3 * max_rows;
     s.jxy = reinterpret_cast<float*>(w + 4 * max_rows);
     s.jz = s.jxy + max_lz;
-    (void)g;
     return s;
 }
 
@@ -144,8 +182,7 @@ __device__ __forceinline__ void load_state(const TaskView& t, const Geo& g, Smem
     const float4* src = reinterpret_cast<const float4*>(t.theta);
     for (uint32_t q = threadIdx.x; q < g.volume / 4; q += blockDim.x) {
         const float4 v = src[q];
-        const uint32_t idx = 4 * q;
-        const Coords c = coords_of(g, idx);
+        const Coords c = coords_of(g, 4 * q);
         const uint32_t p = (c.y + c.z) & 1u; /* colour of the even-x site */
         const uint32_t h = 2 * q;
         s.th[p * g.stride1 + h] = v.x;
@@ -162,24 +199,19 @@ __device__ __forceinline__ void load_state(const TaskView& t, const Geo& g, Smem
 __device__ __forceinline__ void store_state(const TaskView& t, const Geo& g, const Smem& s) {
     float4* dst = reinterpret_cast<float4*>(t.theta);
     for (uint32_t q = threadIdx.x; q < g.volume / 4; q += blockDim.x) {
-        const uint32_t idx = 4 * q;
-        const Coords c = coords_of(g, idx);
+        const Coords c = coords_of(g, 4 * q);
         const uint32_t p = (c.y + c.z) & 1u;
         const uint32_t h = 2 * q;
-        float4 v;
-        v.x = s.th[p * g.stride1 + h];
-        v.y = s.th[(p ^ 1u) * g.stride1 + h];
-        v.z = s.th[p * g.stride1 + h + 1];
-        v.w = s.th[(p ^ 1u) * g.stride1 + h + 1];
-        dst[q] = v;
+        dst[q] = make_float4(s.th[p * g.stride1 + h], s.th[(p ^ 1u) * g.stride1 + h], s.th[p * g.stride1 + h + 1],
+                             s.th[(p ^ 1u) * g.stride1 + h + 1]);
     }
 }
 
 /* One colour half-sweep.  A warp owns 32 consecutive Philox blocks (64
  * sites); lanes exchange words so that lane j updates colour-compact sites
  * 2*base + j and 2*base + 32 + j, i.e. consecutive shared words. */
-__device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, Smem& s,
-                                               uint64_t sweep, uint32_t colour) {
+__device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, Smem& s, uint64_t sweep,
+                                               uint32_t colour) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t nwarps = blockDim.x >> 5;
     const uint32_t npairs = (g.half + 1) >> 1;
@@ -200,7 +232,6 @@ __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, 
             if (h >= g.half) continue;
             const float u_prop = slsf_u24f((lane & 1u) ? wz : wx);
             const float u_acc = slsf_u24f((lane & 1u) ? ww : wy);
-            /* decode the colour-compact index */
             const uint32_t row = slsf_fastdiv_div(h, g.div_hx);
             const uint32_t k = h - row * (g.lx >> 1);
             const uint32_t z = slsf_fastdiv_div(row, g.div_ly);
@@ -235,16 +266,48 @@ __device__ __forceinline__ float site_theta(const Geo& g, const Smem& s, uint32_
     return s.th[slot(g, idx, (c.x + c.y + c.z) & 1u)];
 }
 
-/* One Wolff update; returns the cluster size (valid in every thread). */
-__device__ __forceinline__ uint32_t wolff_update(const TaskView& t, const Geo& g, Smem& s,
-                                                 uint64_t counter, uint32_t* s_count) {
+__device__ __forceinline__ float proj_of(float theta, float cphi, float sphi) {
+    float sn, cn;
+    __sincosf(theta, &sn, &cn);
+    return wolff_projection(cn, sn, cphi, sphi);
+}
+
+/* One growth pass: every row takes the cluster bits that reach it through
+ * its y and z bonds; a row that gained bits is closed along x (stored rows
+ * are always closed).  Returns nonzero if any row changed. */
+__device__ __forceinline__ int grow_pass(const Geo& g, Smem& s) {
+    int changed = 0;
+    for (uint32_t r = threadIdx.x; r < g.rows; r += blockDim.x) {
+        const uint32_t old = s.cl[r];
+        const uint32_t z = slsf_fastdiv_div(r, g.div_ly);
+        const uint32_t y = r - z * g.ly;
+        const uint32_t r_yp = (y + 1 == g.ly) ? r + 1 - g.ly : r + 1;
+        const uint32_t r_ym = (y == 0) ? r + g.ly - 1 : r - 1;
+        const uint32_t r_zp = (z + 1 == g.lz) ? r + g.ly - g.rows : r + g.ly;
+        const uint32_t r_zm = (z == 0) ? r + g.rows - g.ly : r - g.ly;
+        const uint32_t in = (s.cl[r_ym] & s.by[r_ym]) | (s.cl[r_yp] & s.by[r]) | (s.cl[r_zm] & s.bz[r_zm]) |
+                            (s.cl[r_zp] & s.bz[r]);
+        const uint32_t c = old | in;
+        if (c != old) {
+            s.cl[r] = close_row(c, s.bx[r], g.lx, g.xmask);
+            changed = 1;
+        }
+    }
+    return changed;
+}
+
+/* One Wolff update (src/updates.rs:551-620); adds the cluster size to *count. */
+__device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Smem& s, uint64_t counter,
+                                             uint32_t* s_count) {
     const uint32_t lane = threadIdx.x & 31u;
     const slsf_u32x4 pick = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_PICK, 0, 0);
     const float phi = slsf_angle_from_word(pick.x);
     const uint32_t x0 = slsf_range(pick.y, g.lx), y0 = slsf_range(pick.z, g.ly), z0 = slsf_range(pick.w, g.lz);
+    float sphi, cphi;
+    __sincosf(phi, &sphi, &cphi);
     const float m2b = __fmul_rn(-2.0f, t.beta);
 
-    if (!g.lx_divides_warp) {
+    if (!g.lx_tiles_warp) {
         for (uint32_t r = threadIdx.x; r < g.rows; r += blockDim.x) {
             s.bx[r] = 0;
             s.by[r] = 0;
@@ -260,32 +323,31 @@ __device__ __forceinline__ uint32_t wolff_update(const TaskView& t, const Geo& g
         const Coords c = coords_of(g, ii);
         uint32_t xp, yp, zp;
         forward_neighbours(g, ii, c, xp, yp, zp);
-        const float ri = wolff_projection(site_theta(g, s, ii, c), phi);
+        const float ri = proj_of(site_theta(g, s, ii, c), cphi, sphi);
         float rxp;
-        if (g.lx_divides_warp) {
+        if (g.lx_tiles_warp) {
             rxp = __shfl_sync(0xffffffffu, ri, xp_lane(lane, g.lx));
         } else {
             const Coords cx = {c.x + 1 == g.lx ? 0 : c.x + 1, c.y, c.z, c.row};
-            rxp = wolff_projection(site_theta(g, s, xp, cx), phi);
+            rxp = proj_of(site_theta(g, s, xp, cx), cphi, sphi);
         }
         const Coords cy = {c.x, c.y + 1 == g.ly ? 0 : c.y + 1, c.z, 0};
         const Coords cz = {c.x, c.y, c.z + 1 == g.lz ? 0 : c.z + 1, 0};
-        const float ryp = wolff_projection(site_theta(g, s, yp, cy), phi);
-        const float rzp = wolff_projection(site_theta(g, s, zp, cz), phi);
+        const float ryp = proj_of(site_theta(g, s, yp, cy), cphi, sphi);
+        const float rzp = proj_of(site_theta(g, s, zp, cz), cphi, sphi);
         const slsf_u32x4 b = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, ii);
         const float jx = s.jxy[c.z], jzz = s.jz[c.z];
         const bool ax = valid && wolff_bond_active(jx, ri, rxp, m2b, b.x);
         const bool ay = valid && wolff_bond_active(jx, ri, ryp, m2b, b.y);
         const bool az = valid && wolff_bond_active(jzz, ri, rzp, m2b, b.z);
-        if (g.lx_divides_warp) {
+        if (g.lx_tiles_warp) {
             const uint32_t bal_x = __ballot_sync(0xffffffffu, ax);
             const uint32_t bal_y = __ballot_sync(0xffffffffu, ay);
             const uint32_t bal_z = __ballot_sync(0xffffffffu, az);
             if (valid && c.x == 0) {
-                const uint32_t sh = lane; /* lane of x == 0 is the row's first bit */
-                s.bx[c.row] = (bal_x >> sh) & g.xmask;
-                s.by[c.row] = (bal_y >> sh) & g.xmask;
-                s.bz[c.row] = (bal_z >> sh) & g.xmask;
+                s.bx[c.row] = (bal_x >> lane) & g.xmask;
+                s.by[c.row] = (bal_y >> lane) & g.xmask;
+                s.bz[c.row] = (bal_z >> lane) & g.xmask;
             }
         } else if (valid) {
             if (ax) atomicOr(&s.bx[c.row], 1u << c.x);
@@ -296,31 +358,17 @@ __device__ __forceinline__ uint32_t wolff_update(const TaskView& t, const Geo& g
     const uint32_t seed_row = y0 + g.ly * z0;
     for (uint32_t r = threadIdx.x; r < g.rows; r += blockDim.x) s.cl[r] = (r == seed_row) ? (1u << x0) : 0u;
     __syncthreads();
+    if (threadIdx.x == 0) s.cl[seed_row] = close_row(s.cl[seed_row], s.bx[seed_row], g.lx, g.xmask);
+    __syncthreads();
+    SLSF_PHASE(2);
 
     /* Grow the seed's component; bounded by V passes (monotone growth). */
-    for (uint32_t pass = 0; pass <= g.volume; ++pass) {
-        int changed = 0;
-        for (uint32_t r = threadIdx.x; r < g.rows; r += blockDim.x) {
-            const uint32_t old = s.cl[r];
-            const uint32_t z = slsf_fastdiv_div(r, g.div_ly);
-            const uint32_t y = r - z * g.ly;
-            const uint32_t r_yp = (y + 1 == g.ly) ? r + 1 - g.ly : r + 1;
-            const uint32_t r_ym = (y == 0) ? r + g.ly - 1 : r - 1;
-            const uint32_t r_zp = (z + 1 == g.lz) ? r + g.ly - g.rows : r + g.ly;
-            const uint32_t r_zm = (z == 0) ? r + g.rows - g.ly : r - g.ly;
-            uint32_t c = old;
-            c |= s.cl[r_ym] & s.by[r_ym];
-            c |= s.cl[r_yp] & s.by[r];
-            c |= s.cl[r_zm] & s.bz[r_zm];
-            c |= s.cl[r_zp] & s.bz[r];
-            if (c) c = close_row(c, s.bx[r], g.lx, g.xmask);
-            if (c != old) {
-                s.cl[r] = c;
-                changed = 1;
-            }
-        }
-        if (!__syncthreads_or(changed)) break;
-    }
+    uint32_t pass = 0;
+    for (; pass <= g.volume; ++pass)
+        if (!__syncthreads_or(grow_pass(g, s))) break;
+    SLSF_PHASE(3);
+    SLSF_PHASE_COUNT(6, pass + 1);
+    SLSF_PHASE_COUNT(7, 1);
 
     /* Reflect the cluster (src/updates.rs:602-617) and count it. */
     uint32_t members = 0;
@@ -336,15 +384,15 @@ __device__ __forceinline__ uint32_t wolff_update(const TaskView& t, const Geo& g
     for (int off = 16; off > 0; off >>= 1) members += __shfl_down_sync(0xffffffffu, members, off);
     if (lane == 0 && members) atomicAdd(s_count, members);
     __syncthreads();
-    return 0;
+    SLSF_PHASE(4);
 }
 
-/* Fused observables of the resident state (src/observables.rs:99-141):
- * mx, my, cos xyz, sin xyz, FP64 per thread and across the block. */
+/* Fused observables of the resident state (src/observables.rs:99-141): mx,
+ * my, cos xyz, sin xyz; FP32 per thread over its sites, FP64 across the
+ * block (valid in thread 0). */
 __device__ __forceinline__ void measure(const Geo& g, const Smem& s, double (&acc)[8], double* red) {
     const uint32_t lane = threadIdx.x & 31u;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+    float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t i0 = (threadIdx.x & ~31u); i0 < g.volume; i0 += blockDim.x) {
         const uint32_t idx = i0 + lane;
         const bool valid = idx < g.volume;
@@ -354,7 +402,7 @@ __device__ __forceinline__ void measure(const Geo& g, const Smem& s, double (&ac
         forward_neighbours(g, ii, c, xp, yp, zp);
         float si, ci, sx, cx, sy, cy, sz, cz;
         __sincosf(site_theta(g, s, ii, c), &si, &ci);
-        if (g.lx_divides_warp) {
+        if (g.lx_tiles_warp) {
             const uint32_t src = xp_lane(lane, g.lx);
             sx = __shfl_sync(0xffffffffu, si, src);
             cx = __shfl_sync(0xffffffffu, ci, src);
@@ -368,22 +416,23 @@ __device__ __forceinline__ void measure(const Geo& g, const Smem& s, double (&ac
         __sincosf(site_theta(g, s, zp, czp), &sz, &cz);
         if (!valid) continue;
         const float jx = s.jxy[c.z], jzz = s.jz[c.z];
-        acc[0] += ci;
-        acc[1] += si;
-        acc[2] += jx * (ci * cx + si * sx);
-        acc[3] += jx * (ci * cy + si * sy);
-        acc[4] += jzz * (ci * cz + si * sz);
-        acc[5] += jx * (si * cx - ci * sx);
-        acc[6] += jx * (si * cy - ci * sy);
-        acc[7] += jzz * (si * cz - ci * sz);
+        f[0] += ci;
+        f[1] += si;
+        f[2] += jx * (ci * cx + si * sx);
+        f[3] += jx * (ci * cy + si * sy);
+        f[4] += jzz * (ci * cz + si * sz);
+        f[5] += jx * (si * cx - ci * sx);
+        f[6] += jx * (si * cy - ci * sy);
+        f[7] += jzz * (si * cz - ci * sz);
     }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[k] = (double)f[k];
     block_sum<8>(acc, red);
 }
 
 __global__ void __launch_bounds__(kBThreads, 1)
-    k_batched(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps,
-              unsigned int* __restrict__ queue, uint32_t max_volume, uint32_t max_rows,
-              uint32_t max_lz) {
+    k_resident(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
+               uint32_t max_volume, uint32_t max_rows, uint32_t max_lz) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[8 * 32];
     __shared__ double bin_acc[kBinCols];
@@ -398,21 +447,26 @@ __global__ void __launch_bounds__(kBThreads, 1)
         if (item >= n) return;
         const TaskView t = views[item];
         const Geo g = make_geo(t);
-        Smem s = carve(smem_raw, g, max_volume, max_rows, max_lz);
+        Smem s = carve(smem_raw, max_volume, max_rows, max_lz);
         if (threadIdx.x == 0) {
             s_cluster = 0;
             s_accepted = 0;
         }
         load_state(t, g, s);
         __syncthreads();
+#ifdef SLSF_PHASE_TIMING
+        if (threadIdx.x == 0) s_phase_mark = clock64();
+#endif
         uint32_t accepted = 0;
         int64_t bin_cur = -1;
         for (uint32_t sw = 0; sw < n_sweeps; ++sw) {
             const uint64_t sweep = t.metro_sweeps + sw;
             accepted += half_sweep(t, g, s, sweep, 0);
             __syncthreads();
+            SLSF_PHASE(0);
             accepted += half_sweep(t, g, s, sweep, 1);
             __syncthreads();
+            SLSF_PHASE(1);
             for (uint32_t k = 0; k < t.wolff_steps; ++k)
                 wolff_update(t, g, s, t.wolff_done + (uint64_t)sw * t.wolff_steps + k, &s_cluster);
             /* ThetaModel::measure after the sweep, once thermalized. */
@@ -422,6 +476,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
                 const int64_t b = (int64_t)(m / t.binsize);
                 double acc[8];
                 measure(g, s, acc, red);
+                SLSF_PHASE(5);
                 if (threadIdx.x == 0) {
                     if (b != bin_cur) {
                         if (bin_cur >= 0 && bin_cur < (int64_t)t.n_bins)
@@ -475,34 +530,39 @@ int max_dynamic_smem(int device) {
 
 }  // namespace
 
-BatchLimits batched_limits(int device) {
-    BatchLimits l;
-    l.max_volume = (uint32_t)(max_dynamic_smem(device) / 4.5);
-    return l;
-}
-
-bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
+bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
     /* Row words hold L_x <= 32 bits; the float4 colour-split copy needs
      * L_x % 4 == 0 so that four consecutive sites never span two rows. */
-    if (lx > kMaxRowBits || lx < 4 || lx % 4) return false;
+    if (lx > kMaxRowBits || lx < 4 || lx % 4 || ly < 2 || ly % 2 || lz < 2 || lz % 2) return false;
     const uint64_t v = (uint64_t)lx * ly * lz;
     return smem_bytes((uint32_t)v, ly * lz, lz) <= (size_t)max_dynamic_smem(device);
 }
 
-cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps,
-                           unsigned int* queue, int device, cudaStream_t s, uint32_t max_volume,
-                           uint32_t max_rows, uint32_t max_lz) {
+cudaError_t launch_resident(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+                            int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz) {
     const size_t smem = smem_bytes(max_volume, max_rows, max_lz);
-    cudaError_t e = cudaFuncSetAttribute(k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int sms = 0, per_sm = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batched, kBThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resident, kBThreads, smem);
     if (e != cudaSuccess) return e;
-    const uint32_t grid = std::min<uint32_t>(n, (uint32_t)(sms * std::max(1, per_sm)));
-    k_batched<<<grid, kBThreads, smem, s>>>(views_dev, n, n_sweeps, queue, max_volume, max_rows, max_lz);
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const uint32_t grid = std::min<uint32_t>(n, (uint32_t)(sms * per_sm));
+    k_resident<<<grid, kBThreads, smem, s>>>(views_dev, n, n_sweeps, queue, max_volume, max_rows, max_lz);
     return cudaGetLastError();
 }
 
 }  // namespace slsf
+
+#ifdef SLSF_PHASE_TIMING
+extern "C" int slsf_debug_resident_phase_cycles(unsigned long long out[8], int reset) {
+    cudaError_t e = cudaMemcpyFromSymbol(out, slsf::g_res_phase_cycles, sizeof(unsigned long long) * 8);
+    if (e == cudaSuccess && reset) {
+        const unsigned long long zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        e = cudaMemcpyToSymbol(slsf::g_res_phase_cycles, zero, sizeof(zero));
+    }
+    return e == cudaSuccess ? 0 : 1;
+}
+#endif

@@ -136,12 +136,19 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t xp = (x + 1 == lx) ? i + 1 - lx : i + 1;
     const uint32_t yp = (y + 1 == ly) ? i + lx - plane : i + lx;
     const uint32_t zp = (z + 1 == lz) ? i + plane - volume : i + plane;
-    const float ri = wolff_projection(theta[i], phi);
+    float sphi, cphi;
+    __sincosf(phi, &sphi, &cphi);
+    auto proj = [&](uint32_t site) {
+        float s, c;
+        __sincosf(theta[site], &s, &c);
+        return wolff_projection(c, s, cphi, sphi);
+    };
+    const float ri = proj(i);
     const slsf_u32x4 b = slsf_stream(seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, i);
     uint32_t bits = 0;
-    if (wolff_bond_active(jxy[z], ri, wolff_projection(theta[xp], phi), minus_two_beta, b.x)) bits |= 1u;
-    if (wolff_bond_active(jxy[z], ri, wolff_projection(theta[yp], phi), minus_two_beta, b.y)) bits |= 2u;
-    if (wolff_bond_active(jz[z], ri, wolff_projection(theta[zp], phi), minus_two_beta, b.z)) bits |= 4u;
+    if (wolff_bond_active(jxy[z], ri, proj(xp), minus_two_beta, b.x)) bits |= 1u;
+    if (wolff_bond_active(jxy[z], ri, proj(yp), minus_two_beta, b.y)) bits |= 2u;
+    if (wolff_bond_active(jz[z], ri, proj(zp), minus_two_beta, b.z)) bits |= 4u;
     bonds[i] = (uint8_t)bits;
     parent[i] = i;
 }

@@ -78,10 +78,11 @@ __device__ __forceinline__ bool metro_decide(float theta, float ci, float si, fl
     return acc;
 }
 
-/* Projection of a spin on the Wolff axis, r = cos(theta - phi)
- * (src/updates.rs:579-582). */
-__device__ __forceinline__ float wolff_projection(float theta, float phi) {
-    return __cosf(__fsub_rn(theta, phi));
+/* Projection of a spin on the Wolff axis from its cached trig,
+ * r = cos(theta) cos(phi) + sin(theta) sin(phi) (src/updates.rs:579-582),
+ * where (s, c) = __sincosf(theta) and (sphi, cphi) = __sincosf(phi). */
+__device__ __forceinline__ float wolff_projection(float c, float s, float cphi, float sphi) {
+    return __fmaf_rn(s, sphi, __fmul_rn(c, cphi));
 }
 
 /* Bond activation of try_add_wolff_neighbor (src/updates.rs:537-548) with a

@@ -49,7 +49,8 @@ def batched_tasks(slsf, ctx, orc, specs):
 
 
 @pytest.mark.parametrize("dims,wolff", [((8, 8, 8), 0), ((8, 8, 8), 1), ((32, 32, 32), 1), ((16, 8, 12), 2),
-                                        ((24, 24, 24), 1), ((32, 16, 8), 1)])
+                                        ((24, 24, 24), 1), ((32, 16, 8), 1), ((12, 10, 6), 1),
+                                        ((32, 32, 48), 1), ((32, 32, 96), 1), ((20, 24, 16), 1)])
 def test_batched_equals_plain_bitwise(slsf, ctx, orc, dims, wolff):
     ref, _ = plain_run(slsf, ctx, orc, dims, 1.1, seed=42, sweeps=4, wolff=wolff)
     [t] = batched_tasks(slsf, ctx, orc, [(dims, 1.1, 42, wolff, 0, 1, 0, 1)])
