@@ -200,6 +200,30 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n_tasks, uint3
 int slsf_batch_get_bins(slsf_ctx* ctx, slsf_task* const* tasks, size_t n_tasks, size_t n_rows,
                         double* out, uint64_t* measurements);
 
+/* ---------------------------------------------------- no device allocation */
+
+/* Largest lattice slsf_measure_noalloc accepts (2^31 - 1 sites). */
+#define SLSF_NOALLOC_MAX_SITES 2147483647ull
+
+/* The fused measurement of slsf_task_measure for a lattice held in the
+ * caller's own device memory (theta [Lx Ly Lz], j_xy [Lz], j_z [Lz], FP32,
+ * layout x + Lx (y + Ly z)), for callers that cannot allocate device memory:
+ * hosts whose own memory pool owns the device, services under a fixed device
+ * memory budget, and loops that must not risk cudaMalloc/cudaFree's
+ * device-wide synchronisation.  It calls no allocating routine.  Its scratch
+ * (per-block partial sums, about 75 KiB) is a static device array that every
+ * GPU loading this library holds until the process exits.
+ *   - Lattices beyond SLSF_NOALLOC_MAX_SITES sites are rejected.
+ *   - All calls share that array and it keeps the last call's contents;
+ *     calls that overlap on the GPU race on it, so serialise them.
+ *   - The first call on a device sets the scratch up on the current device
+ *     (takes its address, zeroes its counter); make it before any stream
+ *     capture.
+ * `stream` is a cudaStream_t (NULL: the default stream); the call waits for
+ * it.  No counterpart in the reference. */
+int slsf_measure_noalloc(const float* theta, const float* j_xy, const float* j_z, uint32_t lx, uint32_t ly,
+                         uint32_t lz, void* stream, slsf_observables* out);
+
 #ifdef __cplusplus
 }
 #endif

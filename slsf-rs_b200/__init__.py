@@ -101,6 +101,8 @@ SIGNATURES = {
     "slsf_batch_get_bins": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_size_t, _F64P, _U64P]),
     "slsf_ctx_set_stream": (C.c_int, [_P, _P]),
     "slsf_ctx_launch_count": (C.c_int, [_P, _U64P]),
+    "slsf_measure_noalloc": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, _P,
+                                       C.POINTER(Observables)]),
 }
 
 _lib = None

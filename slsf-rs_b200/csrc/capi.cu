@@ -49,6 +49,12 @@ int cuda_error(cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_error(e_, #call); \
     } while (0)
 
+}  // namespace
+
+int slsf::report_error(int code, const std::string& message) { return set_error(code, message); }
+
+namespace {
+
 const char* kErrTemperature = "temperature T must be positive and finite";
 const char* kErrWidth = "proposal_width must be nonnegative and finite";
 const char* kErrEven = "red-black Metropolis sweep requires even lattice dimensions";

@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 namespace slsf {
 
 /* Device-side counters of one task. */
@@ -41,6 +43,10 @@ struct TaskView {
     uint32_t thermalization, binsize, n_bins;
     unsigned long long* stats;
 };
+
+/* Records `message` as the calling thread's slsf_last_error text and returns
+ * `code` (capi.cu). */
+int report_error(int code, const std::string& message);
 
 /* ---- single-task kernels (kernels_plain.cu) ---- */
 void launch_init_random(float* theta, uint32_t volume, uint64_t seed, cudaStream_t s);
