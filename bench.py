@@ -91,7 +91,7 @@ def peaks():
 
 def traffic_per_site():
     """DRAM bytes per replica site per launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "k_batched_traffic.json")
+    path = os.path.join(ROOT, "profiles", "k_resident_c2_traffic.json")
     if os.path.exists(path):
         with open(path) as f:
             return float(json.load(f)["dram_bytes_per_site_per_launch"])

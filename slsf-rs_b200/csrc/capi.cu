@@ -169,6 +169,7 @@ struct slsf_task {
         v.thermalization = thermalization;
         v.binsize = binsize;
         v.n_bins = n_bins;
+        v.sweeps = 0;
         v.stats = stats;
         return v;
     }
@@ -703,7 +704,7 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_
             csize[i] = slsf::batched_cluster_size(t->lx, t->ly, t->lz, ctx->device);
             if (!csize[i])
                 return set_error(SLSF_ERR_INVALID,
-                                 "lattice not supported by the shared-memory batched kernels (needs L_x <= 32, "
+                                 "lattice not supported by the shared-memory batched kernels (needs L_x <= 64, "
                                  "L_x % 4 == 0, even L_y and L_z, and a slab of at most 8 CTAs in shared memory)");
         }
     }
@@ -730,13 +731,14 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_
         const uint32_t c = csize[order[lo]];
         size_t hi = lo;
         const uint32_t parts = c ? c : 1;
-        uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0;
+        uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0, max_lx = 0;
         while (hi < n && csize[order[hi]] == c) {
             const slsf_task* t = tasks[order[hi]];
             max_vs = std::max(max_vs, t->volume / parts);
             max_rows = std::max(max_rows, t->ly * (t->lz / parts));
             max_lz = std::max(max_lz, t->lz);
             max_plane = std::max(max_plane, t->lx * t->ly);
+            max_lx = std::max(max_lx, t->lx);
             ++hi;
         }
         if (c == 0)
@@ -744,7 +746,7 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_
                                             ctx->device, ctx->stream, max_vs, max_rows, max_lz));
         else
             SLSF_CUDA(slsf::launch_batched(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
-                                           ctx->device, ctx->stream, c, max_vs, max_rows, max_lz, max_plane));
+                                           ctx->device, ctx->stream, c, max_vs, max_rows, max_lz, max_plane, max_lx));
         ctx->launches += 1;
         lo = hi;
     }

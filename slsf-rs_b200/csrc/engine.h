@@ -41,6 +41,7 @@ struct TaskView {
     uint64_t wolff_done;   /* Wolff steps done before this launch */
     double* bins;          /* [n_bins][kBinCols] sums */
     uint32_t thermalization, binsize, n_bins;
+    uint32_t sweeps;       /* sweeps of this task in a batched launch; 0: the launch's count */
     unsigned long long* stats;
 };
 
@@ -83,10 +84,10 @@ bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);
 /* Runs n_sweeps sweeps of every task view in `views_dev` (device array of
  * n, all needing the same cluster size) with a persistent grid of clusters;
  * `queue` is a zeroed device counter the kernel consumes.  max_* are the
- * largest per-CTA slab volume, slab row count, Lz and Lx Ly over the views. */
+ * largest per-CTA slab volume, slab row count, Lz, Lx Ly and Lx over the views. */
 cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                            int device, cudaStream_t s, uint32_t cluster, uint32_t max_vs, uint32_t max_rows,
-                           uint32_t max_lz, uint32_t max_plane);
+                           uint32_t max_lz, uint32_t max_plane, uint32_t max_lx);
 
 }  // namespace slsf
 

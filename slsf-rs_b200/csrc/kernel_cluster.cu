@@ -1,38 +1,34 @@
 /*
- * Batched persistent kernel: many replicas of uneven size, each resident in
- * the distributed shared memory of a thread-block cluster for all of its
- * sweeps.  Replaces the carlo-mc Runner's task-by-task loop over
+ * Batched persistent kernel for replicas too large for one CTA: each replica
+ * is split into C z-slabs (C = 1, 2, 4 or 8) held in the distributed shared
+ * memory of a thread-block cluster for all of its sweeps.  Same role as
+ * kernel_resident.cu -- the carlo-mc Runner's task-by-task loop over
  * ThetaModel::sweep + ThetaModel::measure (src/model.rs:379-442,
- * src/results.rs:200-202) for every task of a batch at once.
+ * src/results.rs:200-202) for every task of a batch -- for L_x up to 64
+ * (L = 48 and 64 cubes: 4 and 8 CTAs of about 110 and 130 KiB).
  *
- * A replica is split into C z-slabs (C = cluster size, 1, 2, 4 or 8), one
- * per CTA.  Each CTA keeps, for its slab,
+ * Each CTA keeps, for its slab (planes z0 .. z0 + nz - 1),
  *   theta   FP32, colour-split layout: the colour-c site with slab index li
- *           sits at c * (Vs/2 + 16) + li/2, so a warp reading one colour
- *           reads consecutive words, and the 64-byte pad puts the two colours
- *           of neighbouring sites in different bank halves;
- *   trig    (cos theta, sin theta) FP32 pairs in the same layout (pad 8
- *           pairs = 64 bytes), always equal to __sincosf(theta), like the
- *           reference's ThetaScratch (src/types.rs:163-214);
- *   bonds   Wolff +x/+y/+z active-bond words and cluster words, one 32-bit
- *           word per row of L_x <= 32 sites;
- *   halo    trig of the partner planes just above and below the slab, copied
- *           from the partners' shared memory (DSMEM) before each phase that
- *           needs it, so that the update loops only touch local memory.
+ *           at c * (Vs/2 + 16) + li/2 (consecutive words per warp access; the
+ *           64-byte pad puts the colours of neighbouring sites in different
+ *           bank halves);
+ *   halo    theta of the partner planes just above (z0 + nz) and below
+ *           (z0 - 1), copied from the partners' shared memory through DSMEM
+ *           before every phase that needs them, so the update loops read only
+ *           local shared memory;
+ *   bonds   Wolff +x/+y/+z active-bond words and cluster words, one W-bit
+ *           word per row (W = 32 for L_x <= 32, 64 for L_x <= 64).
+ * Trig values are recomputed with __sincosf from theta where needed, exactly
+ * as in the single-task kernels, so results are bit-identical to them.
  * Cluster barriers separate the phases.  HBM traffic is one read and one
  * write of theta per launch, independent of the sweep count.
  *
- * Per sweep: two colour half-sweeps with the decision code shared with the
- * single-task kernel (xy_device.cuh), `wolff_steps` Wolff updates, and, after
- * thermalization, the fused measurement accumulated into the task's bins.
- *
  * Wolff labelling is bit-parallel: the cluster grows from the seed by OR-ing
- * neighbour rows through the bond words and closing each changed row along
- * x, until a pass changes nothing in the whole cluster.  The result is the
- * seed's connected component over the active bonds -- the set the
- * reference's DFS (src/updates.rs:577-597) collects when fed the same
- * per-bond randoms.  Growth is monotone, so the pass count is bounded by the
- * site count.
+ * neighbour rows through the bond words and closing every row that gained
+ * bits along x, until a pass changes nothing in the whole cluster.  The
+ * result is the seed's connected component over the active bonds -- the set
+ * the reference's DFS (src/updates.rs:577-597) collects when fed the same
+ * per-bond randoms.  Growth is monotone, so the pass count is bounded by V.
  */
 #include <cooperative_groups.h>
 
@@ -49,30 +45,26 @@ namespace slsf {
 namespace {
 
 constexpr int kBThreads = 1024;
-constexpr uint32_t kPadTheta = 16; /* floats: 64 bytes */
-constexpr uint32_t kPadTrig = 8;   /* float2: 64 bytes */
-constexpr uint32_t kMaxRowBits = 32;
+constexpr uint32_t kPad = 16; /* floats: 64 bytes */
+constexpr uint32_t kMaxRowBits = 64;
 constexpr uint32_t kMaxCluster = 8;
 
-/* Optional per-phase cycle accounting (build with -DSLSF_PHASE_TIMING):
- * thread 0 of every CTA adds the clock64 cycles of each phase, measured
- * between block barriers, to g_phase_cycles; slot 6 counts cluster-growth
- * passes and slot 7 Wolff updates. */
+/* Optional per-phase cycle accounting (build with -DSLSF_PHASE_TIMING). */
 #ifdef SLSF_PHASE_TIMING
-__device__ unsigned long long g_phase_cycles[8];
+__device__ unsigned long long g_cl_phase_cycles[8];
 __shared__ long long s_phase_mark;
-#define SLSF_PHASE(k)                                                                 \
-    do {                                                                              \
-        __syncthreads();                                                              \
-        if (threadIdx.x == 0) {                                                       \
-            const long long now_ = clock64();                                         \
-            atomicAdd(&g_phase_cycles[k], (unsigned long long)(now_ - s_phase_mark)); \
-            s_phase_mark = now_;                                                      \
-        }                                                                             \
+#define SLSF_PHASE(k)                                                                    \
+    do {                                                                                 \
+        __syncthreads();                                                                 \
+        if (threadIdx.x == 0) {                                                          \
+            const long long now_ = clock64();                                            \
+            atomicAdd(&g_cl_phase_cycles[k], (unsigned long long)(now_ - s_phase_mark)); \
+            s_phase_mark = now_;                                                         \
+        }                                                                                \
     } while (0)
-#define SLSF_PHASE_COUNT(k, n)                                                          \
-    do {                                                                                \
-        if (threadIdx.x == 0) atomicAdd(&g_phase_cycles[k], (unsigned long long)(n)); \
+#define SLSF_PHASE_COUNT(k, n)                                                             \
+    do {                                                                                   \
+        if (threadIdx.x == 0) atomicAdd(&g_cl_phase_cycles[k], (unsigned long long)(n)); \
     } while (0)
 #else
 #define SLSF_PHASE(k) \
@@ -83,14 +75,68 @@ __shared__ long long s_phase_mark;
     } while (0)
 #endif
 
+/* ---- row words ---- */
+
+template <typename W>
+struct RowOps;
+
+template <>
+struct RowOps<uint32_t> {
+    static __device__ __forceinline__ uint32_t rotl(uint32_t w, uint32_t s, uint32_t lx, uint32_t mask) {
+        return lx == 32 ? __funnelshift_l(w, w, s) : (((w << s) | (w >> (lx - s))) & mask);
+    }
+    static __device__ __forceinline__ uint32_t rotr(uint32_t w, uint32_t s, uint32_t lx, uint32_t mask) {
+        return lx == 32 ? __funnelshift_r(w, w, s) : (((w >> s) | (w << (lx - s))) & mask);
+    }
+    static __device__ __forceinline__ uint32_t popc(uint32_t w) { return __popc(w); }
+};
+
+template <>
+struct RowOps<uint64_t> {
+    static __device__ __forceinline__ uint64_t rotl(uint64_t w, uint32_t s, uint32_t lx, uint64_t mask) {
+        return lx == 64 ? ((w << s) | (w >> (64 - s))) : (((w << s) | (w >> (lx - s))) & mask);
+    }
+    static __device__ __forceinline__ uint64_t rotr(uint64_t w, uint32_t s, uint32_t lx, uint64_t mask) {
+        return lx == 64 ? ((w >> s) | (w << (64 - s))) : (((w >> s) | (w << (lx - s))) & mask);
+    }
+    static __device__ __forceinline__ uint32_t popc(uint64_t w) { return __popcll(w); }
+};
+
+__device__ __forceinline__ void atomic_or_row(uint32_t* p, uint32_t v) { atomicOr(p, v); }
+__device__ __forceinline__ void atomic_or_row(uint64_t* p, uint64_t v) {
+    atomicOr(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
+}
+
+/* Closure of a periodic row's cluster bits c along x through the bond bits b
+ * (bit x: bond x -- x+1).  Kogge-Stone doubling in both directions: after the
+ * step with shift s, every site within 2s - 1 bond steps of a seed is set;
+ * shifts up to 32 cover any row of L_x <= 64 sites. */
+template <typename W>
+__device__ __forceinline__ W close_row(W c, W b, uint32_t lx, W mask) {
+    using R = RowOps<W>;
+    W gr = c, pr = b;                   /* rightward: bond p -> p+1 */
+    W gl = c, pl = R::rotl(b, 1, lx, mask); /* leftward: bond p-1 -> p */
+#pragma unroll
+    for (uint32_t s = 1; s < 8 * sizeof(W); s <<= 1) {
+        if (s >= lx) break;
+        gr |= R::rotl(gr & pr, s, lx, mask);
+        pr &= R::rotr(pr, s, lx, mask);
+        gl |= R::rotr(gl & pl, s, lx, mask);
+        pl &= R::rotl(pl, s, lx, mask);
+    }
+    return gr | gl;
+}
+
+/* ---- geometry ---- */
+
 struct Geo {
     uint32_t lx, ly, lz, volume, plane;
     uint32_t nz, z0, rank, csize; /* slab: planes z0 .. z0 + nz - 1 */
     uint32_t vs, half_s, rows_s;  /* slab sites, per colour, rows */
-    uint32_t tstride, cstride;    /* colour-1 offsets of theta and trig */
+    uint32_t tstride;             /* colour-1 offset of theta */
     uint32_t hp;                  /* sites of one colour in one plane */
-    uint32_t xmask;
-    bool lx_tiles_warp;
+    bool lx_tiles_warp;           /* 32 % lx == 0 */
+    bool lx_two_warps;            /* lx == 64 */
     slsf_fastdiv div_hx, div_ly, div_lx;
 };
 
@@ -108,11 +154,10 @@ __device__ __forceinline__ Geo make_geo(const TaskView& t, uint32_t rank, uint32
     g.vs = g.plane * g.nz;
     g.half_s = g.vs >> 1;
     g.rows_s = t.ly * g.nz;
-    g.tstride = g.half_s + kPadTheta;
-    g.cstride = g.half_s + kPadTrig;
+    g.tstride = g.half_s + kPad;
     g.hp = g.plane >> 1;
-    g.xmask = t.lx >= 32 ? 0xffffffffu : ((1u << t.lx) - 1u);
-    g.lx_tiles_warp = (32u % t.lx) == 0;
+    g.lx_tiles_warp = t.lx <= 32 && (32u % t.lx) == 0;
+    g.lx_two_warps = t.lx == 64;
     g.div_hx = slsf_fastdiv_make(t.lx >> 1);
     g.div_ly = slsf_fastdiv_make(t.ly);
     g.div_lx = slsf_fastdiv_make(t.lx);
@@ -141,77 +186,50 @@ __device__ __forceinline__ uint32_t seg_next(uint32_t lane, uint32_t n) {
     return (lane & ~(n - 1u)) | ((lane + 1u) & (n - 1u));
 }
 
-__device__ __forceinline__ uint32_t rotl_row(uint32_t w, uint32_t s, uint32_t lx, uint32_t mask) {
-    return lx == 32 ? __funnelshift_l(w, w, s) : (((w << s) | (w >> (lx - s))) & mask);
-}
+/* ---- shared memory ---- */
 
-__device__ __forceinline__ uint32_t rotr_row(uint32_t w, uint32_t s, uint32_t lx, uint32_t mask) {
-    return lx == 32 ? __funnelshift_r(w, w, s) : (((w >> s) | (w << (lx - s))) & mask);
-}
-
-/* Closure of a periodic row's cluster bits c along x through the bond bits b
- * (bit x: bond x -- x+1).  Kogge-Stone doubling in both directions: after the
- * step with shift s, every site within 2s - 1 bond steps of a seed is set;
- * shifts 1..16 cover any row of L_x <= 32 sites.  A shift of L_x or more is
- * skipped (the row is already closed by then). */
-__device__ __forceinline__ uint32_t close_row(uint32_t c, uint32_t b, uint32_t lx, uint32_t mask) {
-    uint32_t gr = c, pr = b;                        /* rightward: bond p -> p+1 */
-    uint32_t gl = c, pl = rotl_row(b, 1, lx, mask); /* leftward: bond p-1 -> p */
-#pragma unroll
-    for (uint32_t s = 1; s < 32; s <<= 1) {
-        if (s >= lx) break;
-        gr |= rotl_row(gr & pr, s, lx, mask);
-        pr &= rotr_row(pr, s, lx, mask);
-        gl |= rotr_row(gl & pl, s, lx, mask);
-        pl &= rotl_row(pl, s, lx, mask);
-    }
-    return gr | gl;
-}
-
+template <typename W>
 struct Smem {
-    float2* cs;   /* [2][cstride] (cos, sin) */
-    float* th;    /* [2][tstride] */
-    float2* halo; /* [2][hp] partner-plane trig */
-    uint32_t* bx;
-    uint32_t* by;
-    uint32_t* bz;
-    uint32_t* cl;
+    float* th;   /* [2][tstride] */
+    float* halo; /* [0..1]: plane above, colours 0/1; [2..3]: plane below, colours 0/1; each [hp] */
+    W* bx;
+    W* by;
+    W* bz;
+    W* cl;
     float* jxy;
     float* jz;
 };
 
-/* Per-CTA layout for the largest slab of the launch. */
 struct Limits {
     uint32_t vs, rows, lz, hp;
 };
 
-__device__ __forceinline__ Smem carve(unsigned char* base, const Limits& m) {
-    Smem s;
+template <typename W>
+__device__ __forceinline__ Smem<W> carve(unsigned char* base, const Limits& m) {
+    Smem<W> s;
     unsigned char* p = base;
-    s.cs = reinterpret_cast<float2*>(p);
-    p += 8ull * (m.vs + 2 * kPadTrig);
-    s.halo = reinterpret_cast<float2*>(p);
-    p += 16ull * m.hp;
-    s.th = reinterpret_cast<float*>(p);
-    p += 4ull * (m.vs + 2 * kPadTheta);
-    uint32_t* w = reinterpret_cast<uint32_t*>(p);
+    W* w = reinterpret_cast<W*>(p); /* 8-byte aligned first */
     s.bx = w;
     s.by = w + m.rows;
     s.bz = w + 2 * m.rows;
     s.cl = w + 3 * m.rows;
-    s.jxy = reinterpret_cast<float*>(w + 4 * m.rows);
+    p += 4ull * m.rows * sizeof(W);
+    s.th = reinterpret_cast<float*>(p);
+    p += 4ull * (m.vs + 2 * kPad);
+    s.halo = reinterpret_cast<float*>(p);
+    p += 16ull * m.hp;
+    s.jxy = reinterpret_cast<float*>(p);
     s.jz = s.jxy + m.lz;
     return s;
 }
 
-/* The partner CTAs holding the planes above (up) and below (dn) this slab;
- * with C = 1 both are this CTA. */
+template <typename W>
 struct Remote {
-    const float2* cs_up;
-    const float2* cs_dn;
-    const uint32_t* cl_up;
-    const uint32_t* cl_dn;
-    const uint32_t* bz_dn;
+    const float* th_up; /* partner holding plane z0 + nz */
+    const float* th_dn; /* partner holding plane z0 - 1 */
+    const W* cl_up;
+    const W* cl_dn;
+    const W* bz_dn;
 };
 
 __device__ __forceinline__ void cluster_barrier(const Geo& g, cg::cluster_group& cluster) {
@@ -221,45 +239,44 @@ __device__ __forceinline__ void cluster_barrier(const Geo& g, cg::cluster_group&
         cluster.sync();
 }
 
-/* halo[0][i] <- up plane 0, colour a; halo[1][i] <- (b_from_up ? up plane 0
- * : dn plane nz-1), colour b.  i is the plane-compact index (x + Lx y) / 2.
- * Ends with a block barrier. */
-__device__ __forceinline__ void fill_halo(const Geo& g, Smem& s, const Remote& rm, uint32_t a, uint32_t b,
-                                          bool b_from_up) {
-    const float2* src_a = rm.cs_up + a * g.cstride;
-    const float2* src_b = b_from_up ? rm.cs_up + b * g.cstride
-                                    : rm.cs_dn + b * g.cstride + ((g.plane * (g.nz - 1)) >> 1);
-    for (uint32_t i = threadIdx.x; i < g.hp; i += blockDim.x) {
-        s.halo[i] = src_a[i];
-        s.halo[g.hp + i] = src_b[i];
+/* Copy colour `col` (or both colours when col > 1) of the partner planes
+ * above and below the slab into the halo; ends with a block barrier. */
+template <typename W>
+__device__ __forceinline__ void fill_halo(const Geo& g, Smem<W>& s, const Remote<W>& rm, uint32_t col) {
+    const uint32_t c0 = col > 1 ? 0 : col, c1 = col > 1 ? 1 : col;
+    const uint32_t below = (g.plane * (g.nz - 1)) >> 1; /* compact offset of the partner's last plane */
+    for (uint32_t c = c0; c <= c1; ++c) {
+        const float* up = rm.th_up + c * g.tstride;
+        const float* dn = rm.th_dn + c * g.tstride + below;
+        for (uint32_t i = threadIdx.x; i < g.hp; i += blockDim.x) {
+            s.halo[c * g.hp + i] = up[i];
+            s.halo[(2 + c) * g.hp + i] = dn[i];
+        }
     }
     __syncthreads();
 }
 
+/* theta of the site at plane-compact index pc, colour col, one plane above
+ * (up = true) or below the slab. */
+template <typename W>
+__device__ __forceinline__ float halo_theta(const Geo& g, const Smem<W>& s, bool up, uint32_t col, uint32_t pc) {
+    return s.halo[(up ? 0u : 2u) * g.hp + col * g.hp + pc];
+}
+
 /* ---- load / store ---- */
 
-__device__ __forceinline__ void load_slab(const TaskView& t, const Geo& g, Smem& s) {
+template <typename W>
+__device__ __forceinline__ void load_slab(const TaskView& t, const Geo& g, Smem<W>& s) {
     const float4* src = reinterpret_cast<const float4*>(t.theta + (size_t)g.plane * g.z0);
     for (uint32_t q = threadIdx.x; q < g.vs / 4; q += blockDim.x) {
         const float4 v = src[q];
         const Coords c = coords_of(g, 4 * q);
         const uint32_t p = colour_of(g, 0, c.y, c.zl); /* x = 4q mod lx is even */
         const uint32_t h = 2 * q;
-        const uint32_t ta = p * g.tstride + h, tb = (p ^ 1u) * g.tstride + h;
-        const uint32_t ca = p * g.cstride + h, cb = (p ^ 1u) * g.cstride + h;
-        float sn, cn;
-        s.th[ta] = v.x;
-        __sincosf(v.x, &sn, &cn);
-        s.cs[ca] = make_float2(cn, sn);
-        s.th[tb] = v.y;
-        __sincosf(v.y, &sn, &cn);
-        s.cs[cb] = make_float2(cn, sn);
-        s.th[ta + 1] = v.z;
-        __sincosf(v.z, &sn, &cn);
-        s.cs[ca + 1] = make_float2(cn, sn);
-        s.th[tb + 1] = v.w;
-        __sincosf(v.w, &sn, &cn);
-        s.cs[cb + 1] = make_float2(cn, sn);
+        s.th[p * g.tstride + h] = v.x;
+        s.th[(p ^ 1u) * g.tstride + h] = v.y;
+        s.th[p * g.tstride + h + 1] = v.z;
+        s.th[(p ^ 1u) * g.tstride + h + 1] = v.w;
     }
     for (uint32_t z = threadIdx.x; z < g.lz; z += blockDim.x) {
         s.jxy[z] = t.jxy[z];
@@ -267,31 +284,32 @@ __device__ __forceinline__ void load_slab(const TaskView& t, const Geo& g, Smem&
     }
 }
 
-__device__ __forceinline__ void store_slab(const TaskView& t, const Geo& g, const Smem& s) {
+template <typename W>
+__device__ __forceinline__ void store_slab(const TaskView& t, const Geo& g, const Smem<W>& s) {
     float4* dst = reinterpret_cast<float4*>(t.theta + (size_t)g.plane * g.z0);
     for (uint32_t q = threadIdx.x; q < g.vs / 4; q += blockDim.x) {
         const Coords c = coords_of(g, 4 * q);
         const uint32_t p = colour_of(g, 0, c.y, c.zl);
         const uint32_t h = 2 * q;
-        const uint32_t ta = p * g.tstride + h, tb = (p ^ 1u) * g.tstride + h;
-        dst[q] = make_float4(s.th[ta], s.th[tb], s.th[ta + 1], s.th[tb + 1]);
+        dst[q] = make_float4(s.th[p * g.tstride + h], s.th[(p ^ 1u) * g.tstride + h],
+                             s.th[p * g.tstride + h + 1], s.th[(p ^ 1u) * g.tstride + h + 1]);
     }
 }
 
 /* ---- Metropolis ---- */
 
-/* One colour half-sweep of the slab; the halo holds the colour-(1-c) trig of
- * the partner planes (halo[0]: above, halo[1]: below).  A warp owns 32
- * consecutive Philox blocks (64 sites); lanes exchange words so that lane j
- * updates colour-compact sites 2*base + j and 2*base + 32 + j. */
-__device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, Smem& s, uint64_t sweep,
+/* One colour half-sweep of the slab; the halo holds colour 1-c of the
+ * partner planes.  A warp owns 32 consecutive Philox blocks (64 sites);
+ * lanes exchange words so that lane j updates colour-compact sites
+ * 2*base + j and 2*base + 32 + j. */
+template <typename W>
+__device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, Smem<W>& s, uint64_t sweep,
                                                uint32_t colour) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t nwarps = blockDim.x >> 5;
     const uint32_t npairs = g.half_s >> 1;
-    const uint32_t pair0 = (g.plane * g.z0) >> 2; /* global Philox block of the slab's first pair */
-    const uint32_t own_t = colour * g.tstride, own_c = colour * g.cstride;
-    const uint32_t oth = (colour ^ 1u) * g.cstride;
+    const uint32_t pair0 = (g.plane * g.z0) >> 2;
+    const uint32_t own = colour * g.tstride, oth = (colour ^ 1u) * g.tstride, ocol = colour ^ 1u;
     const uint32_t hx = g.lx >> 1;
     uint32_t accepted = 0;
     for (uint32_t base = warp * 32; base < npairs; base += nwarps * 32) {
@@ -316,27 +334,33 @@ __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, 
             const uint32_t z = g.z0 + zl;
             const uint32_t x = 2u * k + ((colour + y + z) & 1u);
             const uint32_t li = x + g.lx * row;
-            const uint32_t pc = (x + g.lx * y) >> 1; /* plane-compact index */
-            /* in-plane neighbours (slab-local indices) */
+            const uint32_t pc = (x + g.lx * y) >> 1;
             const uint32_t xp = (x + 1 == g.lx) ? li + 1 - g.lx : li + 1;
             const uint32_t xm = (x == 0) ? li + g.lx - 1 : li - 1;
             const uint32_t yp = (y + 1 == g.ly) ? li + g.lx - g.plane : li + g.lx;
             const uint32_t ym = (y == 0) ? li + g.plane - g.lx : li - g.lx;
-            const float2 n0 = s.cs[oth + (xp >> 1)];
-            const float2 n1 = s.cs[oth + (xm >> 1)];
-            const float2 n2 = s.cs[oth + (yp >> 1)];
-            const float2 n3 = s.cs[oth + (ym >> 1)];
-            const float2 n4 = (zl + 1 < g.nz) ? s.cs[oth + ((li + g.plane) >> 1)] : s.halo[pc];
-            const float2 n5 = (zl > 0) ? s.cs[oth + ((li - g.plane) >> 1)] : s.halo[g.hp + pc];
+            const float t0 = s.th[oth + (xp >> 1)];
+            const float t1 = s.th[oth + (xm >> 1)];
+            const float t2 = s.th[oth + (yp >> 1)];
+            const float t3 = s.th[oth + (ym >> 1)];
+            const float t4 = (zl + 1 < g.nz) ? s.th[oth + ((li + g.plane) >> 1)] : halo_theta(g, s, true, ocol, pc);
+            const float t5 = (zl > 0) ? s.th[oth + ((li - g.plane) >> 1)] : halo_theta(g, s, false, ocol, pc);
+            float ns[6], nc[6];
+            __sincosf(t0, &ns[0], &nc[0]);
+            __sincosf(t1, &ns[1], &nc[1]);
+            __sincosf(t2, &ns[2], &nc[2]);
+            __sincosf(t3, &ns[3], &nc[3]);
+            __sincosf(t4, &ns[4], &nc[4]);
+            __sincosf(t5, &ns[5], &nc[5]);
             const float jx = s.jxy[z], jzp = s.jz[z], jzm = s.jz[z == 0 ? g.lz - 1 : z - 1];
-            const float hxf = field_component(jx, jzp, jzm, n0.x, n1.x, n2.x, n3.x, n4.x, n5.x);
-            const float hyf = field_component(jx, jzp, jzm, n0.y, n1.y, n2.y, n3.y, n4.y, n5.y);
-            const float th = s.th[own_t + h];
-            const float2 cur = s.cs[own_c + h];
+            const float hxf = field_component(jx, jzp, jzm, nc[0], nc[1], nc[2], nc[3], nc[4], nc[5]);
+            const float hyf = field_component(jx, jzp, jzm, ns[0], ns[1], ns[2], ns[3], ns[4], ns[5]);
+            const float th = s.th[own + h];
+            float si, ci;
+            __sincosf(th, &si, &ci);
             float tn, sn, cn;
-            if (metro_decide(th, cur.x, cur.y, hxf, hyf, t.beta, t.width, u_prop, u_acc, &tn, &sn, &cn)) {
-                s.th[own_t + h] = tn;
-                s.cs[own_c + h] = make_float2(cn, sn);
+            if (metro_decide(th, ci, si, hxf, hyf, t.beta, t.width, u_prop, u_acc, &tn, &sn, &cn)) {
+                s.th[own + h] = tn;
                 ++accepted;
             }
         }
@@ -346,17 +370,21 @@ __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, 
 
 /* ---- Wolff ---- */
 
-__device__ __forceinline__ float proj(float2 v, float cphi, float sphi) {
-    return wolff_projection(v.x, v.y, cphi, sphi);
+__device__ __forceinline__ float proj_of(float theta, float cphi, float sphi) {
+    float sn, cn;
+    __sincosf(theta, &sn, &cn);
+    return wolff_projection(cn, sn, cphi, sphi);
 }
 
-/* Bond activation for every slab site; fills bx/by/bz and seeds cl.  The
- * halo holds both colours of the plane above the slab. */
-__device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Smem& s, uint64_t counter,
+/* Bond activation for every slab site (the halo holds both colours of the
+ * partner planes); fills bx/by/bz and seeds cl with the closed seed row. */
+template <typename W>
+__device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Smem<W>& s, uint64_t counter,
                                             float cphi, float sphi, uint32_t seed_idx) {
     const uint32_t lane = threadIdx.x & 31u;
     const float m2b = __fmul_rn(-2.0f, t.beta);
-    if (!g.lx_tiles_warp) {
+    const bool ballots = g.lx_tiles_warp || g.lx_two_warps;
+    if (!ballots) {
         for (uint32_t r = threadIdx.x; r < g.rows_s; r += blockDim.x) {
             s.bx[r] = 0;
             s.by[r] = 0;
@@ -370,38 +398,51 @@ __device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Sme
         const bool valid = li < g.vs;
         const uint32_t ll = valid ? li : 0;
         const Coords c = coords_of(g, ll);
-        const uint32_t col = colour_of(g, c.x, c.y, c.zl), oth = (col ^ 1u) * g.cstride;
-        const float ri = proj(s.cs[col * g.cstride + (ll >> 1)], cphi, sphi);
+        const uint32_t col = colour_of(g, c.x, c.y, c.zl), oth = (col ^ 1u) * g.tstride;
+        const float ri = proj_of(s.th[col * g.tstride + (ll >> 1)], cphi, sphi);
         float rxp;
         if (g.lx_tiles_warp) {
             rxp = __shfl_sync(0xffffffffu, ri, seg_next(lane, g.lx));
         } else {
             const uint32_t xp = (c.x + 1 == g.lx) ? ll + 1 - g.lx : ll + 1;
-            rxp = proj(s.cs[oth + (xp >> 1)], cphi, sphi);
+            rxp = proj_of(s.th[oth + (xp >> 1)], cphi, sphi);
         }
         const uint32_t yp = (c.y + 1 == g.ly) ? ll + g.lx - g.plane : ll + g.lx;
-        const float ryp = proj(s.cs[oth + (yp >> 1)], cphi, sphi);
-        const float2 vz = (c.zl + 1 < g.nz) ? s.cs[oth + ((ll + g.plane) >> 1)]
-                                            : s.halo[(col ^ 1u) * g.hp + ((c.x + g.lx * c.y) >> 1)];
-        const float rzp = proj(vz, cphi, sphi);
+        const float ryp = proj_of(s.th[oth + (yp >> 1)], cphi, sphi);
+        const float tz = (c.zl + 1 < g.nz) ? s.th[oth + ((ll + g.plane) >> 1)]
+                                           : halo_theta(g, s, true, col ^ 1u, (c.x + g.lx * c.y) >> 1);
+        const float rzp = proj_of(tz, cphi, sphi);
         const slsf_u32x4 b = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, base_idx + ll);
         const float jx = s.jxy[g.z0 + c.zl], jzz = s.jz[g.z0 + c.zl];
         const bool ax = valid && wolff_bond_active(jx, ri, rxp, m2b, b.x);
         const bool ay = valid && wolff_bond_active(jx, ri, ryp, m2b, b.y);
         const bool az = valid && wolff_bond_active(jzz, ri, rzp, m2b, b.z);
-        if (g.lx_tiles_warp) {
+        if (ballots) {
             const uint32_t bal_x = __ballot_sync(0xffffffffu, ax);
             const uint32_t bal_y = __ballot_sync(0xffffffffu, ay);
             const uint32_t bal_z = __ballot_sync(0xffffffffu, az);
-            if (valid && c.x == 0) {
-                s.bx[c.row] = (bal_x >> lane) & g.xmask;
-                s.by[c.row] = (bal_y >> lane) & g.xmask;
-                s.bz[c.row] = (bal_z >> lane) & g.xmask;
+            if (g.lx_tiles_warp) {
+                if (valid && c.x == 0) {
+                    const W m = (W)((g.lx >= 32) ? 0xffffffffu : ((1u << g.lx) - 1u));
+                    s.bx[c.row] = (W)(bal_x >> lane) & m;
+                    s.by[c.row] = (W)(bal_y >> lane) & m;
+                    s.bz[c.row] = (W)(bal_z >> lane) & m;
+                }
+            } else if (valid && lane == 0) {
+                /* lx == 64: this warp holds half a row; write its 32-bit half */
+                uint32_t* hx32 = reinterpret_cast<uint32_t*>(s.bx);
+                uint32_t* hy32 = reinterpret_cast<uint32_t*>(s.by);
+                uint32_t* hz32 = reinterpret_cast<uint32_t*>(s.bz);
+                const uint32_t half = c.x >> 5;
+                hx32[2 * c.row + half] = bal_x;
+                hy32[2 * c.row + half] = bal_y;
+                hz32[2 * c.row + half] = bal_z;
             }
         } else if (valid) {
-            if (ax) atomicOr(&s.bx[c.row], 1u << c.x);
-            if (ay) atomicOr(&s.by[c.row], 1u << c.x);
-            if (az) atomicOr(&s.bz[c.row], 1u << c.x);
+            const W bit = (W)1 << c.x;
+            if (ax) atomic_or_row(&s.bx[c.row], bit);
+            if (ay) atomic_or_row(&s.by[c.row], bit);
+            if (az) atomic_or_row(&s.bz[c.row], bit);
         }
     }
     /* seed the cluster */
@@ -409,22 +450,27 @@ __device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Sme
     const uint32_t sz = srow / g.ly, sy = srow - sz * g.ly;
     const bool mine = sz >= g.z0 && sz < g.z0 + g.nz;
     const uint32_t seed_row = sy + g.ly * (sz - g.z0);
-    for (uint32_t r = threadIdx.x; r < g.rows_s; r += blockDim.x)
-        s.cl[r] = (mine && r == seed_row) ? (1u << sx) : 0u;
+    for (uint32_t r = threadIdx.x; r < g.rows_s; r += blockDim.x) s.cl[r] = (mine && r == seed_row) ? ((W)1 << sx) : (W)0;
+    __syncthreads();
+    if (mine && threadIdx.x == 0) {
+        const W mask = g.lx >= 8 * sizeof(W) ? ~(W)0 : (((W)1 << g.lx) - 1);
+        s.cl[seed_row] = close_row<W>(s.cl[seed_row], s.bx[seed_row], g.lx, mask);
+    }
 }
 
 /* One growth pass: every row takes the cluster bits that reach it through
- * its y and z bonds; a row that gained bits is closed along x.  Returns
- * nonzero if any row of this CTA changed. */
-__device__ __forceinline__ int grow_pass(const Geo& g, Smem& s, const Remote& rm) {
+ * its y and z bonds; a row that gained bits is closed along x (stored rows
+ * are always closed).  Returns nonzero if any row of this CTA changed. */
+template <typename W>
+__device__ __forceinline__ int grow_pass(const Geo& g, Smem<W>& s, const Remote<W>& rm, W mask) {
     int changed = 0;
     for (uint32_t r = threadIdx.x; r < g.rows_s; r += blockDim.x) {
         const uint32_t zl = slsf_fastdiv_div(r, g.div_ly);
         const uint32_t y = r - zl * g.ly;
-        const uint32_t old = s.cl[r];
+        const W old = s.cl[r];
         const uint32_t r_yp = (y + 1 == g.ly) ? r + 1 - g.ly : r + 1;
         const uint32_t r_ym = (y == 0) ? r + g.ly - 1 : r - 1;
-        uint32_t in = (s.cl[r_ym] & s.by[r_ym]) | (s.cl[r_yp] & s.by[r]);
+        W in = (s.cl[r_ym] & s.by[r_ym]) | (s.cl[r_yp] & s.by[r]);
         if (zl > 0) {
             in |= s.cl[r - g.ly] & s.bz[r - g.ly];
         } else {
@@ -432,9 +478,9 @@ __device__ __forceinline__ int grow_pass(const Geo& g, Smem& s, const Remote& rm
             in |= rm.cl_dn[rr] & rm.bz_dn[rr];
         }
         in |= ((zl + 1 < g.nz) ? s.cl[r + g.ly] : rm.cl_up[y]) & s.bz[r];
-        const uint32_t c = old | in;
+        const W c = old | in;
         if (c != old) {
-            s.cl[r] = close_row(c, s.bx[r], g.lx, g.xmask);
+            s.cl[r] = close_row<W>(c, s.bx[r], g.lx, mask);
             changed = 1;
         }
     }
@@ -442,7 +488,8 @@ __device__ __forceinline__ int grow_pass(const Geo& g, Smem& s, const Remote& rm
 }
 
 /* One Wolff update (src/updates.rs:551-620); adds the cluster size to *count. */
-__device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Smem& s, const Remote& rm,
+template <typename W>
+__device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Smem<W>& s, const Remote<W>& rm,
                                              cg::cluster_group& cluster, uint64_t counter, uint32_t* count,
                                              int* flags) {
     const slsf_u32x4 pick = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_PICK, 0, 0);
@@ -450,20 +497,15 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
     const uint32_t x0 = slsf_range(pick.y, g.lx), y0 = slsf_range(pick.z, g.ly), z0 = slsf_range(pick.w, g.lz);
     float sphi, cphi;
     __sincosf(phi, &sphi, &cphi);
-    fill_halo(g, s, rm, 0, 1, true);
+    const W mask = g.lx >= 8 * sizeof(W) ? ~(W)0 : (((W)1 << g.lx) - 1);
+    fill_halo(g, s, rm, 2);
     wolff_bonds(t, g, s, counter, cphi, sphi, x0 + g.lx * (y0 + g.ly * z0));
-    /* the seed row is closed before the first pass */
-    __syncthreads();
-    if (z0 >= g.z0 && z0 < g.z0 + g.nz && threadIdx.x == 0) {
-        const uint32_t r = y0 + g.ly * (z0 - g.z0);
-        s.cl[r] = close_row(s.cl[r], s.bx[r], g.lx, g.xmask);
-    }
     cluster_barrier(g, cluster);
     SLSF_PHASE(2);
 
     uint32_t pass = 0;
     for (; pass <= g.volume; ++pass) {
-        int any = __syncthreads_or(grow_pass(g, s, rm));
+        int any = __syncthreads_or(grow_pass(g, s, rm, mask));
         if (g.csize > 1) {
             if (threadIdx.x == 0) flags[pass & 1] = any;
             cluster.sync();
@@ -476,19 +518,14 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
     SLSF_PHASE_COUNT(6, pass + 1);
     SLSF_PHASE_COUNT(7, 1);
 
-    /* Reflect the cluster (src/updates.rs:602-617), refresh its trig. */
+    /* Reflect the cluster (src/updates.rs:602-617) and count it. */
     uint32_t members = 0;
-    for (uint32_t r = threadIdx.x; r < g.rows_s; r += blockDim.x) members += __popc(s.cl[r]);
+    for (uint32_t r = threadIdx.x; r < g.rows_s; r += blockDim.x) members += RowOps<W>::popc(s.cl[r]);
     for (uint32_t li = threadIdx.x; li < g.vs; li += blockDim.x) {
         const Coords c = coords_of(g, li);
-        if ((s.cl[c.row] >> c.x) & 1u) {
-            const uint32_t col = colour_of(g, c.x, c.y, c.zl);
-            const uint32_t st = col * g.tstride + (li >> 1), sc = col * g.cstride + (li >> 1);
-            const float nt = slsf_reflect(s.th[st], phi);
-            float sn, cn;
-            __sincosf(nt, &sn, &cn);
-            s.th[st] = nt;
-            s.cs[sc] = make_float2(cn, sn);
+        if ((s.cl[c.row] >> c.x) & (W)1) {
+            const uint32_t sl = colour_of(g, c.x, c.y, c.zl) * g.tstride + (li >> 1);
+            s.th[sl] = slsf_reflect(s.th[sl], phi);
         }
     }
 #pragma unroll
@@ -502,8 +539,9 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
 
 /* Slab sums of mx, my, cos xyz, sin xyz (src/observables.rs:99-141): FP32
  * per thread over its sites, FP64 across the block (valid in thread 0).  The
- * halo holds both colours of the plane above the slab. */
-__device__ __forceinline__ void measure_slab(const Geo& g, const Smem& s, double (&acc)[8], double* red) {
+ * halo holds both colours of the partner planes. */
+template <typename W>
+__device__ __forceinline__ void measure_slab(const Geo& g, const Smem<W>& s, double (&acc)[8], double* red) {
     const uint32_t lane = threadIdx.x & 31u;
     float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t i0 = (threadIdx.x & ~31u); i0 < g.vs; i0 += blockDim.x) {
@@ -511,40 +549,41 @@ __device__ __forceinline__ void measure_slab(const Geo& g, const Smem& s, double
         const bool valid = li < g.vs;
         const uint32_t ll = valid ? li : 0;
         const Coords c = coords_of(g, ll);
-        const uint32_t col = colour_of(g, c.x, c.y, c.zl), oth = (col ^ 1u) * g.cstride;
-        const float2 me = s.cs[col * g.cstride + (ll >> 1)];
-        float2 nx;
+        const uint32_t col = colour_of(g, c.x, c.y, c.zl), oth = (col ^ 1u) * g.tstride;
+        float si, ci, sx, cx, sy, cy, sz, cz;
+        __sincosf(s.th[col * g.tstride + (ll >> 1)], &si, &ci);
         if (g.lx_tiles_warp) {
             const uint32_t src = seg_next(lane, g.lx);
-            nx.x = __shfl_sync(0xffffffffu, me.x, src);
-            nx.y = __shfl_sync(0xffffffffu, me.y, src);
+            sx = __shfl_sync(0xffffffffu, si, src);
+            cx = __shfl_sync(0xffffffffu, ci, src);
         } else {
             const uint32_t xp = (c.x + 1 == g.lx) ? ll + 1 - g.lx : ll + 1;
-            nx = s.cs[oth + (xp >> 1)];
+            __sincosf(s.th[oth + (xp >> 1)], &sx, &cx);
         }
         const uint32_t yp = (c.y + 1 == g.ly) ? ll + g.lx - g.plane : ll + g.lx;
-        const float2 ny = s.cs[oth + (yp >> 1)];
-        const float2 nz = (c.zl + 1 < g.nz) ? s.cs[oth + ((ll + g.plane) >> 1)]
-                                            : s.halo[(col ^ 1u) * g.hp + ((c.x + g.lx * c.y) >> 1)];
+        __sincosf(s.th[oth + (yp >> 1)], &sy, &cy);
+        const float tz = (c.zl + 1 < g.nz) ? s.th[oth + ((ll + g.plane) >> 1)]
+                                           : halo_theta(g, s, true, col ^ 1u, (c.x + g.lx * c.y) >> 1);
+        __sincosf(tz, &sz, &cz);
         if (!valid) continue;
         const float jx = s.jxy[g.z0 + c.zl], jzz = s.jz[g.z0 + c.zl];
-        /* diff_cos_sin (src/observables.rs:9-11) */
-        f[0] += me.x;
-        f[1] += me.y;
-        f[2] += jx * (me.x * nx.x + me.y * nx.y);
-        f[3] += jx * (me.x * ny.x + me.y * ny.y);
-        f[4] += jzz * (me.x * nz.x + me.y * nz.y);
-        f[5] += jx * (me.y * nx.x - me.x * nx.y);
-        f[6] += jx * (me.y * ny.x - me.x * ny.y);
-        f[7] += jzz * (me.y * nz.x - me.x * nz.y);
+        f[0] += ci;
+        f[1] += si;
+        f[2] += jx * (ci * cx + si * sx);
+        f[3] += jx * (ci * cy + si * sy);
+        f[4] += jzz * (ci * cz + si * sz);
+        f[5] += jx * (si * cx - ci * sx);
+        f[6] += jx * (si * cy - ci * sy);
+        f[7] += jzz * (si * cz - ci * sz);
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) acc[k] = (double)f[k];
     block_sum<8>(acc, red);
 }
 
+template <typename W>
 __global__ void __launch_bounds__(kBThreads, 1)
-    k_batched(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
+    k_cluster(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
               Limits lim) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[8 * 32];
@@ -555,12 +594,12 @@ __global__ void __launch_bounds__(kBThreads, 1)
     __shared__ int s_flags[2];
     cg::cluster_group cluster = cg::this_cluster();
     const uint32_t rank = cluster.block_rank(), csize = cluster.num_blocks();
-    Smem s = carve(smem_raw, lim);
-    Remote rm;
+    Smem<W> s = carve<W>(smem_raw, lim);
+    Remote<W> rm;
     {
         const uint32_t up = (rank + 1) % csize, dn = (rank + csize - 1) % csize;
-        rm.cs_up = cluster.map_shared_rank(s.cs, up);
-        rm.cs_dn = cluster.map_shared_rank(s.cs, dn);
+        rm.th_up = cluster.map_shared_rank(s.th, up);
+        rm.th_dn = cluster.map_shared_rank(s.th, dn);
         rm.cl_up = cluster.map_shared_rank(s.cl, up);
         rm.cl_dn = cluster.map_shared_rank(s.cl, dn);
         rm.bz_dn = cluster.map_shared_rank(s.bz, dn);
@@ -576,6 +615,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
         if (item >= n) return;
         const TaskView t = views[item];
         const Geo g = make_geo(t, rank, csize);
+        const uint32_t sweeps = t.sweeps ? t.sweeps : n_sweeps;
         if (threadIdx.x == 0) s_cluster = 0;
         load_slab(t, g, s);
         cluster.sync();
@@ -584,13 +624,13 @@ __global__ void __launch_bounds__(kBThreads, 1)
 #endif
         uint32_t accepted = 0;
         int64_t bin_cur = -1;
-        for (uint32_t sw = 0; sw < n_sweeps; ++sw) {
+        for (uint32_t sw = 0; sw < sweeps; ++sw) {
             const uint64_t sweep = t.metro_sweeps + sw;
-            fill_halo(g, s, rm, 1, 1, false);
+            fill_halo(g, s, rm, 1);
             accepted += half_sweep(t, g, s, sweep, 0);
             cluster_barrier(g, cluster);
             SLSF_PHASE(0);
-            fill_halo(g, s, rm, 0, 0, false);
+            fill_halo(g, s, rm, 0);
             accepted += half_sweep(t, g, s, sweep, 1);
             cluster_barrier(g, cluster);
             SLSF_PHASE(1);
@@ -601,7 +641,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
             const uint64_t done = sweep + 1;
             if (done > t.thermalization && t.n_bins > 0) {
                 double acc[8];
-                fill_halo(g, s, rm, 0, 1, true);
+                fill_halo(g, s, rm, 2);
                 measure_slab(g, s, acc, red);
                 if (threadIdx.x == 0)
                     for (int k = 0; k < 8; ++k) *cluster.map_shared_rank(&cred[rank][k], 0) = acc[k];
@@ -626,7 +666,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
                                                    a[5] * a[5], a[6] * a[6], a[7] * a[7]};
                     for (int q = 0; q < kBinCols; ++q) bin_acc[q] += vals[q];
                 }
-                /* partners must not overwrite cred or trig before rank 0 is done */
+                /* partners must not overwrite cred or theta before rank 0 is done */
                 cluster_barrier(g, cluster);
             }
         }
@@ -639,16 +679,15 @@ __global__ void __launch_bounds__(kBThreads, 1)
         __syncthreads();
         if (threadIdx.x == 0) {
             if (s_cluster) atomicAdd(&t.stats[kStatClusterSites], (unsigned long long)s_cluster);
-            if (rank == 0) atomicAdd(&t.stats[kStatClusters], (unsigned long long)n_sweeps * t.wolff_steps);
+            if (rank == 0) atomicAdd(&t.stats[kStatClusters], (unsigned long long)sweeps * t.wolff_steps);
         }
         /* no CTA may start the next replica while a partner still reads its slab */
         cluster.sync();
     }
 }
 
-size_t smem_bytes(const Limits& m) {
-    return 8ull * (m.vs + 2 * kPadTrig) + 16ull * m.hp + 4ull * (m.vs + 2 * kPadTheta) + 16ull * m.rows +
-           8ull * m.lz;
+size_t smem_bytes(const Limits& m, size_t word) {
+    return 4ull * m.rows * word + 4ull * (m.vs + 2 * kPad) + 16ull * m.hp + 8ull * m.lz;
 }
 
 int max_dynamic_smem(int device) {
@@ -658,32 +697,11 @@ int max_dynamic_smem(int device) {
     return v - 4096;
 }
 
-}  // namespace
-
-uint32_t batched_cluster_size(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
-    /* Row words hold L_x <= 32 bits; the float4 colour-split copy needs
-     * L_x % 4 == 0 so that four consecutive sites never span two rows. */
-    if (lx > kMaxRowBits || lx < 4 || lx % 4 || ly < 2 || ly % 2 || lz < 2 || lz % 2) return 0;
-    for (uint32_t c = 1; c <= kMaxCluster; c <<= 1) {
-        if (lz % c) continue;
-        const uint32_t nz = lz / c;
-        const Limits m = {lx * ly * nz, ly * nz, lz, (lx * ly) / 2};
-        if (smem_bytes(m) <= (size_t)max_dynamic_smem(device)) return c;
-    }
-    return 0;
-}
-
-bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
-    return batched_cluster_size(lx, ly, lz, device) != 0;
-}
-
-cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
-                           int device, cudaStream_t s, uint32_t cluster, uint32_t max_vs, uint32_t max_rows,
-                           uint32_t max_lz, uint32_t max_plane) {
-    (void)device;
-    const Limits lim = {max_vs, max_rows, max_lz, max_plane / 2};
-    const size_t smem = smem_bytes(lim);
-    cudaError_t e = cudaFuncSetAttribute(k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+template <typename W>
+cudaError_t launch_w(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+                     cudaStream_t s, uint32_t cluster, const Limits& lim) {
+    const size_t smem = smem_bytes(lim, sizeof(W));
+    cudaError_t e = cudaFuncSetAttribute(k_cluster<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
@@ -698,22 +716,51 @@ cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_swe
     cfg.numAttrs = 1;
     cfg.gridDim = dim3(cluster, 1, 1);
     int clusters = 0;
-    e = cudaOccupancyMaxActiveClusters(&clusters, k_batched, &cfg);
+    e = cudaOccupancyMaxActiveClusters(&clusters, k_cluster<W>, &cfg);
     if (e != cudaSuccess) return e;
     if (clusters < 1) return cudaErrorInvalidConfiguration;
     const uint32_t grid_clusters = std::min<uint32_t>(n, (uint32_t)clusters);
     cfg.gridDim = dim3(grid_clusters * cluster, 1, 1);
-    return cudaLaunchKernelEx(&cfg, k_batched, views_dev, n, n_sweeps, queue, lim);
+    return cudaLaunchKernelEx(&cfg, k_cluster<W>, views_dev, n, n_sweeps, queue, lim);
+}
+
+}  // namespace
+
+uint32_t batched_cluster_size(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
+    /* Row words hold L_x <= 64 bits; the float4 colour-split copy needs
+     * L_x % 4 == 0 so that four consecutive sites never span two rows. */
+    if (lx > kMaxRowBits || lx < 4 || lx % 4 || ly < 2 || ly % 2 || lz < 2 || lz % 2) return 0;
+    const size_t word = lx > 32 ? 8 : 4;
+    for (uint32_t c = 1; c <= kMaxCluster; c <<= 1) {
+        if (lz % c) continue;
+        const uint32_t nz = lz / c;
+        const Limits m = {lx * ly * nz, ly * nz, lz, (lx * ly) / 2};
+        if (smem_bytes(m, word) <= (size_t)max_dynamic_smem(device)) return c;
+    }
+    return 0;
+}
+
+bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
+    return batched_cluster_size(lx, ly, lz, device) != 0;
+}
+
+cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+                           int device, cudaStream_t s, uint32_t cluster, uint32_t max_vs, uint32_t max_rows,
+                           uint32_t max_lz, uint32_t max_plane, uint32_t max_lx) {
+    (void)device;
+    const Limits lim = {max_vs, max_rows, max_lz, max_plane / 2};
+    if (max_lx > 32) return launch_w<uint64_t>(views_dev, n, n_sweeps, queue, s, cluster, lim);
+    return launch_w<uint32_t>(views_dev, n, n_sweeps, queue, s, cluster, lim);
 }
 
 }  // namespace slsf
 
 #ifdef SLSF_PHASE_TIMING
 extern "C" int slsf_debug_phase_cycles(unsigned long long out[8], int reset) {
-    cudaError_t e = cudaMemcpyFromSymbol(out, slsf::g_phase_cycles, sizeof(unsigned long long) * 8);
+    cudaError_t e = cudaMemcpyFromSymbol(out, slsf::g_cl_phase_cycles, sizeof(unsigned long long) * 8);
     if (e == cudaSuccess && reset) {
         const unsigned long long zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        e = cudaMemcpyToSymbol(slsf::g_phase_cycles, zero, sizeof(zero));
+        e = cudaMemcpyToSymbol(slsf::g_cl_phase_cycles, zero, sizeof(zero));
     }
     return e == cudaSuccess ? 0 : 1;
 }

@@ -457,9 +457,10 @@ __global__ void __launch_bounds__(kBThreads, 1)
 #ifdef SLSF_PHASE_TIMING
         if (threadIdx.x == 0) s_phase_mark = clock64();
 #endif
+        const uint32_t sweeps = t.sweeps ? t.sweeps : n_sweeps;
         uint32_t accepted = 0;
         int64_t bin_cur = -1;
-        for (uint32_t sw = 0; sw < n_sweeps; ++sw) {
+        for (uint32_t sw = 0; sw < sweeps; ++sw) {
             const uint64_t sweep = t.metro_sweeps + sw;
             accepted += half_sweep(t, g, s, sweep, 0);
             __syncthreads();
@@ -512,7 +513,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
         if (threadIdx.x == 0) {
             atomicAdd(&t.stats[kStatAccepted], (unsigned long long)s_accepted);
             atomicAdd(&t.stats[kStatClusterSites], (unsigned long long)s_cluster);
-            atomicAdd(&t.stats[kStatClusters], (unsigned long long)n_sweeps * t.wolff_steps);
+            atomicAdd(&t.stats[kStatClusters], (unsigned long long)sweeps * t.wolff_steps);
         }
     }
 }

@@ -50,7 +50,8 @@ def batched_tasks(slsf, ctx, orc, specs):
 
 @pytest.mark.parametrize("dims,wolff", [((8, 8, 8), 0), ((8, 8, 8), 1), ((32, 32, 32), 1), ((16, 8, 12), 2),
                                         ((24, 24, 24), 1), ((32, 16, 8), 1), ((12, 10, 6), 1),
-                                        ((32, 32, 48), 1), ((32, 32, 96), 1), ((20, 24, 16), 1)])
+                                        ((32, 32, 48), 1), ((32, 32, 96), 1), ((20, 24, 16), 1),
+                                        ((48, 48, 48), 1), ((64, 64, 64), 1), ((40, 16, 8), 1), ((64, 8, 6), 1)])
 def test_batched_equals_plain_bitwise(slsf, ctx, orc, dims, wolff):
     ref, _ = plain_run(slsf, ctx, orc, dims, 1.1, seed=42, sweeps=4, wolff=wolff)
     [t] = batched_tasks(slsf, ctx, orc, [(dims, 1.1, 42, wolff, 0, 1, 0, 1)])
@@ -63,7 +64,8 @@ def test_batched_equals_plain_bitwise(slsf, ctx, orc, dims, wolff):
 def test_same_alone_and_in_the_mix(slsf, ctx, orc):
     specs = [((8, 8, 8), 1.0, 1, 1, 0, 1, 0, 1), ((16, 16, 16), 1.3, 2, 1, 0, 1, 0, 2),
              ((32, 32, 32), 1.5, 3, 1, 0, 1, 0, 3), ((24, 24, 24), 1.2, 4, 1, 0, 1, 0, 4),
-             ((8, 16, 4), 0.9, 5, 2, 0, 1, 0, 5)] * 3
+             ((8, 16, 4), 0.9, 5, 2, 0, 1, 0, 5), ((48, 48, 48), 1.1, 6, 1, 0, 1, 0, 6)] * 2 + \
+            [((64, 64, 64), 1.4, 7, 1, 0, 1, 0, 7)]
     mix = batched_tasks(slsf, ctx, orc, specs)
     ctx.batch_run(mix, 5)
     for spec, t in zip(specs, mix):
@@ -110,7 +112,7 @@ def test_checkpoint_resume_is_bit_exact(slsf, ctx, orc):
 
 
 def test_batched_rejects_unsupported(slsf, ctx, orc):
-    [big] = batched_tasks(slsf, ctx, orc, [((64, 64, 64), 1.2, 1, 1, 0, 1, 0, 1)])
+    [big] = batched_tasks(slsf, ctx, orc, [((128, 4, 4), 1.2, 1, 1, 0, 1, 0, 1)])
     with pytest.raises(slsf.SlsfError):
         ctx.batch_run([big], 1)
 
