@@ -193,6 +193,13 @@ int slsf_task_reset_bins(slsf_task* task);
 int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n_tasks, uint32_t n_sweeps,
                    slsf_sweep_stats* stats);
 
+/* slsf_batch_run with its own sweep count per task (sweeps[i]; tasks with 0
+ * are left out of the launch): how a scheduler advances tasks with different
+ * remaining work in one persistent launch (carlo-mc's dynamic runner,
+ * src/results.rs:211-239, batched). */
+int slsf_batch_run_v(slsf_ctx* ctx, slsf_task* const* tasks, size_t n_tasks, const uint32_t* sweeps,
+                     slsf_sweep_stats* stats);
+
 /* Bin means of many tasks in one device gather and one copy: out is
  * [n_tasks][n_rows][SLSF_BIN_COLS]; measurements (may be NULL) receives each
  * task's measurement count.  The batched form of slsf_task_get_bins, feeding

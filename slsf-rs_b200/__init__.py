@@ -99,6 +99,7 @@ SIGNATURES = {
     "slsf_task_reset_bins": (C.c_int, [_P]),
     "slsf_batch_run": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_uint32, C.POINTER(SweepStats)]),
     "slsf_batch_get_bins": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_size_t, _F64P, _U64P]),
+    "slsf_batch_run_v": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, _U32P, C.POINTER(SweepStats)]),
     "slsf_ctx_set_stream": (C.c_int, [_P, _P]),
     "slsf_ctx_launch_count": (C.c_int, [_P, _U64P]),
     "slsf_measure_noalloc": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, _P,
@@ -374,3 +375,220 @@ def exported_symbols():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(slsf_[a-z_0-9]+)\s*\(", text)))
+
+
+# ---------------------------------------------------------------- host layer (include/slsf_host.h)
+HOST_LIB_PATH = os.path.join(HERE, "libslsf_host.so")
+HOST_HEADER = os.path.join(ROOT, "include", "slsf_host.h")
+DERIVED = ("Magnetization", "Chi", "SpecificHeat", "RhoXY", "RhoZ")
+
+
+class Estimates(C.Structure):
+    _fields_ = [("measurements", C.c_uint64), ("n_bins", C.c_uint32), ("acceptance", C.c_double),
+                ("mean", C.c_double * BIN_COLS), ("err", C.c_double * BIN_COLS),
+                ("derived", C.c_double * 5), ("derived_err", C.c_double * 5)]
+
+    def as_dict(self):
+        d = {"measurements": self.measurements, "n_bins": self.n_bins, "acceptance": self.acceptance}
+        for k, name in enumerate(BIN_NAMES):
+            d[name] = (self.mean[k], self.err[k])
+        for k, name in enumerate(DERIVED):
+            d[name] = (self.derived[k], self.derived_err[k])
+        return d
+
+
+class ThetaTaskDesc(C.Structure):
+    _fields_ = [("lx", C.c_uint32), ("ly", C.c_uint32), ("lz", C.c_uint32), ("temperature", C.c_double),
+                ("j_xy", C.c_double), ("delta_j_xy", C.c_double), ("j_z_mean", C.c_double),
+                ("delta_j_z", C.c_double), ("disorder_seed", C.c_uint64), ("seed", C.c_uint64),
+                ("sweeps", C.c_uint32), ("thermalization", C.c_uint32), ("binsize", C.c_uint32),
+                ("proposal_width", C.c_double), ("wolff_steps", C.c_uint32),
+                ("j_xy_array", C.POINTER(C.c_double)), ("j_z_array", C.POINTER(C.c_double))]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("epoch_sweeps", C.c_uint32), ("max_active", C.c_uint32), ("budget_bytes", C.c_uint64)]
+
+
+class Request(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("lx", C.c_uint32), ("ly", C.c_uint32), ("lz", C.c_uint32),
+                ("temperature", C.c_double), ("proposal_width", C.c_double), ("wolff_steps", C.c_uint32),
+                ("seed", C.c_uint64), ("j_xy", C.POINTER(C.c_double)), ("j_z", C.POINTER(C.c_double)),
+                ("sweeps", C.c_uint32), ("thermalization", C.c_uint32), ("n_bins", C.c_uint32)]
+
+
+class Result(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("status", C.c_int), ("message", C.c_char * 160), ("submit_s", C.c_double),
+                ("admit_s", C.c_double), ("finish_s", C.c_double), ("sweeps", C.c_uint64),
+                ("accepted", C.c_uint64), ("cluster_sites", C.c_uint64), ("est", Estimates)]
+
+    def as_dict(self):
+        return {"tag": self.tag, "status": self.status, "message": self.message.decode(), "submit_s": self.submit_s,
+                "admit_s": self.admit_s, "finish_s": self.finish_s, "sweeps": self.sweeps,
+                "accepted": self.accepted, "cluster_sites": self.cluster_sites, "est": self.est.as_dict()}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("cancelled", C.c_uint64), ("epochs", C.c_uint64), ("launches", C.c_uint64),
+                ("site_updates", C.c_uint64), ("busy_s", C.c_double), ("peak_active", C.c_uint64),
+                ("peak_bytes", C.c_uint64)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+HOST_SIGNATURES = {
+    "slsf_host_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "slsf_binned_estimate": (C.c_int, [_F64P, C.c_size_t, C.c_size_t, _F64P, _F64P, C.POINTER(C.c_size_t)]),
+    "slsf_estimates_from_bins": (C.c_int, [_F64P, C.c_size_t, C.c_double, C.c_double, C.POINTER(Estimates)]),
+    "slsf_task_seed": (C.c_uint64, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double]),
+    "slsf_task_couplings": (C.c_int, [C.POINTER(ThetaTaskDesc), _F64P, _F64P]),
+    "slsf_model_run": (C.c_int, [_P, C.POINTER(ThetaTaskDesc), C.c_int, C.POINTER(Estimates)]),
+    "slsf_server_create": (C.c_int, [_P, C.POINTER(ServerConfig), C.POINTER(_P)]),
+    "slsf_server_destroy": (C.c_int, [_P]),
+    "slsf_server_submit": (C.c_int, [_P, C.POINTER(Request)]),
+    "slsf_server_cancel": (C.c_int, [_P, C.c_uint64]),
+    "slsf_server_step": (C.c_int, [_P, _U32P, _U32P]),
+    "slsf_server_start": (C.c_int, [_P]),
+    "slsf_server_stop": (C.c_int, [_P]),
+    "slsf_server_wait_idle": (C.c_int, [_P, C.c_double]),
+    "slsf_server_poll": (C.c_int, [_P, C.POINTER(Result), C.c_size_t, C.POINTER(C.c_size_t)]),
+    "slsf_server_stats_get": (C.c_int, [_P, C.POINTER(ServerStats)]),
+}
+
+_host = None
+
+
+def load_host():
+    global _host
+    if _host is not None:
+        return _host
+    load()
+    if not os.path.exists(HOST_LIB_PATH):
+        raise RuntimeError(f"{HOST_LIB_PATH} is missing: run build() first")
+    lib = C.CDLL(HOST_LIB_PATH)
+    for name, (res, args) in HOST_SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _host = lib
+    return lib
+
+
+def host_last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    load_host().slsf_host_last_error(buf, len(buf))
+    return buf.value.decode("utf-8")
+
+
+def host_check(code):
+    if code != OK:
+        raise SlsfError(code, host_last_error())
+
+
+def host_declared_symbols():
+    import re
+
+    text = re.sub(r"/\*.*?\*/", "", open(HOST_HEADER).read(), flags=re.S)
+    return sorted(set(re.findall(r"\b(slsf_[a-z_0-9]+)\s*\(", text)))
+
+
+def binned_estimate(samples, binsize):
+    a = np.ascontiguousarray(samples, np.float64)
+    mean, err, nb = C.c_double(), C.c_double(), C.c_size_t()
+    host_check(load_host().slsf_binned_estimate(_ptr(a, C.c_double), a.size, binsize, C.byref(mean), C.byref(err),
+                                                C.byref(nb)))
+    return {"mean": mean.value, "stderr": err.value, "n_bins": nb.value}
+
+
+def theta_task(dims, temperature, sweeps, thermalization, binsize, seed, disorder_seed=0, j_xy=1.0, delta_j_xy=0.0,
+               j_z_mean=0.1, delta_j_z=0.0, proposal_width=np.pi, wolff_steps=1, j_xy_array=None, j_z_array=None):
+    """A ThetaTask (src/model.rs:20-47); keeps the J arrays alive on the struct."""
+    d = ThetaTaskDesc(lx=dims[0], ly=dims[1], lz=dims[2], temperature=temperature, j_xy=j_xy, delta_j_xy=delta_j_xy,
+                      j_z_mean=j_z_mean, delta_j_z=delta_j_z, disorder_seed=disorder_seed, seed=seed, sweeps=sweeps,
+                      thermalization=thermalization, binsize=binsize, proposal_width=proposal_width,
+                      wolff_steps=wolff_steps)
+    keep = []
+    if j_xy_array is not None:
+        a = np.ascontiguousarray(j_xy_array, np.float64)
+        keep.append(a)
+        d.j_xy_array = _ptr(a, C.c_double)
+    if j_z_array is not None:
+        b = np.ascontiguousarray(j_z_array, np.float64)
+        keep.append(b)
+        d.j_z_array = _ptr(b, C.c_double)
+    d._keep = keep
+    return d
+
+
+def task_couplings(desc):
+    jx, jz = np.zeros(desc.lz), np.zeros(desc.lz)
+    host_check(load_host().slsf_task_couplings(C.byref(desc), _ptr(jx, C.c_double), _ptr(jz, C.c_double)))
+    return jx, jz
+
+
+def model_run(ctx, desc, batched=True):
+    """ThetaModel driven the way carlo-mc drives it; returns binned estimates."""
+    e = Estimates()
+    host_check(load_host().slsf_model_run(ctx.h, C.byref(desc), int(batched), C.byref(e)))
+    return e.as_dict()
+
+
+class Server:
+    """Continuous-batching server (slsf_server_*)."""
+
+    def __init__(self, ctx, epoch_sweeps=100, max_active=0, budget_bytes=0):
+        h = _P()
+        cfg = ServerConfig(epoch_sweeps=epoch_sweeps, max_active=max_active, budget_bytes=budget_bytes)
+        host_check(load_host().slsf_server_create(ctx.h, C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.ctx = ctx
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_host().slsf_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, tag, dims, temperature, seed, j_xy, j_z, sweeps, thermalization=0, n_bins=1,
+               proposal_width=np.pi, wolff_steps=1):
+        jx = np.ascontiguousarray(j_xy, np.float64)
+        jz = np.ascontiguousarray(j_z, np.float64)
+        r = Request(tag=tag, lx=dims[0], ly=dims[1], lz=dims[2], temperature=temperature,
+                    proposal_width=proposal_width, wolff_steps=wolff_steps, seed=seed, j_xy=_ptr(jx, C.c_double),
+                    j_z=_ptr(jz, C.c_double), sweeps=sweeps, thermalization=thermalization, n_bins=n_bins)
+        host_check(load_host().slsf_server_submit(self.h, C.byref(r)))
+
+    def cancel(self, tag):
+        host_check(load_host().slsf_server_cancel(self.h, tag))
+
+    def step(self):
+        a, p = C.c_uint32(), C.c_uint32()
+        host_check(load_host().slsf_server_step(self.h, C.byref(a), C.byref(p)))
+        return a.value, p.value
+
+    def start(self):
+        host_check(load_host().slsf_server_start(self.h))
+
+    def stop(self):
+        host_check(load_host().slsf_server_stop(self.h))
+
+    def wait_idle(self, timeout_s=600.0):
+        host_check(load_host().slsf_server_wait_idle(self.h, timeout_s))
+
+    def poll(self, max_results=4096):
+        buf = (Result * max_results)()
+        n = C.c_size_t()
+        host_check(load_host().slsf_server_poll(self.h, buf, max_results, C.byref(n)))
+        return [buf[i].as_dict() for i in range(n.value)]
+
+    def stats(self):
+        st = ServerStats()
+        host_check(load_host().slsf_server_stats_get(self.h, C.byref(st)))
+        return st.as_dict()

@@ -686,42 +686,86 @@ int slsf_task_reset_bins(slsf_task* t) {
     return SLSF_OK;
 }
 
-int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_sweeps,
-                   slsf_sweep_stats* stats) {
-    if (!ctx || (!tasks && n)) return set_error(SLSF_ERR_INVALID, "NULL argument");
-    if (n == 0 || n_sweeps == 0) return SLSF_OK;
+/* `v.sweeps` sweeps of one task through the grid-wide kernels, measuring
+ * after every sweep past thermalization into the task's bin sums as the
+ * persistent kernels do; counters accumulate into v.stats. */
+static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v) {
+    for (uint32_t sw = 0; sw < v.sweeps; ++sw) {
+        const uint64_t sweep = t->metro_sweeps + sw;
+        slsf::launch_metro_colour(v, sweep, 0, nullptr, ctx->stream);
+        slsf::launch_metro_colour(v, sweep, 1, nullptr, ctx->stream);
+        ctx->launches += 2;
+        for (uint32_t k = 0; k < t->wolff_steps; ++k) {
+            slsf::launch_wolff(v, t->wolff_done + (uint64_t)sw * t->wolff_steps + k, t->bonds, t->parent, nullptr,
+                               ctx->stream, nullptr, nullptr);
+            ctx->launches += 3;
+        }
+        const uint64_t done = sweep + 1;
+        if (done > t->thermalization && t->n_bins) {
+            const uint64_t b = (done - t->thermalization - 1) / t->binsize;
+            if (b < t->n_bins) {
+                slsf::launch_measure_into_bin(v, t->partials, t->done, t->result, t->bins + b * slsf::kBinCols,
+                                              ctx->stream);
+                ctx->launches += 1;
+            }
+        }
+    }
+}
+
+/* Shared body of slsf_batch_run (every task n_sweeps) and slsf_batch_run_v
+ * (task i per_task[i] sweeps; tasks with 0 sweeps are left out of the launch). */
+static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_all, uint32_t n_sweeps,
+                          const uint32_t* per_task, slsf_sweep_stats* all_stats) {
+    if (!ctx || (!all_tasks && n_all)) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    std::vector<slsf_task*> task_list;
+    std::vector<size_t> slot_of;
+    std::vector<uint32_t> sweeps_of;
+    for (size_t i = 0; i < n_all; ++i) {
+        const uint32_t sw = per_task ? per_task[i] : n_sweeps;
+        if (all_stats) all_stats[i] = slsf_sweep_stats{0, 0, 0, 0};
+        if (sw == 0) continue;
+        task_list.push_back(all_tasks[i]);
+        slot_of.push_back(i);
+        sweeps_of.push_back(sw);
+    }
+    const size_t n = task_list.size();
+    slsf_task* const* tasks = task_list.data();
+    if (n == 0) return SLSF_OK;
     if (int rc = bind_device(ctx)) return rc;
+    /* Kernel of each task: 0 = one CTA holds the replica
+     * (kernel_resident.cu); 1..8 = the cluster size of kernel_cluster.cu;
+     * kGrid = a lattice too large for one cluster's shared memory, swept by
+     * the grid-wide single-task kernels (kernels_plain.cu), which fill the
+     * GPU on their own. */
+    constexpr uint32_t kGrid = 0xFFFFFFFFu;
     std::vector<uint32_t> csize(n);
     for (size_t i = 0; i < n; ++i) {
         slsf_task* t = tasks[i];
         if (!t || t->ctx != ctx) return set_error(SLSF_ERR_INVALID, "task does not belong to this context");
         if (int rc = check_sweepable(t)) return rc;
-        /* 0: one CTA holds the replica (kernel_resident.cu); else the
-         * cluster size of kernel_cluster.cu. */
         if (slsf::resident_supports(t->lx, t->ly, t->lz, ctx->device)) {
             csize[i] = 0;
         } else {
             csize[i] = slsf::batched_cluster_size(t->lx, t->ly, t->lz, ctx->device);
-            if (!csize[i])
-                return set_error(SLSF_ERR_INVALID,
-                                 "lattice not supported by the shared-memory batched kernels (needs L_x <= 64, "
-                                 "L_x % 4 == 0, even L_y and L_z, and a slab of at most 8 CTAs in shared memory)");
+            if (!csize[i]) csize[i] = kGrid;
         }
     }
     if (int rc = ensure_batch_capacity(ctx, n)) return rc;
-    /* Grouped by kernel (one persistent launch each, cluster groups first),
-     * largest replicas first within a group so the grid ends evenly; each
-     * view accumulates its counters into its own slot of the batch stats
-     * array. */
+    /* Grouped by kernel (one persistent launch each, cluster groups first,
+     * grid-wide tasks last), largest replicas first within a group so the
+     * grid ends evenly; each view accumulates its counters into its own slot
+     * of the batch stats array. */
     std::vector<size_t> order(n);
     for (size_t i = 0; i < n; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-        if (csize[a] != csize[b]) return csize[a] > csize[b];
+        const uint32_t ka = csize[a] == kGrid ? 0u : csize[a] + 1, kb = csize[b] == kGrid ? 0u : csize[b] + 1;
+        if (ka != kb) return ka > kb;
         return tasks[a]->volume > tasks[b]->volume;
     });
     for (size_t k = 0; k < n; ++k) {
         TaskView v = tasks[order[k]]->view();
         v.stats = ctx->d_batch_stats + slsf::kStatSlots * order[k];
+        v.sweeps = sweeps_of[order[k]];
         ctx->h_views[k] = v;
     }
     SLSF_CUDA(cudaMemcpyAsync(ctx->d_views, ctx->h_views, sizeof(TaskView) * n, cudaMemcpyHostToDevice, ctx->stream));
@@ -729,6 +773,10 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_
     SLSF_CUDA(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int) * kQueues, ctx->stream));
     for (size_t lo = 0, q = 0; lo < n; ++q) {
         const uint32_t c = csize[order[lo]];
+        if (c == kGrid) {
+            for (size_t k = lo; k < n; ++k) run_grid_task(ctx, tasks[order[k]], ctx->h_views[k]);
+            break;
+        }
         size_t hi = lo;
         const uint32_t parts = c ? c : 1;
         uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0, max_lx = 0;
@@ -756,22 +804,35 @@ int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_
     int rc = SLSF_OK;
     for (size_t i = 0; i < n; ++i) {
         slsf_task* t = tasks[i];
+        const uint32_t sw = sweeps_of[i];
         const uint64_t before = t->metro_sweeps;
-        t->metro_sweeps += n_sweeps;
-        t->wolff_done += (uint64_t)n_sweeps * t->wolff_steps;
+        t->metro_sweeps += sw;
+        t->wolff_done += (uint64_t)sw * t->wolff_steps;
         /* Measurements happen after sweeps past the thermalization count. */
         const uint64_t lo = std::max<uint64_t>(before, t->thermalization);
         if (t->metro_sweeps > lo && t->n_bins) t->measurements += t->metro_sweeps - lo;
         const unsigned long long* s = &ctx->h_batch_stats[i * slsf::kStatSlots];
         if (s[slsf::kStatError]) rc = set_error(SLSF_ERR_TIMEOUT, "a bounded device loop hit its iteration limit");
-        if (stats) {
-            stats[i].sweeps = n_sweeps;
-            stats[i].accepted = s[slsf::kStatAccepted];
-            stats[i].wolff_clusters = s[slsf::kStatClusters];
-            stats[i].wolff_cluster_sites = s[slsf::kStatClusterSites];
+        if (all_stats) {
+            slsf_sweep_stats& o = all_stats[slot_of[i]];
+            o.sweeps = sw;
+            o.accepted = s[slsf::kStatAccepted];
+            o.wolff_clusters = csize[i] == kGrid ? (uint64_t)sw * t->wolff_steps : s[slsf::kStatClusters];
+            o.wolff_cluster_sites = s[slsf::kStatClusterSites];
         }
     }
     return rc;
+}
+
+int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_sweeps, slsf_sweep_stats* stats) {
+    if (n_sweeps == 0) return SLSF_OK;
+    return batch_run_impl(ctx, tasks, n, n_sweeps, nullptr, stats);
+}
+
+int slsf_batch_run_v(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, const uint32_t* sweeps,
+                     slsf_sweep_stats* stats) {
+    if (!sweeps && n) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    return batch_run_impl(ctx, tasks, n, 0, sweeps, stats);
 }
 
 int slsf_batch_get_bins(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, size_t n_rows, double* out,

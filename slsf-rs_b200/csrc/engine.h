@@ -58,6 +58,10 @@ void launch_wolff(const TaskView& t, uint64_t wolff_counter, uint8_t* bonds, uin
 /* Fused observables: writes 8 FP64 sums (mx, my, cos xyz, sin xyz) to result. */
 void launch_measure(const TaskView& t, double* partials, unsigned int* done, double* result,
                     cudaStream_t s);
+/* launch_measure that also adds the measurement's kBinCols stream values to
+ * bin_row (a task's bin sums row). */
+void launch_measure_into_bin(const TaskView& t, double* partials, unsigned int* done, double* result,
+                             double* bin_row, cudaStream_t s);
 int measure_partial_blocks(uint32_t volume);
 /* Correlation sums: sx[lz][rmax_xy], sy[lz][rmax_xy], sz[rmax_z] (FP64). */
 void launch_correlations(const TaskView& t, uint32_t rmax_xy, uint32_t rmax_z, double* work,

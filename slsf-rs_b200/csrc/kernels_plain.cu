@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kMeasureThreads)
     k_measure(const float* __restrict__ theta, const float* __restrict__ jxy,
               const float* __restrict__ jz, uint32_t lx, uint32_t ly, uint32_t lz,
               double* __restrict__ partials, unsigned int* __restrict__ done,
-              double* __restrict__ result) {
+              double* __restrict__ result, double* __restrict__ bin_row) {
     __shared__ double scratch[8 * 32];
     __shared__ bool last;
     const uint32_t volume = lx * ly * lz, plane = lx * ly;
@@ -238,6 +238,17 @@ __global__ void __launch_bounds__(kMeasureThreads)
     block_sum<8>(tot, scratch);
     if (threadIdx.x == 0) {
         for (int k = 0; k < 8; ++k) result[k] = tot[k];
+        if (bin_row) {
+            /* ThetaModel::measure's stream (src/model.rs:406-409) added to
+             * the bin's sums, in the batched kernels' column order. */
+            const double v = (double)volume;
+            const double e = -(tot[2] + tot[3] + tot[4]) / v;
+            const double vals[kBinCols] = {e,      e * e,  (tot[0] * tot[0] + tot[1] * tot[1]) / (v * v),
+                                           tot[2], tot[3], tot[4],
+                                           tot[5], tot[6], tot[7],
+                                           tot[5] * tot[5], tot[6] * tot[6], tot[7] * tot[7]};
+            for (int q = 0; q < kBinCols; ++q) bin_row[q] += vals[q];
+        }
         *done = 0;
     }
 }
@@ -397,7 +408,14 @@ void launch_measure(const TaskView& t, double* partials, unsigned int* done, dou
                     cudaStream_t s) {
     const uint32_t volume = t.lx * t.ly * t.lz;
     k_measure<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly,
-                                                                         t.lz, partials, done, result);
+                                                                         t.lz, partials, done, result, nullptr);
+}
+
+void launch_measure_into_bin(const TaskView& t, double* partials, unsigned int* done, double* result,
+                             double* bin_row, cudaStream_t s) {
+    const uint32_t volume = t.lx * t.ly * t.lz;
+    k_measure<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly,
+                                                                         t.lz, partials, done, result, bin_row);
 }
 
 size_t correlation_work_doubles(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rmax_xy,

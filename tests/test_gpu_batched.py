@@ -111,10 +111,33 @@ def test_checkpoint_resume_is_bit_exact(slsf, ctx, orc):
     assert a.counters == c.counters
 
 
-def test_batched_rejects_unsupported(slsf, ctx, orc):
-    [big] = batched_tasks(slsf, ctx, orc, [((128, 4, 4), 1.2, 1, 1, 0, 1, 0, 1)])
-    with pytest.raises(slsf.SlsfError):
-        ctx.batch_run([big], 1)
+def test_batched_grid_tasks_in_the_mix(slsf, ctx, orc):
+    # Lattices too large for one cluster's shared memory run through the
+    # grid-wide kernels inside the same batch call: same trajectory as the
+    # single-task path, bins equal to the plain measure stream.
+    dims, T, therm, binsize, sweeps = (128, 4, 4), 1.2, 1, 2, 5
+    n_bins = (sweeps - therm) // binsize
+    ref, series = plain_run(slsf, ctx, orc, dims, T, seed=11, sweeps=sweeps, wolff=1, therm=therm)
+    specs = [(dims, T, 11, 1, therm, binsize, n_bins, 1), ((8, 8, 8), 1.0, 3, 1, 0, 1, 0, 2),
+             ((48, 48, 48), 1.1, 6, 1, 0, 1, 0, 6)]
+    mix = batched_tasks(slsf, ctx, orc, specs)
+    stats = ctx.batch_run(mix, sweeps)
+    big = mix[0]
+    assert np.array_equal(big.theta.view(np.uint32), ref.theta.view(np.uint32))
+    assert big.counters == ref.counters
+    assert stats[0]["sweeps"] == sweeps and stats[0]["wolff_clusters"] == sweeps
+    bins, m = big.bins()
+    assert m == sweeps - therm
+    rows = np.array([[o["energy"], o["energy"] ** 2, o["magnetization_squared"], o["cos_x"], o["cos_y"], o["cos_z"],
+                      o["sin_x"], o["sin_y"], o["sin_z"], o["sin_x"] ** 2, o["sin_y"] ** 2, o["sin_z"] ** 2]
+                     for o in series])
+    for b in range(n_bins):
+        # same measure kernel on both paths: equal up to the host's FP64 averaging order
+        assert np.allclose(bins[b], rows[b * binsize:(b + 1) * binsize].mean(axis=0), rtol=1e-12, atol=1e-12)
+    for spec, t in zip(specs[1:], mix[1:]):
+        [alone] = batched_tasks(slsf, ctx, orc, [spec])
+        ctx.batch_run([alone], sweeps)
+        assert np.array_equal(t.theta.view(np.uint32), alone.theta.view(np.uint32))
 
 
 def _binned(bin_means):
