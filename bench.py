@@ -49,6 +49,10 @@ def parse():
     p.add_argument("--no-plain", action="store_true", help="skip the single-task L=64 comparison")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
+    p.add_argument("--no-serve", action="store_true", help="skip the served-stream side figure")
+    p.add_argument("--serve-tasks", type=int, default=4096, help="tasks of the served stream")
+    p.add_argument("--serve-epoch", type=int, default=100, help="sweeps per server epoch")
+    p.add_argument("--serve-only", action="store_true", help="run only the served stream (prints its own line)")
     return p.parse_args()
 
 
@@ -226,10 +230,108 @@ def plain_rate(pkg, ctx, L=64, T=1.3, sweeps=1000):
             "config": f"c1 single replica L={L}, T={T}, {sweeps} sweeps, Metropolis + 1 Wolff + measure per sweep"}
 
 
+SERVE_L = (8, 16, 24, 32, 48, 64)
+
+
+def serve_requests(pkg, n_tasks, seed=BASE_SEED):
+    """Served-stream tasks: L ~ U{8,16,24,32,48,64}, T ~ U[1.0,1.6], sweeps ~
+    U{200..2000}, disorder seed per task (J_xy = 1.2, J_z ~ U[0.5,1.5]); the
+    first 20% of sweeps thermalize, the rest go into 32 bins."""
+    rng = np.random.default_rng(seed)
+    Ls = rng.choice(SERVE_L, n_tasks)
+    Ts = rng.uniform(1.0, 1.6, n_tasks)
+    sweeps = rng.integers(200, 2001, n_tasks)
+    out = []
+    jz_cache = {}
+    for i in range(n_tasks):
+        L, T, sw = int(Ls[i]), float(Ts[i]), int(sweeps[i])
+        dseed = BASE_SEED + i
+        key = (L, dseed)
+        if key not in jz_cache:
+            jz_cache[key] = pkg.uniform_layer_disorder(L, 0.5, 1.5, dseed)
+        out.append(dict(tag=i + 1, dims=(L, L, L), T=T, seed=pkg.task_seed(BASE_SEED, L, i + 1, T),
+                        jxy=np.full(L, 1.2), jz=jz_cache[key], sweeps=sw, therm=sw // 5, n_bins=32))
+    return out
+
+
+def serve_run(pkg, ctx, reqs, rate, epoch_sweeps):
+    """Submits `reqs` as a Poisson stream of `rate` tasks/s (all at once when
+    rate is None) to a continuous-batching server running on its worker
+    thread; returns throughput and latency figures from the server's clock."""
+    srv = pkg.Server(ctx, epoch_sweeps=epoch_sweeps)
+    rng = np.random.default_rng(BASE_SEED + 1)
+    gaps = rng.exponential(1.0 / rate, len(reqs)) if rate else np.zeros(len(reqs))
+    arrivals = np.cumsum(gaps)
+    results = []
+    srv.start()
+    t0 = time.perf_counter()
+    for r, at in zip(reqs, arrivals):
+        delay = at - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        srv.submit(r["tag"], r["dims"], r["T"], r["seed"], r["jxy"], r["jz"], r["sweeps"],
+                   thermalization=r["therm"], n_bins=r["n_bins"])
+        if len(results) < len(reqs):
+            results.extend(srv.poll(256))
+    srv.wait_idle(3600)
+    srv.stop()
+    results.extend(srv.poll(len(reqs)))
+    st = srv.stats()
+    srv.close()
+    ok = [r for r in results if r["status"] == pkg.OK]
+    lat = np.array([r["finish_s"] - r["submit_s"] for r in ok])
+    wait = np.array([r["admit_s"] - r["submit_s"] for r in ok])
+    first = min(r["submit_s"] for r in results)
+    last = max(r["finish_s"] for r in results)
+    updates = sum(r["dims"][0] ** 3 * r["sweeps"] for r in reqs)
+    return {"tasks": len(reqs), "completed": len(ok), "failed": len(results) - len(ok),
+            "offered_tasks_per_s": rate, "makespan_s": last - first,
+            "throughput": updates / (last - first), "unit": "site-updates/s",
+            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+            "p50_queue_s": float(np.percentile(wait, 50)), "p99_queue_s": float(np.percentile(wait, 99)),
+            "epochs": st["epochs"], "launch_groups": st["launches"], "peak_active": st["peak_active"],
+            "peak_bytes": st["peak_bytes"], "busy_s": st["busy_s"]}
+
+
+def served_stream(pkg, ctx, n_tasks, epoch_sweeps):
+    """Served stream: capacity with every task queued at t = 0, then Poisson
+    arrivals offering 0.8x and 1.5x that capacity."""
+    reqs = serve_requests(pkg, n_tasks)
+    mean_work = float(np.mean([r["dims"][0] ** 3 * r["sweeps"] for r in reqs]))
+    warm = serve_requests(pkg, 64, seed=BASE_SEED + 7)
+    serve_run(pkg, ctx, warm, None, epoch_sweeps)
+    sat = serve_run(pkg, ctx, reqs, None, epoch_sweeps)
+    capacity = sat["throughput"]
+    out = {"workload": f"c3 served stream: {n_tasks} tasks, L~U{{8..64}}, T~U[1.0,1.6], sweeps~U{{200..2000}}, "
+                       f"J_xy=1.2, J_z~U[0.5,1.5] per task, 20% thermalization, 32 bins, epoch {epoch_sweeps} sweeps",
+           "mean_site_updates_per_task": mean_work, "saturation": sat, "capacity": capacity}
+    for load in (0.8, 1.5):
+        rate = load * capacity / mean_work
+        r = serve_run(pkg, ctx, reqs, rate, epoch_sweeps)
+        r["offered_load"] = load
+        out[f"load_{load}"] = r
+    return out
+
+
+def serve_only(args):
+    import torch
+
+    torch.cuda.set_device(0)
+    pkg = load_pkg()
+    pkg.load()
+    ctx = pkg.Context(0)
+    res = served_stream(pkg, ctx, args.serve_tasks, args.serve_epoch)
+    ctx.close()
+    print(json.dumps(res))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.serve_only:
+        return serve_only(args)
 
     import torch
 
@@ -328,7 +430,7 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (tps * n * L ** 3) if tps is not None else None,
                 "peak_kind": peak_kind,
-                "kernel": "k_batched (one launch = S sweeps of every replica, state resident in shared memory)",
+                "kernel": "k_resident (one launch = S sweeps of every replica, each replica resident in one CTA's shared memory)",
                 "algorithmic_bytes_per_launch": alg_bytes}
 
     extra = {}
@@ -336,6 +438,8 @@ def main():
         if not args.no_plain:
             extra["plain"] = plain_rate(pkg, ctx)
             extra["plain"]["batched_over_plain"] = value / extra["plain"]["value"]
+        if not args.no_serve:
+            extra["served"] = served_stream(pkg, ctx, args.serve_tasks, args.serve_epoch)
         if not args.no_cpu:
             extra["cpu_baseline"] = cpu_baseline(L, list(np.linspace(1.1, 1.5, args.temperatures)), 2000,
                                                  args.cpu_seconds)

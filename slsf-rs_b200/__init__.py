@@ -150,10 +150,13 @@ class Context:
         check(load().slsf_ctx_create(device, budget_bytes, 0, C.byref(h)))
         self.h = h
         self._tasks = weakref.WeakSet()
+        self._servers = weakref.WeakSet()
 
     def close(self):
-        """Destroy every live task of this context, then the context."""
+        """Destroy every live server and task of this context, then the context."""
         if getattr(self, "h", None):
+            for srv in list(self._servers):
+                srv.close()
             for t in list(self._tasks):
                 t.close()
             check(load().slsf_ctx_destroy(self.h))
@@ -544,6 +547,7 @@ class Server:
         host_check(load_host().slsf_server_create(ctx.h, C.byref(cfg), C.byref(h)))
         self.h = h
         self.ctx = ctx
+        ctx._servers.add(self)
 
     def close(self):
         if getattr(self, "h", None):

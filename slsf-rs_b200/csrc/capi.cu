@@ -64,9 +64,10 @@ bool width_ok(double w) { return w >= 0.0 && std::isfinite(w); }
 
 uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
 
-/* One work-queue counter per kernel group of a batch: the one-CTA kernel and
- * the cluster kernel at sizes 1, 2, 4, 8. */
-constexpr int kQueues = 5;
+/* One work-queue counter (and side stream) per kernel group of a batch: the
+ * one-CTA kernel, the cluster kernel at sizes 1, 2, 4, 8, and the grid-wide
+ * kernels. */
+constexpr int kQueues = 6;
 
 /* Offsets of the arrays inside a task's block. */
 struct TaskLayout {
@@ -120,6 +121,12 @@ struct slsf_ctx {
     unsigned long long* h_batch_stats = nullptr; /* pinned */
     uint32_t views_cap = 0;
     unsigned int* d_queue = nullptr;
+    /* one side stream per extra kernel group of a batch, forked from and
+     * joined back into `stream` with events, so that groups that do not
+     * fill the GPU alone overlap */
+    cudaStream_t side[kQueues] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kQueues] = {};
     /* bins gather scratch */
     const double** d_bin_src = nullptr;
     const double** h_bin_src = nullptr; /* pinned */
@@ -280,6 +287,16 @@ uint64_t slsf_task_bytes(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t n_bins)
     return layout_of(lx, ly, lz, n_bins).total;
 }
 
+static void destroy_streams(slsf_ctx* ctx) {
+    for (int q = 0; q < kQueues; ++q) {
+        if (ctx->side[q]) cudaStreamSynchronize(ctx->side[q]);
+        if (ctx->side[q]) cudaStreamDestroy(ctx->side[q]);
+        if (ctx->join[q]) cudaEventDestroy(ctx->join[q]);
+    }
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+}
+
 int slsf_ctx_create(int device, uint64_t budget_bytes, uint32_t flags, slsf_ctx** out) {
     (void)flags;
     if (!out) return set_error(SLSF_ERR_INVALID, "output handle pointer is NULL");
@@ -301,8 +318,14 @@ int slsf_ctx_create(int device, uint64_t budget_bytes, uint32_t flags, slsf_ctx*
     ctx->budget = budget_bytes ? budget_bytes : (uint64_t)(0.9 * (double)free_b);
     e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_queue, sizeof(unsigned int) * kQueues);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming);
+    for (int q = 0; q < kQueues && e == cudaSuccess; ++q) {
+        e = cudaStreamCreateWithFlags(&ctx->side[q], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join[q], cudaEventDisableTiming);
+    }
     if (e != cudaSuccess) {
-        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+        destroy_streams(ctx);
+        if (ctx->d_queue) cudaFree(ctx->d_queue);
         delete ctx;
         return cuda_error(e, "context set-up");
     }
@@ -324,7 +347,7 @@ int slsf_ctx_destroy(slsf_ctx* ctx) {
     for (void* p : host)
         if (p) cudaFreeHost(p);
     ctx->pool.release();
-    cudaStreamDestroy(ctx->own_stream);
+    destroy_streams(ctx);
     delete ctx;
     return SLSF_OK;
 }
@@ -689,15 +712,15 @@ int slsf_task_reset_bins(slsf_task* t) {
 /* `v.sweeps` sweeps of one task through the grid-wide kernels, measuring
  * after every sweep past thermalization into the task's bin sums as the
  * persistent kernels do; counters accumulate into v.stats. */
-static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v) {
+static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v, cudaStream_t st) {
     for (uint32_t sw = 0; sw < v.sweeps; ++sw) {
         const uint64_t sweep = t->metro_sweeps + sw;
-        slsf::launch_metro_colour(v, sweep, 0, nullptr, ctx->stream);
-        slsf::launch_metro_colour(v, sweep, 1, nullptr, ctx->stream);
+        slsf::launch_metro_colour(v, sweep, 0, nullptr, st);
+        slsf::launch_metro_colour(v, sweep, 1, nullptr, st);
         ctx->launches += 2;
         for (uint32_t k = 0; k < t->wolff_steps; ++k) {
             slsf::launch_wolff(v, t->wolff_done + (uint64_t)sw * t->wolff_steps + k, t->bonds, t->parent, nullptr,
-                               ctx->stream, nullptr, nullptr);
+                               st, nullptr, nullptr);
             ctx->launches += 3;
         }
         const uint64_t done = sweep + 1;
@@ -705,7 +728,7 @@ static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v) 
             const uint64_t b = (done - t->thermalization - 1) / t->binsize;
             if (b < t->n_bins) {
                 slsf::launch_measure_into_bin(v, t->partials, t->done, t->result, t->bins + b * slsf::kBinCols,
-                                              ctx->stream);
+                                              st);
                 ctx->launches += 1;
             }
         }
@@ -771,10 +794,23 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
     SLSF_CUDA(cudaMemcpyAsync(ctx->d_views, ctx->h_views, sizeof(TaskView) * n, cudaMemcpyHostToDevice, ctx->stream));
     SLSF_CUDA(cudaMemsetAsync(ctx->d_batch_stats, 0, 8 * slsf::kStatSlots * n, ctx->stream));
     SLSF_CUDA(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int) * kQueues, ctx->stream));
+    /* Group g runs on ctx->stream (g == 0) or on side stream g, forked after
+     * the uploads above and joined before the stats read-back below. */
+    size_t n_groups = 0;
+    for (size_t k = 0; k < n; ++k)
+        if (k == 0 || csize[order[k]] != csize[order[k - 1]]) ++n_groups;
+    if (n_groups > 1) SLSF_CUDA(cudaEventRecord(ctx->fork, ctx->stream));
     for (size_t lo = 0, q = 0; lo < n; ++q) {
         const uint32_t c = csize[order[lo]];
+        cudaStream_t st = ctx->stream;
+        if (q > 0) {
+            st = ctx->side[q];
+            SLSF_CUDA(cudaStreamWaitEvent(st, ctx->fork, 0));
+        }
         if (c == kGrid) {
-            for (size_t k = lo; k < n; ++k) run_grid_task(ctx, tasks[order[k]], ctx->h_views[k]);
+            for (size_t k = lo; k < n; ++k) run_grid_task(ctx, tasks[order[k]], ctx->h_views[k], st);
+            if (q > 0) SLSF_CUDA(cudaEventRecord(ctx->join[q], st));
+            if (q > 0) SLSF_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join[q], 0));
             break;
         }
         size_t hi = lo;
@@ -791,11 +827,15 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
         }
         if (c == 0)
             SLSF_CUDA(slsf::launch_resident(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
-                                            ctx->device, ctx->stream, max_vs, max_rows, max_lz));
+                                            ctx->device, st, max_vs, max_rows, max_lz));
         else
             SLSF_CUDA(slsf::launch_batched(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
-                                           ctx->device, ctx->stream, c, max_vs, max_rows, max_lz, max_plane, max_lx));
+                                           ctx->device, st, c, max_vs, max_rows, max_lz, max_plane, max_lx));
         ctx->launches += 1;
+        if (q > 0) {
+            SLSF_CUDA(cudaEventRecord(ctx->join[q], st));
+            SLSF_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join[q], 0));
+        }
         lo = hi;
     }
     SLSF_CUDA(cudaMemcpyAsync(ctx->h_batch_stats, ctx->d_batch_stats, 8 * slsf::kStatSlots * n,

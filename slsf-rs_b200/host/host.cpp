@@ -14,7 +14,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
-#include <deque>
+#include <list>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -280,7 +280,7 @@ struct slsf_server {
     std::mutex mu;                /* guards queue, results, cancel set, stats */
     std::condition_variable cv;   /* new work or stop */
     std::condition_variable idle; /* queue and active set empty */
-    std::deque<Pending> queue;
+    std::list<Pending> queue; /* stable iterators: submissions append while admission scans */
     std::vector<slsf_result> results;
     std::unordered_set<uint64_t> cancel;
     slsf_server_stats stats = {};
@@ -291,6 +291,8 @@ struct slsf_server {
     std::atomic<bool> running{false};
     std::thread worker;
     std::atomic<uint32_t> n_active{0};
+    uint32_t admitting = 0; /* requests between the queue and the active set (guarded by mu) */
+    std::vector<uint64_t> admitting_tags;
     std::string worker_error; /* set when the worker stopped on a device error */
 };
 
@@ -333,78 +335,105 @@ std::string validate(const Pending& p) {
 /* Admission: FIFO, but a request that does not fit may be passed by later
  * ones that do, at most 8 epochs in a row (then admission waits for it). */
 void admit(slsf_server* s) {
+    struct Pick {
+        Pending p;
+        uint64_t bytes;
+        uint32_t binsize, n_bins;
+        slsf_task* task;
+        int rc;
+        std::string msg;
+    };
     const uint64_t budget = s->cfg.budget_bytes;
-    std::unique_lock<std::mutex> lock(s->mu);
-    bool head_blocked = false;
-    for (auto it = s->queue.begin(); it != s->queue.end();) {
-        Pending& p = *it;
-        if (s->cfg.max_active && s->active.size() >= s->cfg.max_active) break;
-        const uint32_t measured = p.req.sweeps > p.req.thermalization ? p.req.sweeps - p.req.thermalization : 0;
-        const uint32_t n_bins = std::max<uint32_t>(1, std::min<uint32_t>(p.req.n_bins ? p.req.n_bins : 1,
-                                                                         std::max<uint32_t>(measured, 1)));
-        /* complete bins only (carlo drops a partial last bin) */
-        const uint32_t binsize = std::max<uint32_t>(1, measured / n_bins);
-        const uint64_t bytes = slsf_task_bytes(p.req.lx, p.req.ly, p.req.lz, n_bins);
-        if (bytes > budget) {
-            /* can never fit: reject now */
-            s->results.push_back(make_result(p, SLSF_ERR_BUDGET, "request does not fit in the server's device "
-                                                                 "memory budget", now_s(s->t0)));
-            s->stats.failed++;
-            it = s->queue.erase(it);
-            continue;
-        }
-        if (s->used + bytes > budget) {
-            if (it == s->queue.begin()) {
-                if (++p.bypassed > 8) break;
-                head_blocked = true;
+    std::vector<Pick> picks;
+    {
+        /* Choose under the lock; s->used and s->active change only on the
+         * thread that runs epochs, which is this one. */
+        std::lock_guard<std::mutex> lock(s->mu);
+        uint64_t used = s->used;
+        size_t n_active = s->active.size();
+        for (auto it = s->queue.begin(); it != s->queue.end();) {
+            if (s->cfg.max_active && n_active >= s->cfg.max_active) break;
+            Pending& p = *it;
+            const uint32_t measured = p.req.sweeps > p.req.thermalization ? p.req.sweeps - p.req.thermalization : 0;
+            const uint32_t n_bins = std::max<uint32_t>(
+                1, std::min<uint32_t>(p.req.n_bins ? p.req.n_bins : 1, std::max<uint32_t>(measured, 1)));
+            /* complete bins only (carlo drops a partial last bin) */
+            const uint32_t binsize = std::max<uint32_t>(1, measured / n_bins);
+            const uint64_t bytes = slsf_task_bytes(p.req.lx, p.req.ly, p.req.lz, n_bins);
+            if (bytes > budget) {
+                /* can never fit: reject now */
+                s->results.push_back(make_result(p, SLSF_ERR_BUDGET,
+                                                 "request does not fit in the server's device memory budget",
+                                                 now_s(s->t0)));
+                s->stats.failed++;
+                it = s->queue.erase(it);
+                continue;
             }
-            ++it;
-            continue;
+            if (used + bytes > budget) {
+                /* later requests may pass a blocked head at most 8 epochs in a row */
+                if (it == s->queue.begin() && ++p.bypassed > 8) break;
+                ++it;
+                continue;
+            }
+            s->admitting_tags.push_back(p.req.tag);
+            picks.push_back(Pick{std::move(p), bytes, binsize, n_bins, nullptr, SLSF_OK, ""});
+            it = s->queue.erase(it);
+            used += bytes;
+            ++n_active;
         }
-        (void)head_blocked;
-        Pending mine = std::move(p);
-        it = s->queue.erase(it);
-        lock.unlock();
+        s->admitting += (uint32_t)picks.size();
+    }
+    /* Device set-up outside the lock: submissions continue meanwhile. */
+    for (Pick& k : picks) {
         slsf_task_desc d = {};
-        d.lx = mine.req.lx;
-        d.ly = mine.req.ly;
-        d.lz = mine.req.lz;
-        d.temperature = mine.req.temperature;
-        d.proposal_width = mine.req.proposal_width;
-        d.wolff_steps = mine.req.wolff_steps;
-        d.seed = mine.req.seed;
-        d.j_xy = mine.jxy.data();
-        d.n_j_xy = mine.jxy.size();
-        d.j_z = mine.jz.data();
-        d.n_j_z = mine.jz.size();
-        d.thermalization = mine.req.thermalization;
-        d.binsize = binsize;
-        d.n_bins = n_bins;
-        slsf_task* task = nullptr;
-        int rc = slsf_task_create(s->ctx, &d, &task);
-        if (rc == SLSF_OK) rc = slsf_task_init_random(task);
-        lock.lock();
-        if (rc != SLSF_OK) {
+        d.lx = k.p.req.lx;
+        d.ly = k.p.req.ly;
+        d.lz = k.p.req.lz;
+        d.temperature = k.p.req.temperature;
+        d.proposal_width = k.p.req.proposal_width;
+        d.wolff_steps = k.p.req.wolff_steps;
+        d.seed = k.p.req.seed;
+        d.j_xy = k.p.jxy.data();
+        d.n_j_xy = k.p.jxy.size();
+        d.j_z = k.p.jz.data();
+        d.n_j_z = k.p.jz.size();
+        d.thermalization = k.p.req.thermalization;
+        d.binsize = k.binsize;
+        d.n_bins = k.n_bins;
+        k.rc = slsf_task_create(s->ctx, &d, &k.task);
+        if (k.rc == SLSF_OK) k.rc = slsf_task_init_random(k.task);
+        if (k.rc != SLSF_OK) {
             char buf[160];
             slsf_last_error(buf, sizeof(buf));
-            if (task) slsf_task_destroy(task);
-            s->results.push_back(make_result(mine, rc, buf, now_s(s->t0)));
+            k.msg = buf;
+            if (k.task) slsf_task_destroy(k.task);
+            k.task = nullptr;
+        }
+    }
+    std::lock_guard<std::mutex> lock(s->mu);
+    const double t = now_s(s->t0);
+    s->admitting_tags.clear();
+    for (Pick& k : picks) {
+        s->admitting--;
+        if (k.rc != SLSF_OK) {
+            s->cancel.erase(k.p.req.tag);
+            s->results.push_back(make_result(k.p, k.rc, k.msg, t));
             s->stats.failed++;
             continue;
         }
         Active a;
-        a.p = std::move(mine);
-        a.task = task;
-        a.bytes = bytes;
+        a.p = std::move(k.p);
+        a.task = k.task;
+        a.bytes = k.bytes;
         a.remaining = a.p.req.sweeps;
-        a.binsize = binsize;
-        a.n_bins = n_bins;
-        a.admit_s = now_s(s->t0);
-        s->used += bytes;
+        a.binsize = k.binsize;
+        a.n_bins = k.n_bins;
+        a.admit_s = t;
+        s->used += k.bytes;
         s->active.push_back(std::move(a));
-        s->stats.peak_active = std::max<uint64_t>(s->stats.peak_active, s->active.size());
-        s->stats.peak_bytes = std::max<uint64_t>(s->stats.peak_bytes, s->used);
     }
+    s->stats.peak_active = std::max<uint64_t>(s->stats.peak_active, s->active.size());
+    s->stats.peak_bytes = std::max<uint64_t>(s->stats.peak_bytes, s->used);
 }
 
 /* Retire finished or cancelled tasks: one gather of their bins, estimates,
@@ -505,7 +534,7 @@ int retire(slsf_server* s) {
 
 void notify_if_idle(slsf_server* s) {
     std::lock_guard<std::mutex> lock(s->mu);
-    if (s->queue.empty() && s->active.empty()) s->idle.notify_all();
+    if (s->queue.empty() && s->active.empty() && !s->admitting) s->idle.notify_all();
 }
 
 /* One epoch: retire cancelled tasks, admit, advance every active task by up
@@ -630,6 +659,11 @@ int slsf_server_cancel(slsf_server* s, uint64_t tag) {
             s->cancel.insert(tag);
             return SLSF_OK;
         }
+    /* being admitted: cancelled at the next retire */
+    if (std::find(s->admitting_tags.begin(), s->admitting_tags.end(), tag) != s->admitting_tags.end()) {
+        s->cancel.insert(tag);
+        return SLSF_OK;
+    }
     return fail(SLSF_ERR_INVALID, "unknown request tag");
 }
 
@@ -672,7 +706,7 @@ int slsf_server_wait_idle(slsf_server* s, double timeout_s) {
     if (!s) return fail(SLSF_ERR_INVALID, "NULL argument");
     std::unique_lock<std::mutex> lock(s->mu);
     const bool ok = s->idle.wait_for(lock, std::chrono::duration<double>(timeout_s), [&] {
-        return (s->queue.empty() && s->active.empty()) || !s->worker_error.empty();
+        return (s->queue.empty() && s->active.empty() && !s->admitting) || !s->worker_error.empty();
     });
     if (!s->worker_error.empty()) return fail(SLSF_ERR_CUDA, "server worker stopped: " + s->worker_error);
     return ok ? SLSF_OK : fail(SLSF_ERR_TIMEOUT, "server still has queued or running requests");

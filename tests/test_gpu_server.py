@@ -206,3 +206,37 @@ def test_server_worker_and_idle(slsf, ctx, orc):
     assert r["status"] == slsf.OK and r["sweeps"] == 40
     assert srv.stats()["launches"] >= 4
     srv.close()
+
+
+def test_server_admits_while_submissions_continue(slsf, ctx, orc):
+    # Requests arrive while the worker thread admits and runs others; every
+    # one completes, and each equals the same request run alone.
+    import time
+
+    srv = slsf.Server(ctx, epoch_sweeps=4)
+    srv.start()
+    reqs = [(k + 1, ((8, 8, 8), (16, 16, 16), (16, 8, 4))[k % 3], 1.0 + 0.01 * k, 100 + k, 12 + (k % 5), 2, 2)
+            for k in range(150)]
+    for r in reqs:
+        submit(srv, orc, r)
+        if r[0] % 10 == 0:
+            srv.cancel(r[0])  # queued, being admitted or running: all are cancellable
+        time.sleep(0.0005)
+    srv.wait_idle(120)
+    srv.stop()
+    res = {r["tag"]: r for r in srv.poll(1000)}
+    srv.close()
+    assert sorted(res) == [r[0] for r in reqs]
+    for r in reqs:
+        got = res[r[0]]
+        if r[0] % 10 == 0:
+            assert got["status"] in (slsf.OK, slsf.ERR_STATE)
+            continue
+        assert got["status"] == slsf.OK, got["message"]
+        assert got["sweeps"] == r[4]
+    one = slsf.Server(ctx, epoch_sweeps=4)
+    submit(one, orc, reqs[4])
+    drain(one)
+    [alone] = one.poll()
+    one.close()
+    assert alone["est"]["Energy"] == res[reqs[4][0]]["est"]["Energy"]
