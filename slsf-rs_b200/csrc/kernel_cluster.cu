@@ -34,6 +34,7 @@
 
 #include <algorithm>
 
+#include "bins.cuh"
 #include "engine.h"
 #include "fastdiv.h"
 #include "xy_device.cuh"
@@ -301,10 +302,14 @@ __device__ __forceinline__ void store_slab(const TaskView& t, const Geo& g, cons
 /* One colour half-sweep of the slab; the halo holds colour 1-c of the
  * partner planes.  A warp owns 32 consecutive Philox blocks (64 sites);
  * lanes exchange words so that lane j updates colour-compact sites
- * 2*base + j and 2*base + 32 + j. */
-template <typename W>
+ * 2*base + j and 2*base + 32 + j.  With kMeasure (colour 0) it also adds the
+ * slab's share of the observables of the state it starts from: the three
+ * forward and three backward bonds of every colour-0 site (every bond has
+ * exactly one colour-0 end) and the magnetisation of the site and of its +x
+ * neighbour, with the bond_cos / bond_sin terms of the measurement pass. */
+template <bool kMeasure, typename W>
 __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, Smem<W>& s, uint64_t sweep,
-                                               uint32_t colour) {
+                                               uint32_t colour, float (&acc)[8]) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t nwarps = blockDim.x >> 5;
     const uint32_t npairs = g.half_s >> 1;
@@ -339,25 +344,38 @@ __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, 
             const uint32_t xm = (x == 0) ? li + g.lx - 1 : li - 1;
             const uint32_t yp = (y + 1 == g.ly) ? li + g.lx - g.plane : li + g.lx;
             const uint32_t ym = (y == 0) ? li + g.plane - g.lx : li - g.lx;
-            const float t0 = s.th[oth + (xp >> 1)];
-            const float t1 = s.th[oth + (xm >> 1)];
-            const float t2 = s.th[oth + (yp >> 1)];
-            const float t3 = s.th[oth + (ym >> 1)];
-            const float t4 = (zl + 1 < g.nz) ? s.th[oth + ((li + g.plane) >> 1)] : halo_theta(g, s, true, ocol, pc);
-            const float t5 = (zl > 0) ? s.th[oth + ((li - g.plane) >> 1)] : halo_theta(g, s, false, ocol, pc);
-            float ns[6], nc[6];
-            __sincosf(t0, &ns[0], &nc[0]);
-            __sincosf(t1, &ns[1], &nc[1]);
-            __sincosf(t2, &ns[2], &nc[2]);
-            __sincosf(t3, &ns[3], &nc[3]);
-            __sincosf(t4, &ns[4], &nc[4]);
-            __sincosf(t5, &ns[5], &nc[5]);
             const float jx = s.jxy[z], jzp = s.jz[z], jzm = s.jz[z == 0 ? g.lz - 1 : z - 1];
-            const float hxf = field_component(jx, jzp, jzm, nc[0], nc[1], nc[2], nc[3], nc[4], nc[5]);
-            const float hyf = field_component(jx, jzp, jzm, ns[0], ns[1], ns[2], ns[3], ns[4], ns[5]);
             const float th = s.th[own + h];
             float si, ci;
             __sincosf(th, &si, &ci);
+            /* neighbours in pairs (+x -x, +y -y, +z -z), folded into the field as they come */
+            float sa, ca, sb, cb;
+            __sincosf(s.th[oth + (xp >> 1)], &sa, &ca);
+            __sincosf(s.th[oth + (xm >> 1)], &sb, &cb);
+            if (kMeasure) {
+                acc[0] += ci + ca;
+                acc[1] += si + sa;
+                acc[2] += bond_cos(jx, ci, si, ca, sa) + bond_cos(jx, cb, sb, ci, si);
+                acc[5] += bond_sin(jx, ci, si, ca, sa) + bond_sin(jx, cb, sb, ci, si);
+            }
+            const float hx01 = __fadd_rn(ca, cb), hy01 = __fadd_rn(sa, sb);
+            __sincosf(s.th[oth + (yp >> 1)], &sa, &ca);
+            __sincosf(s.th[oth + (ym >> 1)], &sb, &cb);
+            if (kMeasure) {
+                acc[3] += bond_cos(jx, ci, si, ca, sa) + bond_cos(jx, cb, sb, ci, si);
+                acc[6] += bond_sin(jx, ci, si, ca, sa) + bond_sin(jx, cb, sb, ci, si);
+            }
+            const float hx23 = __fadd_rn(ca, cb), hy23 = __fadd_rn(sa, sb);
+            const float t4 = (zl + 1 < g.nz) ? s.th[oth + ((li + g.plane) >> 1)] : halo_theta(g, s, true, ocol, pc);
+            const float t5 = (zl > 0) ? s.th[oth + ((li - g.plane) >> 1)] : halo_theta(g, s, false, ocol, pc);
+            __sincosf(t4, &sa, &ca);
+            __sincosf(t5, &sb, &cb);
+            if (kMeasure) {
+                acc[4] += bond_cos(jzp, ci, si, ca, sa) + bond_cos(jzm, cb, sb, ci, si);
+                acc[7] += bond_sin(jzp, ci, si, ca, sa) + bond_sin(jzm, cb, sb, ci, si);
+            }
+            const float hxf = field_from_pairs(jx, jzp, jzm, hx01, hx23, ca, cb);
+            const float hyf = field_from_pairs(jx, jzp, jzm, hy01, hy23, sa, sb);
             float tn, sn, cn;
             if (metro_decide(th, ci, si, hxf, hyf, t.beta, t.width, u_prop, u_acc, &tn, &sn, &cn)) {
                 s.th[own + h] = tn;
@@ -569,16 +587,25 @@ __device__ __forceinline__ void measure_slab(const Geo& g, const Smem<W>& s, dou
         const float jx = s.jxy[g.z0 + c.zl], jzz = s.jz[g.z0 + c.zl];
         f[0] += ci;
         f[1] += si;
-        f[2] += jx * (ci * cx + si * sx);
-        f[3] += jx * (ci * cy + si * sy);
-        f[4] += jzz * (ci * cz + si * sz);
-        f[5] += jx * (si * cx - ci * sx);
-        f[6] += jx * (si * cy - ci * sy);
-        f[7] += jzz * (si * cz - ci * sz);
+        f[2] += bond_cos(jx, ci, si, cx, sx);
+        f[3] += bond_cos(jx, ci, si, cy, sy);
+        f[4] += bond_cos(jzz, ci, si, cz, sz);
+        f[5] += bond_sin(jx, ci, si, cx, sx);
+        f[6] += bond_sin(jx, ci, si, cy, sy);
+        f[7] += bond_sin(jzz, ci, si, cz, sz);
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) acc[k] = (double)f[k];
     block_sum<8>(acc, red);
+}
+
+/* Rank 0, thread 0: totals of the slab sums and their bin entry. */
+__device__ __forceinline__ void bin_cluster_sums(const TaskView& t, const Geo& g, uint64_t done,
+                                                 const double (*cred)[8], double* bin_acc, int64_t& bin_cur) {
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t q = 0; q < g.csize; ++q)
+        for (int k = 0; k < 8; ++k) a[k] += cred[q][k];
+    bin_measurement(t, g.volume, done, a, bin_acc, bin_cur);
 }
 
 template <typename W>
@@ -624,54 +651,51 @@ __global__ void __launch_bounds__(kBThreads, 1)
 #endif
         uint32_t accepted = 0;
         int64_t bin_cur = -1;
+        /* ThetaModel::measure after every sweep past thermalization: the state
+         * after sweep k is measured inside sweep k+1's colour-0 half-sweep,
+         * the launch's last state by the measurement pass below; each CTA
+         * sends its slab sums to rank 0, which bins them. */
+        const bool measuring = t.n_bins > 0;
         for (uint32_t sw = 0; sw < sweeps; ++sw) {
             const uint64_t sweep = t.metro_sweeps + sw;
+            const bool meas = measuring && sw > 0 && sweep > t.thermalization;
+            float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             fill_halo(g, s, rm, 1);
-            accepted += half_sweep(t, g, s, sweep, 0);
+            if (meas) {
+                accepted += half_sweep<true>(t, g, s, sweep, 0, acc);
+                double tot[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) tot[k] = acc[k];
+                block_sum<8>(tot, red);
+                if (threadIdx.x == 0)
+                    for (int k = 0; k < 8; ++k) *cluster.map_shared_rank(&cred[rank][k], 0) = tot[k];
+            } else {
+                accepted += half_sweep<false>(t, g, s, sweep, 0, acc);
+            }
             cluster_barrier(g, cluster);
             SLSF_PHASE(0);
+            /* cred is written again only after two more cluster barriers */
+            if (meas && rank == 0 && threadIdx.x == 0) bin_cluster_sums(t, g, sweep, cred, bin_acc, bin_cur);
             fill_halo(g, s, rm, 0);
-            accepted += half_sweep(t, g, s, sweep, 1);
+            accepted += half_sweep<false>(t, g, s, sweep, 1, acc);
             cluster_barrier(g, cluster);
             SLSF_PHASE(1);
             for (uint32_t k = 0; k < t.wolff_steps; ++k)
                 wolff_update(t, g, s, rm, cluster, t.wolff_done + (uint64_t)sw * t.wolff_steps + k, &s_cluster,
                              s_flags);
-            /* ThetaModel::measure after the sweep, once thermalized. */
-            const uint64_t done = sweep + 1;
-            if (done > t.thermalization && t.n_bins > 0) {
-                double acc[8];
-                fill_halo(g, s, rm, 2);
-                measure_slab(g, s, acc, red);
-                if (threadIdx.x == 0)
-                    for (int k = 0; k < 8; ++k) *cluster.map_shared_rank(&cred[rank][k], 0) = acc[k];
-                cluster_barrier(g, cluster);
-                SLSF_PHASE(5);
-                if (rank == 0 && threadIdx.x == 0) {
-                    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                    for (uint32_t q = 0; q < csize; ++q)
-                        for (int k = 0; k < 8; ++k) a[k] += cred[q][k];
-                    const int64_t b = (int64_t)((done - t.thermalization - 1) / t.binsize);
-                    if (b != bin_cur) {
-                        if (bin_cur >= 0 && bin_cur < (int64_t)t.n_bins)
-                            for (int q = 0; q < kBinCols; ++q) t.bins[bin_cur * kBinCols + q] += bin_acc[q];
-                        for (int q = 0; q < kBinCols; ++q) bin_acc[q] = 0.0;
-                        bin_cur = b;
-                    }
-                    const double v = (double)g.volume;
-                    const double e = -(a[2] + a[3] + a[4]) / v;
-                    const double vals[kBinCols] = {e,    e * e, (a[0] * a[0] + a[1] * a[1]) / (v * v),
-                                                   a[2], a[3],  a[4],
-                                                   a[5], a[6],  a[7],
-                                                   a[5] * a[5], a[6] * a[6], a[7] * a[7]};
-                    for (int q = 0; q < kBinCols; ++q) bin_acc[q] += vals[q];
-                }
-                /* partners must not overwrite cred or theta before rank 0 is done */
-                cluster_barrier(g, cluster);
-            }
         }
-        if (rank == 0 && threadIdx.x == 0 && bin_cur >= 0 && bin_cur < (int64_t)t.n_bins)
-            for (int q = 0; q < kBinCols; ++q) t.bins[bin_cur * kBinCols + q] += bin_acc[q];
+        const uint64_t last = t.metro_sweeps + sweeps;
+        if (measuring && sweeps > 0 && last > t.thermalization) {
+            double acc[8];
+            fill_halo(g, s, rm, 2);
+            measure_slab(g, s, acc, red);
+            if (threadIdx.x == 0)
+                for (int k = 0; k < 8; ++k) *cluster.map_shared_rank(&cred[rank][k], 0) = acc[k];
+            cluster_barrier(g, cluster);
+            SLSF_PHASE(5);
+            if (rank == 0 && threadIdx.x == 0) bin_cluster_sums(t, g, last, cred, bin_acc, bin_cur);
+        }
+        if (rank == 0 && threadIdx.x == 0) flush_bin(t, bin_acc, bin_cur);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) accepted += __shfl_down_sync(0xffffffffu, accepted, off);
         if ((threadIdx.x & 31u) == 0 && accepted) atomicAdd(&t.stats[kStatAccepted], (unsigned long long)accepted);

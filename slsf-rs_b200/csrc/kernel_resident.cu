@@ -29,6 +29,7 @@
  */
 #include <algorithm>
 
+#include "bins.cuh"
 #include "engine.h"
 #include "fastdiv.h"
 #include "xy_device.cuh"
@@ -209,9 +210,20 @@ __device__ __forceinline__ void store_state(const TaskView& t, const Geo& g, con
 
 /* One colour half-sweep.  A warp owns 32 consecutive Philox blocks (64
  * sites); lanes exchange words so that lane j updates colour-compact sites
- * 2*base + j and 2*base + 32 + j, i.e. consecutive shared words. */
+ * 2*base + j and 2*base + 32 + j, i.e. consecutive shared words.
+ *
+ * With kMeasure (colour 0 only) it also measures the state the half-sweep
+ * starts from, at no extra trig: every bond joins a colour-0 site to a
+ * colour-1 site, and before its update a colour-0 site has the trig of
+ * itself and of all six neighbours, so it adds the terms of its three
+ * forward bonds and of the three backward bonds that end on it, and the
+ * magnetisation of itself and of its +x neighbour (each colour-1 site is the
+ * +x neighbour of exactly one colour-0 site).  Each term is the bond_cos /
+ * bond_sin value the measurement pass computes; FP32 sums per thread, FP64
+ * across the block, as in the measurement pass. */
+template <bool kMeasure>
 __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, Smem& s, uint64_t sweep,
-                                               uint32_t colour) {
+                                               uint32_t colour, float (&acc)[8]) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t nwarps = blockDim.x >> 5;
     const uint32_t npairs = (g.half + 1) >> 1;
@@ -243,15 +255,37 @@ __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, 
             st.idx = st.x + g.lx * row;
             uint32_t nb[6];
             neighbour_indices(st, g.lx, g.ly, g.lz, nb);
-            float ns[6], nc[6];
-#pragma unroll
-            for (int q = 0; q < 6; ++q) __sincosf(s.th[other + (nb[q] >> 1)], &ns[q], &nc[q]);
             const float jx = s.jxy[z], jzp = s.jz[z], jzm = s.jz[z == 0 ? g.lz - 1 : z - 1];
-            const float hx = field_component(jx, jzp, jzm, nc[0], nc[1], nc[2], nc[3], nc[4], nc[5]);
-            const float hy = field_component(jx, jzp, jzm, ns[0], ns[1], ns[2], ns[3], ns[4], ns[5]);
             const float th = s.th[own + h];
             float si, ci;
             __sincosf(th, &si, &ci);
+            /* neighbours in pairs, folded into the field as they come */
+            float sa, ca, sb, cb;
+            __sincosf(s.th[other + (nb[0] >> 1)], &sa, &ca);
+            __sincosf(s.th[other + (nb[1] >> 1)], &sb, &cb);
+            if (kMeasure) {
+                /* forward bonds i -> i+mu, backward bonds i-mu -> i */
+                acc[0] += ci + ca;
+                acc[1] += si + sa;
+                acc[2] += bond_cos(jx, ci, si, ca, sa) + bond_cos(jx, cb, sb, ci, si);
+                acc[5] += bond_sin(jx, ci, si, ca, sa) + bond_sin(jx, cb, sb, ci, si);
+            }
+            const float hx01 = __fadd_rn(ca, cb), hy01 = __fadd_rn(sa, sb);
+            __sincosf(s.th[other + (nb[2] >> 1)], &sa, &ca);
+            __sincosf(s.th[other + (nb[3] >> 1)], &sb, &cb);
+            if (kMeasure) {
+                acc[3] += bond_cos(jx, ci, si, ca, sa) + bond_cos(jx, cb, sb, ci, si);
+                acc[6] += bond_sin(jx, ci, si, ca, sa) + bond_sin(jx, cb, sb, ci, si);
+            }
+            const float hx23 = __fadd_rn(ca, cb), hy23 = __fadd_rn(sa, sb);
+            __sincosf(s.th[other + (nb[4] >> 1)], &sa, &ca);
+            __sincosf(s.th[other + (nb[5] >> 1)], &sb, &cb);
+            if (kMeasure) {
+                acc[4] += bond_cos(jzp, ci, si, ca, sa) + bond_cos(jzm, cb, sb, ci, si);
+                acc[7] += bond_sin(jzp, ci, si, ca, sa) + bond_sin(jzm, cb, sb, ci, si);
+            }
+            const float hx = field_from_pairs(jx, jzp, jzm, hx01, hx23, ca, cb);
+            const float hy = field_from_pairs(jx, jzp, jzm, hy01, hy23, sa, sb);
             float tn, sn, cn;
             if (metro_decide(th, ci, si, hx, hy, t.beta, t.width, u_prop, u_acc, &tn, &sn, &cn)) {
                 s.th[own + h] = tn;
@@ -388,8 +422,8 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
 }
 
 /* Fused observables of the resident state (src/observables.rs:99-141): mx,
- * my, cos xyz, sin xyz; FP32 per thread over its sites, FP64 across the
- * block (valid in thread 0). */
+ * my, cos xyz, sin xyz; FP32 sums per thread, FP64 across the block (valid
+ * in thread 0). */
 __device__ __forceinline__ void measure(const Geo& g, const Smem& s, double (&acc)[8], double* red) {
     const uint32_t lane = threadIdx.x & 31u;
     float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -418,17 +452,18 @@ __device__ __forceinline__ void measure(const Geo& g, const Smem& s, double (&ac
         const float jx = s.jxy[c.z], jzz = s.jz[c.z];
         f[0] += ci;
         f[1] += si;
-        f[2] += jx * (ci * cx + si * sx);
-        f[3] += jx * (ci * cy + si * sy);
-        f[4] += jzz * (ci * cz + si * sz);
-        f[5] += jx * (si * cx - ci * sx);
-        f[6] += jx * (si * cy - ci * sy);
-        f[7] += jzz * (si * cz - ci * sz);
+        f[2] += bond_cos(jx, ci, si, cx, sx);
+        f[3] += bond_cos(jx, ci, si, cy, sy);
+        f[4] += bond_cos(jzz, ci, si, cz, sz);
+        f[5] += bond_sin(jx, ci, si, cx, sx);
+        f[6] += bond_sin(jx, ci, si, cy, sy);
+        f[7] += bond_sin(jzz, ci, si, cz, sz);
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) acc[k] = (double)f[k];
     block_sum<8>(acc, red);
 }
+
 
 __global__ void __launch_bounds__(kBThreads, 1)
     k_resident(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
@@ -460,51 +495,39 @@ __global__ void __launch_bounds__(kBThreads, 1)
         const uint32_t sweeps = t.sweeps ? t.sweeps : n_sweeps;
         uint32_t accepted = 0;
         int64_t bin_cur = -1;
+        /* ThetaModel::measure after every sweep past thermalization: the state
+         * after sweep k is measured inside sweep k+1's colour-0 half-sweep,
+         * the launch's last state by the measurement pass below. */
+        const bool measuring = t.n_bins > 0;
         for (uint32_t sw = 0; sw < sweeps; ++sw) {
             const uint64_t sweep = t.metro_sweeps + sw;
-            accepted += half_sweep(t, g, s, sweep, 0);
+            float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            if (measuring && sw > 0 && sweep > t.thermalization) {
+                accepted += half_sweep<true>(t, g, s, sweep, 0, acc);
+                double tot[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) tot[k] = acc[k];
+                block_sum<8>(tot, red);
+                if (threadIdx.x == 0) bin_measurement(t, g.volume, sweep, tot, bin_acc, bin_cur);
+            } else {
+                accepted += half_sweep<false>(t, g, s, sweep, 0, acc);
+            }
             __syncthreads();
             SLSF_PHASE(0);
-            accepted += half_sweep(t, g, s, sweep, 1);
+            accepted += half_sweep<false>(t, g, s, sweep, 1, acc);
             __syncthreads();
             SLSF_PHASE(1);
             for (uint32_t k = 0; k < t.wolff_steps; ++k)
                 wolff_update(t, g, s, t.wolff_done + (uint64_t)sw * t.wolff_steps + k, &s_cluster);
-            /* ThetaModel::measure after the sweep, once thermalized. */
-            const uint64_t done = sweep + 1;
-            if (done > t.thermalization && t.n_bins > 0) {
-                const uint64_t m = done - t.thermalization - 1;
-                const int64_t b = (int64_t)(m / t.binsize);
-                double acc[8];
-                measure(g, s, acc, red);
-                SLSF_PHASE(5);
-                if (threadIdx.x == 0) {
-                    if (b != bin_cur) {
-                        if (bin_cur >= 0 && bin_cur < (int64_t)t.n_bins)
-                            for (int q = 0; q < kBinCols; ++q) t.bins[bin_cur * kBinCols + q] += bin_acc[q];
-                        for (int q = 0; q < kBinCols; ++q) bin_acc[q] = 0.0;
-                        bin_cur = b;
-                    }
-                    const double v = (double)g.volume;
-                    const double e = -(acc[2] + acc[3] + acc[4]) / v;
-                    const double vals[kBinCols] = {e,
-                                                   e * e,
-                                                   (acc[0] * acc[0] + acc[1] * acc[1]) / (v * v),
-                                                   acc[2],
-                                                   acc[3],
-                                                   acc[4],
-                                                   acc[5],
-                                                   acc[6],
-                                                   acc[7],
-                                                   acc[5] * acc[5],
-                                                   acc[6] * acc[6],
-                                                   acc[7] * acc[7]};
-                    for (int q = 0; q < kBinCols; ++q) bin_acc[q] += vals[q];
-                }
-            }
         }
-        if (threadIdx.x == 0 && bin_cur >= 0 && bin_cur < (int64_t)t.n_bins)
-            for (int q = 0; q < kBinCols; ++q) t.bins[bin_cur * kBinCols + q] += bin_acc[q];
+        const uint64_t last = t.metro_sweeps + sweeps;
+        if (measuring && sweeps > 0 && last > t.thermalization) {
+            double acc[8];
+            measure(g, s, acc, red);
+            SLSF_PHASE(5);
+            if (threadIdx.x == 0) bin_measurement(t, g.volume, last, acc, bin_acc, bin_cur);
+        }
+        if (threadIdx.x == 0) flush_bin(t, bin_acc, bin_cur);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) accepted += __shfl_down_sync(0xffffffffu, accepted, off);
         if ((threadIdx.x & 31u) == 0 && accepted) atomicAdd(&s_accepted, accepted);

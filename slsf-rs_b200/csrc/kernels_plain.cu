@@ -215,12 +215,12 @@ __global__ void __launch_bounds__(kMeasureThreads)
         /* diff_cos_sin (src/observables.rs:9-11): cos(a-b), sin(a-b) from trig. */
         acc[0] += ci;
         acc[1] += si;
-        acc[2] += jx * (ci * cx + si * sx);
-        acc[3] += jx * (ci * cy + si * sy);
-        acc[4] += jzz * (ci * cz + si * sz);
-        acc[5] += jx * (si * cx - ci * sx);
-        acc[6] += jx * (si * cy - ci * sy);
-        acc[7] += jzz * (si * cz - ci * sz);
+        acc[2] += bond_cos(jx, ci, si, cx, sx);
+        acc[3] += bond_cos(jx, ci, si, cy, sy);
+        acc[4] += bond_cos(jzz, ci, si, cz, sz);
+        acc[5] += bond_sin(jx, ci, si, cx, sx);
+        acc[6] += bond_sin(jx, ci, si, cy, sy);
+        acc[7] += bond_sin(jzz, ci, si, cz, sz);
     }
     block_sum<8>(acc, scratch);
     if (threadIdx.x == 0) {

@@ -52,12 +52,18 @@ __device__ __forceinline__ void neighbour_indices(const SiteXYZ& s, uint32_t lx,
 }
 
 /* One component of the local field (src/updates.rs:215-228):
- * J_xy (a0 + a1 + a2 + a3) + J_z+ a4 + J_z- a5, with a fixed rounding order. */
+ * J_xy (a0 + a1 + a2 + a3) + J_z+ a4 + J_z- a5, with a fixed rounding order;
+ * field_from_pairs takes the in-plane pairs a0 + a1 and a2 + a3 already
+ * rounded, so a kernel can fold neighbours in as it loads them. */
+__device__ __forceinline__ float field_from_pairs(float jxy, float jzp, float jzm, float a01, float a23,
+                                                  float a4, float a5) {
+    return __fmaf_rn(jzm, a5, __fmaf_rn(jzp, a4, __fmul_rn(jxy, __fadd_rn(a01, a23))));
+}
+
 __device__ __forceinline__ float field_component(float jxy, float jzp, float jzm, float a0,
                                                  float a1, float a2, float a3, float a4,
                                                  float a5) {
-    const float inplane = __fadd_rn(__fadd_rn(a0, a1), __fadd_rn(a2, a3));
-    return __fmaf_rn(jzm, a5, __fmaf_rn(jzp, a4, __fmul_rn(jxy, inplane)));
+    return field_from_pairs(jxy, jzp, jzm, __fadd_rn(a0, a1), __fadd_rn(a2, a3), a4, a5);
 }
 
 /* The Metropolis decision of local_metropolis_step_at_unchecked
@@ -93,6 +99,20 @@ __device__ __forceinline__ bool wolff_bond_active(float coupling, float ri, floa
     if (!(prod > 0.0f)) return false;
     const float p = __fsub_rn(1.0f, __expf(__fmul_rn(minus_two_beta, prod)));
     return slsf_u24f(word) < p;
+}
+
+/* Terms of one bond a -> b = a + mu of the observables
+ * (src/observables.rs:108-137): J cos(theta_a - theta_b) and
+ * J sin(theta_a - theta_b) from the two sites' trig, with a fixed rounding
+ * order so that every kernel that measures (the single-task kernel, the
+ * batched kernels' measurement pass and the measurement fused into their
+ * Metropolis half-sweep) computes each bond's terms bit-identically. */
+__device__ __forceinline__ float bond_cos(float j, float ca, float sa, float cb, float sb) {
+    return __fmul_rn(j, __fmaf_rn(ca, cb, __fmul_rn(sa, sb)));
+}
+
+__device__ __forceinline__ float bond_sin(float j, float ca, float sa, float cb, float sb) {
+    return __fmul_rn(j, __fmaf_rn(sa, cb, -__fmul_rn(ca, sb)));
 }
 
 template <int N>
