@@ -23,12 +23,15 @@
  * Cluster barriers separate the phases.  HBM traffic is one read and one
  * write of theta per launch, independent of the sweep count.
  *
- * Wolff labelling is bit-parallel: the cluster grows from the seed by OR-ing
- * neighbour rows through the bond words and closing every row that gained
- * bits along x, until a pass changes nothing in the whole cluster.  The
- * result is the seed's connected component over the active bonds -- the set
- * the reference's DFS (src/updates.rs:577-597) collects when fed the same
- * per-bond randoms.  Growth is monotone, so the pass count is bounded by V.
+ * Wolff labelling is bit-parallel: the cluster grows from the seed in
+ * rounds; a round closes every column along z (sequentially per column,
+ * across the slab faces through the partners' rows), then every row along y
+ * (a segmented scan over the lanes of a warp) and along x (a doubling scan
+ * inside the row word), until a round changes nothing in the whole cluster.
+ * The result is the seed's connected component over the active bonds -- the
+ * set the reference's DFS (src/updates.rs:577-597) collects when fed the
+ * same per-bond randoms.  Growth is monotone, so the round count is bounded
+ * by V.
  */
 #include <cooperative_groups.h>
 
@@ -199,6 +202,9 @@ struct Smem {
     W* cl;
     float* jxy;
     float* jz;
+    uint8_t* dirty; /* per row: changed by growth stage Z, not yet x-closed */
+    W* zc;          /* stage Z: carry out of each column segment */
+    W* zp;          /* stage Z: product of each column segment's links */
 };
 
 struct Limits {
@@ -214,13 +220,16 @@ __device__ __forceinline__ Smem<W> carve(unsigned char* base, const Limits& m) {
     s.by = w + m.rows;
     s.bz = w + 2 * m.rows;
     s.cl = w + 3 * m.rows;
-    p += 4ull * m.rows * sizeof(W);
+    s.zc = w + 4 * m.rows;
+    s.zp = w + 5 * m.rows;
+    p += 6ull * m.rows * sizeof(W);
     s.th = reinterpret_cast<float*>(p);
     p += 4ull * (m.vs + 2 * kPad);
     s.halo = reinterpret_cast<float*>(p);
     p += 16ull * m.hp;
     s.jxy = reinterpret_cast<float*>(p);
     s.jz = s.jxy + m.lz;
+    s.dirty = reinterpret_cast<uint8_t*>(s.jz + m.lz);
     return s;
 }
 
@@ -422,8 +431,12 @@ __device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Sme
         if (g.lx_tiles_warp) {
             rxp = __shfl_sync(0xffffffffu, ri, seg_next(lane, g.lx));
         } else {
-            const uint32_t xp = (c.x + 1 == g.lx) ? ll + 1 - g.lx : ll + 1;
-            rxp = proj_of(s.th[oth + (xp >> 1)], cphi, sphi);
+            /* the +x neighbour is the next lane unless the row or the warp ends */
+            rxp = __shfl_down_sync(0xffffffffu, ri, 1);
+            if (lane == 31 || c.x + 1 == g.lx) {
+                const uint32_t xp = (c.x + 1 == g.lx) ? ll + 1 - g.lx : ll + 1;
+                rxp = proj_of(s.th[oth + (xp >> 1)], cphi, sphi);
+            }
         }
         const uint32_t yp = (c.y + 1 == g.ly) ? ll + g.lx - g.plane : ll + g.lx;
         const float ryp = proj_of(s.th[oth + (yp >> 1)], cphi, sphi);
@@ -456,11 +469,23 @@ __device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Sme
                 hy32[2 * c.row + half] = bal_y;
                 hz32[2 * c.row + half] = bal_z;
             }
-        } else if (valid) {
-            const W bit = (W)1 << c.x;
-            if (ax) atomic_or_row(&s.bx[c.row], bit);
-            if (ay) atomic_or_row(&s.by[c.row], bit);
-            if (az) atomic_or_row(&s.bz[c.row], bit);
+        } else {
+            /* The warp's 32 consecutive sites cover pieces of a few rows; the
+             * first lane of each piece ORs the piece's ballot bits into its
+             * row (rows shared with another warp need the atomic). */
+            const uint32_t bal_x = __ballot_sync(0xffffffffu, ax);
+            const uint32_t bal_y = __ballot_sync(0xffffffffu, ay);
+            const uint32_t bal_z = __ballot_sync(0xffffffffu, az);
+            if (valid && (lane == 0 || c.x == 0)) {
+                const uint32_t len = min(g.lx - c.x, 32u - lane);
+                const uint32_t m = len >= 32 ? 0xffffffffu : ((1u << len) - 1u);
+                const W px = (W)((bal_x >> lane) & m) << c.x;
+                const W py = (W)((bal_y >> lane) & m) << c.x;
+                const W pz = (W)((bal_z >> lane) & m) << c.x;
+                if (px) atomic_or_row(&s.bx[c.row], px);
+                if (py) atomic_or_row(&s.by[c.row], py);
+                if (pz) atomic_or_row(&s.bz[c.row], pz);
+            }
         }
     }
     /* seed the cluster */
@@ -468,7 +493,10 @@ __device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Sme
     const uint32_t sz = srow / g.ly, sy = srow - sz * g.ly;
     const bool mine = sz >= g.z0 && sz < g.z0 + g.nz;
     const uint32_t seed_row = sy + g.ly * (sz - g.z0);
-    for (uint32_t r = threadIdx.x; r < g.rows_s; r += blockDim.x) s.cl[r] = (mine && r == seed_row) ? ((W)1 << sx) : (W)0;
+    for (uint32_t r = threadIdx.x; r < g.rows_s; r += blockDim.x) {
+        s.cl[r] = (mine && r == seed_row) ? ((W)1 << sx) : (W)0;
+        s.dirty[r] = 0;
+    }
     __syncthreads();
     if (mine && threadIdx.x == 0) {
         const W mask = g.lx >= 8 * sizeof(W) ? ~(W)0 : (((W)1 << g.lx) - 1);
@@ -476,29 +504,157 @@ __device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Sme
     }
 }
 
-/* One growth pass: every row takes the cluster bits that reach it through
- * its y and z bonds; a row that gained bits is closed along x (stored rows
- * are always closed).  Returns nonzero if any row of this CTA changed. */
+constexpr uint32_t kZSeg = 4; /* planes per column segment in growth stage Z */
+
+/* Growth stage Z: every column of the slab (the rows of one y) carries its
+ * cluster bits along z through its bz words, forward and backward, fed
+ * across the slab faces by the partner rows (for a one-CTA cluster the
+ * partner is this CTA: the periodic wrap).  A column is cut into segments of
+ * kZSeg planes, one thread each (lanes over consecutive columns, so shared
+ * accesses are conflict-free): each segment runs its chain with no carry in,
+ * publishes its carry out and the product of its links, then runs again
+ * from the carry that the segments before it deliver, stopping where the
+ * carry adds nothing.  Changed rows are stored unclosed along x and marked
+ * dirty.  Returns nonzero if any row changed. */
 template <typename W>
-__device__ __forceinline__ int grow_pass(const Geo& g, Smem<W>& s, const Remote<W>& rm, W mask) {
+__device__ __forceinline__ int grow_z(const Geo& g, Smem<W>& s, const Remote<W>& rm) {
+    const uint32_t nseg = (g.nz + kZSeg - 1) / kZSeg;
+    const uint32_t n = nseg * g.ly;
+    const uint32_t top = g.ly * (g.nz - 1);
     int changed = 0;
-    for (uint32_t r = threadIdx.x; r < g.rows_s; r += blockDim.x) {
-        const uint32_t zl = slsf_fastdiv_div(r, g.div_ly);
-        const uint32_t y = r - zl * g.ly;
-        const W old = s.cl[r];
-        const uint32_t r_yp = (y + 1 == g.ly) ? r + 1 - g.ly : r + 1;
-        const uint32_t r_ym = (y == 0) ? r + g.ly - 1 : r - 1;
-        W in = (s.cl[r_ym] & s.by[r_ym]) | (s.cl[r_yp] & s.by[r]);
-        if (zl > 0) {
-            in |= s.cl[r - g.ly] & s.bz[r - g.ly];
-        } else {
-            const uint32_t rr = y + g.ly * (g.nz - 1);
-            in |= rm.cl_dn[rr] & rm.bz_dn[rr];
+    /* forward: plane zl feeds plane zl + 1 through bz[zl] */
+    for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
+        const uint32_t j = slsf_fastdiv_div(t, g.div_ly), y = t - j * g.ly;
+        const uint32_t z0 = j * kZSeg, z1 = min(z0 + kZSeg, g.nz);
+        W acc = j == 0 ? (rm.cl_dn[top + y] & rm.bz_dn[top + y]) : (W)0, prod = ~(W)0;
+        for (uint32_t zl = z0; zl < z1; ++zl) {
+            const uint32_t r = y + g.ly * zl;
+            const W c = s.cl[r], b = s.bz[r];
+            const W v = c | acc;
+            if (v != c) {
+                s.cl[r] = v;
+                s.dirty[r] = 1;
+                changed = 1;
+            }
+            acc = v & b;
+            prod &= b;
         }
-        in |= ((zl + 1 < g.nz) ? s.cl[r + g.ly] : rm.cl_up[y]) & s.bz[r];
-        const W c = old | in;
-        if (c != old) {
-            s.cl[r] = close_row<W>(c, s.bx[r], g.lx, mask);
+        s.zc[t] = acc;
+        s.zp[t] = prod;
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
+        const uint32_t j = slsf_fastdiv_div(t, g.div_ly), y = t - j * g.ly;
+        if (j == 0) continue;
+        W acc = s.zc[y];
+        for (uint32_t q = 1; q < j; ++q) acc = (acc & s.zp[q * g.ly + y]) | s.zc[q * g.ly + y];
+        const uint32_t z1 = min(j * kZSeg + kZSeg, g.nz);
+        for (uint32_t zl = j * kZSeg; zl < z1 && acc; ++zl) {
+            const uint32_t r = y + g.ly * zl;
+            const W c = s.cl[r];
+            const W v = c | acc;
+            if (v == c) break; /* from here on the first run's chain stands */
+            s.cl[r] = v;
+            s.dirty[r] = 1;
+            changed = 1;
+            acc = v & s.bz[r];
+        }
+    }
+    __syncthreads();
+    /* backward: plane zl feeds plane zl - 1 through bz[zl - 1] */
+    for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
+        const uint32_t j = slsf_fastdiv_div(t, g.div_ly), y = t - j * g.ly;
+        const uint32_t z0 = j * kZSeg, z1 = min(z0 + kZSeg, g.nz);
+        W acc = j == nseg - 1 ? (rm.cl_up[y] & s.bz[top + y]) : (W)0, prod = ~(W)0;
+        for (uint32_t zl = z1; zl-- > z0;) {
+            const uint32_t r = y + g.ly * zl;
+            const W c = s.cl[r], b = zl > 0 ? s.bz[r - g.ly] : (W)0;
+            const W v = c | acc;
+            if (v != c) {
+                s.cl[r] = v;
+                s.dirty[r] = 1;
+                changed = 1;
+            }
+            acc = v & b;
+            prod &= b;
+        }
+        s.zc[t] = acc;
+        s.zp[t] = prod;
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
+        const uint32_t j = slsf_fastdiv_div(t, g.div_ly), y = t - j * g.ly;
+        if (j == nseg - 1) continue;
+        W acc = s.zc[(nseg - 1) * g.ly + y];
+        for (uint32_t q = nseg - 2; q > j; --q) acc = (acc & s.zp[q * g.ly + y]) | s.zc[q * g.ly + y];
+        const uint32_t z0 = j * kZSeg, z1 = min(z0 + kZSeg, g.nz);
+        for (uint32_t zl = z1; zl-- > z0 && acc;) {
+            const uint32_t r = y + g.ly * zl;
+            const W c = s.cl[r];
+            const W v = c | acc;
+            if (v == c) break;
+            s.cl[r] = v;
+            s.dirty[r] = 1;
+            changed = 1;
+            acc = zl > 0 ? (v & s.bz[r - g.ly]) : (W)0;
+        }
+    }
+    return changed;
+}
+
+/* Growth stage XY: one thread per row, warps over consecutive rows.  A row
+ * takes the bits of its y neighbours through their by words, then each warp
+ * closes its rows along x (a doubling scan in the row word) and along y (a
+ * segmented Kogge-Stone scan, forward and backward over the lanes that hold
+ * consecutive y of one plane), and along x again where the y scan added
+ * bits.  A warp whose rows are all x-closed (none dirty from stage Z) and
+ * gain nothing from their neighbours is skipped: its rows are closed along
+ * x and along the y bonds inside the warp.  Returns nonzero if any row
+ * changed. */
+template <typename W>
+__device__ __forceinline__ int grow_xy(const Geo& g, Smem<W>& s, W mask) {
+    const uint32_t lane = threadIdx.x & 31u;
+    int changed = 0;
+    for (uint32_t r0 = threadIdx.x & ~31u; r0 < g.rows_s; r0 += blockDim.x) {
+        const uint32_t r = r0 + lane;
+        const bool valid = r < g.rows_s;
+        const uint32_t rr = valid ? r : 0;
+        const uint32_t zl = slsf_fastdiv_div(rr, g.div_ly);
+        const uint32_t y = rr - zl * g.ly;
+        const uint32_t r_yp = (y + 1 == g.ly) ? rr + 1 - g.ly : rr + 1;
+        const uint32_t r_ym = (y == 0) ? rr + g.ly - 1 : rr - 1;
+        const W old = s.cl[rr], by_r = s.by[rr];
+        W c = old | (s.cl[r_ym] & s.by[r_ym]) | (s.cl[r_yp] & by_r);
+        const bool is_dirty = valid && s.dirty[rr];
+        if (__all_sync(0xffffffffu, !is_dirty && (!valid || c == old))) continue;
+        if (is_dirty) s.dirty[rr] = 0;
+        if (is_dirty || c != old) c = close_row<W>(c, s.bx[rr], g.lx, mask);
+        /* forward: lane - 1 holds row rr - 1 of the same plane when y > 0 */
+        W gsum = c;
+        W link = (lane > 0 && y > 0) ? s.by[rr - 1] : (W)0;
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const W up = __shfl_up_sync(0xffffffffu, gsum, d);
+            const W lk = __shfl_up_sync(0xffffffffu, link, d);
+            if (lane >= d) {
+                gsum |= up & link;
+                link &= lk;
+            }
+        }
+        /* backward: lane + 1 holds row rr + 1 of the same plane */
+        link = (lane < 31 && y + 1 < g.ly && rr + 1 < g.rows_s) ? by_r : (W)0;
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const W dn = __shfl_down_sync(0xffffffffu, gsum, d);
+            const W lk = __shfl_down_sync(0xffffffffu, link, d);
+            if (lane + d < 32) {
+                gsum |= dn & link;
+                link &= lk;
+            }
+        }
+        if (gsum != c) gsum = close_row<W>(gsum, s.bx[rr], g.lx, mask);
+        if (valid && gsum != old) {
+            s.cl[rr] = gsum;
             changed = 1;
         }
     }
@@ -521,14 +677,19 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
     cluster_barrier(g, cluster);
     SLSF_PHASE(2);
 
+    /* Rounds of stage Z then stage XY until a round changes nothing in the
+     * whole cluster; every round that goes on adds at least one site. */
     uint32_t pass = 0;
     for (; pass <= g.volume; ++pass) {
-        int any = __syncthreads_or(grow_pass(g, s, rm, mask));
+        int any = grow_z(g, s, rm);
+        __syncthreads();
+        any = __syncthreads_or(grow_xy(g, s, mask) | any);
         if (g.csize > 1) {
+            /* lane q of warp 0 reads rank q's flag; one block barrier spreads the OR */
             if (threadIdx.x == 0) flags[pass & 1] = any;
             cluster.sync();
-            any = 0;
-            for (uint32_t q = 0; q < g.csize; ++q) any |= *cluster.map_shared_rank(&flags[pass & 1], q);
+            const int mine = threadIdx.x < g.csize ? *cluster.map_shared_rank(&flags[pass & 1], threadIdx.x) : 0;
+            any = __syncthreads_or(mine);
         }
         if (!any) break;
     }
@@ -711,7 +872,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
 }
 
 size_t smem_bytes(const Limits& m, size_t word) {
-    return 4ull * m.rows * word + 4ull * (m.vs + 2 * kPad) + 16ull * m.hp + 8ull * m.lz;
+    return 6ull * m.rows * word + 4ull * (m.vs + 2 * kPad) + 16ull * m.hp + 8ull * m.lz + m.rows;
 }
 
 int max_dynamic_smem(int device) {

@@ -11,21 +11,24 @@
  *      one colour reads consecutive words, and the 64-byte pad puts the two
  *      colours of neighbouring sites in different bank halves;
  *   2. per sweep: two colour half-sweeps (the same decision code as the
- *      single-task kernel, xy_device.cuh), `wolff_steps` Wolff updates, and,
- *      after thermalization, the fused measurement added to the task's bins;
+ *      single-task kernel, xy_device.cuh) and `wolff_steps` Wolff updates;
+ *      after thermalization each sweep's state is measured inside the next
+ *      sweep's colour-0 half-sweep (the launch's last state by a separate
+ *      pass) and added to the task's bins;
  *   3. copies theta back.
  * HBM traffic is 8 bytes per site per launch, independent of the sweep
  * count.  Trig values are recomputed with __sincosf where needed (a 32^3
- * replica leaves no room for a cos/sin cache next to theta; the cluster
- * kernel, kernel_cluster.cu, holds larger replicas with one).
+ * replica leaves no room for a cos/sin cache next to theta).
  *
  * Wolff labelling is bit-parallel: the active +x/+y/+z bonds of a row of
  * L_x <= 32 sites are three 32-bit words; the cluster grows from the seed by
  * OR-ing neighbour rows through the bond words and closing every row that
- * gained bits along x, until a pass changes nothing.  The result is the
- * seed's connected component over the active bonds -- the set the
- * reference's DFS (src/updates.rs:577-597) collects when fed the same
- * per-bond randoms.  Growth is monotone, so the pass count is bounded by V.
+ * gained bits along x, until a pass changes nothing.  (In one CTA a pass is
+ * a single block barrier, which for replicas of this size beats the
+ * column-scan rounds of kernel_cluster.cu.)  The result is the seed's
+ * connected component over the active bonds -- the set the reference's DFS
+ * (src/updates.rs:577-597) collects when fed the same per-bond randoms.
+ * Growth is monotone, so the pass count is bounded by V.
  */
 #include <algorithm>
 
@@ -308,7 +311,9 @@ __device__ __forceinline__ float proj_of(float theta, float cphi, float sphi) {
 
 /* One growth pass: every row takes the cluster bits that reach it through
  * its y and z bonds; a row that gained bits is closed along x (stored rows
- * are always closed).  Returns nonzero if any row changed. */
+ * are always closed).  Returns nonzero if any row changed.  Rows updated
+ * earlier in the same pass are seen by later ones, so bits can travel more
+ * than one row per pass. */
 __device__ __forceinline__ int grow_pass(const Geo& g, Smem& s) {
     int changed = 0;
     for (uint32_t r = threadIdx.x; r < g.rows; r += blockDim.x) {
@@ -362,8 +367,12 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
         if (g.lx_tiles_warp) {
             rxp = __shfl_sync(0xffffffffu, ri, xp_lane(lane, g.lx));
         } else {
-            const Coords cx = {c.x + 1 == g.lx ? 0 : c.x + 1, c.y, c.z, c.row};
-            rxp = proj_of(site_theta(g, s, xp, cx), cphi, sphi);
+            /* the +x neighbour is the next lane unless the row or the warp ends */
+            rxp = __shfl_down_sync(0xffffffffu, ri, 1);
+            if (lane == 31 || c.x + 1 == g.lx) {
+                const Coords cx = {c.x + 1 == g.lx ? 0 : c.x + 1, c.y, c.z, c.row};
+                rxp = proj_of(site_theta(g, s, xp, cx), cphi, sphi);
+            }
         }
         const Coords cy = {c.x, c.y + 1 == g.ly ? 0 : c.y + 1, c.z, 0};
         const Coords cz = {c.x, c.y, c.z + 1 == g.lz ? 0 : c.z + 1, 0};
@@ -383,10 +392,23 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
                 s.by[c.row] = (bal_y >> lane) & g.xmask;
                 s.bz[c.row] = (bal_z >> lane) & g.xmask;
             }
-        } else if (valid) {
-            if (ax) atomicOr(&s.bx[c.row], 1u << c.x);
-            if (ay) atomicOr(&s.by[c.row], 1u << c.x);
-            if (az) atomicOr(&s.bz[c.row], 1u << c.x);
+        } else {
+            /* The warp's 32 consecutive sites cover pieces of a few rows; the
+             * first lane of each piece ORs the piece's ballot bits into its
+             * row (rows shared with another warp need the atomic). */
+            const uint32_t bal_x = __ballot_sync(0xffffffffu, ax);
+            const uint32_t bal_y = __ballot_sync(0xffffffffu, ay);
+            const uint32_t bal_z = __ballot_sync(0xffffffffu, az);
+            if (valid && (lane == 0 || c.x == 0)) {
+                const uint32_t len = min(g.lx - c.x, 32u - lane);
+                const uint32_t m = len >= 32 ? 0xffffffffu : ((1u << len) - 1u);
+                const uint32_t px = ((bal_x >> lane) & m) << c.x;
+                const uint32_t py = ((bal_y >> lane) & m) << c.x;
+                const uint32_t pz = ((bal_z >> lane) & m) << c.x;
+                if (px) atomicOr(&s.bx[c.row], px);
+                if (py) atomicOr(&s.by[c.row], py);
+                if (pz) atomicOr(&s.bz[c.row], pz);
+            }
         }
     }
     const uint32_t seed_row = y0 + g.ly * z0;
@@ -396,7 +418,8 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
     __syncthreads();
     SLSF_PHASE(2);
 
-    /* Grow the seed's component; bounded by V passes (monotone growth). */
+    /* Grow the seed's component; every pass that goes on adds at least one
+     * site, so the count is bounded by V. */
     uint32_t pass = 0;
     for (; pass <= g.volume; ++pass)
         if (!__syncthreads_or(grow_pass(g, s))) break;
