@@ -646,8 +646,8 @@ int slsf_task_correlations(slsf_task* t, uint32_t rmax_xy, uint32_t rmax_z, doub
     rmax_xy = std::min(std::min(rmax_xy, t->lx / 2), t->ly / 2);
     rmax_z = std::min(rmax_z, t->lz / 2);
     if (rmax_xy == 0 && rmax_z == 0) return SLSF_OK;
-    if ((size_t)2 * std::max(t->ly, t->lz) * 32 * sizeof(float) > 200 * 1024)
-        return set_error(SLSF_ERR_INVALID, "correlation lines longer than 800 sites are not supported");
+    if (slsf::corr_tile_bytes(std::max(t->ly + rmax_xy, t->lz + rmax_z)) > 200 * 1024)
+        return set_error(SLSF_ERR_INVALID, "correlation lines plus lags longer than 800 sites are not supported");
     if (int rc = bind_device(t->ctx)) return rc;
     const size_t work_n = slsf::correlation_work_doubles(t->lx, t->ly, t->lz, rmax_xy, rmax_z);
     const size_t nsx = (size_t)t->lz * rmax_xy, nsz = rmax_z;

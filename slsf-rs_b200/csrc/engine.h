@@ -63,6 +63,8 @@ void launch_measure(const TaskView& t, double* partials, unsigned int* done, dou
 void launch_measure_into_bin(const TaskView& t, double* partials, unsigned int* done, double* result,
                              double* bin_row, cudaStream_t s);
 int measure_partial_blocks(uint32_t volume);
+/* Shared bytes of the correlation kernel's tile for lines of n sites at lags up to rmax: corr_tile_bytes(n + rmax). */
+size_t corr_tile_bytes(uint32_t entries);
 /* Correlation sums: sx[lz][rmax_xy], sy[lz][rmax_xy], sz[rmax_z] (FP64). */
 void launch_correlations(const TaskView& t, uint32_t rmax_xy, uint32_t rmax_z, double* work,
                          size_t work_doubles, double* sx, double* sy, double* sz,

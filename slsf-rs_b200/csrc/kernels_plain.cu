@@ -5,10 +5,13 @@
  *   k_metro_colour       one colour of metropolis_sweep_with_scratch
  *                        (src/updates.rs:440-486), one thread per Philox block
  *                        (two same-colour sites)
- *   k_wolff_bonds        per-site +x/+y/+z bond activation of
- *   k_wolff_union        wolff_cluster_step_with_theta_scratch
- *   k_wolff_flip         (src/updates.rs:551-620): lock-free union-find over
- *                        the active bonds, then reflect the seed's component
+ *   k_wolff_tiles        per-site +x/+y/+z bond activation of
+ *   k_wolff_boundary     wolff_cluster_step_with_theta_scratch
+ *   k_wolff_flip         (src/updates.rs:551-620): components inside
+ *                        32x8x4 tiles by union-find in shared memory, the
+ *                        bonds between tiles by a lock-free global
+ *                        union-find over the tile roots, then reflect the
+ *                        seed's component
  *   k_measure            measure_theta_observables_with_scratch
  *                        (src/observables.rs:80-154), FP64 block sums, fixed
  *                        summation order (last block reduces the partials)
@@ -123,50 +126,128 @@ __device__ __forceinline__ bool uf_union(uint32_t* parent, uint32_t a, uint32_t 
     return false;
 }
 
+/* Wolff tiles: a CTA labels one tile of kTileX x kTileY x kTileZ sites. */
+constexpr uint32_t kTileX = 32, kTileY = 8, kTileZ = 4;
+constexpr uint32_t kTileSites = kTileX * kTileY * kTileZ;
+
+/* Local union-find in shared memory: hook the larger root under the smaller
+ * with a CAS; bounded like the global one. */
+__device__ __forceinline__ uint32_t tile_find(uint32_t* lpar, uint32_t x, bool* ok) {
+    volatile uint32_t* par = lpar;
+    for (uint32_t it = 0; it <= kTileSites; ++it) {
+        const uint32_t p = par[x];
+        if (p == x) return x;
+        const uint32_t gp = par[p];
+        if (gp != p) par[x] = gp;
+        x = p;
+    }
+    *ok = false;
+    return x;
+}
+
+__device__ __forceinline__ bool tile_union(uint32_t* lpar, uint32_t a, uint32_t b) {
+    bool ok = true;
+    for (uint32_t it = 0; it < 4 * kTileSites; ++it) {
+        a = tile_find(lpar, a, &ok);
+        b = tile_find(lpar, b, &ok);
+        if (!ok) return false;
+        if (a == b) return true;
+        if (a > b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(&lpar[b], b, a) == b) return true;
+    }
+    return false;
+}
+
+/* Bond activation (try_add_wolff_neighbor, src/updates.rs:537-548) for every
+ * site of a tile, then the tile's components over its inner bonds: each site
+ * gets parent = the smallest site of its component inside the tile (local
+ * order is global order inside a tile, so parent[i] <= i holds).  Bonds that
+ * leave the tile are joined by k_wolff_boundary. */
 __global__ void __launch_bounds__(kThreads)
-    k_wolff_bonds(const float* __restrict__ theta, const float* __restrict__ jxy,
+    k_wolff_tiles(const float* __restrict__ theta, const float* __restrict__ jxy,
                   const float* __restrict__ jz, uint32_t lx, uint32_t ly, uint32_t lz,
                   float minus_two_beta, float phi, uint64_t seed, uint64_t counter,
-                  uint8_t* __restrict__ bonds, uint32_t* __restrict__ parent) {
-    const uint32_t volume = lx * ly * lz;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= volume) return;
-    const uint32_t x = i % lx, row = i / lx, y = row % ly, z = row / ly;
-    const uint32_t plane = lx * ly;
-    const uint32_t xp = (x + 1 == lx) ? i + 1 - lx : i + 1;
-    const uint32_t yp = (y + 1 == ly) ? i + lx - plane : i + lx;
-    const uint32_t zp = (z + 1 == lz) ? i + plane - volume : i + plane;
+                  uint8_t* __restrict__ bonds, uint32_t* __restrict__ parent,
+                  unsigned long long* __restrict__ stats) {
+    __shared__ uint32_t lpar[kTileSites];
+    __shared__ uint8_t lbits[kTileSites];
+    const uint32_t ntx = (lx + kTileX - 1) / kTileX, nty = (ly + kTileY - 1) / kTileY;
+    const uint32_t tx = blockIdx.x % ntx, rest = blockIdx.x / ntx;
+    const uint32_t ty = rest % nty, tz = rest / nty;
+    const uint32_t x0 = tx * kTileX, y0 = ty * kTileY, z0 = tz * kTileZ;
+    const uint32_t ex = min(kTileX, lx - x0), ey = min(kTileY, ly - y0), ez = min(kTileZ, lz - z0);
+    const uint32_t plane = lx * ly, volume = plane * lz;
     float sphi, cphi;
     __sincosf(phi, &sphi, &cphi);
     auto proj = [&](uint32_t site) {
-        float s, c;
-        __sincosf(theta[site], &s, &c);
-        return wolff_projection(c, s, cphi, sphi);
+        float sn, cn;
+        __sincosf(theta[site], &sn, &cn);
+        return wolff_projection(cn, sn, cphi, sphi);
     };
-    const float ri = proj(i);
-    const slsf_u32x4 b = slsf_stream(seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, i);
-    uint32_t bits = 0;
-    if (wolff_bond_active(jxy[z], ri, proj(xp), minus_two_beta, b.x)) bits |= 1u;
-    if (wolff_bond_active(jxy[z], ri, proj(yp), minus_two_beta, b.y)) bits |= 2u;
-    if (wolff_bond_active(jz[z], ri, proj(zp), minus_two_beta, b.z)) bits |= 4u;
-    bonds[i] = (uint8_t)bits;
-    parent[i] = i;
+    for (uint32_t l = threadIdx.x; l < kTileSites; l += blockDim.x) {
+        const uint32_t ax = l % kTileX, ay = (l / kTileX) % kTileY, az = l / (kTileX * kTileY);
+        uint32_t bits = 0;
+        if (ax < ex && ay < ey && az < ez) {
+            const uint32_t x = x0 + ax, y = y0 + ay, z = z0 + az;
+            const uint32_t i = x + lx * (y + ly * z);
+            const uint32_t xp = (x + 1 == lx) ? i + 1 - lx : i + 1;
+            const uint32_t yp = (y + 1 == ly) ? i + lx - plane : i + lx;
+            const uint32_t zp = (z + 1 == lz) ? i + plane - volume : i + plane;
+            const float ri = proj(i);
+            const slsf_u32x4 b = slsf_stream(seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, i);
+            if (wolff_bond_active(jxy[z], ri, proj(xp), minus_two_beta, b.x)) bits |= 1u;
+            if (wolff_bond_active(jxy[z], ri, proj(yp), minus_two_beta, b.y)) bits |= 2u;
+            if (wolff_bond_active(jz[z], ri, proj(zp), minus_two_beta, b.z)) bits |= 4u;
+            bonds[i] = (uint8_t)bits;
+        }
+        lbits[l] = (uint8_t)bits;
+        lpar[l] = l;
+    }
+    __syncthreads();
+    bool ok = true;
+    for (uint32_t l = threadIdx.x; l < kTileSites; l += blockDim.x) {
+        const uint32_t bits = lbits[l];
+        if (!bits) continue;
+        const uint32_t ax = l % kTileX, ay = (l / kTileX) % kTileY, az = l / (kTileX * kTileY);
+        if ((bits & 1u) && ax + 1 < ex) ok &= tile_union(lpar, l, l + 1);
+        if ((bits & 2u) && ay + 1 < ey) ok &= tile_union(lpar, l, l + kTileX);
+        if ((bits & 4u) && az + 1 < ez) ok &= tile_union(lpar, l, l + kTileX * kTileY);
+    }
+    __syncthreads();
+    for (uint32_t l = threadIdx.x; l < kTileSites; l += blockDim.x) {
+        const uint32_t ax = l % kTileX, ay = (l / kTileX) % kTileY, az = l / (kTileX * kTileY);
+        if (ax >= ex || ay >= ey || az >= ez) continue;
+        const uint32_t r = tile_find(lpar, l, &ok);
+        const uint32_t rx = r % kTileX, ry = (r / kTileX) % kTileY, rz = r / (kTileX * kTileY);
+        parent[(x0 + ax) + lx * ((y0 + ay) + ly * (z0 + az))] = (x0 + rx) + lx * ((y0 + ry) + ly * (z0 + rz));
+    }
+    if (!ok) atomicOr(&stats[kStatError], kErrUnionFindLimit);
 }
 
+/* The active bonds that leave a tile (the tile's last x, y or z, periodic
+ * wraps included), joined in the global union-find over the tile roots. */
 __global__ void __launch_bounds__(kThreads)
-    k_wolff_union(const uint8_t* __restrict__ bonds, uint32_t lx, uint32_t ly, uint32_t lz,
-                  uint32_t* parent, unsigned long long* stats) {
+    k_wolff_boundary(const uint8_t* __restrict__ bonds, uint32_t lx, uint32_t ly, uint32_t lz,
+                     uint32_t* parent, unsigned long long* stats) {
     const uint32_t volume = lx * ly * lz;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= volume) return;
     const uint32_t bits = bonds[i];
     if (!bits) return;
     const uint32_t x = i % lx, row = i / lx, y = row % ly, z = row / ly;
+    const bool ex = (x % kTileX == kTileX - 1) || (x + 1 == lx);
+    const bool ey = (y % kTileY == kTileY - 1) || (y + 1 == ly);
+    const bool ez = (z % kTileZ == kTileZ - 1) || (z + 1 == lz);
+    if (!((ex && (bits & 1u)) || (ey && (bits & 2u)) || (ez && (bits & 4u)))) return;
     const uint32_t plane = lx * ly;
     bool ok = true;
-    if (bits & 1u) ok &= uf_union(parent, i, (x + 1 == lx) ? i + 1 - lx : i + 1, volume);
-    if (bits & 2u) ok &= uf_union(parent, i, (y + 1 == ly) ? i + lx - plane : i + lx, volume);
-    if (bits & 4u) ok &= uf_union(parent, i, (z + 1 == lz) ? i + plane - volume : i + plane, volume);
+    if (ex && (bits & 1u)) ok &= uf_union(parent, i, (x + 1 == lx) ? i + 1 - lx : i + 1, volume);
+    if (ey && (bits & 2u)) ok &= uf_union(parent, i, (y + 1 == ly) ? i + lx - plane : i + lx, volume);
+    if (ez && (bits & 4u)) ok &= uf_union(parent, i, (z + 1 == lz) ? i + plane - volume : i + plane, volume);
     if (!ok) atomicOr(&stats[kStatError], kErrUnionFindLimit);
 }
 
@@ -263,43 +344,75 @@ constexpr int kCorrThreads = 256;
 constexpr int kCorrCols = 32;
 
 /* Lines along an axis with stride `stride` (lx for y, lx*ly for z), n sites
- * each; a block takes kCorrCols consecutive x at one (other-axis) offset.
- * out[block][r] = sum over its columns of the lag-r sums. */
+ * each; a block takes kCorrCols consecutive x at one (other-axis) offset and
+ * writes out[block][r - 1] = sum over its columns and all k of
+ * s_k . s_{(k+r) mod n}, r = 1..rmax.
+ *
+ * The block's lines sit in shared memory as (cos, sin) pairs [n + rmax][32]
+ * (the first rmax entries repeated after the last, so k + r needs no
+ * modulo).  Lane c of a warp owns column c; warp w owns the kCorrLags
+ * consecutive lags from 1 + w kCorrLags (then + nwarps kCorrLags, ...) and
+ * slides a register window of those lags' partners along k: one new shared
+ * load per k for kCorrLags products.  Products are summed in FP32 over runs
+ * of kCorrRun values of k, and the runs in FP64, in a fixed order. */
+constexpr uint32_t kCorrLags = 8;
+constexpr uint32_t kCorrRun = 32;
+
 __global__ void __launch_bounds__(kCorrThreads)
     k_corr_strided(const float* __restrict__ theta, uint32_t lx, uint32_t n, uint32_t stride,
                    uint32_t outer_count, uint32_t outer_stride, uint32_t rmax,
                    double* __restrict__ out) {
-    extern __shared__ float tile[]; /* [n][kCorrCols][2] (cos, sin) */
+    extern __shared__ float2 tile[]; /* [n + rmax][kCorrCols] (cos, sin) */
     const uint32_t col_blocks = (lx + kCorrCols - 1) / kCorrCols;
     const uint32_t outer = blockIdx.x / col_blocks;
     const uint32_t x0 = (blockIdx.x % col_blocks) * kCorrCols;
     const uint32_t cols = min((uint32_t)kCorrCols, lx - x0);
     const uint32_t base = outer * outer_stride + x0;
-    for (uint32_t e = threadIdx.x; e < n * kCorrCols; e += blockDim.x) {
+    const uint32_t ext = n + rmax;
+    for (uint32_t e = threadIdx.x; e < ext * kCorrCols; e += blockDim.x) {
         const uint32_t k = e / kCorrCols, c = e % kCorrCols;
-        float s = 0.0f, co = 0.0f;
-        if (c < cols) __sincosf(theta[base + k * stride + c], &s, &co);
-        tile[2 * e] = co;
-        tile[2 * e + 1] = s;
+        const uint32_t kk = k < n ? k : k - n;
+        float sn = 0.0f, cn = 0.0f;
+        if (c < cols) __sincosf(theta[base + kk * stride + c], &sn, &cn);
+        tile[e] = make_float2(cn, sn);
     }
     __syncthreads();
-    __shared__ double red[kCorrThreads];
-    for (uint32_t r = 1; r <= rmax; ++r) {
-        double acc = 0.0;
-        for (uint32_t e = threadIdx.x; e < n * kCorrCols; e += blockDim.x) {
-            const uint32_t k = e / kCorrCols, c = e % kCorrCols;
-            const uint32_t k2 = (k + r) % n;
-            const uint32_t f = k2 * kCorrCols + c;
-            acc += (double)(tile[2 * e] * tile[2 * f] + tile[2 * e + 1] * tile[2 * f + 1]);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (uint32_t r0 = 1 + warp * kCorrLags; r0 <= rmax; r0 += nwarps * kCorrLags) {
+        /* window w[j] = partner of lag r0 + j at the current k */
+        float2 w[kCorrLags];
+#pragma unroll
+        for (uint32_t j = 0; j < kCorrLags; ++j) w[j] = tile[min(r0 + j, ext - 1) * kCorrCols + lane];
+        double tot[kCorrLags];
+        float part[kCorrLags];
+#pragma unroll
+        for (uint32_t j = 0; j < kCorrLags; ++j) {
+            tot[j] = 0.0;
+            part[j] = 0.0f;
         }
-        red[threadIdx.x] = acc;
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-            __syncthreads();
+        for (uint32_t k = 0; k < n; ++k) {
+            const float2 a = tile[k * kCorrCols + lane];
+#pragma unroll
+            for (uint32_t j = 0; j < kCorrLags; ++j) part[j] = __fmaf_rn(a.y, w[j].y, __fmaf_rn(a.x, w[j].x, part[j]));
+            /* slide: the partner of lag r0 + j at k + 1 is the one of lag r0 + j + 1 at k */
+#pragma unroll
+            for (uint32_t j = 0; j + 1 < kCorrLags; ++j) w[j] = w[j + 1];
+            w[kCorrLags - 1] = tile[min(k + 1 + r0 + kCorrLags - 1, ext - 1) * kCorrCols + lane];
+            if ((k + 1) % kCorrRun == 0 || k + 1 == n) {
+#pragma unroll
+                for (uint32_t j = 0; j < kCorrLags; ++j) {
+                    tot[j] += (double)part[j];
+                    part[j] = 0.0f;
+                }
+            }
         }
-        if (threadIdx.x == 0) out[(size_t)blockIdx.x * rmax + (r - 1)] = red[0];
-        __syncthreads();
+#pragma unroll
+        for (uint32_t j = 0; j < kCorrLags; ++j) {
+            double v = tot[j];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0 && r0 + j <= rmax) out[(size_t)blockIdx.x * rmax + (r0 + j - 1)] = v;
+        }
     }
     (void)outer_count;
 }
@@ -334,18 +447,28 @@ __global__ void __launch_bounds__(kCorrThreads)
     }
 }
 
-/* out[g][r] = sum_{j < per_group} in[(g * per_group + j)][r], fixed order. */
+/* out[g][r] = sum_{j < per_group} in[(g * per_group + j)][r] in a fixed
+ * order: one warp per (g, r), lanes over j, then a shuffle tree. */
 __global__ void k_sum_groups(const double* __restrict__ in, uint32_t groups, uint32_t per_group,
                              uint32_t rmax, double* __restrict__ out) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
     if (t >= groups * rmax) return;
     const uint32_t g = t / rmax, r = t % rmax;
     double acc = 0.0;
-    for (uint32_t j = 0; j < per_group; ++j) acc += in[((size_t)g * per_group + j) * rmax + r];
-    out[t] = acc;
+    for (uint32_t j = lane; j < per_group; j += 32) acc += in[((size_t)g * per_group + j) * rmax + r];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (lane == 0) out[t] = acc;
 }
 
 inline uint32_t blocks_for(uint64_t n, int threads) { return (uint32_t)((n + threads - 1) / threads); }
+
+}  // namespace
+
+/* Shared bytes of a k_corr_strided tile of `entries` (cos, sin) rows. */
+size_t corr_tile_bytes(uint32_t entries) { return (size_t)entries * kCorrCols * sizeof(float2); }
+
+namespace {
 
 /* One block per source array; coalesced copy into the contiguous output. */
 __global__ void k_gather(const double* const* __restrict__ src, uint32_t per, double* __restrict__ dst) {
@@ -388,9 +511,11 @@ void launch_wolff(const TaskView& t, uint64_t counter, uint8_t* bonds, uint32_t*
     const uint32_t volume = t.lx * t.ly * t.lz;
     const uint32_t seed_idx = x0 + t.lx * (y0 + t.ly * z0);
     const uint32_t grid = blocks_for(volume, kThreads);
-    k_wolff_bonds<<<grid, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, -2.0f * t.beta, phi,
-                                            t.seed, counter, bonds, parent);
-    k_wolff_union<<<grid, kThreads, 0, s>>>(bonds, t.lx, t.ly, t.lz, parent, t.stats);
+    const uint32_t tiles = ((t.lx + kTileX - 1) / kTileX) * ((t.ly + kTileY - 1) / kTileY) *
+                           ((t.lz + kTileZ - 1) / kTileZ);
+    k_wolff_tiles<<<tiles, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, -2.0f * t.beta, phi,
+                                             t.seed, counter, bonds, parent, t.stats);
+    k_wolff_boundary<<<grid, kThreads, 0, s>>>(bonds, t.lx, t.ly, t.lz, parent, t.stats);
     k_wolff_flip<<<grid, kThreads, 0, s>>>(t.theta, volume, parent, seed_idx, phi, t.stats, cluster_out);
     if (phi_out) *phi_out = phi;
     if (seed_site) {
@@ -432,7 +557,7 @@ void launch_correlations(const TaskView& t, uint32_t rmax_xy, uint32_t rmax_z, d
                          cudaStream_t s) {
     (void)work_doubles;
     const uint32_t col_blocks = (t.lx + kCorrCols - 1) / kCorrCols;
-    const size_t smem_max = (size_t)2 * std::max(t.ly, t.lz) * kCorrCols * sizeof(float);
+    const size_t smem_max = corr_tile_bytes(std::max(t.ly + rmax_xy, t.lz + rmax_z));
     if (smem_max > 48 * 1024)
         cudaFuncSetAttribute(k_corr_strided, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
     if ((size_t)2 * t.lx * sizeof(float) > 48 * 1024)
@@ -440,19 +565,17 @@ void launch_correlations(const TaskView& t, uint32_t rmax_xy, uint32_t rmax_z, d
     if (rmax_xy > 0) {
         /* x: one block per row, then sum the ly rows of each layer. */
         k_corr_rows<<<t.ly * t.lz, kCorrThreads, 2 * t.lx * sizeof(float), s>>>(t.theta, t.lx, rmax_xy, work);
-        k_sum_groups<<<blocks_for((uint64_t)t.lz * rmax_xy, 128), 128, 0, s>>>(work, t.lz, t.ly, rmax_xy, sx);
+        k_sum_groups<<<blocks_for(32ull * t.lz * rmax_xy, 128), 128, 0, s>>>(work, t.lz, t.ly, rmax_xy, sx);
         /* y: lines of ly sites with stride lx; one block per (z, x-chunk). */
-        const size_t smem_y = (size_t)2 * t.ly * kCorrCols * sizeof(float);
-        k_corr_strided<<<t.lz * col_blocks, kCorrThreads, smem_y, s>>>(t.theta, t.lx, t.ly, t.lx, t.lz,
-                                                                        t.lx * t.ly, rmax_xy, work);
-        k_sum_groups<<<blocks_for((uint64_t)t.lz * rmax_xy, 128), 128, 0, s>>>(work, t.lz, col_blocks, rmax_xy, sy);
+        k_corr_strided<<<t.lz * col_blocks, kCorrThreads, corr_tile_bytes(t.ly + rmax_xy), s>>>(
+            t.theta, t.lx, t.ly, t.lx, t.lz, t.lx * t.ly, rmax_xy, work);
+        k_sum_groups<<<blocks_for(32ull * t.lz * rmax_xy, 128), 128, 0, s>>>(work, t.lz, col_blocks, rmax_xy, sy);
     }
     if (rmax_z > 0) {
         /* z: lines of lz sites with stride lx*ly; one block per (y, x-chunk). */
-        const size_t smem_z = (size_t)2 * t.lz * kCorrCols * sizeof(float);
-        k_corr_strided<<<t.ly * col_blocks, kCorrThreads, smem_z, s>>>(t.theta, t.lx, t.lz, t.lx * t.ly, t.ly,
-                                                                        t.lx, rmax_z, work);
-        k_sum_groups<<<blocks_for(rmax_z, 128), 128, 0, s>>>(work, 1, t.ly * col_blocks, rmax_z, sz);
+        k_corr_strided<<<t.ly * col_blocks, kCorrThreads, corr_tile_bytes(t.lz + rmax_z), s>>>(
+            t.theta, t.lx, t.lz, t.lx * t.ly, t.ly, t.lx, rmax_z, work);
+        k_sum_groups<<<blocks_for(32ull * rmax_z, 128), 128, 0, s>>>(work, 1, t.ly * col_blocks, rmax_z, sz);
     }
 }
 

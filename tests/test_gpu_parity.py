@@ -110,7 +110,8 @@ def test_metropolis_width_zero_and_wrap(slsf, ctx, orc):
     assert np.array_equal(t3.theta.view(np.uint32)[same], ref["theta"].view(np.uint32)[same])
 
 
-@pytest.mark.parametrize("dims,T", [((8, 8, 8), 1.1), ((12, 6, 8), 0.9), ((64, 64, 64), 1.3), ((32, 32, 32), 3.0)])
+@pytest.mark.parametrize("dims,T", [((8, 8, 8), 1.1), ((12, 6, 8), 0.9), ((64, 64, 64), 1.3), ((32, 32, 32), 3.0),
+                                    ((40, 12, 6), 1.0), ((96, 16, 10), 0.8), ((128, 24, 10), 1.2)])
 def test_wolff_cluster_bit_exact(slsf, ctx, orc, dims, T):
     t, jxy, jz = make_task(slsf, ctx, orc, dims, T, seed=31)
     t.init_random()
@@ -182,13 +183,17 @@ def test_cold_state_kat(slsf, ctx, L):
     assert np.allclose(c["corr_xy_by_z"], 1.0, atol=1e-6)
 
 
-@pytest.mark.parametrize("dims,rxy,rz", [((8, 8, 8), 4, 4), ((16, 12, 20), 5, 10), ((64, 64, 64), 32, 32)])
+@pytest.mark.parametrize("dims,rxy,rz", [((8, 8, 8), 4, 4), ((16, 12, 20), 5, 10), ((64, 64, 64), 32, 32),
+                                         ((40, 24, 256), 3, 128), ((32, 48, 30), 24, 9)])
 def test_correlations_match_oracle(slsf, ctx, orc, dims, rxy, rz):
     t, _, _ = make_task(slsf, ctx, orc, dims, 1.3, seed=4)
     t.init_random()
     t.sweep(2)
     got = t.correlations(rxy, rz)
-    ref = orc.correlations_f32(dims, t.theta, rxy, rz)
+    # lags clamp to L/2 (src/observables.rs:177-181); the oracle entry takes clamped lags
+    lx, ly, lz = dims
+    ref = orc.correlations_f32(dims, t.theta, min(rxy, lx // 2, ly // 2), min(rz, lz // 2))
+    assert len(got["corr_x"]) == min(rxy, lx // 2, ly // 2) and len(got["corr_z"]) == min(rz, lz // 2)
     assert np.allclose(got["corr_x"], ref["corr_x"], atol=2e-6)
     assert np.allclose(got["corr_y"], ref["corr_y"], atol=2e-6)
     assert np.allclose(got["corr_z"], ref["corr_z"], atol=2e-6)
