@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     p.add_argument("--no-serve", action="store_true", help="skip the served-stream side figure")
+    p.add_argument("--no-large", action="store_true", help="skip the L=256 large-lattice side figure")
     p.add_argument("--serve-tasks", type=int, default=4096, help="tasks of the served stream")
     p.add_argument("--serve-epoch", type=int, default=100, help="sweeps per server epoch")
     p.add_argument("--serve-only", action="store_true", help="run only the served stream (prints its own line)")
@@ -71,7 +72,8 @@ def load_pkg():
 
 
 def workload(pkg, samples, n_temps, L, rank):
-    """(disorder seed, T, run seed, J_xy, J_z) per replica; samples are offset by rank."""
+    """(disorder seed, T, run seed, J_xy, J_z) per replica of one rank: samples
+    rank*samples + 1 .. (rank+1)*samples, so ranks hold disjoint replicas."""
     temps = np.linspace(1.1, 1.5, n_temps)
     out = []
     for s in range(1, samples + 1):
@@ -82,6 +84,18 @@ def workload(pkg, samples, n_temps, L, rank):
         for T in temps:
             out.append((dseed, float(T), pkg.task_seed(BASE_SEED, L, sample, float(T)), jxy, jz))
     return out
+
+
+def max_over_ranks(value, dist, device):
+    """The job time of a multi-rank run: the max of the ranks' times (one
+    all_reduce of a scalar; no data-path collective)."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def peaks():
@@ -228,6 +242,49 @@ def plain_rate(pkg, ctx, L=64, T=1.3, sweeps=1000):
     t.close()
     return {"value": sweeps * L ** 3 / dt, "unit": "site-updates/s",
             "config": f"c1 single replica L={L}, T={T}, {sweeps} sweeps, Metropolis + 1 Wolff + measure per sweep"}
+
+
+def large_lattice(pkg, ctx, stream, L=256, T=1.22, sweeps=50, warmup=5):
+    """Large lattice near the transition: one L^3 replica (J_xy = 1.2, J_z ~
+    U[0.5, 1.5]) through the single-task kernels; every sweep is Metropolis +
+    one Wolff update, then the observables (energy, m^2, helicity sums) and
+    C_z(r) for r = 1..L/2, as ThetaModel::sweep + ThetaModel::measure with
+    z correlations.  Timed with CUDA events on the context's stream."""
+    import torch
+
+    jz = pkg.uniform_layer_disorder(L, 0.5, 1.5, BASE_SEED)
+    t = pkg.Task(ctx, (L, L, L), np.full(L, 1.2), jz, T, wolff_steps=1, seed=pkg.task_seed(BASE_SEED, L, 1, T))
+    t.init_random()
+    for _ in range(warmup):
+        t.sweep(1)
+        t.measure()
+        t.correlations(0, L // 2)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    parts = {"sweep_ms": 0.0, "measure_ms": 0.0, "correlations_ms": 0.0}
+    cluster = 0
+    with torch.cuda.stream(stream):
+        for _ in range(sweeps):
+            ev[0].record(stream)
+            st = t.sweep(1)
+            ev[1].record(stream)
+            t.measure()
+            ev[2].record(stream)
+            t.correlations(0, L // 2)
+            ev[3].record(stream)
+            torch.cuda.synchronize()
+            parts["sweep_ms"] += ev[0].elapsed_time(ev[1])
+            parts["measure_ms"] += ev[1].elapsed_time(ev[2])
+            parts["correlations_ms"] += ev[2].elapsed_time(ev[3])
+            cluster += st["wolff_cluster_sites"]
+    t.close()
+    total_ms = sum(parts.values())
+    out = {"value": sweeps * L ** 3 / (total_ms / 1e3), "unit": "site-updates/s",
+           "config": f"c4 large lattice: L={L} (V={L ** 3}), T={T}, J_xy=1.2, J_z~U[0.5,1.5], Metropolis + 1 Wolff, "
+                     f"observables and C_z(r<={L // 2}) every sweep; {sweeps} timed sweeps after {warmup}",
+           "ms_per_sweep": total_ms / sweeps, "mean_cluster_fraction": cluster / (sweeps * L ** 3)}
+    out.update({k: v / sweeps for k, v in parts.items()})
+    return out
 
 
 SERVE_L = (8, 16, 24, 32, 48, 64)
@@ -394,10 +451,7 @@ def main():
     clk = clocks.stop()
     step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     elapsed = sum(step_ms) / 1e3
-    if dist:
-        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(elapsed, dist, dev)
     updates_rank = n * S * args.steps * L ** 3
     value = updates_rank * world / elapsed
 
@@ -413,10 +467,7 @@ def main():
         ctx.batch_run(tasks, S, handles=handles)
         ctx.batch_bins(tasks, n_bins, out=bins_out, handles=handles)
     e2e_dt = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_dt], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_dt = float(t.item())
+    e2e_dt = max_over_ranks(e2e_dt, dist, dev)
     e2e_value = n * S * e2e_steps * L ** 3 * world / e2e_dt
     view_bytes = 104  # sizeof(slsf::TaskView) uploaded per task per batch launch
     h2d = n * view_bytes + 8 * n  # task table + handle table of the gather
@@ -438,6 +489,8 @@ def main():
         if not args.no_plain:
             extra["plain"] = plain_rate(pkg, ctx)
             extra["plain"]["batched_over_plain"] = value / extra["plain"]["value"]
+        if not args.no_large:
+            extra["large"] = large_lattice(pkg, ctx, stream)
         if not args.no_serve:
             extra["served"] = served_stream(pkg, ctx, args.serve_tasks, args.serve_epoch)
         if not args.no_cpu:
