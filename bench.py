@@ -469,7 +469,7 @@ def main():
     e2e_dt = time.perf_counter() - t0
     e2e_dt = max_over_ranks(e2e_dt, dist, dev)
     e2e_value = n * S * e2e_steps * L ** 3 * world / e2e_dt
-    view_bytes = 104  # sizeof(slsf::TaskView) uploaded per task per batch launch
+    view_bytes = 112  # sizeof(slsf::TaskView) uploaded per task per batch launch
     h2d = n * view_bytes + 8 * n  # task table + handle table of the gather
     d2h = n * 32 + n * n_bins * pkg.BIN_COLS * 8  # per-task counters + bins
 

@@ -113,6 +113,14 @@ uint64_t slsf_task_bytes(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t n_bins)
 int slsf_ctx_set_stream(slsf_ctx* ctx, void* stream);
 /* Number of kernels the library has launched on this context. */
 int slsf_ctx_launch_count(const slsf_ctx* ctx, uint64_t* launches);
+/* Lowers the bound of every device loop of this context's later launches
+ * (union-find path lengths and retries, Wolff growth passes) to `limit`;
+ * 0 restores the defaults (paths <= V, 2^22 union retries, growth <= V
+ * passes).  A loop that reaches its bound makes the kernel record the
+ * failure and return, and the call reports SLSF_ERR_TIMEOUT.  For testing
+ * the error path without faulting a GPU; the task's state after such a
+ * failure is undefined.  No reference counterpart. */
+int slsf_ctx_set_loop_limit(slsf_ctx* ctx, uint32_t limit);
 
 /* ---------------------------------------------------------------- one task */
 

@@ -102,6 +102,7 @@ SIGNATURES = {
     "slsf_batch_run_v": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, _U32P, C.POINTER(SweepStats)]),
     "slsf_ctx_set_stream": (C.c_int, [_P, _P]),
     "slsf_ctx_launch_count": (C.c_int, [_P, _U64P]),
+    "slsf_ctx_set_loop_limit": (C.c_int, [_P, C.c_uint32]),
     "slsf_measure_noalloc": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, _P,
                                        C.POINTER(Observables)]),
 }
@@ -173,6 +174,10 @@ class Context:
 
     def __exit__(self, *exc):
         self.close()
+
+    def set_loop_limit(self, limit):
+        """Bound of every device loop of later launches (0: defaults)."""
+        check(load().slsf_ctx_set_loop_limit(self.h, limit))
 
     def memory(self):
         used, budget = C.c_uint64(), C.c_uint64()

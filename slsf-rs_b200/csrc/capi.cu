@@ -112,6 +112,7 @@ struct slsf_ctx {
     uint64_t used = 0;
     uint64_t live_tasks = 0;
     uint64_t launches = 0;
+    uint32_t loop_limit = 0; /* slsf_ctx_set_loop_limit */
     int sm_count = 0;
     slsf::DevicePool pool;
     /* batched engine scratch */
@@ -177,6 +178,7 @@ struct slsf_task {
         v.binsize = binsize;
         v.n_bins = n_bins;
         v.sweeps = 0;
+        v.loop_limit = ctx->loop_limit;
         v.stats = stats;
         return v;
     }
@@ -364,6 +366,12 @@ int slsf_ctx_set_stream(slsf_ctx* ctx, void* stream) {
     if (int rc = bind_device(ctx)) return rc;
     SLSF_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return SLSF_OK;
+}
+
+int slsf_ctx_set_loop_limit(slsf_ctx* ctx, uint32_t limit) {
+    if (!ctx) return set_error(SLSF_ERR_INVALID, "context is NULL");
+    ctx->loop_limit = limit;
     return SLSF_OK;
 }
 

@@ -24,6 +24,7 @@ enum StatSlot : int {
 /* Error bits written to stats[kStatError]. */
 constexpr unsigned long long kErrUnionFindLimit = 1ull;
 constexpr unsigned long long kErrQueueLimit = 2ull;
+constexpr unsigned long long kErrGrowthLimit = 4ull; /* a Wolff growth did not converge */
 
 constexpr int kBinCols = 12;
 
@@ -42,6 +43,7 @@ struct TaskView {
     double* bins;          /* [n_bins][kBinCols] sums */
     uint32_t thermalization, binsize, n_bins;
     uint32_t sweeps;       /* sweeps of this task in a batched launch; 0: the launch's count */
+    uint32_t loop_limit;   /* 0, or a lower bound on device loops (slsf_ctx_set_loop_limit) */
     unsigned long long* stats;
 };
 

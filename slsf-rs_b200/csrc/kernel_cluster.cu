@@ -679,8 +679,10 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
 
     /* Rounds of stage Z then stage XY until a round changes nothing in the
      * whole cluster; every round that goes on adds at least one site. */
+    const uint32_t bound = t.loop_limit ? min(t.loop_limit, g.volume) : g.volume;
     uint32_t pass = 0;
-    for (; pass <= g.volume; ++pass) {
+    bool converged = false;
+    for (; pass <= bound; ++pass) {
         int any = grow_z(g, s, rm);
         __syncthreads();
         any = __syncthreads_or(grow_xy(g, s, mask) | any);
@@ -691,8 +693,12 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
             const int mine = threadIdx.x < g.csize ? *cluster.map_shared_rank(&flags[pass & 1], threadIdx.x) : 0;
             any = __syncthreads_or(mine);
         }
-        if (!any) break;
+        if (!any) {
+            converged = true;
+            break;
+        }
     }
+    if (!converged && threadIdx.x == 0) atomicOr(&t.stats[kStatError], kErrGrowthLimit);
     SLSF_PHASE(3);
     SLSF_PHASE_COUNT(6, pass + 1);
     SLSF_PHASE_COUNT(7, 1);

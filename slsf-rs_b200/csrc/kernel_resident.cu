@@ -419,10 +419,16 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
     SLSF_PHASE(2);
 
     /* Grow the seed's component; every pass that goes on adds at least one
-     * site, so the count is bounded by V. */
+     * site, so the count is bounded by V (or the context's loop limit). */
+    const uint32_t bound = t.loop_limit ? min(t.loop_limit, g.volume) : g.volume;
     uint32_t pass = 0;
-    for (; pass <= g.volume; ++pass)
-        if (!__syncthreads_or(grow_pass(g, s))) break;
+    bool converged = false;
+    for (; pass <= bound; ++pass)
+        if (!__syncthreads_or(grow_pass(g, s))) {
+            converged = true;
+            break;
+        }
+    if (!converged && threadIdx.x == 0) atomicOr(&t.stats[kStatError], kErrGrowthLimit);
     SLSF_PHASE(3);
     SLSF_PHASE_COUNT(6, pass + 1);
     SLSF_PHASE_COUNT(7, 1);

@@ -89,12 +89,23 @@ __global__ void __launch_bounds__(kThreads)
 
 /* ---- Wolff: union-find with links from larger to smaller roots ---- */
 
+/* Loop bounds of the union-find: a path is strictly decreasing, so at most
+ * `volume` long; a union retries at most 2^22 times.  A nonzero `limit`
+ * (slsf_ctx_set_loop_limit) lowers both, to exercise the error path. */
+struct UfBounds {
+    uint32_t find, uni;
+};
+
+__device__ __forceinline__ UfBounds uf_bounds(uint32_t volume, uint32_t limit) {
+    const uint32_t u = 1u << 22;
+    return {limit ? min(limit, volume) : volume, limit ? min(limit, u) : u};
+}
+
 /* Root of x with path splitting.  parent[i] <= i always holds, so every path
- * is strictly decreasing and at most `volume` long; the loop is bounded by it. */
-__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x, uint32_t volume,
-                                            bool* ok) {
+ * is strictly decreasing; the loop is bounded by b.find. */
+__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x, UfBounds b, bool* ok) {
     volatile uint32_t* par = parent;
-    for (uint32_t it = 0; it <= volume; ++it) {
+    for (uint32_t it = 0; it <= b.find; ++it) {
         const uint32_t p = par[x];
         if (p == x) return x;
         const uint32_t gp = par[p];
@@ -108,11 +119,11 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x, uint32
 /* Lock-free union: hook the larger root under the smaller with a CAS.  A
  * failed CAS means another thread linked that root; every retry follows some
  * other thread's progress, and the retry count is bounded. */
-__device__ __forceinline__ bool uf_union(uint32_t* parent, uint32_t a, uint32_t b, uint32_t volume) {
+__device__ __forceinline__ bool uf_union(uint32_t* parent, uint32_t a, uint32_t b, UfBounds bd) {
     bool ok = true;
-    for (uint32_t it = 0; it < (1u << 22); ++it) {
-        a = uf_find(parent, a, volume, &ok);
-        b = uf_find(parent, b, volume, &ok);
+    for (uint32_t it = 0; it < bd.uni; ++it) {
+        a = uf_find(parent, a, bd, &ok);
+        b = uf_find(parent, b, bd, &ok);
         if (!ok) return false;
         if (a == b) return true;
         if (a > b) {
@@ -132,9 +143,9 @@ constexpr uint32_t kTileSites = kTileX * kTileY * kTileZ;
 
 /* Local union-find in shared memory: hook the larger root under the smaller
  * with a CAS; bounded like the global one. */
-__device__ __forceinline__ uint32_t tile_find(uint32_t* lpar, uint32_t x, bool* ok) {
+__device__ __forceinline__ uint32_t tile_find(uint32_t* lpar, uint32_t x, UfBounds bd, bool* ok) {
     volatile uint32_t* par = lpar;
-    for (uint32_t it = 0; it <= kTileSites; ++it) {
+    for (uint32_t it = 0; it <= bd.find; ++it) {
         const uint32_t p = par[x];
         if (p == x) return x;
         const uint32_t gp = par[p];
@@ -145,11 +156,11 @@ __device__ __forceinline__ uint32_t tile_find(uint32_t* lpar, uint32_t x, bool* 
     return x;
 }
 
-__device__ __forceinline__ bool tile_union(uint32_t* lpar, uint32_t a, uint32_t b) {
+__device__ __forceinline__ bool tile_union(uint32_t* lpar, uint32_t a, uint32_t b, UfBounds bd) {
     bool ok = true;
-    for (uint32_t it = 0; it < 4 * kTileSites; ++it) {
-        a = tile_find(lpar, a, &ok);
-        b = tile_find(lpar, b, &ok);
+    for (uint32_t it = 0; it < bd.uni; ++it) {
+        a = tile_find(lpar, a, bd, &ok);
+        b = tile_find(lpar, b, bd, &ok);
         if (!ok) return false;
         if (a == b) return true;
         if (a > b) {
@@ -172,8 +183,10 @@ __global__ void __launch_bounds__(kThreads)
                   const float* __restrict__ jz, uint32_t lx, uint32_t ly, uint32_t lz,
                   float minus_two_beta, float phi, uint64_t seed, uint64_t counter,
                   uint8_t* __restrict__ bonds, uint32_t* __restrict__ parent,
-                  unsigned long long* __restrict__ stats) {
+                  unsigned long long* __restrict__ stats, uint32_t limit) {
     __shared__ uint32_t lpar[kTileSites];
+    const UfBounds bd = uf_bounds(kTileSites, limit);
+    const UfBounds bu = {bd.find, limit ? min(limit, 4 * kTileSites) : 4 * kTileSites};
     __shared__ uint8_t lbits[kTileSites];
     const uint32_t ntx = (lx + kTileX - 1) / kTileX, nty = (ly + kTileY - 1) / kTileY;
     const uint32_t tx = blockIdx.x % ntx, rest = blockIdx.x / ntx;
@@ -213,15 +226,15 @@ __global__ void __launch_bounds__(kThreads)
         const uint32_t bits = lbits[l];
         if (!bits) continue;
         const uint32_t ax = l % kTileX, ay = (l / kTileX) % kTileY, az = l / (kTileX * kTileY);
-        if ((bits & 1u) && ax + 1 < ex) ok &= tile_union(lpar, l, l + 1);
-        if ((bits & 2u) && ay + 1 < ey) ok &= tile_union(lpar, l, l + kTileX);
-        if ((bits & 4u) && az + 1 < ez) ok &= tile_union(lpar, l, l + kTileX * kTileY);
+        if ((bits & 1u) && ax + 1 < ex) ok &= tile_union(lpar, l, l + 1, bu);
+        if ((bits & 2u) && ay + 1 < ey) ok &= tile_union(lpar, l, l + kTileX, bu);
+        if ((bits & 4u) && az + 1 < ez) ok &= tile_union(lpar, l, l + kTileX * kTileY, bu);
     }
     __syncthreads();
     for (uint32_t l = threadIdx.x; l < kTileSites; l += blockDim.x) {
         const uint32_t ax = l % kTileX, ay = (l / kTileX) % kTileY, az = l / (kTileX * kTileY);
         if (ax >= ex || ay >= ey || az >= ez) continue;
-        const uint32_t r = tile_find(lpar, l, &ok);
+        const uint32_t r = tile_find(lpar, l, bd, &ok);
         const uint32_t rx = r % kTileX, ry = (r / kTileX) % kTileY, rz = r / (kTileX * kTileY);
         parent[(x0 + ax) + lx * ((y0 + ay) + ly * (z0 + az))] = (x0 + rx) + lx * ((y0 + ry) + ly * (z0 + rz));
     }
@@ -232,7 +245,7 @@ __global__ void __launch_bounds__(kThreads)
  * wraps included), joined in the global union-find over the tile roots. */
 __global__ void __launch_bounds__(kThreads)
     k_wolff_boundary(const uint8_t* __restrict__ bonds, uint32_t lx, uint32_t ly, uint32_t lz,
-                     uint32_t* parent, unsigned long long* stats) {
+                     uint32_t* parent, unsigned long long* stats, uint32_t limit) {
     const uint32_t volume = lx * ly * lz;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= volume) return;
@@ -244,22 +257,24 @@ __global__ void __launch_bounds__(kThreads)
     const bool ez = (z % kTileZ == kTileZ - 1) || (z + 1 == lz);
     if (!((ex && (bits & 1u)) || (ey && (bits & 2u)) || (ez && (bits & 4u)))) return;
     const uint32_t plane = lx * ly;
+    const UfBounds bd = uf_bounds(volume, limit);
     bool ok = true;
-    if (ex && (bits & 1u)) ok &= uf_union(parent, i, (x + 1 == lx) ? i + 1 - lx : i + 1, volume);
-    if (ey && (bits & 2u)) ok &= uf_union(parent, i, (y + 1 == ly) ? i + lx - plane : i + lx, volume);
-    if (ez && (bits & 4u)) ok &= uf_union(parent, i, (z + 1 == lz) ? i + plane - volume : i + plane, volume);
+    if (ex && (bits & 1u)) ok &= uf_union(parent, i, (x + 1 == lx) ? i + 1 - lx : i + 1, bd);
+    if (ey && (bits & 2u)) ok &= uf_union(parent, i, (y + 1 == ly) ? i + lx - plane : i + lx, bd);
+    if (ez && (bits & 4u)) ok &= uf_union(parent, i, (z + 1 == lz) ? i + plane - volume : i + plane, bd);
     if (!ok) atomicOr(&stats[kStatError], kErrUnionFindLimit);
 }
 
 __global__ void __launch_bounds__(kThreads)
     k_wolff_flip(float* __restrict__ theta, uint32_t volume, uint32_t* parent, uint32_t seed_idx,
-                 float phi, unsigned long long* stats, uint8_t* __restrict__ cluster_out) {
+                 float phi, unsigned long long* stats, uint8_t* __restrict__ cluster_out, uint32_t limit) {
+    const UfBounds bd = uf_bounds(volume, limit);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool ok = true;
     uint32_t in = 0;
     if (i < volume) {
-        const uint32_t root = uf_find(parent, seed_idx, volume, &ok);
-        in = (uf_find(parent, i, volume, &ok) == root) ? 1u : 0u;
+        const uint32_t root = uf_find(parent, seed_idx, bd, &ok);
+        in = (uf_find(parent, i, bd, &ok) == root) ? 1u : 0u;
         if (in) theta[i] = slsf_reflect(theta[i], phi);
         if (cluster_out) cluster_out[i] = (uint8_t)in;
     }
@@ -514,9 +529,10 @@ void launch_wolff(const TaskView& t, uint64_t counter, uint8_t* bonds, uint32_t*
     const uint32_t tiles = ((t.lx + kTileX - 1) / kTileX) * ((t.ly + kTileY - 1) / kTileY) *
                            ((t.lz + kTileZ - 1) / kTileZ);
     k_wolff_tiles<<<tiles, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, -2.0f * t.beta, phi,
-                                             t.seed, counter, bonds, parent, t.stats);
-    k_wolff_boundary<<<grid, kThreads, 0, s>>>(bonds, t.lx, t.ly, t.lz, parent, t.stats);
-    k_wolff_flip<<<grid, kThreads, 0, s>>>(t.theta, volume, parent, seed_idx, phi, t.stats, cluster_out);
+                                             t.seed, counter, bonds, parent, t.stats, t.loop_limit);
+    k_wolff_boundary<<<grid, kThreads, 0, s>>>(bonds, t.lx, t.ly, t.lz, parent, t.stats, t.loop_limit);
+    k_wolff_flip<<<grid, kThreads, 0, s>>>(t.theta, volume, parent, seed_idx, phi, t.stats, cluster_out,
+                                           t.loop_limit);
     if (phi_out) *phi_out = phi;
     if (seed_site) {
         seed_site[0] = x0;
