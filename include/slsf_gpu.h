@@ -122,6 +122,40 @@ int slsf_ctx_launch_count(const slsf_ctx* ctx, uint64_t* launches);
  * failure is undefined.  No reference counterpart. */
 int slsf_ctx_set_loop_limit(slsf_ctx* ctx, uint32_t limit);
 
+/* ---------------------------------------------------------------- tuning
+ * How the batched entry points run each lattice shape: the one-CTA kernel
+ * with a CTA of `threads`, the cluster kernel with `cluster` CTAs per replica
+ * (a power of two up to 16) of `threads` each, or the grid-wide single-task
+ * kernels.  The choice changes neither a task's trajectory nor its bins
+ * beyond FP32 partial-sum rounding, only the speed.  A context starts from a
+ * default per shape; slsf_autotune times every feasible choice on scratch
+ * replicas and keeps the fastest; the table can be saved and loaded.  No
+ * reference counterpart (the reference's tasks are single-threaded). */
+#define SLSF_KERNEL_RESIDENT 0
+#define SLSF_KERNEL_CLUSTER 1
+#define SLSF_KERNEL_GRID 2
+
+typedef struct slsf_kernel_choice {
+    uint32_t kind;    /* SLSF_KERNEL_* */
+    uint32_t cluster; /* CTAs per replica (SLSF_KERNEL_CLUSTER), else 1 */
+    uint32_t threads; /* threads per CTA */
+} slsf_kernel_choice;
+
+/* The choice the context uses for this shape (its table entry or the default). */
+int slsf_tune_get(slsf_ctx* ctx, uint32_t lx, uint32_t ly, uint32_t lz, slsf_kernel_choice* out);
+/* Sets the shape's choice; SLSF_ERR_INVALID if it cannot hold the lattice. */
+int slsf_tune_set(slsf_ctx* ctx, uint32_t lx, uint32_t ly, uint32_t lz, const slsf_kernel_choice* c);
+/* Times every feasible choice for the shape over `sweeps` sweeps of scratch
+ * replicas that fill the GPU (0: a default that runs ~20 ms per choice),
+ * stores the fastest in the table and returns it with its rate in
+ * site-updates/s.  Uses device memory for the scratch replicas while it runs. */
+int slsf_autotune(slsf_ctx* ctx, uint32_t lx, uint32_t ly, uint32_t lz, uint32_t sweeps, slsf_kernel_choice* best,
+                  double* site_updates_per_s);
+/* The table as text lines "lx ly lz kind cluster threads rate"; loading
+ * skips entries that this device cannot run. */
+int slsf_tune_save(const slsf_ctx* ctx, const char* path);
+int slsf_tune_load(slsf_ctx* ctx, const char* path);
+
 /* ---------------------------------------------------------------- one task */
 
 /* Replaces ThetaModel::new (src/model.rs:314-371): validates the lattice

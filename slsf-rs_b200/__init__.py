@@ -58,6 +58,16 @@ class SweepStats(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+KERNEL_KINDS = ("resident", "cluster", "grid")
+
+
+class KernelChoice(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("cluster", C.c_uint32), ("threads", C.c_uint32)]
+
+    def as_dict(self):
+        return {"kind": KERNEL_KINDS[self.kind], "cluster": self.cluster, "threads": self.threads}
+
+
 def build(force: bool = False) -> str:
     """Compile the library with nvcc for sm_100a (works without a GPU)."""
     if force:
@@ -103,6 +113,12 @@ SIGNATURES = {
     "slsf_ctx_set_stream": (C.c_int, [_P, _P]),
     "slsf_ctx_launch_count": (C.c_int, [_P, _U64P]),
     "slsf_ctx_set_loop_limit": (C.c_int, [_P, C.c_uint32]),
+    "slsf_tune_get": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KernelChoice)]),
+    "slsf_tune_set": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KernelChoice)]),
+    "slsf_autotune": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KernelChoice),
+                                C.POINTER(C.c_double)]),
+    "slsf_tune_save": (C.c_int, [_P, C.c_char_p]),
+    "slsf_tune_load": (C.c_int, [_P, C.c_char_p]),
     "slsf_measure_noalloc": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, _P,
                                        C.POINTER(Observables)]),
 }
@@ -178,6 +194,27 @@ class Context:
     def set_loop_limit(self, limit):
         """Bound of every device loop of later launches (0: defaults)."""
         check(load().slsf_ctx_set_loop_limit(self.h, limit))
+
+    def tune_get(self, dims):
+        c = KernelChoice()
+        check(load().slsf_tune_get(self.h, *dims, C.byref(c)))
+        return c.as_dict()
+
+    def tune_set(self, dims, kind, cluster=1, threads=1024):
+        c = KernelChoice(KERNEL_KINDS.index(kind), cluster, threads)
+        check(load().slsf_tune_set(self.h, *dims, C.byref(c)))
+
+    def autotune(self, dims, sweeps=0):
+        """Times every feasible kernel choice for the shape; keeps and returns the fastest."""
+        c, r = KernelChoice(), C.c_double()
+        check(load().slsf_autotune(self.h, *dims, sweeps, C.byref(c), C.byref(r)))
+        return dict(c.as_dict(), site_updates_per_s=r.value)
+
+    def tune_save(self, path):
+        check(load().slsf_tune_save(self.h, str(path).encode()))
+
+    def tune_load(self, path):
+        check(load().slsf_tune_load(self.h, str(path).encode()))
 
     def memory(self):
         used, budget = C.c_uint64(), C.c_uint64()

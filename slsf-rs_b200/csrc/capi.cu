@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/slsf_gpu.h"
@@ -64,10 +65,10 @@ bool width_ok(double w) { return w >= 0.0 && std::isfinite(w); }
 
 uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
 
-/* One work-queue counter (and side stream) per kernel group of a batch: the
- * one-CTA kernel, the cluster kernel at sizes 1, 2, 4, 8, and the grid-wide
- * kernels. */
-constexpr int kQueues = 6;
+/* Side streams for the kernel groups of a batch after the first (group g
+ * runs on side[(g - 1) % kSideStreams]); each group has its own work-queue
+ * counter. */
+constexpr int kSideStreams = 7;
 
 /* Offsets of the arrays inside a task's block. */
 struct TaskLayout {
@@ -121,13 +122,17 @@ struct slsf_ctx {
     unsigned long long* d_batch_stats = nullptr;
     unsigned long long* h_batch_stats = nullptr; /* pinned */
     uint32_t views_cap = 0;
-    unsigned int* d_queue = nullptr;
-    /* one side stream per extra kernel group of a batch, forked from and
-     * joined back into `stream` with events, so that groups that do not
-     * fill the GPU alone overlap */
-    cudaStream_t side[kQueues] = {};
+    unsigned int* d_queue = nullptr; /* one counter per kernel group */
+    uint32_t queue_cap = 0;
+    /* side streams for the kernel groups of a batch, forked from and joined
+     * back into `stream` with events, so that groups that do not fill the
+     * GPU alone overlap */
+    cudaStream_t side[kSideStreams] = {};
     cudaEvent_t fork = nullptr;
-    cudaEvent_t join[kQueues] = {};
+    cudaEvent_t join[kSideStreams] = {};
+    /* kernel choice per lattice shape (slsf_tune_set / slsf_autotune) */
+    std::unordered_map<uint64_t, slsf::KernelChoice> tune;
+    std::unordered_map<uint64_t, double> tune_rate; /* site-updates/s measured by slsf_autotune */
     /* bins gather scratch */
     const double** d_bin_src = nullptr;
     const double** h_bin_src = nullptr; /* pinned */
@@ -290,7 +295,7 @@ uint64_t slsf_task_bytes(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t n_bins)
 }
 
 static void destroy_streams(slsf_ctx* ctx) {
-    for (int q = 0; q < kQueues; ++q) {
+    for (int q = 0; q < kSideStreams; ++q) {
         if (ctx->side[q]) cudaStreamSynchronize(ctx->side[q]);
         if (ctx->side[q]) cudaStreamDestroy(ctx->side[q]);
         if (ctx->join[q]) cudaEventDestroy(ctx->join[q]);
@@ -319,9 +324,8 @@ int slsf_ctx_create(int device, uint64_t budget_bytes, uint32_t flags, slsf_ctx*
     ctx->sm_count = prop.multiProcessorCount;
     ctx->budget = budget_bytes ? budget_bytes : (uint64_t)(0.9 * (double)free_b);
     e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_queue, sizeof(unsigned int) * kQueues);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming);
-    for (int q = 0; q < kQueues && e == cudaSuccess; ++q) {
+    for (int q = 0; q < kSideStreams && e == cudaSuccess; ++q) {
         e = cudaStreamCreateWithFlags(&ctx->side[q], cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join[q], cudaEventDisableTiming);
     }
@@ -743,10 +747,69 @@ static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v, 
     }
 }
 
-/* Shared body of slsf_batch_run (every task n_sweeps) and slsf_batch_run_v
- * (task i per_task[i] sweeps; tasks with 0 sweeps are left out of the launch). */
+namespace {
+
+uint64_t shape_key(uint32_t lx, uint32_t ly, uint32_t lz) {
+    return (uint64_t)lx | ((uint64_t)ly << 21) | ((uint64_t)lz << 42);
+}
+
+bool choice_feasible(const slsf::KernelChoice& c, uint32_t lx, uint32_t ly, uint32_t lz, int device) {
+    switch (c.kind) {
+        case slsf::kKernelResident:
+            return c.cluster == 1 && c.threads >= 64 && c.threads <= 1024 && c.threads % 32 == 0 &&
+                   slsf::resident_supports(lx, ly, lz, device);
+        case slsf::kKernelCluster:
+            return c.threads >= 64 && c.threads <= 1024 && c.threads % 32 == 0 &&
+                   slsf::cluster_feasible(lx, ly, lz, c.cluster, device);
+        case slsf::kKernelGrid:
+            return true;
+        default:
+            return false;
+    }
+}
+
+/* Without a tuned entry: the one-CTA kernel when the replica fits, with a CTA
+ * of about one thread per 8 sites (128 .. 1024); else the smallest cluster
+ * that holds it; else the grid-wide kernels. */
+slsf::KernelChoice default_choice(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
+    if (slsf::resident_supports(lx, ly, lz, device)) {
+        const uint64_t v = (uint64_t)lx * ly * lz;
+        uint32_t t = 128;
+        while (t < 1024 && 8ull * t < v) t <<= 1;
+        return {slsf::kKernelResident, 1, t};
+    }
+    if (const uint32_t c = slsf::batched_cluster_size(lx, ly, lz, device)) return {slsf::kKernelCluster, c, 1024};
+    return {slsf::kKernelGrid, 1, 256};
+}
+
+slsf::KernelChoice choice_for(const slsf_ctx* ctx, uint32_t lx, uint32_t ly, uint32_t lz) {
+    const auto it = ctx->tune.find(shape_key(lx, ly, lz));
+    if (it != ctx->tune.end()) return it->second;
+    return default_choice(lx, ly, lz, ctx->device);
+}
+
+int ensure_queue_capacity(slsf_ctx* ctx, uint32_t n) {
+    if (n <= ctx->queue_cap) return SLSF_OK;
+    if (ctx->d_queue) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->d_queue);
+        ctx->d_queue = nullptr;
+        ctx->queue_cap = 0;
+    }
+    const uint32_t cap = std::max<uint32_t>(16, n);
+    SLSF_CUDA(cudaMalloc(&ctx->d_queue, sizeof(unsigned int) * cap));
+    ctx->queue_cap = cap;
+    return SLSF_OK;
+}
+
+}  // namespace
+
+/* Shared body of slsf_batch_run (every task n_sweeps), slsf_batch_run_v
+ * (task i per_task[i] sweeps; tasks with 0 sweeps are left out of the
+ * launch) and the autotuner (`force`: one kernel choice for every task). */
 static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_all, uint32_t n_sweeps,
-                          const uint32_t* per_task, slsf_sweep_stats* all_stats) {
+                          const uint32_t* per_task, slsf_sweep_stats* all_stats,
+                          const slsf::KernelChoice* force = nullptr) {
     if (!ctx || (!all_tasks && n_all)) return set_error(SLSF_ERR_INVALID, "NULL argument");
     std::vector<slsf_task*> task_list;
     std::vector<size_t> slot_of;
@@ -763,36 +826,40 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
     slsf_task* const* tasks = task_list.data();
     if (n == 0) return SLSF_OK;
     if (int rc = bind_device(ctx)) return rc;
-    /* Kernel of each task: 0 = one CTA holds the replica
-     * (kernel_resident.cu); 1..8 = the cluster size of kernel_cluster.cu;
-     * kGrid = a lattice too large for one cluster's shared memory, swept by
-     * the grid-wide single-task kernels (kernels_plain.cu), which fill the
-     * GPU on their own. */
-    constexpr uint32_t kGrid = 0xFFFFFFFFu;
-    std::vector<uint32_t> csize(n);
+    /* Kernel of each task (kernel_resident.cu, kernel_cluster.cu, or the
+     * grid-wide single-task kernels of kernels_plain.cu for lattices too
+     * large for one cluster's shared memory, which fill the GPU on their
+     * own), from the context's tuning table or the default. */
+    std::vector<slsf::KernelChoice> ch(n);
     for (size_t i = 0; i < n; ++i) {
         slsf_task* t = tasks[i];
         if (!t || t->ctx != ctx) return set_error(SLSF_ERR_INVALID, "task does not belong to this context");
         if (int rc = check_sweepable(t)) return rc;
-        if (slsf::resident_supports(t->lx, t->ly, t->lz, ctx->device)) {
-            csize[i] = 0;
-        } else {
-            csize[i] = slsf::batched_cluster_size(t->lx, t->ly, t->lz, ctx->device);
-            if (!csize[i]) csize[i] = kGrid;
-        }
+        ch[i] = force ? *force : choice_for(ctx, t->lx, t->ly, t->lz);
+        if (!choice_feasible(ch[i], t->lx, t->ly, t->lz, ctx->device))
+            return set_error(SLSF_ERR_INVALID, "the kernel choice does not hold this lattice");
     }
     if (int rc = ensure_batch_capacity(ctx, n)) return rc;
-    /* Grouped by kernel (one persistent launch each, cluster groups first,
-     * grid-wide tasks last), largest replicas first within a group so the
-     * grid ends evenly; each view accumulates its counters into its own slot
-     * of the batch stats array. */
+    /* Grouped by kernel choice (one persistent launch each; cluster groups
+     * first, grid-wide tasks last), largest replicas first within a group so
+     * the grid ends evenly; each view accumulates its counters into its own
+     * slot of the batch stats array. */
+    auto rank = [&](size_t i) {
+        const slsf::KernelChoice& c = ch[i];
+        const uint32_t k = c.kind == slsf::kKernelCluster ? 2u : (c.kind == slsf::kKernelResident ? 1u : 0u);
+        return ((uint64_t)k << 48) | ((uint64_t)c.cluster << 16) | c.threads;
+    };
     std::vector<size_t> order(n);
     for (size_t i = 0; i < n; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-        const uint32_t ka = csize[a] == kGrid ? 0u : csize[a] + 1, kb = csize[b] == kGrid ? 0u : csize[b] + 1;
-        if (ka != kb) return ka > kb;
+        const uint64_t ra = rank(a), rb = rank(b);
+        if (ra != rb) return ra > rb;
         return tasks[a]->volume > tasks[b]->volume;
     });
+    uint32_t n_groups = 0;
+    for (size_t k = 0; k < n; ++k)
+        if (k == 0 || rank(order[k]) != rank(order[k - 1])) ++n_groups;
+    if (int rc = ensure_queue_capacity(ctx, n_groups)) return rc;
     for (size_t k = 0; k < n; ++k) {
         TaskView v = tasks[order[k]]->view();
         v.stats = ctx->d_batch_stats + slsf::kStatSlots * order[k];
@@ -801,30 +868,23 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
     }
     SLSF_CUDA(cudaMemcpyAsync(ctx->d_views, ctx->h_views, sizeof(TaskView) * n, cudaMemcpyHostToDevice, ctx->stream));
     SLSF_CUDA(cudaMemsetAsync(ctx->d_batch_stats, 0, 8 * slsf::kStatSlots * n, ctx->stream));
-    SLSF_CUDA(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int) * kQueues, ctx->stream));
-    /* Group g runs on ctx->stream (g == 0) or on side stream g, forked after
+    SLSF_CUDA(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int) * n_groups, ctx->stream));
+    /* Group g runs on ctx->stream (g == 0) or on a side stream, forked after
      * the uploads above and joined before the stats read-back below. */
-    size_t n_groups = 0;
-    for (size_t k = 0; k < n; ++k)
-        if (k == 0 || csize[order[k]] != csize[order[k - 1]]) ++n_groups;
     if (n_groups > 1) SLSF_CUDA(cudaEventRecord(ctx->fork, ctx->stream));
     for (size_t lo = 0, q = 0; lo < n; ++q) {
-        const uint32_t c = csize[order[lo]];
+        const slsf::KernelChoice c = ch[order[lo]];
+        const uint64_t key = rank(order[lo]);
         cudaStream_t st = ctx->stream;
-        if (q > 0) {
-            st = ctx->side[q];
+        const int side = q > 0 ? (int)((q - 1) % kSideStreams) : -1;
+        if (side >= 0) {
+            st = ctx->side[side];
             SLSF_CUDA(cudaStreamWaitEvent(st, ctx->fork, 0));
         }
-        if (c == kGrid) {
-            for (size_t k = lo; k < n; ++k) run_grid_task(ctx, tasks[order[k]], ctx->h_views[k], st);
-            if (q > 0) SLSF_CUDA(cudaEventRecord(ctx->join[q], st));
-            if (q > 0) SLSF_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join[q], 0));
-            break;
-        }
         size_t hi = lo;
-        const uint32_t parts = c ? c : 1;
+        const uint32_t parts = c.kind == slsf::kKernelCluster ? c.cluster : 1;
         uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0, max_lx = 0;
-        while (hi < n && csize[order[hi]] == c) {
+        while (hi < n && rank(order[hi]) == key) {
             const slsf_task* t = tasks[order[hi]];
             max_vs = std::max(max_vs, t->volume / parts);
             max_rows = std::max(max_rows, t->ly * (t->lz / parts));
@@ -833,16 +893,21 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
             max_lx = std::max(max_lx, t->lx);
             ++hi;
         }
-        if (c == 0)
+        if (c.kind == slsf::kKernelGrid) {
+            for (size_t k = lo; k < hi; ++k) run_grid_task(ctx, tasks[order[k]], ctx->h_views[k], st);
+        } else if (c.kind == slsf::kKernelResident) {
             SLSF_CUDA(slsf::launch_resident(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
-                                            ctx->device, st, max_vs, max_rows, max_lz));
-        else
+                                            ctx->device, st, max_vs, max_rows, max_lz, c.threads));
+            ctx->launches += 1;
+        } else {
             SLSF_CUDA(slsf::launch_batched(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
-                                           ctx->device, st, c, max_vs, max_rows, max_lz, max_plane, max_lx));
-        ctx->launches += 1;
-        if (q > 0) {
-            SLSF_CUDA(cudaEventRecord(ctx->join[q], st));
-            SLSF_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join[q], 0));
+                                           ctx->device, st, c.cluster, c.threads, max_vs, max_rows, max_lz,
+                                           max_plane, max_lx));
+            ctx->launches += 1;
+        }
+        if (side >= 0) {
+            SLSF_CUDA(cudaEventRecord(ctx->join[side], st));
+            SLSF_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join[side], 0));
         }
         lo = hi;
     }
@@ -865,11 +930,155 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
             slsf_sweep_stats& o = all_stats[slot_of[i]];
             o.sweeps = sw;
             o.accepted = s[slsf::kStatAccepted];
-            o.wolff_clusters = csize[i] == kGrid ? (uint64_t)sw * t->wolff_steps : s[slsf::kStatClusters];
+            o.wolff_clusters =
+                ch[i].kind == slsf::kKernelGrid ? (uint64_t)sw * t->wolff_steps : s[slsf::kStatClusters];
             o.wolff_cluster_sites = s[slsf::kStatClusterSites];
         }
     }
     return rc;
+}
+
+static slsf::KernelChoice to_choice(const slsf_kernel_choice& c) { return {c.kind, c.cluster, c.threads}; }
+static slsf_kernel_choice from_choice(const slsf::KernelChoice& c) { return {c.kind, c.cluster, c.threads}; }
+
+int slsf_tune_get(slsf_ctx* ctx, uint32_t lx, uint32_t ly, uint32_t lz, slsf_kernel_choice* out) {
+    if (!ctx || !out) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    *out = from_choice(choice_for(ctx, lx, ly, lz));
+    return SLSF_OK;
+}
+
+int slsf_tune_set(slsf_ctx* ctx, uint32_t lx, uint32_t ly, uint32_t lz, const slsf_kernel_choice* c) {
+    if (!ctx || !c) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    const slsf::KernelChoice k = to_choice(*c);
+    if (!choice_feasible(k, lx, ly, lz, ctx->device))
+        return set_error(SLSF_ERR_INVALID, "the kernel choice does not hold this lattice");
+    ctx->tune[shape_key(lx, ly, lz)] = k;
+    ctx->tune_rate.erase(shape_key(lx, ly, lz));
+    return SLSF_OK;
+}
+
+int slsf_autotune(slsf_ctx* ctx, uint32_t lx, uint32_t ly, uint32_t lz, uint32_t sweeps, slsf_kernel_choice* best,
+                  double* rate) {
+    if (!ctx) return set_error(SLSF_ERR_INVALID, "context is NULL");
+    if (lx == 0 || ly == 0 || lz == 0 || lx % 2 || ly % 2 || lz % 2)
+        return set_error(SLSF_ERR_INVALID, kErrEven);
+    if (int rc = bind_device(ctx)) return rc;
+    /* candidates */
+    std::vector<slsf::KernelChoice> cand;
+    for (uint32_t t : {128u, 256u, 512u, 1024u}) {
+        const slsf::KernelChoice c = {slsf::kKernelResident, 1, t};
+        if (choice_feasible(c, lx, ly, lz, ctx->device)) cand.push_back(c);
+    }
+    for (uint32_t cl = 1; cl <= 16; cl <<= 1)
+        for (uint32_t t : {512u, 1024u}) {
+            const slsf::KernelChoice c = {slsf::kKernelCluster, cl, t};
+            if (choice_feasible(c, lx, ly, lz, ctx->device)) cand.push_back(c);
+        }
+    if (cand.empty()) cand.push_back({slsf::kKernelGrid, 1, 256});
+    /* scratch replicas: about 2^25 sites, at most 4096, within the budget */
+    const uint64_t v = (uint64_t)lx * ly * lz;
+    uint64_t n = std::max<uint64_t>(1, std::min<uint64_t>(4096, (1ull << 25) / v));
+    const uint64_t per = slsf_task_bytes(lx, ly, lz, 1);
+    if (ctx->budget > ctx->used) n = std::min<uint64_t>(n, (ctx->budget - ctx->used) / per);
+    if (n == 0) return set_error(SLSF_ERR_BUDGET, "task does not fit in the context's device memory budget");
+    std::vector<double> jx(lz, 1.2), jz(lz, 1.0);
+    std::vector<slsf_task*> tasks;
+    int rc = SLSF_OK;
+    for (uint64_t i = 0; i < n && rc == SLSF_OK; ++i) {
+        slsf_task_desc d = {};
+        d.lx = lx;
+        d.ly = ly;
+        d.lz = lz;
+        d.temperature = 1.1 + 0.4 * (double)(i % 16) / 15.0;
+        d.proposal_width = 3.141592653589793;
+        d.wolff_steps = 1;
+        d.seed = 0x5eed0000ull + i;
+        d.j_xy = jx.data();
+        d.n_j_xy = lz;
+        d.j_z = jz.data();
+        d.n_j_z = lz;
+        d.binsize = 1;
+        d.n_bins = 1;
+        slsf_task* t = nullptr;
+        rc = slsf_task_create(ctx, &d, &t);
+        if (rc == SLSF_OK) {
+            tasks.push_back(t);
+            rc = slsf_task_init_random(t);
+        }
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (rc == SLSF_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        rc = set_error(SLSF_ERR_CUDA, "event creation failed");
+    double best_rate = -1.0;
+    slsf::KernelChoice best_c = cand[0];
+    for (const slsf::KernelChoice& c : cand) {
+        if (rc != SLSF_OK) break;
+        /* warm-up, then a run sized to ~20 ms unless `sweeps` is given */
+        rc = batch_run_impl(ctx, tasks.data(), tasks.size(), 1, nullptr, nullptr, &c);
+        uint32_t s_run = sweeps ? sweeps : 2;
+        for (int pass = 0; pass < 2 && rc == SLSF_OK; ++pass) {
+            cudaEventRecord(e0, ctx->stream);
+            rc = batch_run_impl(ctx, tasks.data(), tasks.size(), s_run, nullptr, nullptr, &c);
+            cudaEventRecord(e1, ctx->stream);
+            cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rc != SLSF_OK) break;
+            const double r = (double)tasks.size() * (double)v * s_run / (ms * 1e-3);
+            if (sweeps || pass == 1) {
+                if (r > best_rate) {
+                    best_rate = r;
+                    best_c = c;
+                }
+                break;
+            }
+            s_run = (uint32_t)std::min<double>(200.0, std::max<double>(2.0, s_run * 20.0 / std::max(ms, 1e-3f)));
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    for (slsf_task* t : tasks) slsf_task_destroy(t);
+    if (rc != SLSF_OK) return rc;
+    ctx->tune[shape_key(lx, ly, lz)] = best_c;
+    ctx->tune_rate[shape_key(lx, ly, lz)] = best_rate;
+    if (best) *best = from_choice(best_c);
+    if (rate) *rate = best_rate;
+    return SLSF_OK;
+}
+
+int slsf_tune_save(const slsf_ctx* ctx, const char* path) {
+    if (!ctx || !path) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    FILE* f = std::fopen(path, "w");
+    if (!f) return set_error(SLSF_ERR_INVALID, std::string("cannot write ") + path);
+    std::fprintf(f, "# slsf-b200 kernel choices: lx ly lz kind cluster threads site_updates_per_s\n");
+    for (const auto& kv : ctx->tune) {
+        const uint64_t k = kv.first;
+        const auto r = ctx->tune_rate.find(k);
+        std::fprintf(f, "%u %u %u %u %u %u %.6e\n", (unsigned)(k & 0x1fffff), (unsigned)((k >> 21) & 0x1fffff),
+                     (unsigned)(k >> 42), kv.second.kind, kv.second.cluster, kv.second.threads,
+                     r == ctx->tune_rate.end() ? 0.0 : r->second);
+    }
+    const bool ok = std::fclose(f) == 0;
+    return ok ? SLSF_OK : set_error(SLSF_ERR_INVALID, std::string("cannot write ") + path);
+}
+
+int slsf_tune_load(slsf_ctx* ctx, const char* path) {
+    if (!ctx || !path) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    FILE* f = std::fopen(path, "r");
+    if (!f) return set_error(SLSF_ERR_INVALID, std::string("cannot read ") + path);
+    char line[256];
+    while (std::fgets(line, sizeof(line), f)) {
+        if (line[0] == '#') continue;
+        unsigned lx, ly, lz, kind, cl, th;
+        double r = 0.0;
+        if (std::sscanf(line, "%u %u %u %u %u %u %lf", &lx, &ly, &lz, &kind, &cl, &th, &r) < 6) continue;
+        const slsf::KernelChoice c = {kind, cl, th};
+        if (!choice_feasible(c, lx, ly, lz, ctx->device)) continue;
+        ctx->tune[shape_key(lx, ly, lz)] = c;
+        if (r > 0.0) ctx->tune_rate[shape_key(lx, ly, lz)] = r;
+    }
+    std::fclose(f);
+    return SLSF_OK;
 }
 
 int slsf_batch_run(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_sweeps, slsf_sweep_stats* stats) {

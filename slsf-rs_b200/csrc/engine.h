@@ -47,6 +47,17 @@ struct TaskView {
     unsigned long long* stats;
 };
 
+/* How a batched launch runs one lattice shape: which kernel, how many CTAs
+ * hold a replica (cluster kernel) and how many threads a CTA has.  The
+ * choice changes neither a task's trajectory nor its bins beyond FP32
+ * partial-sum rounding. */
+struct KernelChoice {
+    uint32_t kind;    /* kKernelResident, kKernelCluster or kKernelGrid */
+    uint32_t cluster; /* CTAs per replica (cluster kernel), else 1 */
+    uint32_t threads; /* threads per CTA (batched kernels) */
+};
+constexpr uint32_t kKernelResident = 0, kKernelCluster = 1, kKernelGrid = 2;
+
 /* Records `message` as the calling thread's slsf_last_error text and returns
  * `code` (capi.cu). */
 int report_error(int code, const std::string& message);
@@ -82,11 +93,14 @@ bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);
  * `queue` is a zeroed device counter.  max_* are the largest volume, row
  * count (Ly Lz) and Lz over the views. */
 cudaError_t launch_resident(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
-                            int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz);
+                            int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
+                            uint32_t threads);
 
 /* ---- batched persistent engine, one cluster per replica (kernel_cluster.cu) ---- */
-/* Thread-block cluster size that holds one replica of these dimensions in
- * shared memory (1, 2, 4 or 8 CTAs), or 0 if the kernel cannot hold it. */
+/* Whether a cluster of c CTAs (a power of two up to 16) holds one replica of
+ * these dimensions in shared memory. */
+bool cluster_feasible(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t c, int device);
+/* Smallest portable cluster size (1, 2, 4 or 8) that holds the replica, or 0. */
 uint32_t batched_cluster_size(uint32_t lx, uint32_t ly, uint32_t lz, int device);
 bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);
 /* Runs n_sweeps sweeps of every task view in `views_dev` (device array of
@@ -94,8 +108,8 @@ bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);
  * `queue` is a zeroed device counter the kernel consumes.  max_* are the
  * largest per-CTA slab volume, slab row count, Lz, Lx Ly and Lx over the views. */
 cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
-                           int device, cudaStream_t s, uint32_t cluster, uint32_t max_vs, uint32_t max_rows,
-                           uint32_t max_lz, uint32_t max_plane, uint32_t max_lx);
+                           int device, cudaStream_t s, uint32_t cluster, uint32_t threads, uint32_t max_vs,
+                           uint32_t max_rows, uint32_t max_lz, uint32_t max_plane, uint32_t max_lx);
 
 }  // namespace slsf
 

@@ -51,7 +51,7 @@ namespace {
 constexpr int kBThreads = 1024;
 constexpr uint32_t kPad = 16; /* floats: 64 bytes */
 constexpr uint32_t kMaxRowBits = 64;
-constexpr uint32_t kMaxCluster = 8;
+constexpr uint32_t kMaxCluster = 16; /* 16 needs the non-portable cluster size opt-in */
 
 /* Optional per-phase cycle accounting (build with -DSLSF_PHASE_TIMING). */
 #ifdef SLSF_PHASE_TIMING
@@ -318,7 +318,7 @@ __device__ __forceinline__ void store_slab(const TaskView& t, const Geo& g, cons
  * neighbour, with the bond_cos / bond_sin terms of the measurement pass. */
 template <bool kMeasure, typename W>
 __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, Smem<W>& s, uint64_t sweep,
-                                               uint32_t colour, float (&acc)[8]) {
+                                               uint32_t colour, double (&acc)[8]) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t nwarps = blockDim.x >> 5;
     const uint32_t npairs = g.half_s >> 1;
@@ -362,17 +362,17 @@ __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, 
             __sincosf(s.th[oth + (xp >> 1)], &sa, &ca);
             __sincosf(s.th[oth + (xm >> 1)], &sb, &cb);
             if (kMeasure) {
-                acc[0] += ci + ca;
-                acc[1] += si + sa;
-                acc[2] += bond_cos(jx, ci, si, ca, sa) + bond_cos(jx, cb, sb, ci, si);
-                acc[5] += bond_sin(jx, ci, si, ca, sa) + bond_sin(jx, cb, sb, ci, si);
+                acc[0] += (double)ci + (double)ca;
+                acc[1] += (double)si + (double)sa;
+                acc[2] += (double)bond_cos(jx, ci, si, ca, sa) + (double)bond_cos(jx, cb, sb, ci, si);
+                acc[5] += (double)bond_sin(jx, ci, si, ca, sa) + (double)bond_sin(jx, cb, sb, ci, si);
             }
             const float hx01 = __fadd_rn(ca, cb), hy01 = __fadd_rn(sa, sb);
             __sincosf(s.th[oth + (yp >> 1)], &sa, &ca);
             __sincosf(s.th[oth + (ym >> 1)], &sb, &cb);
             if (kMeasure) {
-                acc[3] += bond_cos(jx, ci, si, ca, sa) + bond_cos(jx, cb, sb, ci, si);
-                acc[6] += bond_sin(jx, ci, si, ca, sa) + bond_sin(jx, cb, sb, ci, si);
+                acc[3] += (double)bond_cos(jx, ci, si, ca, sa) + (double)bond_cos(jx, cb, sb, ci, si);
+                acc[6] += (double)bond_sin(jx, ci, si, ca, sa) + (double)bond_sin(jx, cb, sb, ci, si);
             }
             const float hx23 = __fadd_rn(ca, cb), hy23 = __fadd_rn(sa, sb);
             const float t4 = (zl + 1 < g.nz) ? s.th[oth + ((li + g.plane) >> 1)] : halo_theta(g, s, true, ocol, pc);
@@ -380,8 +380,8 @@ __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, 
             __sincosf(t4, &sa, &ca);
             __sincosf(t5, &sb, &cb);
             if (kMeasure) {
-                acc[4] += bond_cos(jzp, ci, si, ca, sa) + bond_cos(jzm, cb, sb, ci, si);
-                acc[7] += bond_sin(jzp, ci, si, ca, sa) + bond_sin(jzm, cb, sb, ci, si);
+                acc[4] += (double)bond_cos(jzp, ci, si, ca, sa) + (double)bond_cos(jzm, cb, sb, ci, si);
+                acc[7] += (double)bond_sin(jzp, ci, si, ca, sa) + (double)bond_sin(jzm, cb, sb, ci, si);
             }
             const float hxf = field_from_pairs(jx, jzp, jzm, hx01, hx23, ca, cb);
             const float hyf = field_from_pairs(jx, jzp, jzm, hy01, hy23, sa, sb);
@@ -722,13 +722,13 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
 
 /* ---- measurement ---- */
 
-/* Slab sums of mx, my, cos xyz, sin xyz (src/observables.rs:99-141): FP32
- * per thread over its sites, FP64 across the block (valid in thread 0).  The
- * halo holds both colours of the partner planes. */
+/* Slab sums of mx, my, cos xyz, sin xyz (src/observables.rs:99-141): FP64
+ * sums of the FP32 bond terms, block total valid in thread 0.  The halo
+ * holds both colours of the partner planes. */
 template <typename W>
 __device__ __forceinline__ void measure_slab(const Geo& g, const Smem<W>& s, double (&acc)[8], double* red) {
     const uint32_t lane = threadIdx.x & 31u;
-    float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t i0 = (threadIdx.x & ~31u); i0 < g.vs; i0 += blockDim.x) {
         const uint32_t li = i0 + lane;
         const bool valid = li < g.vs;
@@ -762,7 +762,7 @@ __device__ __forceinline__ void measure_slab(const Geo& g, const Smem<W>& s, dou
         f[7] += bond_sin(jzz, ci, si, cz, sz);
     }
 #pragma unroll
-    for (int k = 0; k < 8; ++k) acc[k] = (double)f[k];
+    for (int k = 0; k < 8; ++k) acc[k] = f[k];
     block_sum<8>(acc, red);
 }
 
@@ -826,7 +826,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
         for (uint32_t sw = 0; sw < sweeps; ++sw) {
             const uint64_t sweep = t.metro_sweeps + sw;
             const bool meas = measuring && sw > 0 && sweep > t.thermalization;
-            float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             fill_halo(g, s, rm, 1);
             if (meas) {
                 accepted += half_sweep<true>(t, g, s, sweep, 0, acc);
@@ -890,17 +890,21 @@ int max_dynamic_smem(int device) {
 
 template <typename W>
 cudaError_t launch_w(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
-                     cudaStream_t s, uint32_t cluster, const Limits& lim) {
+                     cudaStream_t s, uint32_t cluster, uint32_t threads, const Limits& lim) {
     const size_t smem = smem_bytes(lim, sizeof(W));
     cudaError_t e = cudaFuncSetAttribute(k_cluster<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    if (cluster > 8) {
+        e = cudaFuncSetAttribute(k_cluster<W>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = cluster;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(kBThreads, 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cfg.attrs = attr;
@@ -917,17 +921,20 @@ cudaError_t launch_w(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, u
 
 }  // namespace
 
-uint32_t batched_cluster_size(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
+bool cluster_feasible(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t c, int device) {
     /* Row words hold L_x <= 64 bits; the float4 colour-split copy needs
      * L_x % 4 == 0 so that four consecutive sites never span two rows. */
-    if (lx > kMaxRowBits || lx < 4 || lx % 4 || ly < 2 || ly % 2 || lz < 2 || lz % 2) return 0;
+    if (lx > kMaxRowBits || lx < 4 || lx % 4 || ly < 2 || ly % 2 || lz < 2 || lz % 2) return false;
+    if (c < 1 || c > kMaxCluster || (c & (c - 1)) || lz % c) return false;
     const size_t word = lx > 32 ? 8 : 4;
-    for (uint32_t c = 1; c <= kMaxCluster; c <<= 1) {
-        if (lz % c) continue;
-        const uint32_t nz = lz / c;
-        const Limits m = {lx * ly * nz, ly * nz, lz, (lx * ly) / 2};
-        if (smem_bytes(m, word) <= (size_t)max_dynamic_smem(device)) return c;
-    }
+    const uint32_t nz = lz / c;
+    const Limits m = {lx * ly * nz, ly * nz, lz, (lx * ly) / 2};
+    return smem_bytes(m, word) <= (size_t)max_dynamic_smem(device);
+}
+
+uint32_t batched_cluster_size(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
+    for (uint32_t c = 1; c <= 8; c <<= 1)
+        if (cluster_feasible(lx, ly, lz, c, device)) return c;
     return 0;
 }
 
@@ -936,12 +943,13 @@ bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
 }
 
 cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
-                           int device, cudaStream_t s, uint32_t cluster, uint32_t max_vs, uint32_t max_rows,
-                           uint32_t max_lz, uint32_t max_plane, uint32_t max_lx) {
+                           int device, cudaStream_t s, uint32_t cluster, uint32_t threads, uint32_t max_vs,
+                           uint32_t max_rows, uint32_t max_lz, uint32_t max_plane, uint32_t max_lx) {
     (void)device;
+    if (threads < 64 || threads > (uint32_t)kBThreads || threads % 32) return cudaErrorInvalidConfiguration;
     const Limits lim = {max_vs, max_rows, max_lz, max_plane / 2};
-    if (max_lx > 32) return launch_w<uint64_t>(views_dev, n, n_sweeps, queue, s, cluster, lim);
-    return launch_w<uint32_t>(views_dev, n, n_sweeps, queue, s, cluster, lim);
+    if (max_lx > 32) return launch_w<uint64_t>(views_dev, n, n_sweeps, queue, s, cluster, threads, lim);
+    return launch_w<uint32_t>(views_dev, n, n_sweeps, queue, s, cluster, threads, lim);
 }
 
 }  // namespace slsf

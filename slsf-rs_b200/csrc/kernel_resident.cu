@@ -222,11 +222,10 @@ __device__ __forceinline__ void store_state(const TaskView& t, const Geo& g, con
  * forward bonds and of the three backward bonds that end on it, and the
  * magnetisation of itself and of its +x neighbour (each colour-1 site is the
  * +x neighbour of exactly one colour-0 site).  Each term is the bond_cos /
- * bond_sin value the measurement pass computes; FP32 sums per thread, FP64
- * across the block, as in the measurement pass. */
+ * bond_sin value the measurement pass computes; sums are FP64. */
 template <bool kMeasure>
 __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, Smem& s, uint64_t sweep,
-                                               uint32_t colour, float (&acc)[8]) {
+                                               uint32_t colour, double (&acc)[8]) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t nwarps = blockDim.x >> 5;
     const uint32_t npairs = (g.half + 1) >> 1;
@@ -268,24 +267,24 @@ __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, 
             __sincosf(s.th[other + (nb[1] >> 1)], &sb, &cb);
             if (kMeasure) {
                 /* forward bonds i -> i+mu, backward bonds i-mu -> i */
-                acc[0] += ci + ca;
-                acc[1] += si + sa;
-                acc[2] += bond_cos(jx, ci, si, ca, sa) + bond_cos(jx, cb, sb, ci, si);
-                acc[5] += bond_sin(jx, ci, si, ca, sa) + bond_sin(jx, cb, sb, ci, si);
+                acc[0] += (double)ci + (double)ca;
+                acc[1] += (double)si + (double)sa;
+                acc[2] += (double)bond_cos(jx, ci, si, ca, sa) + (double)bond_cos(jx, cb, sb, ci, si);
+                acc[5] += (double)bond_sin(jx, ci, si, ca, sa) + (double)bond_sin(jx, cb, sb, ci, si);
             }
             const float hx01 = __fadd_rn(ca, cb), hy01 = __fadd_rn(sa, sb);
             __sincosf(s.th[other + (nb[2] >> 1)], &sa, &ca);
             __sincosf(s.th[other + (nb[3] >> 1)], &sb, &cb);
             if (kMeasure) {
-                acc[3] += bond_cos(jx, ci, si, ca, sa) + bond_cos(jx, cb, sb, ci, si);
-                acc[6] += bond_sin(jx, ci, si, ca, sa) + bond_sin(jx, cb, sb, ci, si);
+                acc[3] += (double)bond_cos(jx, ci, si, ca, sa) + (double)bond_cos(jx, cb, sb, ci, si);
+                acc[6] += (double)bond_sin(jx, ci, si, ca, sa) + (double)bond_sin(jx, cb, sb, ci, si);
             }
             const float hx23 = __fadd_rn(ca, cb), hy23 = __fadd_rn(sa, sb);
             __sincosf(s.th[other + (nb[4] >> 1)], &sa, &ca);
             __sincosf(s.th[other + (nb[5] >> 1)], &sb, &cb);
             if (kMeasure) {
-                acc[4] += bond_cos(jzp, ci, si, ca, sa) + bond_cos(jzm, cb, sb, ci, si);
-                acc[7] += bond_sin(jzp, ci, si, ca, sa) + bond_sin(jzm, cb, sb, ci, si);
+                acc[4] += (double)bond_cos(jzp, ci, si, ca, sa) + (double)bond_cos(jzm, cb, sb, ci, si);
+                acc[7] += (double)bond_sin(jzp, ci, si, ca, sa) + (double)bond_sin(jzm, cb, sb, ci, si);
             }
             const float hx = field_from_pairs(jx, jzp, jzm, hx01, hx23, ca, cb);
             const float hy = field_from_pairs(jx, jzp, jzm, hy01, hy23, sa, sb);
@@ -451,11 +450,11 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
 }
 
 /* Fused observables of the resident state (src/observables.rs:99-141): mx,
- * my, cos xyz, sin xyz; FP32 sums per thread, FP64 across the block (valid
- * in thread 0). */
+ * my, cos xyz, sin xyz; FP64 sums of the FP32 bond terms, block total valid
+ * in thread 0. */
 __device__ __forceinline__ void measure(const Geo& g, const Smem& s, double (&acc)[8], double* red) {
     const uint32_t lane = threadIdx.x & 31u;
-    float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t i0 = (threadIdx.x & ~31u); i0 < g.volume; i0 += blockDim.x) {
         const uint32_t idx = i0 + lane;
         const bool valid = idx < g.volume;
@@ -489,7 +488,7 @@ __device__ __forceinline__ void measure(const Geo& g, const Smem& s, double (&ac
         f[7] += bond_sin(jzz, ci, si, cz, sz);
     }
 #pragma unroll
-    for (int k = 0; k < 8; ++k) acc[k] = (double)f[k];
+    for (int k = 0; k < 8; ++k) acc[k] = f[k];
     block_sum<8>(acc, red);
 }
 
@@ -530,7 +529,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
         const bool measuring = t.n_bins > 0;
         for (uint32_t sw = 0; sw < sweeps; ++sw) {
             const uint64_t sweep = t.metro_sweeps + sw;
-            float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             if (measuring && sw > 0 && sweep > t.thermalization) {
                 accepted += half_sweep<true>(t, g, s, sweep, 0, acc);
                 double tot[8];
@@ -592,18 +591,20 @@ bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
 }
 
 cudaError_t launch_resident(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
-                            int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz) {
+                            int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
+                            uint32_t threads) {
+    if (threads < 32 || threads > (uint32_t)kBThreads || threads % 32) return cudaErrorInvalidConfiguration;
     const size_t smem = smem_bytes(max_volume, max_rows, max_lz);
     cudaError_t e = cudaFuncSetAttribute(k_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int sms = 0, per_sm = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resident, kBThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resident, (int)threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const uint32_t grid = std::min<uint32_t>(n, (uint32_t)(sms * per_sm));
-    k_resident<<<grid, kBThreads, smem, s>>>(views_dev, n, n_sweeps, queue, max_volume, max_rows, max_lz);
+    k_resident<<<grid, threads, smem, s>>>(views_dev, n, n_sweeps, queue, max_volume, max_rows, max_lz);
     return cudaGetLastError();
 }
 

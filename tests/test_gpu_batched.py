@@ -91,12 +91,11 @@ def test_bins_match_plain_measure_stream(slsf, ctx, orc):
                      o["sin_x"], o["sin_y"], o["sin_z"], o["sin_x"] ** 2, o["sin_y"] ** 2, o["sin_z"] ** 2])
     rows = np.array(rows)
     # The batched kernels measure inside the next sweep's colour-0 half-sweep
-    # (the launch's last state in a separate pass) with FP32 sums per thread
-    # and FP64 across threads; the single-task stream sums the same FP32 bond
-    # terms in FP64.  They agree to FP32 partial-sum rounding.
+    # (the launch's last state in a separate pass); both paths sum the same
+    # FP32 bond terms in FP64, in different orders.
     for b in range(n_bins):
         expect = rows[b * binsize:(b + 1) * binsize].mean(axis=0)
-        assert np.allclose(bins[b], expect, rtol=1e-6, atol=1e-7 * v), (b, bins[b], expect)
+        assert np.allclose(bins[b], expect, rtol=1e-10, atol=1e-10 * v), (b, bins[b], expect)
 
 
 def test_checkpoint_resume_is_bit_exact(slsf, ctx, orc):
