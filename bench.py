@@ -355,13 +355,15 @@ def served_stream(pkg, ctx, n_tasks, epoch_sweeps):
     arrivals offering 0.8x and 1.5x that capacity."""
     reqs = serve_requests(pkg, n_tasks)
     mean_work = float(np.mean([r["dims"][0] ** 3 * r["sweeps"] for r in reqs]))
+    # kernel choice per request size from the autotuner (the server's launches use the context's table)
+    tuned = {str(L): ctx.autotune((L, L, L)) for L in SERVE_L}
     warm = serve_requests(pkg, 64, seed=BASE_SEED + 7)
     serve_run(pkg, ctx, warm, None, epoch_sweeps)
     sat = serve_run(pkg, ctx, reqs, None, epoch_sweeps)
     capacity = sat["throughput"]
     out = {"workload": f"c3 served stream: {n_tasks} tasks, L~U{{8..64}}, T~U[1.0,1.6], sweeps~U{{200..2000}}, "
                        f"J_xy=1.2, J_z~U[0.5,1.5] per task, 20% thermalization, 32 bins, epoch {epoch_sweeps} sweeps",
-           "mean_site_updates_per_task": mean_work, "saturation": sat, "capacity": capacity}
+           "mean_site_updates_per_task": mean_work, "saturation": sat, "capacity": capacity, "kernel_choice": tuned}
     for load in (0.8, 1.5):
         rate = load * capacity / mean_work
         r = serve_run(pkg, ctx, reqs, rate, epoch_sweeps)
@@ -413,6 +415,7 @@ def main():
     ctx.set_stream(stream.cuda_stream)
 
     L, S = args.L, args.sweeps_per_step
+    choice = ctx.autotune((L, L, L))  # kernel, cluster and CTA size for this shape
     wl = workload(pkg, args.samples, args.temperatures, L, rank)
     n = len(wl)
     total_sweeps = (args.warmup + args.steps) * S
@@ -481,7 +484,8 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (tps * n * L ** 3) if tps is not None else None,
                 "peak_kind": peak_kind,
-                "kernel": "k_resident (one launch = S sweeps of every replica, each replica resident in one CTA's shared memory)",
+                "kernel": "k_resident (one launch = S sweeps of every replica, each replica resident in one CTA's shared memory)"
+                if choice["kind"] == "resident" else f"k_cluster ({choice['cluster']} CTAs per replica)",
                 "algorithmic_bytes_per_launch": alg_bytes}
 
     extra = {}
@@ -508,7 +512,8 @@ def main():
                                    f"in [1.1,1.5], L={L}, J_xy=1.2, J_z~U[0.5,1.5], Metropolis (width pi) + 1 Wolff "
                                    f"+ measure per sweep, {total_sweeps} sweeps total, {S} sweeps per step",
                        "replicas_per_gpu": n, "L": L, "sweeps_per_step": S, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (state 512 MiB per GPU)", "reductions": "fp64"},
+                       "l2": "inputs larger than L2 (state 512 MiB per GPU)", "reductions": "fp64",
+                       "kernel_choice": choice},
             "clocks": clk, "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": "site-updates/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps},

@@ -122,6 +122,23 @@ int slsf_ctx_launch_count(const slsf_ctx* ctx, uint64_t* launches);
  * failure is undefined.  No reference counterpart. */
 int slsf_ctx_set_loop_limit(slsf_ctx* ctx, uint32_t limit);
 
+/* ---------------------------------------------------------------- sessions
+ * A batch session captures one batched step -- n_sweeps sweeps of every task,
+ * with the kernel groups of slsf_batch_run -- in a CUDA graph once, keeps the
+ * task table on the device and replays the graph per step; the tasks'
+ * counters advance on the device and are mirrored on the host after each
+ * step.  While a session is open its tasks refuse the calls that change
+ * their state (SLSF_ERR_STATE); measuring and reading angles, counters and
+ * bins work between steps.  Lattices too large for one thread-block cluster
+ * (run by the grid-wide kernels) are refused.  No reference counterpart. */
+typedef struct slsf_batch slsf_batch;
+
+int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_sweeps, slsf_batch** out);
+/* Replays the step and waits for it; stats (may be NULL) receives each
+ * task's counters of this step, in the order of the tasks at open. */
+int slsf_batch_step(slsf_batch* b, slsf_sweep_stats* stats);
+int slsf_batch_close(slsf_batch* b);
+
 /* ---------------------------------------------------------------- tuning
  * How the batched entry points run each lattice shape: the one-CTA kernel
  * with a CTA of `threads`, the cluster kernel with `cluster` CTAs per replica

@@ -113,6 +113,9 @@ SIGNATURES = {
     "slsf_ctx_set_stream": (C.c_int, [_P, _P]),
     "slsf_ctx_launch_count": (C.c_int, [_P, _U64P]),
     "slsf_ctx_set_loop_limit": (C.c_int, [_P, C.c_uint32]),
+    "slsf_batch_open": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_uint32, C.POINTER(_P)]),
+    "slsf_batch_step": (C.c_int, [_P, C.POINTER(SweepStats)]),
+    "slsf_batch_close": (C.c_int, [_P]),
     "slsf_tune_get": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KernelChoice)]),
     "slsf_tune_set": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KernelChoice)]),
     "slsf_autotune": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KernelChoice),
@@ -168,12 +171,15 @@ class Context:
         self.h = h
         self._tasks = weakref.WeakSet()
         self._servers = weakref.WeakSet()
+        self._sessions = weakref.WeakSet()
 
     def close(self):
         """Destroy every live server and task of this context, then the context."""
         if getattr(self, "h", None):
             for srv in list(self._servers):
                 srv.close()
+            for ses in list(self._sessions):
+                ses.close()
             for t in list(self._tasks):
                 t.close()
             check(load().slsf_ctx_destroy(self.h))
@@ -231,6 +237,10 @@ class Context:
         check(load().slsf_batch_run(self.h, arr, len(tasks), n_sweeps, stats))
         return [s.as_dict() for s in stats]
 
+    def session(self, tasks, n_sweeps):
+        """A batch session: one captured step of n_sweeps sweeps, replayed by step()."""
+        return BatchSession(self, tasks, n_sweeps)
+
     @staticmethod
     def handle_array(tasks):
         return (_P * len(tasks))(*[t.h for t in tasks])
@@ -254,6 +264,42 @@ class Context:
         n = C.c_uint64()
         check(load().slsf_ctx_launch_count(self.h, C.byref(n)))
         return n.value
+
+
+class BatchSession:
+    """slsf_batch_open / slsf_batch_step / slsf_batch_close: one batched step
+    captured in a CUDA graph and replayed."""
+
+    def __init__(self, ctx, tasks, n_sweeps):
+        h = _P()
+        arr = ctx.handle_array(tasks)
+        check(load().slsf_batch_open(ctx.h, arr, len(tasks), n_sweeps, C.byref(h)))
+        self.h = h
+        self.n = len(tasks)
+        self.ctx = ctx
+        ctx._sessions.add(self)
+
+    def step(self):
+        st = (SweepStats * self.n)()
+        check(load().slsf_batch_step(self.h, st))
+        return [x.as_dict() for x in st]
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().slsf_batch_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class Task:

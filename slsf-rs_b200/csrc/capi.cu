@@ -163,6 +163,7 @@ struct slsf_task {
     unsigned int* done = nullptr;
     unsigned long long* stats = nullptr;
     double* bins = nullptr;
+    slsf_batch* session = nullptr; /* open batch session holding the task's device view */
 
     TaskView view() const {
         TaskView v;
@@ -193,10 +194,20 @@ namespace {
 
 /* Checks the state a sweep needs, with the reference's messages
  * (src/updates.rs:447-450). */
+int check_free(const slsf_task* t);
+
 int check_sweepable(const slsf_task* t) {
+    if (int rc = check_free(t)) return rc;
     if (!temperature_ok(t->temperature)) return set_error(SLSF_ERR_INVALID, kErrTemperature);
     if (!width_ok(t->width)) return set_error(SLSF_ERR_INVALID, kErrWidth);
     if (t->lx % 2 || t->ly % 2 || t->lz % 2) return set_error(SLSF_ERR_INVALID, kErrEven);
+    return SLSF_OK;
+}
+
+/* Calls that change a task's state or counters are refused while an open
+ * batch session owns its device view. */
+int check_free(const slsf_task* t) {
+    if (t->session) return set_error(SLSF_ERR_STATE, "task belongs to an open batch session; close it first");
     return SLSF_OK;
 }
 
@@ -459,6 +470,7 @@ int slsf_task_create(slsf_ctx* ctx, const slsf_task_desc* d, slsf_task** out) {
 
 int slsf_task_destroy(slsf_task* t) {
     if (!t) return SLSF_OK;
+    if (int rc = check_free(t)) return rc;
     slsf_ctx* ctx = t->ctx;
     cudaSetDevice(ctx->device);
     /* Work queued on the stream may still use the block. */
@@ -472,6 +484,7 @@ int slsf_task_destroy(slsf_task* t) {
 
 int slsf_task_init_random(slsf_task* t) {
     if (!t) return set_error(SLSF_ERR_INVALID, "task is NULL");
+    if (int rc = check_free(t)) return rc;
     if (int rc = bind_device(t->ctx)) return rc;
     slsf::launch_init_random(t->theta, t->volume, t->seed, t->ctx->stream);
     t->ctx->launches += 1;
@@ -482,6 +495,7 @@ int slsf_task_init_random(slsf_task* t) {
 
 int slsf_task_init_cold(slsf_task* t) {
     if (!t) return set_error(SLSF_ERR_INVALID, "task is NULL");
+    if (int rc = check_free(t)) return rc;
     if (int rc = bind_device(t->ctx)) return rc;
     SLSF_CUDA(cudaMemsetAsync(t->theta, 0, 4ull * t->volume, t->ctx->stream));
     SLSF_CUDA(cudaStreamSynchronize(t->ctx->stream));
@@ -490,6 +504,7 @@ int slsf_task_init_cold(slsf_task* t) {
 
 int slsf_task_set_angles(slsf_task* t, const float* theta, size_t n) {
     if (!t || !theta) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    if (int rc = check_free(t)) return rc;
     if (n != t->volume) return set_error(SLSF_ERR_INVALID, "angle array length must equal the lattice volume");
     if (int rc = bind_device(t->ctx)) return rc;
     SLSF_CUDA(cudaMemcpyAsync(t->theta, theta, 4ull * n, cudaMemcpyHostToDevice, t->ctx->stream));
@@ -515,6 +530,7 @@ int slsf_task_get_counters(const slsf_task* t, uint64_t* metro_sweeps, uint64_t*
 
 int slsf_task_set_counters(slsf_task* t, uint64_t metro_sweeps, uint64_t wolff_steps) {
     if (!t) return set_error(SLSF_ERR_INVALID, "task is NULL");
+    if (int rc = check_free(t)) return rc;
     t->metro_sweeps = metro_sweeps;
     t->wolff_done = wolff_steps;
     return SLSF_OK;
@@ -563,6 +579,7 @@ int slsf_task_metropolis_sweep(slsf_task* t, double* acceptance) {
 int slsf_task_wolff_step_debug(slsf_task* t, uint8_t* bonds, uint8_t* cluster, float* phi,
                                uint32_t seed_site[3], uint64_t* cluster_size) {
     if (!t) return set_error(SLSF_ERR_INVALID, "task is NULL");
+    if (int rc = check_free(t)) return rc;
     /* wolff_cluster_step_with_theta_scratch validates T (src/updates.rs:558). */
     if (!temperature_ok(t->temperature)) return set_error(SLSF_ERR_INVALID, kErrTemperature);
     if (int rc = bind_device(t->ctx)) return rc;
@@ -713,6 +730,7 @@ int slsf_task_get_bins(const slsf_task* t, double* bins, size_t n_rows, uint64_t
 
 int slsf_task_reset_bins(slsf_task* t) {
     if (!t) return set_error(SLSF_ERR_INVALID, "task is NULL");
+    if (int rc = check_free(t)) return rc;
     if (int rc = bind_device(t->ctx)) return rc;
     if (t->n_bins)
         SLSF_CUDA(cudaMemsetAsync(t->bins, 0, 8ull * slsf::kBinCols * t->n_bins, t->ctx->stream));
@@ -769,13 +787,15 @@ bool choice_feasible(const slsf::KernelChoice& c, uint32_t lx, uint32_t ly, uint
 }
 
 /* Without a tuned entry: the one-CTA kernel when the replica fits, with a CTA
- * of about one thread per 8 sites (128 .. 1024); else the smallest cluster
- * that holds it; else the grid-wide kernels. */
+ * of about one thread per 32 sites (128 .. 1024; measured on B200: L = 8 and
+ * 16 run 1.4-2x faster on 128 threads than on 1024, L = 24 best on 512, L = 32
+ * on 1024); else the smallest cluster that holds it, 1024 threads; else the
+ * grid-wide kernels. */
 slsf::KernelChoice default_choice(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
     if (slsf::resident_supports(lx, ly, lz, device)) {
         const uint64_t v = (uint64_t)lx * ly * lz;
         uint32_t t = 128;
-        while (t < 1024 && 8ull * t < v) t <<= 1;
+        while (t < 1024 && 32ull * t < v) t <<= 1;
         return {slsf::kKernelResident, 1, t};
     }
     if (const uint32_t c = slsf::batched_cluster_size(lx, ly, lz, device)) return {slsf::kKernelCluster, c, 1024};
@@ -936,6 +956,173 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
         }
     }
     return rc;
+}
+
+/* ---- batch sessions: one captured step replayed as a CUDA graph ---- */
+
+struct slsf_batch {
+    slsf_ctx* ctx = nullptr;
+    std::vector<slsf_task*> tasks; /* in the caller's order */
+    uint32_t n_sweeps = 0;
+    TaskView* d_views = nullptr;
+    unsigned long long* d_stats = nullptr;
+    unsigned long long* h_stats = nullptr; /* pinned */
+    unsigned int* d_queue = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+static void batch_free(slsf_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->d_views) cudaFree(b->d_views);
+    if (b->d_stats) cudaFree(b->d_stats);
+    if (b->d_queue) cudaFree(b->d_queue);
+    if (b->h_stats) cudaFreeHost(b->h_stats);
+    for (slsf_task* t : b->tasks)
+        if (t && t->session == b) t->session = nullptr;
+    delete b;
+}
+
+int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n_sweeps, slsf_batch** out) {
+    if (!ctx || !out || (!tasks && n)) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    *out = nullptr;
+    if (n == 0 || n_sweeps == 0) return set_error(SLSF_ERR_INVALID, "a session needs tasks and sweeps");
+    if (int rc = bind_device(ctx)) return rc;
+    std::vector<slsf::KernelChoice> ch(n);
+    for (size_t i = 0; i < n; ++i) {
+        slsf_task* t = tasks[i];
+        if (!t || t->ctx != ctx) return set_error(SLSF_ERR_INVALID, "task does not belong to this context");
+        if (int rc = check_sweepable(t)) return rc;
+        for (size_t j = 0; j < i; ++j)
+            if (tasks[j] == t) return set_error(SLSF_ERR_INVALID, "a task appears twice in the session");
+        ch[i] = choice_for(ctx, t->lx, t->ly, t->lz);
+        if (ch[i].kind == slsf::kKernelGrid || !choice_feasible(ch[i], t->lx, t->ly, t->lz, ctx->device))
+            return set_error(SLSF_ERR_INVALID,
+                             "batch sessions hold lattices that fit one thread-block cluster's shared memory");
+    }
+    auto rank = [&](size_t i) {
+        const slsf::KernelChoice& c = ch[i];
+        return ((uint64_t)(c.kind == slsf::kKernelCluster ? 2u : 1u) << 48) | ((uint64_t)c.cluster << 16) | c.threads;
+    };
+    std::vector<size_t> order(n);
+    for (size_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        const uint64_t ra = rank(a), rb = rank(b);
+        if (ra != rb) return ra > rb;
+        return tasks[a]->volume > tasks[b]->volume;
+    });
+    uint32_t n_groups = 0;
+    for (size_t k = 0; k < n; ++k)
+        if (k == 0 || rank(order[k]) != rank(order[k - 1])) ++n_groups;
+    slsf_batch* b = new slsf_batch;
+    b->ctx = ctx;
+    b->tasks.assign(tasks, tasks + n);
+    b->n_sweeps = n_sweeps;
+    cudaError_t e = cudaMalloc(&b->d_views, sizeof(TaskView) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_stats, 8 * slsf::kStatSlots * n);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, sizeof(unsigned int) * n_groups);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_stats, 8 * slsf::kStatSlots * n);
+    std::vector<TaskView> views(n);
+    for (size_t k = 0; k < n && e == cudaSuccess; ++k) {
+        TaskView v = tasks[order[k]]->view();
+        v.stats = b->d_stats + slsf::kStatSlots * order[k];
+        v.sweeps = n_sweeps;
+        views[k] = v;
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_views, views.data(), sizeof(TaskView) * n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        batch_free(b);
+        return cuda_error(e, "batch session set-up");
+    }
+    /* capture one step */
+    cudaStream_t main = ctx->stream;
+    e = cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_stats, 0, 8 * slsf::kStatSlots * n, main);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned int) * n_groups, main);
+    if (e == cudaSuccess && n_groups > 1) e = cudaEventRecord(ctx->fork, main);
+    uint64_t launches = 0;
+    for (size_t lo = 0, q = 0; lo < n && e == cudaSuccess; ++q) {
+        const slsf::KernelChoice c = ch[order[lo]];
+        const uint64_t key = rank(order[lo]);
+        cudaStream_t st = main;
+        const int side = q > 0 ? (int)((q - 1) % kSideStreams) : -1;
+        if (side >= 0) {
+            st = ctx->side[side];
+            e = cudaStreamWaitEvent(st, ctx->fork, 0);
+        }
+        size_t hi = lo;
+        const uint32_t parts = c.kind == slsf::kKernelCluster ? c.cluster : 1;
+        uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0, max_lx = 0;
+        while (hi < n && rank(order[hi]) == key) {
+            const slsf_task* t = tasks[order[hi]];
+            max_vs = std::max(max_vs, t->volume / parts);
+            max_rows = std::max(max_rows, t->ly * (t->lz / parts));
+            max_lz = std::max(max_lz, t->lz);
+            max_plane = std::max(max_plane, t->lx * t->ly);
+            max_lx = std::max(max_lx, t->lx);
+            ++hi;
+        }
+        if (e == cudaSuccess) {
+            if (c.kind == slsf::kKernelResident)
+                e = slsf::launch_resident(b->d_views + lo, (uint32_t)(hi - lo), n_sweeps, b->d_queue + q, ctx->device,
+                                          st, max_vs, max_rows, max_lz, c.threads);
+            else
+                e = slsf::launch_batched(b->d_views + lo, (uint32_t)(hi - lo), n_sweeps, b->d_queue + q, ctx->device,
+                                         st, c.cluster, c.threads, max_vs, max_rows, max_lz, max_plane, max_lx);
+            ++launches;
+        }
+        if (e == cudaSuccess && side >= 0) {
+            e = cudaEventRecord(ctx->join[side], st);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(main, ctx->join[side], 0);
+        }
+        lo = hi;
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->h_stats, b->d_stats, 8 * slsf::kStatSlots * n, cudaMemcpyDeviceToHost, main);
+    const cudaError_t e_end = cudaStreamEndCapture(main, &b->graph);
+    if (e == cudaSuccess) e = e_end;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        batch_free(b);
+        return cuda_error(e, "batch session capture");
+    }
+    (void)launches;
+    for (slsf_task* t : b->tasks) t->session = b;
+    *out = b;
+    return SLSF_OK;
+}
+
+int slsf_batch_step(slsf_batch* b, slsf_sweep_stats* stats) {
+    if (!b) return set_error(SLSF_ERR_INVALID, "session is NULL");
+    slsf_ctx* ctx = b->ctx;
+    if (int rc = bind_device(ctx)) return rc;
+    SLSF_CUDA(cudaGraphLaunch(b->exec, ctx->stream));
+    SLSF_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->launches += 1;
+    int rc = SLSF_OK;
+    for (size_t i = 0; i < b->tasks.size(); ++i) {
+        slsf_task* t = b->tasks[i];
+        const uint64_t before = t->metro_sweeps;
+        t->metro_sweeps += b->n_sweeps;
+        t->wolff_done += (uint64_t)b->n_sweeps * t->wolff_steps;
+        const uint64_t lo = std::max<uint64_t>(before, t->thermalization);
+        if (t->metro_sweeps > lo && t->n_bins) t->measurements += t->metro_sweeps - lo;
+        const unsigned long long* s = &b->h_stats[i * slsf::kStatSlots];
+        if (s[slsf::kStatError]) rc = set_error(SLSF_ERR_TIMEOUT, "a bounded device loop hit its iteration limit");
+        if (stats) stats[i] = slsf_sweep_stats{b->n_sweeps, s[slsf::kStatAccepted], s[slsf::kStatClusters],
+                                               s[slsf::kStatClusterSites]};
+    }
+    return rc;
+}
+
+int slsf_batch_close(slsf_batch* b) {
+    if (!b) return SLSF_OK;
+    bind_device(b->ctx);
+    cudaStreamSynchronize(b->ctx->stream);
+    batch_free(b);
+    return SLSF_OK;
 }
 
 static slsf::KernelChoice to_choice(const slsf_kernel_choice& c) { return {c.kind, c.cluster, c.threads}; }

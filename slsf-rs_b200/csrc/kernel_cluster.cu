@@ -777,7 +777,7 @@ __device__ __forceinline__ void bin_cluster_sums(const TaskView& t, const Geo& g
 
 template <typename W>
 __global__ void __launch_bounds__(kBThreads, 1)
-    k_cluster(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
+    k_cluster(TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
               Limits lim) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[8 * 32];
@@ -874,6 +874,12 @@ __global__ void __launch_bounds__(kBThreads, 1)
         }
         /* no CTA may start the next replica while a partner still reads its slab */
         cluster.sync();
+        /* the view's counters advance on the device, so that a replayed
+         * launch (slsf_batch_open / slsf_batch_step) continues the streams */
+        if (rank == 0 && threadIdx.x == 0) {
+            views[item].metro_sweeps = t.metro_sweeps + sweeps;
+            views[item].wolff_done = t.wolff_done + (uint64_t)sweeps * t.wolff_steps;
+        }
     }
 }
 
@@ -889,7 +895,7 @@ int max_dynamic_smem(int device) {
 }
 
 template <typename W>
-cudaError_t launch_w(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+cudaError_t launch_w(TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                      cudaStream_t s, uint32_t cluster, uint32_t threads, const Limits& lim) {
     const size_t smem = smem_bytes(lim, sizeof(W));
     cudaError_t e = cudaFuncSetAttribute(k_cluster<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -942,7 +948,7 @@ bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
     return batched_cluster_size(lx, ly, lz, device) != 0;
 }
 
-cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+cudaError_t launch_batched(TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                            int device, cudaStream_t s, uint32_t cluster, uint32_t threads, uint32_t max_vs,
                            uint32_t max_rows, uint32_t max_lz, uint32_t max_plane, uint32_t max_lx) {
     (void)device;

@@ -494,7 +494,7 @@ __device__ __forceinline__ void measure(const Geo& g, const Smem& s, double (&ac
 
 
 __global__ void __launch_bounds__(kBThreads, 1)
-    k_resident(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
+    k_resident(TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
                uint32_t max_volume, uint32_t max_rows, uint32_t max_lz) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[8 * 32];
@@ -565,6 +565,10 @@ __global__ void __launch_bounds__(kBThreads, 1)
             atomicAdd(&t.stats[kStatAccepted], (unsigned long long)s_accepted);
             atomicAdd(&t.stats[kStatClusterSites], (unsigned long long)s_cluster);
             atomicAdd(&t.stats[kStatClusters], (unsigned long long)sweeps * t.wolff_steps);
+            /* the view's counters advance on the device, so that a replayed
+             * launch (slsf_batch_open / slsf_batch_step) continues the streams */
+            views[item].metro_sweeps = t.metro_sweeps + sweeps;
+            views[item].wolff_done = t.wolff_done + (uint64_t)sweeps * t.wolff_steps;
         }
     }
 }
@@ -590,7 +594,7 @@ bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
     return smem_bytes((uint32_t)v, ly * lz, lz) <= (size_t)max_dynamic_smem(device);
 }
 
-cudaError_t launch_resident(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+cudaError_t launch_resident(TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                             int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
                             uint32_t threads) {
     if (threads < 32 || threads > (uint32_t)kBThreads || threads % 32) return cudaErrorInvalidConfiguration;

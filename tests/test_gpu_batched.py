@@ -194,3 +194,30 @@ def test_two_sigma_config0(slsf, ctx, orc):
     print("config0 2-sigma:", report)
     for name, (_, _, _, z) in report.items():
         assert abs(z) < 2.0, (name, report)
+
+
+def test_session_graph_replay_equals_batch_run(slsf, ctx, orc):
+    # One step captured in a CUDA graph and replayed: same trajectories, bins and
+    # counters as batch_run, with tasks of several kernels in the session.
+    specs = [((8, 8, 8), 1.0, 1, 1, 2, 2, 4, 1), ((16, 16, 16), 1.3, 2, 1, 2, 2, 4, 2),
+             ((32, 32, 32), 1.5, 3, 1, 2, 2, 4, 3), ((48, 48, 48), 1.1, 6, 1, 2, 2, 4, 6),
+             ((24, 16, 32), 1.2, 7, 2, 2, 2, 4, 7)]
+    a = batched_tasks(slsf, ctx, orc, specs)
+    b = batched_tasks(slsf, ctx, orc, specs)
+    with ctx.session(a, 3) as ses:
+        for _ in range(3):
+            st = ses.step()
+        with pytest.raises(slsf.SlsfError) as e:
+            a[0].sweep(1)  # the session owns the task's device view
+        assert e.value.code == slsf.ERR_STATE
+        assert a[0].counters == (9, 9) and a[4].counters == (9, 18)
+    for _ in range(3):
+        ref = ctx.batch_run(b, 3)
+    for ta, tb in zip(a, b):
+        assert np.array_equal(ta.theta.view(np.uint32), tb.theta.view(np.uint32))
+        assert ta.counters == tb.counters
+        ba, ma = ta.bins()
+        bb, mb = tb.bins()
+        assert ma == mb and np.array_equal(ba, bb)
+    assert [s["accepted"] for s in st] == [s["accepted"] for s in ref]
+    a[0].sweep(1)  # usable again after close
