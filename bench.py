@@ -7,7 +7,7 @@ realisations x 16 temperatures uniformly spaced in [1.1, 1.5], L = 32 cubes,
 J_xy = 1.2, J_z(z) ~ U[0.5, 1.5] per realisation from its disorder seed, one
 Wolff update per sweep, every sweep after thermalization measured into 32
 bins (FP64 reductions).  A step is one persistent launch of S sweeps over all
-4096 replicas; the default W + K = 3 + 17 steps of S = 100 sweeps is the
+4096 replicas, replayed from a CUDA graph; the default W + K = 3 + 17 steps of S = 100 sweeps is the
 whole 2000-sweep job.  The state (512 MiB FP32) is larger than L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
@@ -429,10 +429,12 @@ def main():
         t.init_random()
         tasks.append(t)
     handles = ctx.handle_array(tasks)
+    # one step = one replay of a CUDA graph holding the persistent launch
+    session = ctx.session(tasks, S)
 
     # warm-up steps = thermalization sweeps
     for _ in range(args.warmup):
-        ctx.batch_run(tasks, S, handles=handles)
+        session.step()
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
@@ -447,11 +449,12 @@ def main():
     with torch.cuda.stream(stream):
         ev[0].record(stream)
         for k in range(args.steps):
-            ctx.batch_run(tasks, S, handles=handles)
+            session.step()
             ev[k + 1].record(stream)
     torch.cuda.synchronize(dev)
     launches = ctx.launches - launches0
     clk = clocks.stop()
+    session.close()
     step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     elapsed = sum(step_ms) / 1e3
     elapsed = max_over_ranks(elapsed, dist, dev)
