@@ -917,12 +917,12 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
             for (size_t k = lo; k < hi; ++k) run_grid_task(ctx, tasks[order[k]], ctx->h_views[k], st);
         } else if (c.kind == slsf::kKernelResident) {
             SLSF_CUDA(slsf::launch_resident(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
-                                            ctx->device, st, max_vs, max_rows, max_lz, c.threads));
+                                            ctx->device, st, max_vs, max_rows, max_lz, c.threads, nullptr));
             ctx->launches += 1;
         } else {
             SLSF_CUDA(slsf::launch_batched(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
                                            ctx->device, st, c.cluster, c.threads, max_vs, max_rows, max_lz,
-                                           max_plane, max_lx));
+                                           max_plane, max_lx, nullptr));
             ctx->launches += 1;
         }
         if (side >= 0) {
@@ -968,6 +968,7 @@ struct slsf_batch {
     unsigned long long* d_stats = nullptr;
     unsigned long long* h_stats = nullptr; /* pinned */
     unsigned int* d_queue = nullptr;
+    unsigned long long* d_counters = nullptr; /* [view][Metropolis, Wolff], advanced by the kernels */
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -978,6 +979,7 @@ static void batch_free(slsf_batch* b) {
     if (b->d_views) cudaFree(b->d_views);
     if (b->d_stats) cudaFree(b->d_stats);
     if (b->d_queue) cudaFree(b->d_queue);
+    if (b->d_counters) cudaFree(b->d_counters);
     if (b->h_stats) cudaFreeHost(b->h_stats);
     for (slsf_task* t : b->tasks)
         if (t && t->session == b) t->session = nullptr;
@@ -1023,6 +1025,13 @@ int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n
     if (e == cudaSuccess) e = cudaMalloc(&b->d_stats, 8 * slsf::kStatSlots * n);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, sizeof(unsigned int) * n_groups);
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_stats, 8 * slsf::kStatSlots * n);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counters, 16 * n);
+    std::vector<unsigned long long> counters(2 * n);
+    for (size_t k = 0; k < n; ++k) {
+        counters[2 * k] = tasks[order[k]]->metro_sweeps;
+        counters[2 * k + 1] = tasks[order[k]]->wolff_done;
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_counters, counters.data(), 16 * n, cudaMemcpyHostToDevice);
     std::vector<TaskView> views(n);
     for (size_t k = 0; k < n && e == cudaSuccess; ++k) {
         TaskView v = tasks[order[k]]->view();
@@ -1066,10 +1075,11 @@ int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n
         if (e == cudaSuccess) {
             if (c.kind == slsf::kKernelResident)
                 e = slsf::launch_resident(b->d_views + lo, (uint32_t)(hi - lo), n_sweeps, b->d_queue + q, ctx->device,
-                                          st, max_vs, max_rows, max_lz, c.threads);
+                                          st, max_vs, max_rows, max_lz, c.threads, b->d_counters + 2 * lo);
             else
                 e = slsf::launch_batched(b->d_views + lo, (uint32_t)(hi - lo), n_sweeps, b->d_queue + q, ctx->device,
-                                         st, c.cluster, c.threads, max_vs, max_rows, max_lz, max_plane, max_lx);
+                                         st, c.cluster, c.threads, max_vs, max_rows, max_lz, max_plane, max_lx,
+                                         b->d_counters + 2 * lo);
             ++launches;
         }
         if (e == cudaSuccess && side >= 0) {

@@ -89,13 +89,14 @@ void launch_gather(const double* const* src, uint32_t n, uint32_t per, double* d
 
 /* ---- batched persistent engine, one CTA per replica (kernel_resident.cu) ---- */
 bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);
-/* Runs n_sweeps sweeps of every view in `views_dev` (device array of n;
- * each view's Metropolis and Wolff counters are advanced in place);
- * `queue` is a zeroed device counter.  max_* are the largest volume, row
+/* Runs n_sweeps sweeps of every view in `views_dev` (device array of n);
+ * `queue` is a zeroed device counter.  With `counters` (2 per view, may be
+ * NULL) the Metropolis and Wolff counters come from there instead of the
+ * views and are advanced in place, so a replayed launch continues.  max_* are the largest volume, row
  * count (Ly Lz) and Lz over the views. */
-cudaError_t launch_resident(TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+cudaError_t launch_resident(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                             int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
-                            uint32_t threads);
+                            uint32_t threads, unsigned long long* counters);
 
 /* ---- batched persistent engine, one cluster per replica (kernel_cluster.cu) ---- */
 /* Whether a cluster of c CTAs (a power of two up to 16) holds one replica of
@@ -108,9 +109,10 @@ bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);
  * n, all needing the same cluster size) with a persistent grid of clusters;
  * `queue` is a zeroed device counter the kernel consumes.  max_* are the
  * largest per-CTA slab volume, slab row count, Lz, Lx Ly and Lx over the views. */
-cudaError_t launch_batched(TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                            int device, cudaStream_t s, uint32_t cluster, uint32_t threads, uint32_t max_vs,
-                           uint32_t max_rows, uint32_t max_lz, uint32_t max_plane, uint32_t max_lx);
+                           uint32_t max_rows, uint32_t max_lz, uint32_t max_plane, uint32_t max_lx,
+                           unsigned long long* counters);
 
 }  // namespace slsf
 

@@ -777,8 +777,8 @@ __device__ __forceinline__ void bin_cluster_sums(const TaskView& t, const Geo& g
 
 template <typename W>
 __global__ void __launch_bounds__(kBThreads, 1)
-    k_cluster(TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
-              Limits lim) {
+    k_cluster(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
+              Limits lim, unsigned long long* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[8 * 32];
     __shared__ double cred[kMaxCluster][8]; /* slab sums gathered in rank 0 */
@@ -807,7 +807,11 @@ __global__ void __launch_bounds__(kBThreads, 1)
         cluster.sync();
         const uint32_t item = s_item;
         if (item >= n) return;
-        const TaskView t = views[item];
+        TaskView t = views[item];
+        if (counters) { /* a replayed launch: the counters live in their own array */
+            t.metro_sweeps = counters[2 * item];
+            t.wolff_done = counters[2 * item + 1];
+        }
         const Geo g = make_geo(t, rank, csize);
         const uint32_t sweeps = t.sweeps ? t.sweeps : n_sweeps;
         if (threadIdx.x == 0) s_cluster = 0;
@@ -852,6 +856,13 @@ __global__ void __launch_bounds__(kBThreads, 1)
                              s_flags);
         }
         const uint64_t last = t.metro_sweeps + sweeps;
+        /* the counters advance on the device, so that a replayed launch
+         * (slsf_batch_open / slsf_batch_step) continues the streams; every
+         * CTA of the cluster read them before the first barrier of the item */
+        if (counters && rank == 0 && threadIdx.x == 0) {
+            counters[2 * item] = last;
+            counters[2 * item + 1] = t.wolff_done + (uint64_t)sweeps * t.wolff_steps;
+        }
         if (measuring && sweeps > 0 && last > t.thermalization) {
             double acc[8];
             fill_halo(g, s, rm, 2);
@@ -874,12 +885,6 @@ __global__ void __launch_bounds__(kBThreads, 1)
         }
         /* no CTA may start the next replica while a partner still reads its slab */
         cluster.sync();
-        /* the view's counters advance on the device, so that a replayed
-         * launch (slsf_batch_open / slsf_batch_step) continues the streams */
-        if (rank == 0 && threadIdx.x == 0) {
-            views[item].metro_sweeps = t.metro_sweeps + sweeps;
-            views[item].wolff_done = t.wolff_done + (uint64_t)sweeps * t.wolff_steps;
-        }
     }
 }
 
@@ -895,8 +900,9 @@ int max_dynamic_smem(int device) {
 }
 
 template <typename W>
-cudaError_t launch_w(TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
-                     cudaStream_t s, uint32_t cluster, uint32_t threads, const Limits& lim) {
+cudaError_t launch_w(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+                     cudaStream_t s, uint32_t cluster, uint32_t threads, const Limits& lim,
+                     unsigned long long* counters) {
     const size_t smem = smem_bytes(lim, sizeof(W));
     cudaError_t e = cudaFuncSetAttribute(k_cluster<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -922,7 +928,7 @@ cudaError_t launch_w(TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigne
     if (clusters < 1) return cudaErrorInvalidConfiguration;
     const uint32_t grid_clusters = std::min<uint32_t>(n, (uint32_t)clusters);
     cfg.gridDim = dim3(grid_clusters * cluster, 1, 1);
-    return cudaLaunchKernelEx(&cfg, k_cluster<W>, views_dev, n, n_sweeps, queue, lim);
+    return cudaLaunchKernelEx(&cfg, k_cluster<W>, views_dev, n, n_sweeps, queue, lim, counters);
 }
 
 }  // namespace
@@ -948,14 +954,15 @@ bool batched_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
     return batched_cluster_size(lx, ly, lz, device) != 0;
 }
 
-cudaError_t launch_batched(TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+cudaError_t launch_batched(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                            int device, cudaStream_t s, uint32_t cluster, uint32_t threads, uint32_t max_vs,
-                           uint32_t max_rows, uint32_t max_lz, uint32_t max_plane, uint32_t max_lx) {
+                           uint32_t max_rows, uint32_t max_lz, uint32_t max_plane, uint32_t max_lx,
+                           unsigned long long* counters) {
     (void)device;
     if (threads < 64 || threads > (uint32_t)kBThreads || threads % 32) return cudaErrorInvalidConfiguration;
     const Limits lim = {max_vs, max_rows, max_lz, max_plane / 2};
-    if (max_lx > 32) return launch_w<uint64_t>(views_dev, n, n_sweeps, queue, s, cluster, threads, lim);
-    return launch_w<uint32_t>(views_dev, n, n_sweeps, queue, s, cluster, threads, lim);
+    if (max_lx > 32) return launch_w<uint64_t>(views_dev, n, n_sweeps, queue, s, cluster, threads, lim, counters);
+    return launch_w<uint32_t>(views_dev, n, n_sweeps, queue, s, cluster, threads, lim, counters);
 }
 
 }  // namespace slsf

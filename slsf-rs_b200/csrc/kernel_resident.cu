@@ -494,8 +494,8 @@ __device__ __forceinline__ void measure(const Geo& g, const Smem& s, double (&ac
 
 
 __global__ void __launch_bounds__(kBThreads, 1)
-    k_resident(TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
-               uint32_t max_volume, uint32_t max_rows, uint32_t max_lz) {
+    k_resident(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
+               uint32_t max_volume, uint32_t max_rows, uint32_t max_lz, unsigned long long* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[8 * 32];
     __shared__ double bin_acc[kBinCols];
@@ -508,7 +508,11 @@ __global__ void __launch_bounds__(kBThreads, 1)
         __syncthreads();
         const uint32_t item = s_item;
         if (item >= n) return;
-        const TaskView t = views[item];
+        TaskView t = views[item];
+        if (counters) { /* a replayed launch: the counters live in their own array */
+            t.metro_sweeps = counters[2 * item];
+            t.wolff_done = counters[2 * item + 1];
+        }
         const Geo g = make_geo(t);
         Smem s = carve(smem_raw, max_volume, max_rows, max_lz);
         if (threadIdx.x == 0) {
@@ -549,6 +553,13 @@ __global__ void __launch_bounds__(kBThreads, 1)
                 wolff_update(t, g, s, t.wolff_done + (uint64_t)sw * t.wolff_steps + k, &s_cluster);
         }
         const uint64_t last = t.metro_sweeps + sweeps;
+        /* the counters advance on the device, so that a replayed launch
+         * (slsf_batch_open / slsf_batch_step) continues the streams; every
+         * thread read them before the first barrier of the item */
+        if (counters && threadIdx.x == 0) {
+            counters[2 * item] = last;
+            counters[2 * item + 1] = t.wolff_done + (uint64_t)sweeps * t.wolff_steps;
+        }
         if (measuring && sweeps > 0 && last > t.thermalization) {
             double acc[8];
             measure(g, s, acc, red);
@@ -565,10 +576,6 @@ __global__ void __launch_bounds__(kBThreads, 1)
             atomicAdd(&t.stats[kStatAccepted], (unsigned long long)s_accepted);
             atomicAdd(&t.stats[kStatClusterSites], (unsigned long long)s_cluster);
             atomicAdd(&t.stats[kStatClusters], (unsigned long long)sweeps * t.wolff_steps);
-            /* the view's counters advance on the device, so that a replayed
-             * launch (slsf_batch_open / slsf_batch_step) continues the streams */
-            views[item].metro_sweeps = t.metro_sweeps + sweeps;
-            views[item].wolff_done = t.wolff_done + (uint64_t)sweeps * t.wolff_steps;
         }
     }
 }
@@ -594,9 +601,9 @@ bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
     return smem_bytes((uint32_t)v, ly * lz, lz) <= (size_t)max_dynamic_smem(device);
 }
 
-cudaError_t launch_resident(TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+cudaError_t launch_resident(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                             int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
-                            uint32_t threads) {
+                            uint32_t threads, unsigned long long* counters) {
     if (threads < 32 || threads > (uint32_t)kBThreads || threads % 32) return cudaErrorInvalidConfiguration;
     const size_t smem = smem_bytes(max_volume, max_rows, max_lz);
     cudaError_t e = cudaFuncSetAttribute(k_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -608,7 +615,7 @@ cudaError_t launch_resident(TaskView* views_dev, uint32_t n, uint32_t n_sweeps, 
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const uint32_t grid = std::min<uint32_t>(n, (uint32_t)(sms * per_sm));
-    k_resident<<<grid, threads, smem, s>>>(views_dev, n, n_sweeps, queue, max_volume, max_rows, max_lz);
+    k_resident<<<grid, threads, smem, s>>>(views_dev, n, n_sweeps, queue, max_volume, max_rows, max_lz, counters);
     return cudaGetLastError();
 }
 
