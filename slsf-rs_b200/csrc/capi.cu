@@ -595,7 +595,7 @@ int slsf_task_wolff_step_debug(slsf_task* t, uint8_t* bonds, uint8_t* cluster, f
     uint32_t site[3] = {0, 0, 0};
     slsf::launch_wolff(t->view(), t->wolff_done, t->bonds, t->parent, (uint8_t*)d_cluster, t->ctx->stream, &phi_h,
                        site);
-    t->ctx->launches += 3;
+    t->ctx->launches += 4;
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && bonds)
         e = cudaMemcpyAsync(bonds, t->bonds, t->volume, cudaMemcpyDeviceToHost, t->ctx->stream);
@@ -604,6 +604,8 @@ int slsf_task_wolff_step_debug(slsf_task* t, uint8_t* bonds, uint8_t* cluster, f
     if (e == cudaSuccess) e = cudaStreamSynchronize(t->ctx->stream);
     if (d_cluster) t->ctx->pool.free(d_cluster, align256(t->volume));
     if (e != cudaSuccess) return cuda_error(e, "wolff step");
+    if (bonds) /* the bond bits only (the kernels mark tile roots in bit 3) */
+        for (uint32_t i = 0; i < t->volume; ++i) bonds[i] &= 7u;
     unsigned long long st[slsf::kStatSlots];
     if (int rc = read_stats(t, st)) return rc;
     t->wolff_done += 1;
@@ -631,7 +633,7 @@ int slsf_task_sweep(slsf_task* t, uint32_t n_sweeps, slsf_sweep_stats* stats) {
         for (uint32_t k = 0; k < t->wolff_steps; ++k) {
             slsf::launch_wolff(v, t->wolff_done, t->bonds, t->parent, nullptr, t->ctx->stream, nullptr, nullptr);
             t->wolff_done += 1;
-            t->ctx->launches += 3;
+            t->ctx->launches += 4;
         }
     }
     SLSF_CUDA(cudaGetLastError());
@@ -751,7 +753,7 @@ static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v, 
         for (uint32_t k = 0; k < t->wolff_steps; ++k) {
             slsf::launch_wolff(v, t->wolff_done + (uint64_t)sw * t->wolff_steps + k, t->bonds, t->parent, nullptr,
                                st, nullptr, nullptr);
-            ctx->launches += 3;
+            ctx->launches += 4;
         }
         const uint64_t done = sweep + 1;
         if (done > t->thermalization && t->n_bins) {

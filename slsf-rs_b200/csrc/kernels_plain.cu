@@ -7,11 +7,12 @@
  *                        (two same-colour sites)
  *   k_wolff_tiles        per-site +x/+y/+z bond activation of
  *   k_wolff_boundary     wolff_cluster_step_with_theta_scratch
- *   k_wolff_flip         (src/updates.rs:551-620): components inside
- *                        32x8x4 tiles by union-find in shared memory, the
+ *   k_wolff_compress     (src/updates.rs:551-620): components inside
+ *   k_wolff_flip         32x8x4 tiles by union-find in shared memory, the
  *                        bonds between tiles by a lock-free global
- *                        union-find over the tile roots, then reflect the
- *                        seed's component
+ *                        union-find over the tile roots, the tile roots
+ *                        pointed at their component's root, then reflect
+ *                        the seed's component
  *   k_measure            measure_theta_observables_with_scratch
  *                        (src/observables.rs:80-154), FP64 block sums, fixed
  *                        summation order (last block reduces the partials)
@@ -140,6 +141,9 @@ __device__ __forceinline__ bool uf_union(uint32_t* parent, uint32_t a, uint32_t 
 /* Wolff tiles: a CTA labels one tile of kTileX x kTileY x kTileZ sites. */
 constexpr uint32_t kTileX = 32, kTileY = 8, kTileZ = 4;
 constexpr uint32_t kTileSites = kTileX * kTileY * kTileZ;
+/* Bit 3 of a site's bond byte: the site is the root of its component inside
+ * its tile (bits 0-2 are the +x/+y/+z bonds). */
+constexpr uint8_t kTileRoot = 8;
 
 /* Local union-find in shared memory: hook the larger root under the smaller
  * with a CAS; bounded like the global one. */
@@ -236,49 +240,81 @@ __global__ void __launch_bounds__(kThreads)
         if (ax >= ex || ay >= ey || az >= ez) continue;
         const uint32_t r = tile_find(lpar, l, bd, &ok);
         const uint32_t rx = r % kTileX, ry = (r / kTileX) % kTileY, rz = r / (kTileX * kTileY);
-        parent[(x0 + ax) + lx * ((y0 + ay) + ly * (z0 + az))] = (x0 + rx) + lx * ((y0 + ry) + ly * (z0 + rz));
+        const uint32_t i = (x0 + ax) + lx * ((y0 + ay) + ly * (z0 + az));
+        parent[i] = (x0 + rx) + lx * ((y0 + ry) + ly * (z0 + rz));
+        if (r == l) bonds[i] = (uint8_t)(lbits[l] | kTileRoot); /* marks the tile's roots for k_wolff_compress */
     }
     if (!ok) atomicOr(&stats[kStatError], kErrUnionFindLimit);
 }
 
 /* The active bonds that leave a tile (the tile's last x, y or z, periodic
- * wraps included), joined in the global union-find over the tile roots. */
+ * wraps included), joined in the global union-find over the tile roots.  The
+ * bonds of one direction that a warp holds mostly join the same two tile
+ * components (a tile face crosses one or two components), so the lanes group
+ * them by their (tile root, tile root) pair and one lane per pair joins. */
 __global__ void __launch_bounds__(kThreads)
     k_wolff_boundary(const uint8_t* __restrict__ bonds, uint32_t lx, uint32_t ly, uint32_t lz,
                      uint32_t* parent, unsigned long long* stats, uint32_t limit) {
     const uint32_t volume = lx * ly * lz;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= volume) return;
-    const uint32_t bits = bonds[i];
-    if (!bits) return;
-    const uint32_t x = i % lx, row = i / lx, y = row % ly, z = row / ly;
-    const bool ex = (x % kTileX == kTileX - 1) || (x + 1 == lx);
-    const bool ey = (y % kTileY == kTileY - 1) || (y + 1 == ly);
-    const bool ez = (z % kTileZ == kTileZ - 1) || (z + 1 == lz);
-    if (!((ex && (bits & 1u)) || (ey && (bits & 2u)) || (ez && (bits & 4u)))) return;
+    const bool in = i < volume;
+    const uint32_t bits = in ? bonds[i] : 0u;
+    const uint32_t ii = in ? i : 0u;
+    const uint32_t x = ii % lx, row = ii / lx, y = row % ly, z = row / ly;
     const uint32_t plane = lx * ly;
+    const bool cross[3] = {(x % kTileX == kTileX - 1) || (x + 1 == lx), (y % kTileY == kTileY - 1) || (y + 1 == ly),
+                           (z % kTileZ == kTileZ - 1) || (z + 1 == lz)};
+    const uint32_t nb[3] = {(x + 1 == lx) ? ii + 1 - lx : ii + 1, (y + 1 == ly) ? ii + lx - plane : ii + lx,
+                            (z + 1 == lz) ? ii + plane - volume : ii + plane};
     const UfBounds bd = uf_bounds(volume, limit);
+    const uint32_t lane = threadIdx.x & 31u;
     bool ok = true;
-    if (ex && (bits & 1u)) ok &= uf_union(parent, i, (x + 1 == lx) ? i + 1 - lx : i + 1, bd);
-    if (ey && (bits & 2u)) ok &= uf_union(parent, i, (y + 1 == ly) ? i + lx - plane : i + lx, bd);
-    if (ez && (bits & 4u)) ok &= uf_union(parent, i, (z + 1 == lz) ? i + plane - volume : i + plane, bd);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const bool act = in && cross[d] && (bits & (1u << d));
+        if (!__any_sync(0xffffffffu, act)) continue;
+        uint32_t a = 0, b = 0;
+        if (act) {
+            a = parent[ii];
+            b = parent[nb[d]];
+        }
+        const unsigned long long key = act ? (((unsigned long long)a << 32) | b) : ~0ull;
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        if (act && lane == (uint32_t)(__ffs(grp) - 1) && a != b) ok &= uf_union(parent, a, b, bd);
+    }
     if (!ok) atomicOr(&stats[kStatError], kErrUnionFindLimit);
 }
 
+/* After the joins between tiles, every tile root points at its component's
+ * root (path compression from the roots only: the other sites point at a
+ * tile root, and nobody points at them). */
 __global__ void __launch_bounds__(kThreads)
-    k_wolff_flip(float* __restrict__ theta, uint32_t volume, uint32_t* parent, uint32_t seed_idx,
-                 float phi, unsigned long long* stats, uint8_t* __restrict__ cluster_out, uint32_t limit) {
-    const UfBounds bd = uf_bounds(volume, limit);
+    k_wolff_compress(const uint8_t* __restrict__ bonds, uint32_t volume, uint32_t* parent,
+                     unsigned long long* stats, uint32_t limit) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= volume || !(bonds[i] & kTileRoot)) return;
     bool ok = true;
+    const uint32_t r = uf_find(parent, i, uf_bounds(volume, limit), &ok);
+    if (!ok) {
+        atomicOr(&stats[kStatError], kErrUnionFindLimit);
+        return;
+    }
+    parent[i] = r;
+}
+
+/* Reflect the seed's component (src/updates.rs:602-617).  A site's parent is
+ * a tile root whose parent is the component's root, so two loads find it. */
+__global__ void __launch_bounds__(kThreads)
+    k_wolff_flip(float* __restrict__ theta, uint32_t volume, const uint32_t* __restrict__ parent, uint32_t seed_idx,
+                 float phi, unsigned long long* stats, uint8_t* __restrict__ cluster_out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t in = 0;
     if (i < volume) {
-        const uint32_t root = uf_find(parent, seed_idx, bd, &ok);
-        in = (uf_find(parent, i, bd, &ok) == root) ? 1u : 0u;
+        const uint32_t root = parent[parent[seed_idx]];
+        in = (parent[parent[i]] == root) ? 1u : 0u;
         if (in) theta[i] = slsf_reflect(theta[i], phi);
         if (cluster_out) cluster_out[i] = (uint8_t)in;
     }
-    if (!ok) atomicOr(&stats[kStatError], kErrUnionFindLimit);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) in += __shfl_down_sync(0xffffffffu, in, off);
     if ((threadIdx.x & 31) == 0 && in) atomicAdd(&stats[kStatClusterSites], (unsigned long long)in);
@@ -531,8 +567,8 @@ void launch_wolff(const TaskView& t, uint64_t counter, uint8_t* bonds, uint32_t*
     k_wolff_tiles<<<tiles, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, -2.0f * t.beta, phi,
                                              t.seed, counter, bonds, parent, t.stats, t.loop_limit);
     k_wolff_boundary<<<grid, kThreads, 0, s>>>(bonds, t.lx, t.ly, t.lz, parent, t.stats, t.loop_limit);
-    k_wolff_flip<<<grid, kThreads, 0, s>>>(t.theta, volume, parent, seed_idx, phi, t.stats, cluster_out,
-                                           t.loop_limit);
+    k_wolff_compress<<<grid, kThreads, 0, s>>>(bonds, volume, parent, t.stats, t.loop_limit);
+    k_wolff_flip<<<grid, kThreads, 0, s>>>(t.theta, volume, parent, seed_idx, phi, t.stats, cluster_out);
     if (phi_out) *phi_out = phi;
     if (seed_site) {
         seed_site[0] = x0;
