@@ -141,6 +141,7 @@ __device__ __forceinline__ bool uf_union(uint32_t* parent, uint32_t a, uint32_t 
 /* Wolff tiles: a CTA labels one tile of kTileX x kTileY x kTileZ sites. */
 constexpr uint32_t kTileX = 32, kTileY = 8, kTileZ = 4;
 constexpr uint32_t kTileSites = kTileX * kTileY * kTileZ;
+static_assert(kTileX == 32, "a tile row is one warp");
 /* Bit 3 of a site's bond byte: the site is the root of its component inside
  * its tile (bits 0-2 are the +x/+y/+z bonds). */
 constexpr uint8_t kTileRoot = 8;
@@ -222,15 +223,22 @@ __global__ void __launch_bounds__(kThreads)
             bonds[i] = (uint8_t)bits;
         }
         lbits[l] = (uint8_t)bits;
-        lpar[l] = l;
+        /* A warp holds one row of the tile (kTileX == 32 sites, lane = x):
+         * the sites joined along x form runs, and every site's parent is the
+         * first site of its run (the highest run start at or below its lane),
+         * so the x bonds inside the tile need no union. */
+        const unsigned xb = __ballot_sync(0xffffffffu, (bits & 1u) && ax + 1 < ex);
+        const unsigned starts = ~(xb << 1);
+        const uint32_t lane = l % kTileX;
+        const unsigned upto = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
+        lpar[l] = l - lane + (31u - __clz(starts & upto));
     }
     __syncthreads();
     bool ok = true;
     for (uint32_t l = threadIdx.x; l < kTileSites; l += blockDim.x) {
         const uint32_t bits = lbits[l];
         if (!bits) continue;
-        const uint32_t ax = l % kTileX, ay = (l / kTileX) % kTileY, az = l / (kTileX * kTileY);
-        if ((bits & 1u) && ax + 1 < ex) ok &= tile_union(lpar, l, l + 1, bu);
+        const uint32_t ay = (l / kTileX) % kTileY, az = l / (kTileX * kTileY);
         if ((bits & 2u) && ay + 1 < ey) ok &= tile_union(lpar, l, l + kTileX, bu);
         if ((bits & 4u) && az + 1 < ez) ok &= tile_union(lpar, l, l + kTileX * kTileY, bu);
     }
