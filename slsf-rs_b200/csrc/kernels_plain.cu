@@ -411,7 +411,7 @@ constexpr int kCorrCols = 32;
  * (the first rmax entries repeated after the last, so k + r needs no
  * modulo).  Lane c of a warp owns column c; warp w owns the kCorrLags
  * consecutive lags from 1 + w kCorrLags (then + nwarps kCorrLags, ...) and
- * slides a register window of those lags' partners along k: one new shared
+ * keeps those lags' partners in a register ring along k: one new shared
  * load per k for kCorrLags products.  Products are summed in FP32 over runs
  * of kCorrRun values of k, and the runs in FP64, in a fixed order. */
 constexpr uint32_t kCorrLags = 8;
@@ -449,15 +449,22 @@ __global__ void __launch_bounds__(kCorrThreads)
             tot[j] = 0.0;
             part[j] = 0.0f;
         }
-        for (uint32_t k = 0; k < n; ++k) {
-            const float2 a = tile[k * kCorrCols + lane];
+        /* k in groups of kCorrLags: the window is a ring, the partner of lag
+         * r0 + j at k = k0 + kk sits in slot (kk + j) % kCorrLags, and slot kk
+         * takes the next partner after k -- no register moves */
+        const uint32_t n8 = n - n % kCorrLags;
+        for (uint32_t k0 = 0; k0 < n8; k0 += kCorrLags) {
 #pragma unroll
-            for (uint32_t j = 0; j < kCorrLags; ++j) part[j] = __fmaf_rn(a.y, w[j].y, __fmaf_rn(a.x, w[j].x, part[j]));
-            /* slide: the partner of lag r0 + j at k + 1 is the one of lag r0 + j + 1 at k */
+            for (uint32_t kk = 0; kk < kCorrLags; ++kk) {
+                const float2 a = tile[(k0 + kk) * kCorrCols + lane];
 #pragma unroll
-            for (uint32_t j = 0; j + 1 < kCorrLags; ++j) w[j] = w[j + 1];
-            w[kCorrLags - 1] = tile[min(k + 1 + r0 + kCorrLags - 1, ext - 1) * kCorrCols + lane];
-            if ((k + 1) % kCorrRun == 0 || k + 1 == n) {
+                for (uint32_t j = 0; j < kCorrLags; ++j) {
+                    const float2 wj = w[(kk + j) % kCorrLags];
+                    part[j] = __fmaf_rn(a.y, wj.y, __fmaf_rn(a.x, wj.x, part[j]));
+                }
+                w[kk] = tile[min(k0 + kk + r0 + kCorrLags, ext - 1) * kCorrCols + lane];
+            }
+            if ((k0 + kCorrLags) % kCorrRun == 0) {
 #pragma unroll
                 for (uint32_t j = 0; j < kCorrLags; ++j) {
                     tot[j] += (double)part[j];
@@ -465,6 +472,18 @@ __global__ void __launch_bounds__(kCorrThreads)
                 }
             }
         }
+        /* the ring is aligned again (slot j = lag r0 + j); the last n % 8 k slide it */
+        for (uint32_t k = n8; k < n; ++k) {
+            const float2 a = tile[k * kCorrCols + lane];
+#pragma unroll
+            for (uint32_t j = 0; j < kCorrLags; ++j) part[j] = __fmaf_rn(a.y, w[j].y, __fmaf_rn(a.x, w[j].x, part[j]));
+            /* slide: the partner of lag r0 + j at k + 1 is the one of lag r0 + j + 1 at k */
+#pragma unroll
+            for (uint32_t j = 0; j + 1 < kCorrLags; ++j) w[j] = w[j + 1];
+            w[kCorrLags - 1] = tile[min(k + 1 + r0 + kCorrLags - 1, ext - 1) * kCorrCols + lane];
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kCorrLags; ++j) tot[j] += (double)part[j];
 #pragma unroll
         for (uint32_t j = 0; j < kCorrLags; ++j) {
             double v = tot[j];
