@@ -43,6 +43,20 @@ __global__ void __launch_bounds__(kThreads) k_init_random(float* __restrict__ th
     }
 }
 
+/* Adds a per-thread count to stats[slot] with one global atomic per block
+ * (warp sums, then a shared-memory sum): grid-wide kernels have tens of
+ * thousands of warps, and one same-address atomic per warp serialises. */
+__device__ __forceinline__ void block_count(uint32_t v, unsigned long long* stats, int slot) {
+    __shared__ unsigned int s_sum;
+    if (threadIdx.x == 0) s_sum = 0;
+    __syncthreads();
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&s_sum, v);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_sum) atomicAdd(&stats[slot], (unsigned long long)s_sum);
+}
+
 template <bool kRecord>
 __global__ void __launch_bounds__(kThreads)
     k_metro_colour(float* __restrict__ theta, const float* __restrict__ jxy,
@@ -83,9 +97,7 @@ __global__ void __launch_bounds__(kThreads)
             if (kRecord) record[s.idx] = acc ? 1 : 0;
         }
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) accepted += __shfl_down_sync(0xffffffffu, accepted, off);
-    if ((threadIdx.x & 31) == 0 && accepted) atomicAdd(&stats[kStatAccepted], (unsigned long long)accepted);
+    block_count(accepted, stats, kStatAccepted);
 }
 
 /* ---- Wolff: union-find with links from larger to smaller roots ---- */
@@ -301,13 +313,23 @@ __global__ void __launch_bounds__(kThreads)
                      unsigned long long* stats, uint32_t limit) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= volume || !(bonds[i] & kTileRoot)) return;
-    bool ok = true;
-    const uint32_t r = uf_find(parent, i, uf_bounds(volume, limit), &ok);
-    if (!ok) {
-        atomicOr(&stats[kStatError], kErrUnionFindLimit);
-        return;
+    /* A find without path splitting: the only writes in this kernel set a
+     * tile root's parent to its component's root, so every parent a thread
+     * reads leads to the same root (a split could write back a stale
+     * ancestor over a root already written). */
+    const volatile uint32_t* par = parent;
+    const uint32_t bound = uf_bounds(volume, limit).find;
+    uint32_t x = i;
+    for (uint32_t it = 0;; ++it) {
+        const uint32_t p = par[x];
+        if (p == x) break;
+        if (it >= bound) {
+            atomicOr(&stats[kStatError], kErrUnionFindLimit);
+            return;
+        }
+        x = p;
     }
-    parent[i] = r;
+    parent[i] = x;
 }
 
 /* Reflect the seed's component (src/updates.rs:602-617).  A site's parent is
@@ -323,9 +345,7 @@ __global__ void __launch_bounds__(kThreads)
         if (in) theta[i] = slsf_reflect(theta[i], phi);
         if (cluster_out) cluster_out[i] = (uint8_t)in;
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) in += __shfl_down_sync(0xffffffffu, in, off);
-    if ((threadIdx.x & 31) == 0 && in) atomicAdd(&stats[kStatClusterSites], (unsigned long long)in);
+    block_count(in, stats, kStatClusterSites);
 }
 
 /* ---- fused observables ---- */
