@@ -504,13 +504,15 @@ __device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Sme
     }
 }
 
-constexpr uint32_t kZSeg = 4; /* planes per column segment in growth stage Z */
+constexpr uint32_t kZSeg = 4;    /* planes per column segment in growth stage Z */
+constexpr uint32_t kZChain = 8;  /* slabs up to this many planes run stage Z as one chain per column */
 
 /* Growth stage Z: every column of the slab (the rows of one y) carries its
  * cluster bits along z through its bz words, forward and backward, fed
  * across the slab faces by the partner rows (for a one-CTA cluster the
- * partner is this CTA: the periodic wrap).  A column is cut into segments of
- * kZSeg planes, one thread each (lanes over consecutive columns, so shared
+ * partner is this CTA: the periodic wrap).  A slab of up to kZChain planes
+ * runs one chain per column; a deeper one is cut into segments of kZSeg
+ * planes, one thread each (lanes over consecutive columns, so shared
  * accesses are conflict-free): each segment runs its chain with no carry in,
  * publishes its carry out and the product of its links, then runs again
  * from the carry that the segments before it deliver, stopping where the
@@ -518,10 +520,41 @@ constexpr uint32_t kZSeg = 4; /* planes per column segment in growth stage Z */
  * dirty.  Returns nonzero if any row changed. */
 template <typename W>
 __device__ __forceinline__ int grow_z(const Geo& g, Smem<W>& s, const Remote<W>& rm) {
-    const uint32_t nseg = (g.nz + kZSeg - 1) / kZSeg;
-    const uint32_t n = nseg * g.ly;
     const uint32_t top = g.ly * (g.nz - 1);
     int changed = 0;
+    if (g.nz <= kZChain) {
+        /* A short slab: one thread runs its column's whole chain forward,
+         * then backward, with no barrier inside the stage. */
+        for (uint32_t y = threadIdx.x; y < g.ly; y += blockDim.x) {
+            W acc = rm.cl_dn[top + y] & rm.bz_dn[top + y];
+            for (uint32_t zl = 0; zl < g.nz; ++zl) {
+                const uint32_t r = y + g.ly * zl;
+                const W c = s.cl[r];
+                const W v = c | acc;
+                if (v != c) {
+                    s.cl[r] = v;
+                    s.dirty[r] = 1;
+                    changed = 1;
+                }
+                acc = v & s.bz[r];
+            }
+            acc = rm.cl_up[y] & s.bz[top + y];
+            for (uint32_t zl = g.nz; zl-- > 0;) {
+                const uint32_t r = y + g.ly * zl;
+                const W c = s.cl[r];
+                const W v = c | acc;
+                if (v != c) {
+                    s.cl[r] = v;
+                    s.dirty[r] = 1;
+                    changed = 1;
+                }
+                acc = zl > 0 ? (v & s.bz[r - g.ly]) : (W)0;
+            }
+        }
+        return changed;
+    }
+    const uint32_t nseg = (g.nz + kZSeg - 1) / kZSeg;
+    const uint32_t n = nseg * g.ly;
     /* forward: plane zl feeds plane zl + 1 through bz[zl] */
     for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
         const uint32_t j = slsf_fastdiv_div(t, g.div_ly), y = t - j * g.ly;
