@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     p.add_argument("--no-serve", action="store_true", help="skip the served-stream side figure")
     p.add_argument("--no-large", action="store_true", help="skip the L=256 large-lattice side figure")
+    p.add_argument("--no-tune", action="store_true",
+                   help="use the default kernel choice instead of the autotuner (profiling runs)")
     p.add_argument("--serve-tasks", type=int, default=4096, help="tasks of the served stream")
     p.add_argument("--serve-epoch", type=int, default=100, help="sweeps per server epoch")
     p.add_argument("--serve-only", action="store_true", help="run only the served stream (prints its own line)")
@@ -415,7 +417,8 @@ def main():
     ctx.set_stream(stream.cuda_stream)
 
     L, S = args.L, args.sweeps_per_step
-    choice = ctx.autotune((L, L, L))  # kernel, cluster and CTA size for this shape
+    # kernel, cluster and CTA size for this shape
+    choice = ctx.tune_get((L, L, L)) if args.no_tune else ctx.autotune((L, L, L))
     wl = workload(pkg, args.samples, args.temperatures, L, rank)
     n = len(wl)
     total_sweeps = (args.warmup + args.steps) * S
