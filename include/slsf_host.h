@@ -113,7 +113,9 @@ typedef struct slsf_request {
     const double* j_z;  /* [lz], copied at submission */
     uint32_t sweeps;         /* total sweeps */
     uint32_t thermalization; /* sweeps before the first measurement */
-    uint32_t n_bins;         /* bins of the measured sweeps */
+    uint32_t n_bins;         /* bins of the measured sweeps (used when binsize is 0) */
+    uint32_t binsize;        /* sweeps per bin; 0: measured sweeps / n_bins.  Only complete
+                                bins are kept (carlo drops a partial last bin). */
 } slsf_request;
 
 typedef struct slsf_result {

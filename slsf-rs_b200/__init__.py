@@ -445,18 +445,25 @@ def uniform_layer_disorder(lz: int, lo: float, hi: float, seed: int):
     return lo + (hi - lo) * splitmix64_uniforms(seed, lz)
 
 
-def _round_half_away(x: float) -> int:
-    """f64::round: halves round away from zero."""
+def _round_as_u64(x: float) -> int:
+    """`x.round() as u64`: halves round away from zero, then the cast
+    saturates (NaN and negatives to 0, past the range to 2^64 - 1)."""
     import math
 
-    return int(math.copysign(math.floor(abs(x) + 0.5), x))
+    if math.isnan(x) or x <= 0.0:
+        return 0
+    if math.isinf(x):
+        return _MASK64
+    f = math.floor(x)
+    return min(int(f) + (1 if x - f >= 0.5 else 0), _MASK64)
 
 
 def task_seed(base_seed: int, l_z: int, sample: int, temperature: float, delta_j_xy: float = 0.0,
               delta_j_z: float = 0.0) -> int:
-    """Run seed of a task (ThetaJobConfig::make_theta_tasks, src/model.rs:741-747)."""
-    return (base_seed + 100_000 * l_z + 1_000 * sample + _round_half_away(100.0 * temperature)
-            + _round_half_away(1_000.0 * delta_j_xy) * 10_000 + _round_half_away(1_000.0 * delta_j_z)) & _MASK64
+    """Run seed of a task (ThetaJobConfig::make_theta_tasks, src/model.rs:741-747);
+    the sums wrap modulo 2^64."""
+    return (base_seed + 100_000 * l_z + 1_000 * sample + _round_as_u64(100.0 * temperature)
+            + _round_as_u64(1_000.0 * delta_j_xy) * 10_000 + _round_as_u64(1_000.0 * delta_j_z)) & _MASK64
 
 
 def exported_symbols():
@@ -505,7 +512,8 @@ class Request(C.Structure):
     _fields_ = [("tag", C.c_uint64), ("lx", C.c_uint32), ("ly", C.c_uint32), ("lz", C.c_uint32),
                 ("temperature", C.c_double), ("proposal_width", C.c_double), ("wolff_steps", C.c_uint32),
                 ("seed", C.c_uint64), ("j_xy", C.POINTER(C.c_double)), ("j_z", C.POINTER(C.c_double)),
-                ("sweeps", C.c_uint32), ("thermalization", C.c_uint32), ("n_bins", C.c_uint32)]
+                ("sweeps", C.c_uint32), ("thermalization", C.c_uint32), ("n_bins", C.c_uint32),
+                ("binsize", C.c_uint32)]
 
 
 class Result(C.Structure):
@@ -649,12 +657,14 @@ class Server:
             pass
 
     def submit(self, tag, dims, temperature, seed, j_xy, j_z, sweeps, thermalization=0, n_bins=1,
-               proposal_width=np.pi, wolff_steps=1):
+               proposal_width=np.pi, wolff_steps=1, binsize=0):
+        """Queues a request; `sweeps` counts the thermalization sweeps too."""
         jx = np.ascontiguousarray(j_xy, np.float64)
         jz = np.ascontiguousarray(j_z, np.float64)
         r = Request(tag=tag, lx=dims[0], ly=dims[1], lz=dims[2], temperature=temperature,
                     proposal_width=proposal_width, wolff_steps=wolff_steps, seed=seed, j_xy=_ptr(jx, C.c_double),
-                    j_z=_ptr(jz, C.c_double), sweeps=sweeps, thermalization=thermalization, n_bins=n_bins)
+                    j_z=_ptr(jz, C.c_double), sweeps=sweeps, thermalization=thermalization, n_bins=n_bins,
+                    binsize=binsize)
         host_check(load_host().slsf_server_submit(self.h, C.byref(r)))
 
     def cancel(self, tag):

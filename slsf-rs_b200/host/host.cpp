@@ -13,6 +13,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdint>
 #include <cstring>
 #include <list>
 #include <mutex>
@@ -153,8 +154,14 @@ int slsf_estimates_from_bins(const double* bm, size_t nb, double volume, double 
 }
 
 uint64_t slsf_task_seed(uint64_t base, uint32_t l_z, uint32_t sample, double temperature, double djxy, double djz) {
-    /* f64::round rounds halves away from zero */
-    auto r = [](double x) { return (uint64_t)std::llround(x); };
+    /* f64::round rounds halves away from zero; `as u64` saturates (NaN and
+     * negatives to 0, values past the range to 2^64 - 1) */
+    auto r = [](double x) -> uint64_t {
+        const double v = std::round(x);
+        if (!(v > 0.0)) return 0;
+        if (v >= 18446744073709551616.0) return UINT64_MAX;
+        return (uint64_t)v;
+    };
     return base + 100000ull * l_z + 1000ull * sample + r(100.0 * temperature) + r(1000.0 * djxy) * 10000ull +
            r(1000.0 * djz);
 }
@@ -355,10 +362,16 @@ void admit(slsf_server* s) {
             if (s->cfg.max_active && n_active >= s->cfg.max_active) break;
             Pending& p = *it;
             const uint32_t measured = p.req.sweeps > p.req.thermalization ? p.req.sweeps - p.req.thermalization : 0;
-            const uint32_t n_bins = std::max<uint32_t>(
-                1, std::min<uint32_t>(p.req.n_bins ? p.req.n_bins : 1, std::max<uint32_t>(measured, 1)));
             /* complete bins only (carlo drops a partial last bin) */
-            const uint32_t binsize = std::max<uint32_t>(1, measured / n_bins);
+            uint32_t n_bins, binsize;
+            if (p.req.binsize) {
+                binsize = p.req.binsize;
+                n_bins = std::max<uint32_t>(1, measured / binsize);
+            } else {
+                n_bins = std::max<uint32_t>(
+                    1, std::min<uint32_t>(p.req.n_bins ? p.req.n_bins : 1, std::max<uint32_t>(measured, 1)));
+                binsize = std::max<uint32_t>(1, measured / n_bins);
+            }
             const uint64_t bytes = slsf_task_bytes(p.req.lx, p.req.ly, p.req.lz, n_bins);
             if (bytes > budget) {
                 /* can never fit: reject now */

@@ -1,0 +1,488 @@
+"""Job files for the B200 path: the reference's TOML job schema, its task
+expansion, and a runner that feeds the tasks to the batched kernels.
+
+The reference reads a job file into a `ThetaJobConfig` (src/model.rs:159-213
+for the schema, :552-637 for defaults and key aliases, :1033-1060 for
+durations) and expands it with `make_theta_tasks` (src/model.rs:697-810):
+every lattice shape x delta J_xy x delta J_z x temperature x sample becomes
+one task with disorder seed `base_seed + sample - 1`, its run seed from the
+seed formula and two-point layer couplings drawn J_xy first, then J_z, from
+FastRng(disorder_seed).  This module restates those steps; the seed formula
+and the disorder draw are the host library's (slsf_task_seed,
+slsf_task_couplings).
+
+`run_job` runs a rank's share of the tasks (task index modulo world size,
+ThetaJob::selected_tasks, src/model.rs:60-68):
+
+* tasks without correlation measurements go to the continuous-batching
+  server (batched persistent launches, bins kept on the device);
+* tasks that measure correlations (the reference's default: r_max = L/2) run
+  as groups through the batched kernels too, stopping every
+  `correlation_interval` measurements for the correlation functions of every
+  task of the group (ThetaModel::measure, src/model.rs:402-442).  The
+  trajectories are the ones the single-task path produces.
+
+The result has the reference's ThetaJobResult layout (src/model.rs:72-106:
+job_name, rank, world_size, tasks[] with task, observables{name: {mean,
+error}}, acceptance, measurements) and is written to
+`<output_dir>/<job file stem>.rank<r>.results.json`.
+
+    python slsf-rs_b200/jobs.py job.toml [--output-dir DIR] [--rank R --world-size N]
+"""
+from __future__ import annotations
+
+import dataclasses
+import importlib.util
+import json
+import math
+import os
+import re
+import sys
+from typing import Optional
+
+import numpy as np
+
+
+def _package():
+    """The package this file belongs to (importable by path: its directory
+    name is not a Python identifier)."""
+    if __package__:
+        return sys.modules[__package__]
+    name = "slsf_rs_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    here = os.path.dirname(os.path.abspath(__file__))
+    spec = importlib.util.spec_from_file_location(name, os.path.join(here, "__init__.py"),
+                                                  submodule_search_locations=[here])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+class JobError(ValueError):
+    """A job file or configuration the reference rejects (with its message)."""
+
+
+@dataclasses.dataclass
+class JobConfig:
+    """ThetaJobConfig with the reference's defaults (src/model.rs:519-546)."""
+
+    l: list = dataclasses.field(default_factory=lambda: list(range(4, 21)))
+    l_x: Optional[list] = None
+    l_y: Optional[list] = None
+    l_z: Optional[list] = None
+    temperatures: list = dataclasses.field(default_factory=lambda: [2.8, 2.9, 3.0, 3.1, 3.2, 3.3])
+    delta_j_z: list = dataclasses.field(default_factory=lambda: [0.0])
+    delta_j_xy: list = dataclasses.field(default_factory=lambda: [0.0])
+    samples: int = 16
+    base_seed: int = 20260414
+    j_xy: float = 1.0
+    j_z_mean: float = 0.1
+    sweeps: int = 20_000
+    thermalization: int = 5_000
+    binsize: int = 50
+    proposal_width: float = math.pi
+    wolff_steps: int = 1
+    correlation_rmax: Optional[list] = None
+    correlation_rmax_xy: Optional[list] = None
+    correlation_rmax_z: Optional[list] = None
+    correlation_interval: int = 1
+    run_time_s: int = 12 * 60 * 60
+    checkpoint_time_s: int = 30 * 60
+    job_name: str = "xy_theta_rust"
+    output_dir: Optional[str] = None
+
+
+def _u64(text: str, what: str, value: str) -> int:
+    """str::parse::<u64> (an optional '+', then decimal digits), with Rust's messages."""
+    if text == "":
+        raise JobError(f"failed to parse duration {what} in {value}: cannot parse integer from empty string")
+    if not re.fullmatch(r"\+?[0-9]+", text):
+        raise JobError(f"failed to parse duration {what} in {value}: invalid digit found in string")
+    return int(text)
+
+
+def parse_duration(value: str) -> int:
+    """`[D-][[HH:]MM:]SS` to seconds (parse_duration, src/model.rs:1033-1060)."""
+    days, rest = value.split("-", 1) if "-" in value else ("0", value)
+    d = _u64(days, "days", value)
+    parts = rest.split(":")
+    if len(parts) > 3:
+        raise JobError(f"{value} does not match [[HH:]MM:]SS")
+    nums = [_u64(p, "component", value) for p in parts]
+    h, m, s = ([0, 0] + nums)[-3:]
+    return d * 86400 + h * 3600 + m * 60 + s
+
+
+def _check_types(section: str, table: dict, kinds: dict):
+    """serde's type checks for the keys this schema knows (unknown keys are
+    ignored, as serde does without deny_unknown_fields)."""
+    for key, kind in kinds.items():
+        if key not in table:
+            continue
+        v = table[key]
+        if kind == "usize_list":
+            ok = isinstance(v, list) and all(isinstance(x, int) and not isinstance(x, bool) and x >= 0 for x in v)
+        elif kind == "f64_list":
+            ok = isinstance(v, list) and all(isinstance(x, (int, float)) and not isinstance(x, bool) for x in v)
+        elif kind == "usize":
+            ok = isinstance(v, int) and not isinstance(v, bool) and v >= 0
+        elif kind == "f64":
+            ok = isinstance(v, (int, float)) and not isinstance(v, bool)
+        elif kind == "bool":
+            ok = isinstance(v, bool)
+        else:
+            ok = isinstance(v, str)
+        if not ok:
+            raise JobError(f"invalid type for `{section}{key}`: expected {kind.replace('_list', ' list')}")
+
+
+_TOP = {"name": "str", "output_dir": "str", "output_file": "str", "merged_output_file": "str",
+        "measurement_dir": "str", "checkpoint_dir": "str", "scheduler_dir": "str", "checkpoint": "bool",
+        "run_time": "str", "checkpoint_time": "str"}
+_MODEL = {"l": "usize_list", "L": "usize_list", "l_x": "usize_list", "l_y": "usize_list", "l_z": "usize_list",
+          "temperatures": "f64_list", "T": "f64_list", "t": "f64_list", "delta_j_z": "f64_list", "djz": "f64_list",
+          "samples": "usize", "base_seed": "usize", "j_xy": "f64", "delta_j_xy": "f64_list", "djxy": "f64_list",
+          "j_z_mean": "f64", "j_z": "f64"}
+_RUN = {"sweeps": "usize", "thermalization": "usize", "binsize": "usize", "proposal_width": "f64",
+        "wolff_steps": "usize"}
+_MEASURE = {"corr_rmax": "usize_list", "corr_rmax_xy": "usize_list", "corr_rmax_z": "usize_list",
+            "corr_interval": "usize", "correlation_interval": "usize"}
+
+
+def config_from_toml(text: str) -> JobConfig:
+    """ThetaJobConfig::try_from_toml_spec (src/model.rs:568-637) with the
+    schema's aliases: L for l, T for temperatures, then t; djz, djxy and
+    j_z as fallbacks of delta_j_z, delta_j_xy and j_z_mean; corr_interval
+    for correlation_interval; corr_rmax as the default of corr_rmax_xy and
+    corr_rmax_z."""
+    import tomllib
+
+    try:
+        spec = tomllib.loads(text)
+    except tomllib.TOMLDecodeError as e:
+        raise JobError(str(e)) from None
+    _check_types("", spec, _TOP)
+    model, run, measure = spec.get("model"), spec.get("run"), spec.get("measure")
+    for name, table, kinds in (("model", model, _MODEL), ("run", run, _RUN), ("measure", measure, _MEASURE)):
+        if table is not None:
+            if not isinstance(table, dict):
+                raise JobError(f"invalid type for `{name}`: expected a table")
+            _check_types(name + ".", table, kinds)
+    for a, b in (("l", "L"), ("temperatures", "T")):
+        if model and a in model and b in model:
+            raise JobError(f"duplicate field `{a}`")
+    cfg = JobConfig()
+    if "name" in spec:
+        cfg.job_name = spec["name"]
+    cfg.output_dir = spec.get("output_dir")
+    if "run_time" in spec:
+        try:
+            cfg.run_time_s = parse_duration(spec["run_time"])
+        except JobError as e:
+            raise JobError(f"invalid run_time: {e}") from None
+    if "checkpoint_time" in spec:
+        try:
+            cfg.checkpoint_time_s = parse_duration(spec["checkpoint_time"])
+        except JobError as e:
+            raise JobError(f"invalid checkpoint_time: {e}") from None
+
+    def first(d, *keys):
+        for k in keys:
+            if k in d:
+                return d[k]
+        return None
+
+    if model is not None:
+        if (v := first(model, "l", "L")) is not None:
+            cfg.l = list(v)
+        cfg.l_x, cfg.l_y, cfg.l_z = model.get("l_x"), model.get("l_y"), model.get("l_z")
+        if (v := first(model, "temperatures", "T", "t")) is not None:
+            cfg.temperatures = [float(x) for x in v]
+        if (v := first(model, "delta_j_z", "djz")) is not None:
+            cfg.delta_j_z = [float(x) for x in v]
+        if (v := first(model, "delta_j_xy", "djxy")) is not None:
+            cfg.delta_j_xy = [float(x) for x in v]
+        if "samples" in model:
+            cfg.samples = model["samples"]
+        if "base_seed" in model:
+            cfg.base_seed = model["base_seed"]
+        if "j_xy" in model:
+            cfg.j_xy = float(model["j_xy"])
+        if (v := first(model, "j_z_mean", "j_z")) is not None:
+            cfg.j_z_mean = float(v)
+    if run is not None:
+        for key in ("sweeps", "thermalization", "binsize", "wolff_steps"):
+            if key in run:
+                setattr(cfg, key, run[key])
+        if "proposal_width" in run:
+            cfg.proposal_width = float(run["proposal_width"])
+    if measure is not None:
+        cfg.correlation_rmax = measure.get("corr_rmax")
+        cfg.correlation_rmax_xy = measure.get("corr_rmax_xy", cfg.correlation_rmax)
+        cfg.correlation_rmax_z = measure.get("corr_rmax_z", cfg.correlation_rmax)
+        if (v := first(measure, "correlation_interval", "corr_interval")) is not None:
+            cfg.correlation_interval = v
+    return cfg
+
+
+def load_job(path: str) -> JobConfig:
+    with open(path, encoding="utf-8") as f:
+        return config_from_toml(f.read())
+
+
+def lattice_specs(cfg: JobConfig):
+    """(l_x, l_y, l_z, l) per lattice (ThetaJobConfig::lattice_specs,
+    src/model.rs:812-828): cubic from `l`, else the product of the per-axis
+    lists (an absent list falls back to `l`) with l = l_z."""
+    if cfg.l_x is None and cfg.l_y is None and cfg.l_z is None:
+        return [(l, l, l, l) for l in cfg.l]
+    xs = cfg.l_x if cfg.l_x is not None else cfg.l
+    ys = cfg.l_y if cfg.l_y is not None else cfg.l
+    zs = cfg.l_z if cfg.l_z is not None else cfg.l
+    return [(x, y, z, z) for x in xs for y in ys for z in zs]
+
+
+def make_tasks(cfg: JobConfig):
+    """make_theta_tasks (src/model.rs:697-810): the ThetaTask records, in the
+    reference's order, with its validation messages."""
+    pkg = _package()
+    specs = lattice_specs(cfg)
+    if not specs:
+        raise JobError("at least one lattice size must be configured")
+    for name, values in (("corr_rmax", cfg.correlation_rmax), ("corr_rmax_xy", cfg.correlation_rmax_xy),
+                         ("corr_rmax_z", cfg.correlation_rmax_z)):
+        if values is not None and len(values) != len(specs):
+            raise JobError(f"{name} must contain exactly one value per lattice size: expected {len(specs)}, "
+                           f"got {len(values)}")
+    if not cfg.temperatures:
+        raise JobError("at least one temperature must be configured")
+    if not cfg.delta_j_xy or not cfg.delta_j_z:
+        raise JobError("delta_j_xy and delta_j_z must not be empty")
+    if cfg.samples == 0:
+        raise JobError("samples must be positive")
+    if cfg.binsize == 0:
+        raise JobError("binsize must be positive")
+    if cfg.correlation_interval == 0:
+        raise JobError("correlation_interval must be positive")
+    if cfg.sweeps < cfg.binsize:
+        raise JobError("sweeps must be at least binsize")
+    host = pkg.load_host()
+    tasks = []
+    for li, (lx, ly, lz, l) in enumerate(specs):
+        for djxy in cfg.delta_j_xy:
+            for djz in cfg.delta_j_z:
+                for T in cfg.temperatures:
+                    for sample in range(1, cfg.samples + 1):
+                        dseed = cfg.base_seed + sample - 1
+                        seed = int(host.slsf_task_seed(cfg.base_seed, lz, sample, T, djxy, djz))
+                        desc = pkg.theta_task((lx, ly, lz), T, cfg.sweeps, cfg.thermalization, cfg.binsize, seed,
+                                              disorder_seed=dseed, j_xy=cfg.j_xy, delta_j_xy=djxy,
+                                              j_z_mean=cfg.j_z_mean, delta_j_z=djz)
+                        try:
+                            jx, jz = pkg.task_couplings(desc)
+                        except pkg.SlsfError as e:
+                            raise JobError(str(e)) from None
+                        tasks.append({
+                            "name": f"L{lx}x{ly}x{lz}_T{T:.6f}_dJxy{djxy:.6f}_dJz{djz:.6f}_sample{sample}",
+                            "l": l, "l_x": lx, "l_y": ly, "l_z": lz, "temperature": T, "j_xy": cfg.j_xy,
+                            "delta_j_xy": djxy, "j_z_mean": cfg.j_z_mean, "delta_j_z": djz,
+                            "disorder_seed": dseed, "seed": seed, "sample": sample, "sweeps": cfg.sweeps,
+                            "thermalization": cfg.thermalization, "binsize": cfg.binsize,
+                            "proposal_width": cfg.proposal_width, "wolff_steps": cfg.wolff_steps,
+                            "correlation_rmax": (cfg.correlation_rmax[li] if cfg.correlation_rmax is not None
+                                                 else lz // 2),
+                            "correlation_rmax_xy": (cfg.correlation_rmax_xy[li]
+                                                    if cfg.correlation_rmax_xy is not None else min(lx, ly) // 2),
+                            "correlation_rmax_z": (cfg.correlation_rmax_z[li] if cfg.correlation_rmax_z is not None
+                                                   else lz // 2),
+                            "correlation_interval": cfg.correlation_interval,
+                            "j_xy_array": jx.tolist(), "j_z_array": jz.tolist(),
+                        })
+    return tasks
+
+
+def selected(n_tasks: int, rank: int, world_size: int):
+    """Task indices of one rank (ThetaJob::selected_tasks, src/model.rs:60-68)."""
+    return [k for k in range(n_tasks) if world_size == 1 or k % world_size == rank]
+
+
+def measures_correlations(task) -> bool:
+    """ThetaModel::measure's condition (src/model.rs:410)."""
+    return task["correlation_rmax_xy"] > 0 or task["correlation_rmax_z"] > 0
+
+
+def corr_names(lz, rxy, rz):
+    """Observable names of one correlation measurement, in ThetaModel::measure's
+    order (src/model.rs:420-437); r counts from 1, z from 0."""
+    names = [f"CorrX_r{r}" for r in range(1, rxy + 1)] + [f"CorrY_r{r}" for r in range(1, rxy + 1)]
+    names += [f"CorrXY_r{r}" for r in range(1, rxy + 1)]
+    names += [f"CorrXY_z{z}_r{r}" for z in range(lz) for r in range(1, rxy + 1)]
+    names += [f"CorrZ_r{r}" for r in range(1, rz + 1)]
+    return names
+
+
+def _observables(est: dict, corr: Optional[dict] = None):
+    out = {k: {"mean": v[0], "error": v[1]} for k, v in est.items() if isinstance(v, tuple)}
+    for name, (mean, err) in (corr or {}).items():
+        out[name] = {"mean": mean, "error": err}
+    return dict(sorted(out.items()))
+
+
+def _run_served(pkg, ctx, tasks, epoch_sweeps):
+    """Tasks without correlations through the server: {task index: estimates}."""
+    names = {k: t["name"] for k, t in tasks}
+    srv = pkg.Server(ctx, epoch_sweeps=epoch_sweeps)
+    out = {}
+    try:
+        for k, t in tasks:
+            srv.submit(k, (t["l_x"], t["l_y"], t["l_z"]), t["temperature"], t["seed"], t["j_xy_array"],
+                       t["j_z_array"], t["thermalization"] + t["sweeps"], thermalization=t["thermalization"],
+                       proposal_width=t["proposal_width"], wolff_steps=t["wolff_steps"], binsize=t["binsize"])
+        srv.start()
+        srv.wait_idle(365 * 86400.0)
+        srv.stop()
+        for r in srv.poll(len(tasks) + 16):
+            if r["status"] != pkg.OK:
+                raise pkg.SlsfError(r["status"], f"task {names[r['tag']]}: {r['message']}")
+            out[r["tag"]] = r["est"]
+    finally:
+        srv.close()
+    return out
+
+
+def _run_correlated(pkg, ctx, group):
+    """One group of tasks sharing (thermalization, sweeps, correlation_interval)
+    through the batched kernels: thermalization, then per correlation
+    measurement m (m % interval == 0) the sweeps up to it and the correlation
+    functions of every task; the bins come from the device.  Each correlation
+    observable's series is binned with the task's bin size
+    (BinnedEstimate::from_samples; fewer samples than a bin make one bin)."""
+    import ctypes as C
+
+    t0 = group[0][1]
+    therm, sweeps, interval = t0["thermalization"], t0["sweeps"], t0["correlation_interval"]
+    objs, series, radii = [], [], []
+    try:
+        for _, t in group:
+            o = pkg.Task(ctx, (t["l_x"], t["l_y"], t["l_z"]), t["j_xy_array"], t["j_z_array"], t["temperature"],
+                         proposal_width=t["proposal_width"], wolff_steps=t["wolff_steps"], seed=t["seed"],
+                         thermalization=therm, binsize=t["binsize"], n_bins=t["sweeps"] // t["binsize"])
+            o.init_random()
+            objs.append(o)
+            radii.append((min(t["correlation_rmax_xy"], t["l_x"] // 2, t["l_y"] // 2),
+                          min(t["correlation_rmax_z"], t["l_z"] // 2)))
+            series.append([])
+        handles = ctx.handle_array(objs)
+        accepted = np.zeros(len(objs))
+
+        def advance(n):
+            if n:
+                for i, s in enumerate(ctx.batch_run(objs, n, handles)):
+                    accepted[i] += s["accepted"]
+
+        advance(therm)
+        done = 0
+        for m in range(0, sweeps, interval):
+            advance(m + 1 - done)
+            done = m + 1
+            for i, o in enumerate(objs):
+                c = o.correlations(*radii[i])
+                series[i].append(np.concatenate([c["corr_x"], c["corr_y"], c["corr_xy"],
+                                                 c["corr_xy_by_z"].reshape(-1), c["corr_z"]]))
+        advance(sweeps - done)
+        host = pkg.load_host()
+        out = []
+        for i, ((_, t), o) in enumerate(zip(group, objs)):
+            volume = float(t["l_x"] * t["l_y"] * t["l_z"])
+            bins, meas = o.bins()
+            b = np.ascontiguousarray(bins)
+            e = pkg.Estimates()
+            pkg.host_check(host.slsf_estimates_from_bins(b.ctypes.data_as(C.POINTER(C.c_double)), len(b), volume,
+                                                         1.0 / t["temperature"], C.byref(e)))
+            est = e.as_dict()
+            est["measurements"] = meas
+            est["acceptance"] = accepted[i] / (volume * (therm + sweeps))
+            s = np.array(series[i])
+            corr = {}
+            for j, name in enumerate(corr_names(t["l_z"], *radii[i])):
+                r = pkg.binned_estimate(s[:, j], min(t["binsize"], len(s)))
+                corr[name] = (r["mean"], r["stderr"])
+            out.append((est, corr))
+        return out
+    finally:
+        for o in objs:
+            o.close()
+
+
+def run_job(ctx, cfg: JobConfig, rank: int = 0, world_size: int = 1, epoch_sweeps: int = 100, tasks=None,
+            group_size: int = 1024):
+    """A rank's share of the job; returns the ThetaJobResult record."""
+    pkg = _package()
+    tasks = tasks if tasks is not None else make_tasks(cfg)
+    mine = [(k, tasks[k]) for k in selected(len(tasks), rank, world_size)]
+    served = [(k, t) for k, t in mine if not measures_correlations(t)]
+    est = _run_served(pkg, ctx, served, epoch_sweeps) if served else {}
+    corr = {}
+    groups = {}
+    for k, t in mine:
+        if measures_correlations(t):
+            groups.setdefault((t["thermalization"], t["sweeps"], t["correlation_interval"]), []).append((k, t))
+    for members in groups.values():
+        for lo in range(0, len(members), group_size):
+            chunk = members[lo: lo + group_size]
+            for (k, _), (e, c) in zip(chunk, _run_correlated(pkg, ctx, chunk)):
+                est[k], corr[k] = e, c
+    out = []
+    for k, t in mine:
+        e = est[k]
+        rec = {"task": t}
+        if k:
+            rec["task_index"] = k  # omitted when zero, as the reference's serializer does
+        rec.update(observables=_observables(e, corr.get(k)), acceptance=e["acceptance"],
+                   measurements=int(e["measurements"]))
+        out.append(rec)
+    return {"job_name": cfg.job_name, "rank": rank, "world_size": world_size, "tasks": out}
+
+
+def result_path(cfg: JobConfig, rank: int, output_dir: Optional[str] = None) -> str:
+    """`<dir>/<file name of job_name>.rank<r>.results.json`
+    (rank_result_path_with_options, src/model.rs:948-959): the directory is
+    the given one, else the job file's output_dir, else $XY_OUTPUT_DIR, else
+    the job name's parent directory, else results/."""
+    d = output_dir or cfg.output_dir or os.environ.get("XY_OUTPUT_DIR")
+    if not d:
+        d = os.path.dirname(cfg.job_name) or "results"
+    return os.path.join(d, f"{os.path.basename(cfg.job_name) or cfg.job_name}.rank{rank}.results.json")
+
+
+def write_result(result: dict, path: str) -> str:
+    os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+    with open(path, "w", encoding="utf-8") as f:
+        json.dump(result, f, indent=2)
+    return path
+
+
+def main(argv=None):
+    import argparse
+
+    p = argparse.ArgumentParser(description="Run a theta job file (the reference's TOML schema) on the B200 path.")
+    p.add_argument("job", help="TOML job file")
+    p.add_argument("--output-dir")
+    p.add_argument("--rank", type=int, default=int(os.environ.get("RANK", 0)))
+    p.add_argument("--world-size", type=int, default=int(os.environ.get("WORLD_SIZE", 1)))
+    p.add_argument("--device", type=int, default=int(os.environ.get("LOCAL_RANK", 0)))
+    p.add_argument("--epoch-sweeps", type=int, default=100)
+    args = p.parse_args(argv)
+    cfg = load_job(args.job)
+    pkg = _package()
+    with pkg.Context(args.device) as ctx:
+        res = run_job(ctx, cfg, args.rank, args.world_size, args.epoch_sweeps)
+    path = write_result(res, result_path(cfg, args.rank, args.output_dir))
+    print(f"{len(res['tasks'])} tasks -> {path}")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
