@@ -231,10 +231,30 @@ int slsf_task_measure(slsf_task* task, slsf_observables* out);
 /* Replaces measure_theta_correlations_with_scratch (src/observables.rs:166-265)
  * for explicit rmax values (clamped to L/2 as at :177-181).  Outputs (any may
  * be NULL): corr_x, corr_y, corr_xy [rmax_xy], corr_xy_by_z [lz][rmax_xy],
- * corr_z [rmax_z]. */
+ * corr_z [rmax_z].  Blocks until the values are on the host. */
 int slsf_task_correlations(slsf_task* task, uint32_t rmax_xy, uint32_t rmax_z, double* corr_x,
                            double* corr_y, double* corr_xy, double* corr_xy_by_z,
                            double* corr_z);
+
+/* Correlation measurements binned on the device, for ThetaModel::measure's
+ * correlation observables (src/model.rs:410-438).  slsf_task_corr_setup
+ * gives the task radii (clamped as slsf_task_correlations clamps them; both
+ * 0 turns the measurements off and frees the bins), a bin size and n_bins
+ * rows of bin sums, and resets the measurement count.  One measurement
+ * (slsf_batch_correlations) produces *n_values values in the order
+ *   CorrX_r (r = 1..R), CorrY_r, CorrXY_r, CorrXY_z{z}_r (z-major), CorrZ_r (r = 1..R_z)
+ * with R and R_z the clamped radii, n_values = 3 R + L_z R + R_z, and adds
+ * them into row count / binsize (rows past n_bins are not kept). */
+int slsf_task_corr_setup(slsf_task* task, uint32_t rmax_xy, uint32_t rmax_z, uint32_t binsize, uint32_t n_bins,
+                         size_t* n_values);
+/* The first n_rows rows of bin means ([n_rows][n_values]) and the number of
+ * correlation measurements taken (either output may be NULL).  Blocks. */
+int slsf_task_corr_bins(const slsf_task* task, double* bin_means, size_t n_rows, uint64_t* count);
+/* One correlation measurement of every task (each set up with
+ * slsf_task_corr_setup) in two launches for the whole batch, queued on the
+ * context's stream after the work already queued there (a batched run's
+ * sweeps included); does not wait for it.  Tasks may differ in size. */
+int slsf_batch_correlations(slsf_ctx* ctx, slsf_task* const* tasks, size_t n_tasks);
 
 /* Per-task bin accumulators of the batched engine: n_bins rows of
  * SLSF_BIN_COLS bin means, and the number of measurements taken so far. */

@@ -106,6 +106,9 @@ SIGNATURES = {
     "slsf_task_measure": (C.c_int, [_P, C.POINTER(Observables)]),
     "slsf_task_correlations": (C.c_int, [_P, C.c_uint32, C.c_uint32, _F64P, _F64P, _F64P, _F64P, _F64P]),
     "slsf_task_get_bins": (C.c_int, [_P, _F64P, C.c_size_t, _U64P]),
+    "slsf_task_corr_setup": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_size_t)]),
+    "slsf_task_corr_bins": (C.c_int, [_P, _F64P, C.c_size_t, _U64P]),
+    "slsf_batch_correlations": (C.c_int, [_P, C.POINTER(_P), C.c_size_t]),
     "slsf_task_reset_bins": (C.c_int, [_P]),
     "slsf_batch_run": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_uint32, C.POINTER(SweepStats)]),
     "slsf_batch_get_bins": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_size_t, _F64P, _U64P]),
@@ -237,6 +240,12 @@ class Context:
         check(load().slsf_batch_run(self.h, arr, len(tasks), n_sweeps, stats))
         return [s.as_dict() for s in stats]
 
+    def batch_correlations(self, tasks, handles=None):
+        """One correlation measurement of every task into its device bins
+        (queued on the context's stream; returns without waiting)."""
+        arr = handles if handles is not None else self.handle_array(tasks)
+        check(load().slsf_batch_correlations(self.h, arr, len(tasks)))
+
     def session(self, tasks, n_sweeps):
         """A batch session: one captured step of n_sweeps sweeps, replayed by step()."""
         return BatchSession(self, tasks, n_sweeps)
@@ -323,6 +332,7 @@ class Task:
         self.h = h
         self.ctx = ctx
         self.n_bins = n_bins
+        self.corr_n_values = self.corr_n_bins = 0
         ctx._tasks.add(self)
 
     def close(self):
@@ -410,6 +420,22 @@ class Task:
         check(load().slsf_task_correlations(self.h, rmax_xy, rmax_z, f(cx), f(cy), f(cxy), f(cbz), f(cz)))
         return {"corr_x": cx[:rxy], "corr_y": cy[:rxy], "corr_xy": cxy[:rxy],
                 "corr_xy_by_z": cbz[: lz * rxy].reshape(lz, rxy), "corr_z": cz[:rz]}
+
+    def corr_setup(self, rmax_xy, rmax_z, binsize, n_bins):
+        """Correlation bins on the device (slsf_task_corr_setup); returns the
+        number of values one correlation measurement produces."""
+        nv = C.c_size_t()
+        check(load().slsf_task_corr_setup(self.h, rmax_xy, rmax_z, binsize, n_bins, C.byref(nv)))
+        self.corr_n_values, self.corr_n_bins = nv.value, n_bins
+        return nv.value
+
+    def corr_bins(self, n_rows=None):
+        """(bin means [n_rows][values], correlation measurements so far)."""
+        n_rows = self.corr_n_bins if n_rows is None else n_rows
+        out = np.zeros((max(n_rows, 1), max(self.corr_n_values, 1)))
+        m = C.c_uint64()
+        check(load().slsf_task_corr_bins(self.h, _ptr(out, C.c_double), n_rows, C.byref(m)))
+        return out[:n_rows, : self.corr_n_values], m.value
 
     def bins(self):
         out = np.zeros((max(self.n_bins, 1), BIN_COLS))

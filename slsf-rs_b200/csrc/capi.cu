@@ -22,6 +22,7 @@
 #include <cstring>
 #include <string>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/slsf_gpu.h"
@@ -59,6 +60,7 @@ namespace {
 const char* kErrTemperature = "temperature T must be positive and finite";
 const char* kErrWidth = "proposal_width must be nonnegative and finite";
 const char* kErrEven = "red-black Metropolis sweep requires even lattice dimensions";
+const char* kErrCorrLong = "correlation lines plus lags longer than 775 sites are not supported";
 
 bool temperature_ok(double t) { return t > 0.0 && std::isfinite(t); }
 bool width_ok(double w) { return w >= 0.0 && std::isfinite(w); }
@@ -139,6 +141,12 @@ struct slsf_ctx {
     double* d_bin_out = nullptr;
     double* h_bin_out = nullptr; /* pinned */
     size_t gather_tasks_cap = 0, gather_doubles_cap = 0;
+    /* task table of slsf_batch_correlations; the pinned copy is rewritten
+     * only after the event says its last upload has been read */
+    slsf::CorrTask* d_corr = nullptr;
+    slsf::CorrTask* h_corr = nullptr; /* pinned */
+    size_t corr_cap = 0;
+    cudaEvent_t corr_uploaded = nullptr;
 };
 
 struct slsf_task {
@@ -164,6 +172,15 @@ struct slsf_task {
     unsigned long long* stats = nullptr;
     double* bins = nullptr;
     slsf_batch* session = nullptr; /* open batch session holding the task's device view */
+    /* correlation bins (slsf_task_corr_setup): one pool block holding the
+     * launch scratch, the bin sums and the device measurement count */
+    void* corr_block = nullptr;
+    uint64_t corr_bytes = 0;
+    uint32_t corr_rxy = 0, corr_rz = 0, corr_binsize = 1, corr_n_bins = 0;
+    uint64_t corr_count = 0; /* host mirror of *corr_count_dev */
+    double* corr_partial = nullptr;
+    double* corr_bins = nullptr;
+    unsigned long long* corr_count_dev = nullptr;
 
     TaskView view() const {
         TaskView v;
@@ -360,9 +377,11 @@ int slsf_ctx_destroy(slsf_ctx* ctx) {
     void* dev[] = {ctx->d_views, ctx->d_batch_stats, ctx->d_queue, (void*)ctx->d_bin_src, ctx->d_bin_out};
     for (void* p : dev)
         if (p) cudaFree(p);
-    void* host[] = {ctx->h_views, ctx->h_batch_stats, (void*)ctx->h_bin_src, ctx->h_bin_out};
+    if (ctx->d_corr) cudaFree(ctx->d_corr);
+    void* host[] = {ctx->h_views, ctx->h_batch_stats, (void*)ctx->h_bin_src, ctx->h_bin_out, ctx->h_corr};
     for (void* p : host)
         if (p) cudaFreeHost(p);
+    if (ctx->corr_uploaded) cudaEventDestroy(ctx->corr_uploaded);
     ctx->pool.release();
     destroy_streams(ctx);
     delete ctx;
@@ -475,6 +494,10 @@ int slsf_task_destroy(slsf_task* t) {
     cudaSetDevice(ctx->device);
     /* Work queued on the stream may still use the block. */
     cudaStreamSynchronize(ctx->stream);
+    if (t->corr_block) {
+        ctx->pool.free(t->corr_block, t->corr_bytes);
+        ctx->used -= t->corr_bytes;
+    }
     ctx->pool.free(t->block, t->bytes);
     ctx->used -= t->bytes;
     ctx->live_tasks -= 1;
@@ -677,43 +700,155 @@ int slsf_task_correlations(slsf_task* t, uint32_t rmax_xy, uint32_t rmax_z, doub
     rmax_xy = std::min(std::min(rmax_xy, t->lx / 2), t->ly / 2);
     rmax_z = std::min(rmax_z, t->lz / 2);
     if (rmax_xy == 0 && rmax_z == 0) return SLSF_OK;
-    if (slsf::corr_tile_bytes(std::max(t->ly + rmax_xy, t->lz + rmax_z)) > 200 * 1024)
-        return set_error(SLSF_ERR_INVALID, "correlation lines plus lags longer than 800 sites are not supported");
+    if (!slsf::corr_supports(t->lx, t->ly, t->lz, rmax_xy, rmax_z)) return set_error(SLSF_ERR_INVALID, kErrCorrLong);
     if (int rc = bind_device(t->ctx)) return rc;
-    const size_t work_n = slsf::correlation_work_doubles(t->lx, t->ly, t->lz, rmax_xy, rmax_z);
-    const size_t nsx = (size_t)t->lz * rmax_xy, nsz = rmax_z;
-    const size_t bytes = align256(8 * (work_n + 2 * nsx + nsz + 1));
+    slsf_ctx* ctx = t->ctx;
+    const uint32_t nv = slsf::corr_values(t->lz, rmax_xy, rmax_z);
+    const size_t np = slsf::corr_partial_doubles(t->lx, t->ly, t->lz, rmax_xy, rmax_z);
+    const size_t off_values = align256(8 * np), off_table = off_values + align256(8ull * nv);
+    const size_t bytes = off_table + align256(sizeof(slsf::CorrTask));
     void* dv = nullptr;
-    cudaError_t e = t->ctx->pool.allocate(bytes, &dv);
+    cudaError_t e = ctx->pool.allocate(bytes, &dv);
     if (e != cudaSuccess) return cuda_error(e, "correlation scratch");
-    double* d = static_cast<double*>(dv);
-    double* sx = d + work_n;
-    double* sy = sx + nsx;
-    double* sz = sy + nsx;
-    slsf::launch_correlations(t->view(), rmax_xy, rmax_z, d, work_n, sx, sy, sz, t->ctx->stream);
-    t->ctx->launches += (rmax_xy ? 4 : 0) + (rmax_z ? 2 : 0);
-    e = cudaGetLastError();
-    std::vector<double> h(2 * nsx + nsz);
-    if (e == cudaSuccess && !h.empty())
-        e = cudaMemcpyAsync(h.data(), sx, 8 * h.size(), cudaMemcpyDeviceToHost, t->ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(t->ctx->stream);
-    t->ctx->pool.free(dv, bytes);
+    char* d = static_cast<char*>(dv);
+    slsf::CorrTask ct = {t->theta, t->lx, t->ly, t->lz, rmax_xy, rmax_z, 0, 1, 0,
+                         reinterpret_cast<double*>(d), reinterpret_cast<double*>(d + off_values), nullptr, nullptr};
+    auto* table = reinterpret_cast<slsf::CorrTask*>(d + off_table);
+    std::vector<double> h(nv);
+    e = cudaMemcpyAsync(table, &ct, sizeof(ct), cudaMemcpyHostToDevice, ctx->stream);
+    const uint32_t items = slsf::corr_items(t->lx, t->ly, t->lz, rmax_xy, rmax_z);
+    if (e == cudaSuccess)
+        e = slsf::launch_corr(table, 1, items, slsf::corr_ext(t->lx, t->ly, t->lz, rmax_xy, rmax_z), ctx->sm_count,
+                              ctx->stream);
+    ctx->launches += items ? 2 : 1;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), ct.values, 8ull * nv, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    ctx->pool.free(dv, bytes);
     if (e != cudaSuccess) return cuda_error(e, "correlations");
-    const double volume = (double)t->volume, area = (double)t->lx * t->ly;
-    for (uint32_t r = 0; r < rmax_xy; ++r) {
-        double sxr = 0, syr = 0;
-        for (uint32_t z = 0; z < t->lz; ++z) {
-            const double lsx = h[z * rmax_xy + r], lsy = h[nsx + z * rmax_xy + r];
-            sxr += lsx;
-            syr += lsy;
-            if (corr_xy_by_z) corr_xy_by_z[z * rmax_xy + r] = (lsx + lsy) / (2.0 * area);
-        }
-        if (corr_x) corr_x[r] = sxr / volume;
-        if (corr_y) corr_y[r] = syr / volume;
-        if (corr_xy) corr_xy[r] = (sxr / volume + syr / volume) / 2.0;
+    const uint32_t R = rmax_xy;
+    for (uint32_t r = 0; r < R; ++r) {
+        if (corr_x) corr_x[r] = h[r];
+        if (corr_y) corr_y[r] = h[R + r];
+        if (corr_xy) corr_xy[r] = h[2 * R + r];
     }
-    for (uint32_t r = 0; r < rmax_z; ++r)
-        if (corr_z) corr_z[r] = h[2 * nsx + r] / volume;
+    if (corr_xy_by_z)
+        for (size_t j = 0; j < (size_t)t->lz * R; ++j) corr_xy_by_z[j] = h[3 * R + j];
+    if (corr_z)
+        for (uint32_t r = 0; r < rmax_z; ++r) corr_z[r] = h[3 * R + (size_t)t->lz * R + r];
+    return SLSF_OK;
+}
+
+int slsf_task_corr_setup(slsf_task* t, uint32_t rmax_xy, uint32_t rmax_z, uint32_t binsize, uint32_t n_bins,
+                         size_t* n_values) {
+    if (!t) return set_error(SLSF_ERR_INVALID, "task is NULL");
+    if (int rc = check_free(t)) return rc;
+    if (n_bins > 0 && binsize == 0) return set_error(SLSF_ERR_INVALID, "binsize must be positive");
+    const uint32_t rxy = std::min(std::min(rmax_xy, t->lx / 2), t->ly / 2), rz = std::min(rmax_z, t->lz / 2);
+    const bool on = rxy || rz;
+    if (on && !slsf::corr_supports(t->lx, t->ly, t->lz, rxy, rz)) return set_error(SLSF_ERR_INVALID, kErrCorrLong);
+    slsf_ctx* ctx = t->ctx;
+    const uint32_t nv = on ? slsf::corr_values(t->lz, rxy, rz) : 0;
+    const size_t off_bins = align256(8 * slsf::corr_partial_doubles(t->lx, t->ly, t->lz, rxy, rz));
+    const size_t off_count = off_bins + align256(8ull * nv * n_bins);
+    const uint64_t bytes = on ? off_count + 256 : 0;
+    if (int rc = bind_device(ctx)) return rc;
+    if (t->corr_block) {
+        SLSF_CUDA(cudaStreamSynchronize(ctx->stream)); /* queued launches may still use the block */
+        ctx->pool.free(t->corr_block, t->corr_bytes);
+        ctx->used -= t->corr_bytes;
+        t->corr_block = nullptr;
+        t->corr_bytes = 0;
+        t->corr_partial = t->corr_bins = nullptr;
+        t->corr_count_dev = nullptr;
+    }
+    t->corr_rxy = t->corr_rz = t->corr_n_bins = 0;
+    t->corr_binsize = 1;
+    t->corr_count = 0;
+    if (n_values) *n_values = nv;
+    if (!on) return SLSF_OK;
+    if (ctx->used + bytes > ctx->budget)
+        return set_error(SLSF_ERR_BUDGET, "correlation bins do not fit in the context's device memory budget");
+    void* block = nullptr;
+    SLSF_CUDA(ctx->pool.allocate(bytes, &block));
+    char* b = static_cast<char*>(block);
+    const cudaError_t e = cudaMemsetAsync(block, 0, bytes, ctx->stream);
+    if (e != cudaSuccess) {
+        ctx->pool.free(block, bytes);
+        return cuda_error(e, "correlation bins");
+    }
+    ctx->used += bytes;
+    t->corr_block = block;
+    t->corr_bytes = bytes;
+    t->corr_partial = reinterpret_cast<double*>(b);
+    t->corr_bins = reinterpret_cast<double*>(b + off_bins);
+    t->corr_count_dev = reinterpret_cast<unsigned long long*>(b + off_count);
+    t->corr_rxy = rxy;
+    t->corr_rz = rz;
+    t->corr_binsize = binsize ? binsize : 1;
+    t->corr_n_bins = n_bins;
+    return SLSF_OK;
+}
+
+int slsf_task_corr_bins(const slsf_task* t, double* bin_means, size_t n_rows, uint64_t* count) {
+    if (!t) return set_error(SLSF_ERR_INVALID, "task is NULL");
+    if (count) *count = t->corr_count;
+    if (!bin_means || n_rows == 0) return SLSF_OK;
+    if (n_rows > t->corr_n_bins) return set_error(SLSF_ERR_INVALID, "more bin rows requested than the task keeps");
+    if (int rc = bind_device(t->ctx)) return rc;
+    const size_t nv = slsf::corr_values(t->lz, t->corr_rxy, t->corr_rz);
+    SLSF_CUDA(cudaMemcpyAsync(bin_means, t->corr_bins, 8 * nv * n_rows, cudaMemcpyDeviceToHost, t->ctx->stream));
+    SLSF_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    /* sums -> means: a full row holds binsize measurements, the last fewer */
+    for (size_t row = 0; row < n_rows; ++row) {
+        const uint64_t first = (uint64_t)row * t->corr_binsize;
+        const uint64_t filled = t->corr_count > first ? std::min<uint64_t>(t->corr_binsize, t->corr_count - first) : 0;
+        for (size_t j = 0; j < nv; ++j) bin_means[row * nv + j] = filled ? bin_means[row * nv + j] / (double)filled : 0.0;
+    }
+    return SLSF_OK;
+}
+
+int slsf_batch_correlations(slsf_ctx* ctx, slsf_task* const* tasks, size_t n) {
+    if (!ctx || (!tasks && n)) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    if (n == 0) return SLSF_OK;
+    std::unordered_set<const slsf_task*> seen;
+    for (size_t i = 0; i < n; ++i) {
+        const slsf_task* t = tasks[i];
+        if (!t || t->ctx != ctx) return set_error(SLSF_ERR_INVALID, "task does not belong to this context");
+        if (int rc = check_free(t)) return rc;
+        if (!t->corr_block)
+            return set_error(SLSF_ERR_STATE, "task has no correlation bins; call slsf_task_corr_setup first");
+        if (!seen.insert(t).second) return set_error(SLSF_ERR_INVALID, "a task appears twice in the batch");
+    }
+    if (int rc = bind_device(ctx)) return rc;
+    if (!ctx->corr_uploaded) SLSF_CUDA(cudaEventCreateWithFlags(&ctx->corr_uploaded, cudaEventDisableTiming));
+    /* the pinned table may still be the source of the last queued upload */
+    SLSF_CUDA(cudaEventSynchronize(ctx->corr_uploaded));
+    if (ctx->corr_cap < n) {
+        SLSF_CUDA(cudaStreamSynchronize(ctx->stream)); /* queued launches may still read the device table */
+        if (ctx->d_corr) cudaFree(ctx->d_corr);
+        if (ctx->h_corr) cudaFreeHost(ctx->h_corr);
+        ctx->d_corr = nullptr;
+        ctx->h_corr = nullptr;
+        ctx->corr_cap = 0;
+        SLSF_CUDA(cudaMalloc(&ctx->d_corr, sizeof(slsf::CorrTask) * n));
+        SLSF_CUDA(cudaHostAlloc(&ctx->h_corr, sizeof(slsf::CorrTask) * n, cudaHostAllocDefault));
+        ctx->corr_cap = n;
+    }
+    uint32_t items = 0, max_ext = 0;
+    for (size_t i = 0; i < n; ++i) {
+        slsf_task* t = tasks[i];
+        ctx->h_corr[i] = slsf::CorrTask{t->theta, t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz, items,
+                                        t->corr_binsize, t->corr_n_bins, t->corr_partial, nullptr, t->corr_bins,
+                                        t->corr_count_dev};
+        items += slsf::corr_items(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz);
+        max_ext = std::max(max_ext, slsf::corr_ext(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz));
+    }
+    SLSF_CUDA(cudaMemcpyAsync(ctx->d_corr, ctx->h_corr, sizeof(slsf::CorrTask) * n, cudaMemcpyHostToDevice,
+                              ctx->stream));
+    SLSF_CUDA(cudaEventRecord(ctx->corr_uploaded, ctx->stream));
+    SLSF_CUDA(slsf::launch_corr(ctx->d_corr, (uint32_t)n, items, max_ext, ctx->sm_count, ctx->stream));
+    ctx->launches += items ? 2 : 1;
+    for (size_t i = 0; i < n; ++i) tasks[i]->corr_count += 1;
     return SLSF_OK;
 }
 

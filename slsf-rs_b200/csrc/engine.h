@@ -76,16 +76,36 @@ void launch_measure(const TaskView& t, double* partials, unsigned int* done, dou
 void launch_measure_into_bin(const TaskView& t, double* partials, unsigned int* done, double* result,
                              double* bin_row, cudaStream_t s);
 int measure_partial_blocks(uint32_t volume);
-/* Shared bytes of the correlation kernel's tile for lines of n sites at lags up to rmax: corr_tile_bytes(n + rmax). */
-size_t corr_tile_bytes(uint32_t entries);
-/* Correlation sums: sx[lz][rmax_xy], sy[lz][rmax_xy], sz[rmax_z] (FP64). */
-void launch_correlations(const TaskView& t, uint32_t rmax_xy, uint32_t rmax_z, double* work,
-                         size_t work_doubles, double* sx, double* sy, double* sz,
-                         cudaStream_t s);
-size_t correlation_work_doubles(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rmax_xy,
-                                uint32_t rmax_z);
 /* dst[i * per + k] = src[i][k] for i < n, k < per. */
 void launch_gather(const double* const* src, uint32_t n, uint32_t per, double* dst, cudaStream_t s);
+
+/* ---- correlation functions, batched over tasks (kernel_corr.cu) ---- */
+/* One task of a correlation launch.  `partial` holds corr_partial_doubles()
+ * of scratch; the measurement's corr_values() values (C_x(r), C_y(r),
+ * C_xy(r), C_xy(z, r) z-major, C_z(r)) go to `values` and/or are added into
+ * row *count / binsize of `bins` (rows past n_bins are dropped), after which
+ * *count grows by one. */
+struct CorrTask {
+    const float* theta;
+    uint32_t lx, ly, lz;
+    uint32_t rxy, rz;   /* radii, already clamped to Lx/2, Ly/2 and Lz/2 */
+    uint32_t item0;     /* the task's first work item in the launch */
+    uint32_t binsize, n_bins;
+    double* partial;
+    double* values;     /* or NULL */
+    double* bins;       /* [n_bins][values] sums, or NULL */
+    unsigned long long* count; /* or NULL */
+};
+uint32_t corr_items(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
+size_t corr_partial_doubles(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
+uint32_t corr_values(uint32_t lz, uint32_t rxy, uint32_t rz);
+/* Longest line plus lags of a task (tile rows); corr_supports: the tile fits shared memory. */
+uint32_t corr_ext(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
+bool corr_supports(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
+/* tasks_dev: n_tasks entries in item order (item0 ascending, n_items in
+ * all); max_ext: the largest corr_ext of them. */
+cudaError_t launch_corr(const CorrTask* tasks_dev, uint32_t n_tasks, uint32_t n_items, uint32_t max_ext,
+                        int sm_count, cudaStream_t s);
 
 /* ---- batched persistent engine, one CTA per replica (kernel_resident.cu) ---- */
 bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);

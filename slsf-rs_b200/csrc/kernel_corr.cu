@@ -1,0 +1,275 @@
+/*
+ * Correlation functions of many tasks in two launches
+ * (measure_theta_correlations_with_scratch, src/observables.rs:165-270):
+ *
+ *   C_x(r)     = sum_{x,y,z} s(x,y,z) . s(x+r,y,z) / V
+ *   C_y(r)     = sum s(x,y,z) . s(x,y+r,z) / V
+ *   C_xy(r)    = (C_x(r) + C_y(r)) / 2
+ *   C_xy(z, r) = sum_{x,y} [s . s(x+r) + s . s(y+r)] / (2 Lx Ly)
+ *   C_z(r)     = sum s(x,y,z) . s(x,y,z+r) / V
+ *
+ * with periodic shifts, r = 1..R (R = rmax_xy clamped to Lx/2, Ly/2) and
+ * r = 1..R_z (R_z = rmax_z clamped to Lz/2); s . s' = cos cos' + sin sin'.
+ *
+ * k_corr_lines: a persistent grid walks the work items of all tasks.  An
+ * item is up to 32 parallel lines of one task along one axis -- x lines: 32
+ * consecutive rows y of one layer; y lines: 32 consecutive x of one layer;
+ * z lines: 32 consecutive x of one row y -- staged as (cos, sin) pairs in a
+ * shared tile [n + R][33] (the first R entries of each line repeated after
+ * its end, so k + r needs no modulo; the 33-pair pitch keeps both the
+ * row-wise and the transposed fill free of bank conflicts).  Lane c owns
+ * line c; warp w owns 8 consecutive lags and keeps their partners in a
+ * register ring along k, one shared load per k for 8 products.  Products
+ * are FP32 (fused multiply-add), summed in FP32 over runs of 32 k and the
+ * runs in FP64; the item's per-lag sums (FP64, over its lines) go to the
+ * task's scratch.
+ *
+ * k_corr_finalize: one block per task sums the item partials in a fixed
+ * order (per layer for x and y, over everything for z), forms the values in
+ * ThetaModel::measure's order (src/model.rs:420-437) -- C_x, C_y, C_xy,
+ * C_xy(z, r) z-major, C_z -- and writes them out and/or adds them into row
+ * count / binsize of the task's correlation bin sums.  Everything is
+ * deterministic: a task's values do not depend on the other tasks of the
+ * launch or on the grid size.
+ */
+#include <algorithm>
+
+#include "engine.h"
+
+namespace slsf {
+
+namespace {
+
+constexpr int kCorrThreads = 256;
+constexpr uint32_t kCorrCols = 32;  /* lines per item */
+constexpr uint32_t kCorrPitch = 33; /* (cos, sin) pairs per tile row */
+constexpr uint32_t kCorrLags = 8;   /* lags per warp pass */
+constexpr uint32_t kCorrRun = 32;   /* k per FP32 run */
+constexpr size_t kCorrMaxTile = 200 * 1024;
+
+struct CorrShape {
+    uint32_t cx, cy;     /* items per layer: x lines (chunks of rows), y or z lines (chunks of x) */
+    uint32_t nx, ny, nz; /* items along x, y, z */
+    uint32_t rp;         /* partial row pitch: max(R, R_z) */
+};
+
+__host__ __device__ inline CorrShape corr_shape(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
+    CorrShape s;
+    s.cx = (ly + kCorrCols - 1) / kCorrCols;
+    s.cy = (lx + kCorrCols - 1) / kCorrCols;
+    s.nx = rxy ? lz * s.cx : 0;
+    s.ny = rxy ? lz * s.cy : 0;
+    s.nz = rz ? ly * s.cy : 0;
+    s.rp = rxy > rz ? rxy : rz;
+    return s;
+}
+
+__global__ void __launch_bounds__(kCorrThreads)
+    k_corr_lines(const CorrTask* __restrict__ tasks, uint32_t n_tasks, uint32_t n_items) {
+    extern __shared__ float2 tile[]; /* [n + R][kCorrPitch] */
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (uint32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+        /* the task: the last one whose first item is at or before `item` */
+        uint32_t lo = 0, hi = n_tasks;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (tasks[mid].item0 <= item) lo = mid;
+            else hi = mid;
+        }
+        const CorrTask& T = tasks[lo];
+        const uint32_t lx = T.lx, ly = T.ly, lz = T.lz, plane = lx * ly;
+        const CorrShape sh = corr_shape(lx, ly, lz, T.rxy, T.rz);
+        const uint32_t local = item - T.item0;
+        /* line geometry: n sites per line, `stride` between sites of a line,
+         * `cstride` between lines, `cols` lines, first site `base` */
+        uint32_t n, stride, cstride, cols, base, rmax;
+        if (local < sh.nx) {
+            const uint32_t z = local / sh.cx, y0 = (local % sh.cx) * kCorrCols;
+            n = lx, stride = 1, cstride = lx, cols = min(kCorrCols, ly - y0), base = z * plane + y0 * lx;
+            rmax = T.rxy;
+        } else if (local < sh.nx + sh.ny) {
+            const uint32_t q = local - sh.nx, z = q / sh.cy, x0 = (q % sh.cy) * kCorrCols;
+            n = ly, stride = lx, cstride = 1, cols = min(kCorrCols, lx - x0), base = z * plane + x0;
+            rmax = T.rxy;
+        } else {
+            const uint32_t q = local - sh.nx - sh.ny, y = q / sh.cy, x0 = (q % sh.cy) * kCorrCols;
+            n = lz, stride = plane, cstride = 1, cols = min(kCorrCols, lx - x0), base = y * lx + x0;
+            rmax = T.rz;
+        }
+        const float* __restrict__ theta = T.theta;
+        const uint32_t ext = n + rmax;
+        __syncthreads(); /* the previous item's tile is no longer read */
+        if (cstride == 1) {
+            for (uint32_t e = threadIdx.x; e < ext * kCorrCols; e += blockDim.x) {
+                const uint32_t k = e / kCorrCols, c = e % kCorrCols;
+                const uint32_t kk = k < n ? k : k - n;
+                float sn = 0.0f, cn = 0.0f;
+                if (c < cols) __sincosf(theta[base + kk * stride + c], &sn, &cn);
+                tile[k * kCorrPitch + c] = make_float2(cn, sn);
+            }
+        } else {
+            /* x lines: consecutive threads take consecutive sites of a row */
+            for (uint32_t e = threadIdx.x; e < ext * kCorrCols; e += blockDim.x) {
+                const uint32_t c = e / ext, k = e % ext;
+                const uint32_t kk = k < n ? k : k - n;
+                float sn = 0.0f, cn = 0.0f;
+                if (c < cols) __sincosf(theta[base + c * cstride + kk], &sn, &cn);
+                tile[k * kCorrPitch + c] = make_float2(cn, sn);
+            }
+        }
+        __syncthreads();
+        double* out = T.partial + (size_t)local * sh.rp;
+        for (uint32_t r0 = 1 + warp * kCorrLags; r0 <= rmax; r0 += nwarps * kCorrLags) {
+            /* w[j]: partner of lag r0 + j at the current k */
+            float2 w[kCorrLags];
+#pragma unroll
+            for (uint32_t j = 0; j < kCorrLags; ++j) w[j] = tile[min(r0 + j, ext - 1) * kCorrPitch + lane];
+            double tot[kCorrLags];
+            float part[kCorrLags];
+#pragma unroll
+            for (uint32_t j = 0; j < kCorrLags; ++j) {
+                tot[j] = 0.0;
+                part[j] = 0.0f;
+            }
+            /* k in groups of 8: the partner of lag r0 + j at k = k0 + kk sits
+             * in slot (kk + j) % 8, and slot kk takes the next partner after
+             * k, so the ring needs no register moves */
+            const uint32_t n8 = n - n % kCorrLags;
+            for (uint32_t k0 = 0; k0 < n8; k0 += kCorrLags) {
+#pragma unroll
+                for (uint32_t kk = 0; kk < kCorrLags; ++kk) {
+                    const float2 a = tile[(k0 + kk) * kCorrPitch + lane];
+#pragma unroll
+                    for (uint32_t j = 0; j < kCorrLags; ++j) {
+                        const float2 wj = w[(kk + j) % kCorrLags];
+                        part[j] = __fmaf_rn(a.y, wj.y, __fmaf_rn(a.x, wj.x, part[j]));
+                    }
+                    w[kk] = tile[min(k0 + kk + r0 + kCorrLags, ext - 1) * kCorrPitch + lane];
+                }
+                if ((k0 + kCorrLags) % kCorrRun == 0) {
+#pragma unroll
+                    for (uint32_t j = 0; j < kCorrLags; ++j) {
+                        tot[j] += (double)part[j];
+                        part[j] = 0.0f;
+                    }
+                }
+            }
+            /* the ring is aligned again (slot j = lag r0 + j); the last n % 8
+             * values of k slide it */
+            for (uint32_t k = n8; k < n; ++k) {
+                const float2 a = tile[k * kCorrPitch + lane];
+#pragma unroll
+                for (uint32_t j = 0; j < kCorrLags; ++j)
+                    part[j] = __fmaf_rn(a.y, w[j].y, __fmaf_rn(a.x, w[j].x, part[j]));
+#pragma unroll
+                for (uint32_t j = 0; j + 1 < kCorrLags; ++j) w[j] = w[j + 1];
+                w[kCorrLags - 1] = tile[min(k + kCorrLags + r0, ext - 1) * kCorrPitch + lane];
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kCorrLags; ++j) {
+                double v = tot[j] + (double)part[j];
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+                if (lane == 0 && r0 + j <= rmax) out[r0 + j - 1] = v;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) k_corr_finalize(const CorrTask* __restrict__ tasks) {
+    const CorrTask& T = tasks[blockIdx.x];
+    const uint32_t R = T.rxy, Rz = T.rz, lz = T.lz;
+    if (R == 0 && Rz == 0) return;
+    const CorrShape sh = corr_shape(T.lx, T.ly, lz, R, Rz);
+    const uint32_t items = sh.nx + sh.ny + sh.nz;
+    const uint32_t nv = 3 * R + lz * R + Rz;
+    const double volume = (double)T.lx * T.ly * lz, area = (double)T.lx * T.ly;
+    const double* __restrict__ part = T.partial;
+    double* lsx = T.partial + (size_t)items * sh.rp; /* [lz][R] layer sums */
+    double* lsy = lsx + (size_t)lz * R;
+    __shared__ unsigned long long row_s;
+    if (threadIdx.x == 0) row_s = T.count ? *T.count / (T.binsize ? T.binsize : 1) : 0;
+    __syncthreads();
+    const unsigned long long row = row_s;
+    double* bin = (T.bins && row < T.n_bins) ? T.bins + row * nv : nullptr;
+    auto emit = [&](uint32_t j, double v) {
+        if (T.values) T.values[j] = v;
+        if (bin) bin[j] += v;
+    };
+    for (uint32_t j = threadIdx.x; j < lz * R; j += blockDim.x) {
+        const uint32_t z = j / R, r = j % R;
+        double a = 0.0, b = 0.0;
+        for (uint32_t c = 0; c < sh.cx; ++c) a += part[(size_t)(z * sh.cx + c) * sh.rp + r];
+        for (uint32_t c = 0; c < sh.cy; ++c) b += part[(size_t)(sh.nx + z * sh.cy + c) * sh.rp + r];
+        lsx[j] = a;
+        lsy[j] = b;
+        emit(3 * R + j, (a + b) / (2.0 * area));
+    }
+    __syncthreads(); /* the layer sums are visible to the whole block */
+    for (uint32_t r = threadIdx.x; r < R; r += blockDim.x) {
+        double sx = 0.0, sy = 0.0;
+        for (uint32_t z = 0; z < lz; ++z) {
+            sx += lsx[(size_t)z * R + r];
+            sy += lsy[(size_t)z * R + r];
+        }
+        const double cx = sx / volume, cy = sy / volume;
+        emit(r, cx);
+        emit(R + r, cy);
+        emit(2 * R + r, (cx + cy) / 2.0);
+    }
+    for (uint32_t r = threadIdx.x; r < Rz; r += blockDim.x) {
+        double sz = 0.0;
+        for (uint32_t p = 0; p < sh.nz; ++p) sz += part[(size_t)(sh.nx + sh.ny + p) * sh.rp + r];
+        emit(3 * R + lz * R + r, sz / volume);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && T.count) *T.count += 1;
+}
+
+}  // namespace
+
+uint32_t corr_items(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
+    const CorrShape s = corr_shape(lx, ly, lz, rxy, rz);
+    return s.nx + s.ny + s.nz;
+}
+
+size_t corr_partial_doubles(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
+    const CorrShape s = corr_shape(lx, ly, lz, rxy, rz);
+    return (size_t)(s.nx + s.ny + s.nz) * s.rp + 2ull * lz * rxy;
+}
+
+uint32_t corr_values(uint32_t lz, uint32_t rxy, uint32_t rz) { return 3 * rxy + lz * rxy + rz; }
+
+uint32_t corr_ext(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
+    uint32_t e = 0;
+    if (rxy) e = std::max(lx, ly) + rxy;
+    if (rz) e = std::max(e, lz + rz);
+    return e;
+}
+
+bool corr_supports(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
+    return (size_t)corr_ext(lx, ly, lz, rxy, rz) * kCorrPitch * sizeof(float2) <= kCorrMaxTile;
+}
+
+cudaError_t launch_corr(const CorrTask* tasks_dev, uint32_t n_tasks, uint32_t n_items, uint32_t max_ext,
+                        int sm_count, cudaStream_t s) {
+    if (n_tasks == 0) return cudaSuccess;
+    if (n_items > 0) {
+        const size_t smem = (size_t)max_ext * kCorrPitch * sizeof(float2);
+        cudaError_t e = cudaSuccess;
+        if (smem > 48 * 1024)
+            e = cudaFuncSetAttribute(k_corr_lines, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_corr_lines, kCorrThreads, smem);
+        if (e != cudaSuccess) return e;
+        const uint32_t grid = std::min<uint32_t>(n_items, (uint32_t)std::max(1, per_sm) * (uint32_t)sm_count);
+        k_corr_lines<<<grid, kCorrThreads, smem, s>>>(tasks_dev, n_tasks, n_items);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    k_corr_finalize<<<n_tasks, 128, 0, s>>>(tasks_dev);
+    return cudaGetLastError();
+}
+
+}  // namespace slsf

@@ -16,8 +16,8 @@
  *   k_measure            measure_theta_observables_with_scratch
  *                        (src/observables.rs:80-154), FP64 block sums, fixed
  *                        summation order (last block reduces the partials)
- *   k_corr_*             measure_theta_correlations_with_scratch
- *                        (src/observables.rs:166-265)
+ *
+ * (The correlation functions are in kernel_corr.cu, batched over tasks.)
  */
 #include <algorithm>
 
@@ -413,158 +413,9 @@ __global__ void __launch_bounds__(kMeasureThreads)
     }
 }
 
-/* ---- correlations ----
- * A "line" is a periodic 1-D array of n sites with a fixed stride; the
- * circular correlation of a line at lag r is sum_k s_k . s_{(k+r) mod n}
- * (src/observables.rs:196-220 for x and y rows, :230-244 for z columns).
- * Lines along y and z are taken 32 consecutive x at a time so that the tile
- * loads are coalesced; lines along x are whole rows. */
-constexpr int kCorrThreads = 256;
-constexpr int kCorrCols = 32;
-
-/* Lines along an axis with stride `stride` (lx for y, lx*ly for z), n sites
- * each; a block takes kCorrCols consecutive x at one (other-axis) offset and
- * writes out[block][r - 1] = sum over its columns and all k of
- * s_k . s_{(k+r) mod n}, r = 1..rmax.
- *
- * The block's lines sit in shared memory as (cos, sin) pairs [n + rmax][32]
- * (the first rmax entries repeated after the last, so k + r needs no
- * modulo).  Lane c of a warp owns column c; warp w owns the kCorrLags
- * consecutive lags from 1 + w kCorrLags (then + nwarps kCorrLags, ...) and
- * keeps those lags' partners in a register ring along k: one new shared
- * load per k for kCorrLags products.  Products are summed in FP32 over runs
- * of kCorrRun values of k, and the runs in FP64, in a fixed order. */
-constexpr uint32_t kCorrLags = 8;
-constexpr uint32_t kCorrRun = 32;
-
-__global__ void __launch_bounds__(kCorrThreads)
-    k_corr_strided(const float* __restrict__ theta, uint32_t lx, uint32_t n, uint32_t stride,
-                   uint32_t outer_count, uint32_t outer_stride, uint32_t rmax,
-                   double* __restrict__ out) {
-    extern __shared__ float2 tile[]; /* [n + rmax][kCorrCols] (cos, sin) */
-    const uint32_t col_blocks = (lx + kCorrCols - 1) / kCorrCols;
-    const uint32_t outer = blockIdx.x / col_blocks;
-    const uint32_t x0 = (blockIdx.x % col_blocks) * kCorrCols;
-    const uint32_t cols = min((uint32_t)kCorrCols, lx - x0);
-    const uint32_t base = outer * outer_stride + x0;
-    const uint32_t ext = n + rmax;
-    for (uint32_t e = threadIdx.x; e < ext * kCorrCols; e += blockDim.x) {
-        const uint32_t k = e / kCorrCols, c = e % kCorrCols;
-        const uint32_t kk = k < n ? k : k - n;
-        float sn = 0.0f, cn = 0.0f;
-        if (c < cols) __sincosf(theta[base + kk * stride + c], &sn, &cn);
-        tile[e] = make_float2(cn, sn);
-    }
-    __syncthreads();
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (uint32_t r0 = 1 + warp * kCorrLags; r0 <= rmax; r0 += nwarps * kCorrLags) {
-        /* window w[j] = partner of lag r0 + j at the current k */
-        float2 w[kCorrLags];
-#pragma unroll
-        for (uint32_t j = 0; j < kCorrLags; ++j) w[j] = tile[min(r0 + j, ext - 1) * kCorrCols + lane];
-        double tot[kCorrLags];
-        float part[kCorrLags];
-#pragma unroll
-        for (uint32_t j = 0; j < kCorrLags; ++j) {
-            tot[j] = 0.0;
-            part[j] = 0.0f;
-        }
-        /* k in groups of kCorrLags: the window is a ring, the partner of lag
-         * r0 + j at k = k0 + kk sits in slot (kk + j) % kCorrLags, and slot kk
-         * takes the next partner after k -- no register moves */
-        const uint32_t n8 = n - n % kCorrLags;
-        for (uint32_t k0 = 0; k0 < n8; k0 += kCorrLags) {
-#pragma unroll
-            for (uint32_t kk = 0; kk < kCorrLags; ++kk) {
-                const float2 a = tile[(k0 + kk) * kCorrCols + lane];
-#pragma unroll
-                for (uint32_t j = 0; j < kCorrLags; ++j) {
-                    const float2 wj = w[(kk + j) % kCorrLags];
-                    part[j] = __fmaf_rn(a.y, wj.y, __fmaf_rn(a.x, wj.x, part[j]));
-                }
-                w[kk] = tile[min(k0 + kk + r0 + kCorrLags, ext - 1) * kCorrCols + lane];
-            }
-            if ((k0 + kCorrLags) % kCorrRun == 0) {
-#pragma unroll
-                for (uint32_t j = 0; j < kCorrLags; ++j) {
-                    tot[j] += (double)part[j];
-                    part[j] = 0.0f;
-                }
-            }
-        }
-        /* the ring is aligned again (slot j = lag r0 + j); the last n % 8 k slide it */
-        for (uint32_t k = n8; k < n; ++k) {
-            const float2 a = tile[k * kCorrCols + lane];
-#pragma unroll
-            for (uint32_t j = 0; j < kCorrLags; ++j) part[j] = __fmaf_rn(a.y, w[j].y, __fmaf_rn(a.x, w[j].x, part[j]));
-            /* slide: the partner of lag r0 + j at k + 1 is the one of lag r0 + j + 1 at k */
-#pragma unroll
-            for (uint32_t j = 0; j + 1 < kCorrLags; ++j) w[j] = w[j + 1];
-            w[kCorrLags - 1] = tile[min(k + 1 + r0 + kCorrLags - 1, ext - 1) * kCorrCols + lane];
-        }
-#pragma unroll
-        for (uint32_t j = 0; j < kCorrLags; ++j) tot[j] += (double)part[j];
-#pragma unroll
-        for (uint32_t j = 0; j < kCorrLags; ++j) {
-            double v = tot[j];
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-            if (lane == 0 && r0 + j <= rmax) out[(size_t)blockIdx.x * rmax + (r0 + j - 1)] = v;
-        }
-    }
-    (void)outer_count;
-}
-
-/* Rows along x: a block takes one row (y, z); out[row][r]. */
-__global__ void __launch_bounds__(kCorrThreads)
-    k_corr_rows(const float* __restrict__ theta, uint32_t lx, uint32_t rmax, double* __restrict__ out) {
-    extern __shared__ float row[]; /* [lx][2] */
-    const uint32_t base = blockIdx.x * lx;
-    for (uint32_t k = threadIdx.x; k < lx; k += blockDim.x) {
-        float s, c;
-        __sincosf(theta[base + k], &s, &c);
-        row[2 * k] = c;
-        row[2 * k + 1] = s;
-    }
-    __syncthreads();
-    __shared__ double red[kCorrThreads];
-    for (uint32_t r = 1; r <= rmax; ++r) {
-        double acc = 0.0;
-        for (uint32_t k = threadIdx.x; k < lx; k += blockDim.x) {
-            const uint32_t k2 = (k + r) % lx;
-            acc += (double)(row[2 * k] * row[2 * k2] + row[2 * k + 1] * row[2 * k2 + 1]);
-        }
-        red[threadIdx.x] = acc;
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) out[(size_t)blockIdx.x * rmax + (r - 1)] = red[0];
-        __syncthreads();
-    }
-}
-
-/* out[g][r] = sum_{j < per_group} in[(g * per_group + j)][r] in a fixed
- * order: one warp per (g, r), lanes over j, then a shuffle tree. */
-__global__ void k_sum_groups(const double* __restrict__ in, uint32_t groups, uint32_t per_group,
-                             uint32_t rmax, double* __restrict__ out) {
-    const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
-    if (t >= groups * rmax) return;
-    const uint32_t g = t / rmax, r = t % rmax;
-    double acc = 0.0;
-    for (uint32_t j = lane; j < per_group; j += 32) acc += in[((size_t)g * per_group + j) * rmax + r];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-    if (lane == 0) out[t] = acc;
-}
-
 inline uint32_t blocks_for(uint64_t n, int threads) { return (uint32_t)((n + threads - 1) / threads); }
 
 }  // namespace
-
-/* Shared bytes of a k_corr_strided tile of `entries` (cos, sin) rows. */
-size_t corr_tile_bytes(uint32_t entries) { return (size_t)entries * kCorrCols * sizeof(float2); }
 
 namespace {
 
@@ -640,42 +491,6 @@ void launch_measure_into_bin(const TaskView& t, double* partials, unsigned int* 
     const uint32_t volume = t.lx * t.ly * t.lz;
     k_measure<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly,
                                                                          t.lz, partials, done, result, bin_row);
-}
-
-size_t correlation_work_doubles(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rmax_xy,
-                                uint32_t rmax_z) {
-    const size_t col_blocks = (lx + kCorrCols - 1) / kCorrCols;
-    const size_t rows = (size_t)ly * lz * rmax_xy;          /* x lines */
-    const size_t ycols = col_blocks * lz * rmax_xy;         /* y lines */
-    const size_t zcols = col_blocks * (size_t)ly * rmax_z;  /* z lines */
-    return std::max(std::max(rows, ycols), zcols);
-}
-
-void launch_correlations(const TaskView& t, uint32_t rmax_xy, uint32_t rmax_z, double* work,
-                         size_t work_doubles, double* sx, double* sy, double* sz,
-                         cudaStream_t s) {
-    (void)work_doubles;
-    const uint32_t col_blocks = (t.lx + kCorrCols - 1) / kCorrCols;
-    const size_t smem_max = corr_tile_bytes(std::max(t.ly + rmax_xy, t.lz + rmax_z));
-    if (smem_max > 48 * 1024)
-        cudaFuncSetAttribute(k_corr_strided, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
-    if ((size_t)2 * t.lx * sizeof(float) > 48 * 1024)
-        cudaFuncSetAttribute(k_corr_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * t.lx * sizeof(float)));
-    if (rmax_xy > 0) {
-        /* x: one block per row, then sum the ly rows of each layer. */
-        k_corr_rows<<<t.ly * t.lz, kCorrThreads, 2 * t.lx * sizeof(float), s>>>(t.theta, t.lx, rmax_xy, work);
-        k_sum_groups<<<blocks_for(32ull * t.lz * rmax_xy, 128), 128, 0, s>>>(work, t.lz, t.ly, rmax_xy, sx);
-        /* y: lines of ly sites with stride lx; one block per (z, x-chunk). */
-        k_corr_strided<<<t.lz * col_blocks, kCorrThreads, corr_tile_bytes(t.ly + rmax_xy), s>>>(
-            t.theta, t.lx, t.ly, t.lx, t.lz, t.lx * t.ly, rmax_xy, work);
-        k_sum_groups<<<blocks_for(32ull * t.lz * rmax_xy, 128), 128, 0, s>>>(work, t.lz, col_blocks, rmax_xy, sy);
-    }
-    if (rmax_z > 0) {
-        /* z: lines of lz sites with stride lx*ly; one block per (y, x-chunk). */
-        k_corr_strided<<<t.ly * col_blocks, kCorrThreads, corr_tile_bytes(t.lz + rmax_z), s>>>(
-            t.theta, t.lx, t.lz, t.lx * t.ly, t.ly, t.lx, rmax_z, work);
-        k_sum_groups<<<blocks_for(32ull * rmax_z, 128), 128, 0, s>>>(work, 1, t.ly * col_blocks, rmax_z, sz);
-    }
 }
 
 }  // namespace slsf

@@ -18,9 +18,10 @@ ThetaJob::selected_tasks, src/model.rs:60-68):
   server (batched persistent launches, bins kept on the device);
 * tasks that measure correlations (the reference's default: r_max = L/2) run
   as groups through the batched kernels too, stopping every
-  `correlation_interval` measurements for the correlation functions of every
-  task of the group (ThetaModel::measure, src/model.rs:402-442).  The
-  trajectories are the ones the single-task path produces.
+  `correlation_interval` measurements for one batched launch of the
+  correlation functions of every task of the group, binned on the device
+  (ThetaModel::measure, src/model.rs:402-442).  The trajectories are the
+  ones the single-task path produces.
 
 The result has the reference's ThetaJobResult layout (src/model.rs:72-106:
 job_name, rank, world_size, tasks[] with task, observables{name: {mean,
@@ -355,15 +356,17 @@ def _run_served(pkg, ctx, tasks, epoch_sweeps):
 def _run_correlated(pkg, ctx, group):
     """One group of tasks sharing (thermalization, sweeps, correlation_interval)
     through the batched kernels: thermalization, then per correlation
-    measurement m (m % interval == 0) the sweeps up to it and the correlation
-    functions of every task; the bins come from the device.  Each correlation
-    observable's series is binned with the task's bin size
-    (BinnedEstimate::from_samples; fewer samples than a bin make one bin)."""
+    measurement m (m % interval == 0) the sweeps up to it and one batched
+    correlation launch that adds every task's values into its correlation bins
+    on the device.  A correlation series is binned with the task's bin size
+    (BinnedEstimate::from_samples); a series shorter than one bin forms one
+    bin."""
     import ctypes as C
 
     t0 = group[0][1]
     therm, sweeps, interval = t0["thermalization"], t0["sweeps"], t0["correlation_interval"]
-    objs, series, radii = [], [], []
+    n_corr = (sweeps + interval - 1) // interval
+    objs, radii, corr_bin = [], [], []
     try:
         for _, t in group:
             o = pkg.Task(ctx, (t["l_x"], t["l_y"], t["l_z"]), t["j_xy_array"], t["j_z_array"], t["temperature"],
@@ -373,8 +376,12 @@ def _run_correlated(pkg, ctx, group):
             objs.append(o)
             radii.append((min(t["correlation_rmax_xy"], t["l_x"] // 2, t["l_y"] // 2),
                           min(t["correlation_rmax_z"], t["l_z"] // 2)))
-            series.append([])
+            cb = min(t["binsize"], n_corr)
+            corr_bin.append(cb)
+            o.corr_setup(*radii[-1], cb, n_corr // cb)
         handles = ctx.handle_array(objs)
+        measured = [o for o in objs if o.corr_n_values]
+        corr_handles = ctx.handle_array(measured)
         accepted = np.zeros(len(objs))
 
         def advance(n):
@@ -387,10 +394,8 @@ def _run_correlated(pkg, ctx, group):
         for m in range(0, sweeps, interval):
             advance(m + 1 - done)
             done = m + 1
-            for i, o in enumerate(objs):
-                c = o.correlations(*radii[i])
-                series[i].append(np.concatenate([c["corr_x"], c["corr_y"], c["corr_xy"],
-                                                 c["corr_xy_by_z"].reshape(-1), c["corr_z"]]))
+            if measured:
+                ctx.batch_correlations(measured, corr_handles)
         advance(sweeps - done)
         host = pkg.load_host()
         out = []
@@ -404,11 +409,14 @@ def _run_correlated(pkg, ctx, group):
             est = e.as_dict()
             est["measurements"] = meas
             est["acceptance"] = accepted[i] / (volume * (therm + sweeps))
-            s = np.array(series[i])
             corr = {}
-            for j, name in enumerate(corr_names(t["l_z"], *radii[i])):
-                r = pkg.binned_estimate(s[:, j], min(t["binsize"], len(s)))
-                corr[name] = (r["mean"], r["stderr"])
+            if o.corr_n_values:
+                means, count = o.corr_bins()
+                assert count == n_corr
+                for j, name in enumerate(corr_names(t["l_z"], *radii[i])):
+                    # bins of one mean each: the mean of the bin means and their standard error
+                    r = pkg.binned_estimate(means[:, j], 1)
+                    corr[name] = (r["mean"], r["stderr"])
             out.append((est, corr))
         return out
     finally:

@@ -1,0 +1,129 @@
+"""Correlation bins on the device (marked gpu): one batched launch over tasks
+of mixed shapes gives each task the values its own slsf_task_correlations
+gives, bit for bit, and the oracle's within the FP32 bar; the bins sum the
+measurements in order; set-up, budget and misuse errors."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [((8, 8, 8), 4, 4), ((16, 12, 20), 5, 10), ((2, 2, 2), 1, 1), ((6, 10, 4), 3, 0), ((32, 48, 30), 24, 9),
+          ((40, 24, 256), 3, 128), ((64, 64, 64), 32, 32), ((4, 4, 12), 0, 6)]
+
+
+@pytest.fixture(scope="module")
+def ctx(slsf):
+    slsf.build()
+    c = slsf.Context()
+    yield c
+    c.close()
+
+
+def task(slsf, ctx, orc, dims, seed):
+    jxy, jz = np.full(dims[2], 1.0), orc.uniform_disorder(dims[2], 0.5, 1.5, seed)
+    t = slsf.Task(ctx, dims, jxy, jz, 1.2, seed=seed)
+    t.init_random()
+    return t
+
+
+def flat(c):
+    return np.concatenate([c["corr_x"], c["corr_y"], c["corr_xy"], c["corr_xy_by_z"].ravel(), c["corr_z"]])
+
+
+def test_batched_equals_single_task_and_oracle(slsf, ctx, orc):
+    tasks = [task(slsf, ctx, orc, d, 10 + k) for k, (d, _, _) in enumerate(SHAPES)]
+    for t, (d, rxy, rz) in zip(tasks, SHAPES):
+        nv = t.corr_setup(rxy, rz, 1, 3)
+        R, Rz = min(rxy, d[0] // 2, d[1] // 2), min(rz, d[2] // 2)
+        assert nv == 3 * R + d[2] * R + Rz
+    expect = [[] for _ in tasks]
+    for step in range(3):
+        ctx.batch_run(tasks, 1 + step)
+        for i, (t, (d, rxy, rz)) in enumerate(zip(tasks, SHAPES)):
+            expect[i].append(flat(t.correlations(rxy, rz)))
+        ctx.batch_correlations(tasks)
+    for i, (t, (d, rxy, rz)) in enumerate(zip(tasks, SHAPES)):
+        means, count = t.corr_bins()
+        assert count == 3 and means.shape == (3, t.corr_n_values)
+        # bins of one measurement: the mean is the value itself
+        assert np.array_equal(means, np.array(expect[i])), d
+        R, Rz = min(rxy, d[0] // 2, d[1] // 2), min(rz, d[2] // 2)
+        ref = orc.correlations_f32(d, t.theta, R, Rz)
+        got = expect[i][-1]
+        assert np.allclose(got[:R], ref["corr_x"], atol=2e-6)
+        assert np.allclose(got[R:2 * R], ref["corr_y"], atol=2e-6)
+        assert np.allclose(got[3 * R:3 * R + d[2] * R], ref["corr_xy_by_z"].ravel(), atol=5e-6)
+        assert np.allclose(got[3 * R + d[2] * R:], ref["corr_z"], atol=2e-6)
+    for t in tasks:
+        t.close()
+
+
+def test_bins_sum_in_measurement_order(slsf, ctx, orc):
+    a, b = task(slsf, ctx, orc, (8, 8, 8), 1), task(slsf, ctx, orc, (12, 8, 6), 2)
+    for t in (a, b):
+        t.corr_setup(4, 3, 3, 2)  # two bins of three; the seventh measurement is not kept
+    series = {id(a): [], id(b): []}
+    for _ in range(7):
+        ctx.batch_run([a, b], 1)
+        for t in (a, b):
+            series[id(t)].append(flat(t.correlations(4, 3)))
+        ctx.batch_correlations([b, a])  # order of the batch does not matter
+    for t in (a, b):
+        means, count = t.corr_bins()
+        assert count == 7
+        s = np.array(series[id(t)])
+        for row in range(2):
+            acc = np.zeros(s.shape[1])
+            for k in range(3):
+                acc = acc + s[3 * row + k]
+            assert np.array_equal(means[row], acc / 3.0)
+        # re-setup resets the count and the bins
+        t.corr_setup(4, 3, 3, 2)
+        m2, c2 = t.corr_bins()
+        assert c2 == 0 and not m2.any()
+        t.close()
+
+
+def test_setup_and_misuse_errors(slsf, ctx, orc):
+    before, _ = ctx.memory()
+    t = task(slsf, ctx, orc, (8, 8, 8), 3)
+    u = task(slsf, ctx, orc, (8, 8, 8), 4)
+    with pytest.raises(slsf.SlsfError) as e:
+        ctx.batch_correlations([t])
+    assert e.value.code == slsf.ERR_STATE and "slsf_task_corr_setup" in str(e.value)
+    with pytest.raises(slsf.SlsfError) as e:
+        t.corr_setup(2, 2, 0, 4)
+    assert "binsize must be positive" in str(e.value)
+    assert t.corr_setup(0, 0, 1, 4) == 0  # nothing to measure: no bins
+    used0, _ = ctx.memory()
+    t.corr_setup(4, 4, 1, 8)
+    u.corr_setup(1, 0, 1, 1)
+    assert ctx.memory()[0] > used0
+    with pytest.raises(slsf.SlsfError) as e:
+        ctx.batch_correlations([t, u, t])
+    assert e.value.code == slsf.ERR_INVALID and "twice" in str(e.value)
+    with pytest.raises(slsf.SlsfError) as e:
+        t.corr_bins(9)
+    assert "more bin rows requested than the task keeps" in str(e.value)
+    long = slsf.Task(ctx, (800, 2, 2), np.ones(2), np.ones(2), 1.0)
+    with pytest.raises(slsf.SlsfError) as e:
+        long.corr_setup(1, 1, 1, 1)
+    assert "longer than 775 sites" in str(e.value)
+    with pytest.raises(slsf.SlsfError) as e:
+        long.correlations(1, 1)
+    assert "longer than 775 sites" in str(e.value)
+    long.close()
+    t.close()
+    u.close()
+    assert ctx.memory()[0] == before  # the bins went with their tasks
+
+
+def test_budget_counts_correlation_bins(slsf, orc):
+    one = slsf.load().slsf_task_bytes(8, 8, 8, 0)
+    with slsf.Context(budget_bytes=one + 4096) as small:
+        t = task(slsf, small, orc, (8, 8, 8), 5)
+        with pytest.raises(slsf.SlsfError) as e:
+            t.corr_setup(4, 4, 1, 1000)
+        assert e.value.code == slsf.ERR_BUDGET
+        assert t.corr_setup(1, 1, 1, 1) > 0
+        t.close()
