@@ -261,6 +261,22 @@ int slsf_batch_correlations(slsf_ctx* ctx, slsf_task* const* tasks, size_t n_tas
 int slsf_task_get_bins(const slsf_task* task, double* bins, size_t n_rows, uint64_t* measurements);
 int slsf_task_reset_bins(slsf_task* task);
 
+/* Device state of a task as one byte blob, for checkpoints: the parts of
+ * ThetaModel's serialized state (src/model.rs:255-271) that live on the
+ * device -- angles, counters (Metropolis sweeps, Wolff steps, measurements,
+ * correlation measurements), bin sums and correlation bin sums -- with the
+ * task's configuration to check against.  The random streams are keyed by
+ * (seed, counters, site), so a task loaded from a state continues exactly as
+ * the saved one would have.  `user` carries four caller words through the
+ * blob (e.g. host-side acceptance sums; may be NULL).  Loading requires a
+ * task created with the same description (dimensions, seed, temperature,
+ * proposal width, Wolff steps, couplings, thermalization, bins) and the same
+ * correlation set-up; anything else fails with "state does not match the
+ * task: ...". */
+int slsf_task_state_size(const slsf_task* task, size_t* bytes);
+int slsf_task_state_save(const slsf_task* task, const uint64_t user[4], void* buf, size_t bytes);
+int slsf_task_state_load(slsf_task* task, const void* buf, size_t bytes, uint64_t user[4]);
+
 /* ---------------------------------------------------------------- batches */
 
 /* Runs n_sweeps sweeps of every task in `tasks` in one persistent launch

@@ -162,6 +162,16 @@ int slsf_server_wait_idle(slsf_server* s, double timeout_s);
 /* Moves up to `max` finished results to `out` (thread-safe). */
 int slsf_server_poll(slsf_server* s, slsf_result* out, size_t max, size_t* n);
 int slsf_server_stats_get(slsf_server* s, slsf_server_stats* out);
+/* Checkpoint of the serving loop (carlo-mc's checkpoint directory and
+ * restart, src/results.rs:211-239): with the worker stopped, writes one file
+ * per unfinished request to `dir` -- queued ones as submitted, running ones
+ * with their progress and the task's device state (slsf_task_state_save) --
+ * and keeps running them.  Finished results stay with slsf_server_poll. */
+int slsf_server_checkpoint(slsf_server* s, const char* dir, size_t* n_saved);
+/* Queues the requests a checkpoint saved in `dir`, in tag order; running
+ * ones resume where they stopped and finish with the results they would
+ * have had without the interruption. */
+int slsf_server_restore(slsf_server* s, const char* dir, size_t* n_restored);
 
 #ifdef __cplusplus
 }

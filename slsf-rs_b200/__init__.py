@@ -109,6 +109,9 @@ SIGNATURES = {
     "slsf_task_corr_setup": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_size_t)]),
     "slsf_task_corr_bins": (C.c_int, [_P, _F64P, C.c_size_t, _U64P]),
     "slsf_batch_correlations": (C.c_int, [_P, C.POINTER(_P), C.c_size_t]),
+    "slsf_task_state_size": (C.c_int, [_P, C.POINTER(C.c_size_t)]),
+    "slsf_task_state_save": (C.c_int, [_P, _U64P, _P, C.c_size_t]),
+    "slsf_task_state_load": (C.c_int, [_P, _P, C.c_size_t, _U64P]),
     "slsf_task_reset_bins": (C.c_int, [_P]),
     "slsf_batch_run": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_uint32, C.POINTER(SweepStats)]),
     "slsf_batch_get_bins": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_size_t, _F64P, _U64P]),
@@ -437,6 +440,22 @@ class Task:
         check(load().slsf_task_corr_bins(self.h, _ptr(out, C.c_double), n_rows, C.byref(m)))
         return out[:n_rows, : self.corr_n_values], m.value
 
+    def save_state(self, user=(0, 0, 0, 0)) -> bytes:
+        """The task's device state (slsf_task_state_save) with four caller words."""
+        n = C.c_size_t()
+        check(load().slsf_task_state_size(self.h, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        words = (C.c_uint64 * 4)(*user)
+        check(load().slsf_task_state_save(self.h, words, buf, n.value))
+        return buf.raw
+
+    def load_state(self, blob: bytes):
+        """Restores a saved state; returns its four caller words."""
+        words = (C.c_uint64 * 4)()
+        buf = C.create_string_buffer(blob, len(blob))
+        check(load().slsf_task_state_load(self.h, buf, len(blob), words))
+        return tuple(words)
+
     def bins(self):
         out = np.zeros((max(self.n_bins, 1), BIN_COLS))
         m = C.c_uint64()
@@ -580,6 +599,8 @@ HOST_SIGNATURES = {
     "slsf_server_wait_idle": (C.c_int, [_P, C.c_double]),
     "slsf_server_poll": (C.c_int, [_P, C.POINTER(Result), C.c_size_t, C.POINTER(C.c_size_t)]),
     "slsf_server_stats_get": (C.c_int, [_P, C.POINTER(ServerStats)]),
+    "slsf_server_checkpoint": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_size_t)]),
+    "slsf_server_restore": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_size_t)]),
 }
 
 _host = None
@@ -715,6 +736,18 @@ class Server:
         n = C.c_size_t()
         host_check(load_host().slsf_server_poll(self.h, buf, max_results, C.byref(n)))
         return [buf[i].as_dict() for i in range(n.value)]
+
+    def checkpoint(self, directory):
+        """Writes every unfinished request to `directory` (worker stopped); returns the count."""
+        n = C.c_size_t()
+        host_check(load_host().slsf_server_checkpoint(self.h, str(directory).encode(), C.byref(n)))
+        return n.value
+
+    def restore(self, directory):
+        """Queues the requests saved in `directory`; returns the count."""
+        n = C.c_size_t()
+        host_check(load_host().slsf_server_restore(self.h, str(directory).encode(), C.byref(n)))
+        return n.value
 
     def stats(self):
         st = ServerStats()

@@ -865,6 +865,135 @@ int slsf_task_get_bins(const slsf_task* t, double* bins, size_t n_rows, uint64_t
     return SLSF_OK;
 }
 
+/* ---- device state blob (checkpoints) ----
+ * Layout, little-endian: StateHeader, then J_xy and J_z as stored on the
+ * device (FP32, L_z each), theta (FP32, x fastest), the bin sums
+ * ([n_bins][12] FP64) and the correlation bin sums ([corr_n_bins][values]
+ * FP64), each section padded to 8 bytes. */
+namespace {
+
+struct StateHeader {
+    char magic[8]; /* "SLSFST01" */
+    uint32_t lx, ly, lz, wolff_steps;
+    uint64_t seed;
+    double temperature, width;
+    uint32_t thermalization, binsize, n_bins, corr_rxy;
+    uint32_t corr_rz, corr_binsize, corr_n_bins, corr_values;
+    uint64_t metro_sweeps, wolff_done, measurements, corr_count;
+    uint64_t user[4];
+    uint64_t bytes; /* the whole blob */
+};
+static_assert(sizeof(StateHeader) % 8 == 0, "state header is 8-byte aligned");
+constexpr char kStateMagic[8] = {'S', 'L', 'S', 'F', 'S', 'T', '0', '1'};
+
+uint64_t pad8(uint64_t b) { return (b + 7) & ~7ull; }
+
+struct StateLayout {
+    uint64_t j, theta, bins, corr, total;
+    uint32_t nv;
+};
+
+StateLayout state_layout(const slsf_task* t) {
+    StateLayout L;
+    L.nv = t->corr_block ? slsf::corr_values(t->lz, t->corr_rxy, t->corr_rz) : 0;
+    L.j = sizeof(StateHeader);
+    L.theta = L.j + pad8(8ull * t->lz);
+    L.bins = L.theta + pad8(4ull * t->volume);
+    L.corr = L.bins + 8ull * slsf::kBinCols * t->n_bins;
+    L.total = L.corr + 8ull * L.nv * (t->corr_block ? t->corr_n_bins : 0);
+    return L;
+}
+
+}  // namespace
+
+int slsf_task_state_size(const slsf_task* t, size_t* bytes) {
+    if (!t || !bytes) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    *bytes = state_layout(t).total;
+    return SLSF_OK;
+}
+
+int slsf_task_state_save(const slsf_task* t, const uint64_t user[4], void* buf, size_t bytes) {
+    if (!t || !buf) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    const StateLayout L = state_layout(t);
+    if (bytes < L.total) return set_error(SLSF_ERR_INVALID, "state buffer is smaller than slsf_task_state_size");
+    if (int rc = bind_device(t->ctx)) return rc;
+    char* b = static_cast<char*>(buf);
+    std::memset(b, 0, L.total);
+    StateHeader h;
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, kStateMagic, 8);
+    h.lx = t->lx, h.ly = t->ly, h.lz = t->lz, h.wolff_steps = t->wolff_steps;
+    h.seed = t->seed;
+    h.temperature = t->temperature, h.width = t->width;
+    h.thermalization = t->thermalization, h.binsize = t->binsize, h.n_bins = t->n_bins;
+    h.corr_rxy = t->corr_rxy, h.corr_rz = t->corr_rz, h.corr_binsize = t->corr_binsize;
+    h.corr_n_bins = t->corr_block ? t->corr_n_bins : 0, h.corr_values = L.nv;
+    h.metro_sweeps = t->metro_sweeps, h.wolff_done = t->wolff_done, h.measurements = t->measurements;
+    h.corr_count = t->corr_count;
+    if (user) std::memcpy(h.user, user, sizeof(h.user));
+    h.bytes = L.total;
+    std::memcpy(b, &h, sizeof(h));
+    cudaStream_t st = t->ctx->stream;
+    SLSF_CUDA(cudaMemcpyAsync(b + L.j, t->jxy, 4ull * t->lz, cudaMemcpyDeviceToHost, st));
+    SLSF_CUDA(cudaMemcpyAsync(b + L.j + 4ull * t->lz, t->jz, 4ull * t->lz, cudaMemcpyDeviceToHost, st));
+    SLSF_CUDA(cudaMemcpyAsync(b + L.theta, t->theta, 4ull * t->volume, cudaMemcpyDeviceToHost, st));
+    if (t->n_bins)
+        SLSF_CUDA(cudaMemcpyAsync(b + L.bins, t->bins, L.corr - L.bins, cudaMemcpyDeviceToHost, st));
+    if (L.total > L.corr)
+        SLSF_CUDA(cudaMemcpyAsync(b + L.corr, t->corr_bins, L.total - L.corr, cudaMemcpyDeviceToHost, st));
+    SLSF_CUDA(cudaStreamSynchronize(st));
+    return SLSF_OK;
+}
+
+int slsf_task_state_load(slsf_task* t, const void* buf, size_t bytes, uint64_t user[4]) {
+    if (!t || !buf) return set_error(SLSF_ERR_INVALID, "NULL argument");
+    if (int rc = check_free(t)) return rc;
+    const StateLayout L = state_layout(t);
+    const char* b = static_cast<const char*>(buf);
+    StateHeader h;
+    if (bytes < sizeof(h)) return set_error(SLSF_ERR_INVALID, "not a task state (too short)");
+    std::memcpy(&h, b, sizeof(h));
+    if (std::memcmp(h.magic, kStateMagic, 8) != 0) return set_error(SLSF_ERR_INVALID, "not a task state (bad magic)");
+    auto mismatch = [](const char* what) {
+        return set_error(SLSF_ERR_INVALID, std::string("state does not match the task: ") + what);
+    };
+    if (h.bytes != bytes || bytes != L.total) return mismatch("size");
+    if (h.lx != t->lx || h.ly != t->ly || h.lz != t->lz) return mismatch("lattice dimensions");
+    if (h.seed != t->seed) return mismatch("seed");
+    if (std::memcmp(&h.temperature, &t->temperature, 8) || std::memcmp(&h.width, &t->width, 8))
+        return mismatch("temperature or proposal width");
+    if (h.wolff_steps != t->wolff_steps) return mismatch("wolff_steps");
+    if (h.thermalization != t->thermalization || h.binsize != t->binsize || h.n_bins != t->n_bins)
+        return mismatch("thermalization or bins");
+    const uint32_t corr_n_bins = t->corr_block ? t->corr_n_bins : 0;
+    if (h.corr_rxy != t->corr_rxy || h.corr_rz != t->corr_rz || h.corr_binsize != t->corr_binsize ||
+        h.corr_n_bins != corr_n_bins || h.corr_values != L.nv)
+        return mismatch("correlation set-up");
+    if (int rc = bind_device(t->ctx)) return rc;
+    cudaStream_t st = t->ctx->stream;
+    std::vector<float> j(2ull * t->lz);
+    SLSF_CUDA(cudaMemcpyAsync(j.data(), t->jxy, 4ull * t->lz, cudaMemcpyDeviceToHost, st));
+    SLSF_CUDA(cudaMemcpyAsync(j.data() + t->lz, t->jz, 4ull * t->lz, cudaMemcpyDeviceToHost, st));
+    SLSF_CUDA(cudaStreamSynchronize(st));
+    if (std::memcmp(j.data(), b + L.j, 8ull * t->lz) != 0) return mismatch("layer couplings");
+    SLSF_CUDA(cudaMemcpyAsync(t->theta, b + L.theta, 4ull * t->volume, cudaMemcpyHostToDevice, st));
+    if (t->n_bins)
+        SLSF_CUDA(cudaMemcpyAsync(t->bins, b + L.bins, L.corr - L.bins, cudaMemcpyHostToDevice, st));
+    const unsigned long long corr_count = h.corr_count;
+    if (t->corr_block) {
+        if (L.total > L.corr)
+            SLSF_CUDA(cudaMemcpyAsync(t->corr_bins, b + L.corr, L.total - L.corr, cudaMemcpyHostToDevice, st));
+        SLSF_CUDA(cudaMemcpyAsync(t->corr_count_dev, &corr_count, 8, cudaMemcpyHostToDevice, st));
+    }
+    SLSF_CUDA(cudaStreamSynchronize(st));
+    t->metro_sweeps = h.metro_sweeps;
+    t->wolff_done = h.wolff_done;
+    t->measurements = h.measurements;
+    t->corr_count = t->corr_block ? h.corr_count : 0;
+    if (user) std::memcpy(user, h.user, sizeof(h.user));
+    return SLSF_OK;
+}
+
 int slsf_task_reset_bins(slsf_task* t) {
     if (!t) return set_error(SLSF_ERR_INVALID, "task is NULL");
     if (int rc = check_free(t)) return rc;

@@ -14,7 +14,9 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <list>
 #include <mutex>
 #include <string>
@@ -265,6 +267,11 @@ struct Pending {
     std::vector<double> jxy, jz;
     double submit_s;
     uint32_t bypassed = 0;
+    /* restored from a checkpoint while running: the task's device state,
+     * its bin plan and its progress */
+    std::vector<char> state;
+    uint32_t plan_binsize = 0, plan_n_bins = 0, remaining = 0;
+    uint64_t accepted = 0, cluster_sites = 0;
 };
 
 struct Active {
@@ -364,7 +371,10 @@ void admit(slsf_server* s) {
             const uint32_t measured = p.req.sweeps > p.req.thermalization ? p.req.sweeps - p.req.thermalization : 0;
             /* complete bins only (carlo drops a partial last bin) */
             uint32_t n_bins, binsize;
-            if (p.req.binsize) {
+            if (!p.state.empty()) {
+                binsize = p.plan_binsize;
+                n_bins = p.plan_n_bins;
+            } else if (p.req.binsize) {
                 binsize = p.req.binsize;
                 n_bins = std::max<uint32_t>(1, measured / binsize);
             } else {
@@ -414,7 +424,9 @@ void admit(slsf_server* s) {
         d.binsize = k.binsize;
         d.n_bins = k.n_bins;
         k.rc = slsf_task_create(s->ctx, &d, &k.task);
-        if (k.rc == SLSF_OK) k.rc = slsf_task_init_random(k.task);
+        if (k.rc == SLSF_OK)
+            k.rc = k.p.state.empty() ? slsf_task_init_random(k.task)
+                                     : slsf_task_state_load(k.task, k.p.state.data(), k.p.state.size(), nullptr);
         if (k.rc != SLSF_OK) {
             char buf[160];
             slsf_last_error(buf, sizeof(buf));
@@ -438,7 +450,11 @@ void admit(slsf_server* s) {
         a.p = std::move(k.p);
         a.task = k.task;
         a.bytes = k.bytes;
-        a.remaining = a.p.req.sweeps;
+        a.remaining = a.p.state.empty() ? a.p.req.sweeps : a.p.remaining;
+        a.accepted = a.p.accepted;
+        a.cluster_sites = a.p.cluster_sites;
+        a.p.state.clear();
+        a.p.state.shrink_to_fit();
         a.binsize = k.binsize;
         a.n_bins = k.n_bins;
         a.admit_s = t;
@@ -739,6 +755,136 @@ int slsf_server_stats_get(slsf_server* s, slsf_server_stats* out) {
     if (!s || !out) return fail(SLSF_ERR_INVALID, "NULL argument");
     std::lock_guard<std::mutex> lock(s->mu);
     *out = s->stats;
+    return SLSF_OK;
+}
+
+/* ---- checkpoints ----
+ * One file per unfinished request, request_<tag>.ckpt: RequestRecord, J_xy
+ * and J_z (FP64, L_z each), then, for a running request, the task's device
+ * state (slsf_task_state_save). */
+namespace {
+
+struct RequestRecord {
+    char magic[8]; /* "SLSFRQ01" */
+    uint64_t tag, seed;
+    uint32_t lx, ly, lz, wolff_steps;
+    double temperature, proposal_width;
+    uint32_t sweeps, thermalization, n_bins, binsize;
+    uint32_t running, remaining, plan_binsize, plan_n_bins;
+    uint64_t accepted, cluster_sites, state_bytes;
+};
+constexpr char kRequestMagic[8] = {'S', 'L', 'S', 'F', 'R', 'Q', '0', '1'};
+
+int write_request(const std::string& dir, const Pending& p, const Active* a) {
+    RequestRecord r;
+    std::memset(&r, 0, sizeof(r));
+    std::memcpy(r.magic, kRequestMagic, 8);
+    r.tag = p.req.tag, r.seed = p.req.seed;
+    r.lx = p.req.lx, r.ly = p.req.ly, r.lz = p.req.lz, r.wolff_steps = p.req.wolff_steps;
+    r.temperature = p.req.temperature, r.proposal_width = p.req.proposal_width;
+    r.sweeps = p.req.sweeps, r.thermalization = p.req.thermalization, r.n_bins = p.req.n_bins;
+    r.binsize = p.req.binsize;
+    std::vector<char> state;
+    if (a) {
+        size_t n = 0;
+        if (int rc = slsf_task_state_size(a->task, &n)) return gpu_fail(rc);
+        state.resize(n);
+        if (int rc = slsf_task_state_save(a->task, nullptr, state.data(), n)) return gpu_fail(rc);
+        r.running = 1, r.remaining = a->remaining, r.plan_binsize = a->binsize, r.plan_n_bins = a->n_bins;
+        r.accepted = a->accepted, r.cluster_sites = a->cluster_sites, r.state_bytes = n;
+    }
+    const std::string path = dir + "/request_" + std::to_string(p.req.tag) + ".ckpt";
+    const std::string tmp = path + ".tmp";
+    std::FILE* f = std::fopen(tmp.c_str(), "wb");
+    if (!f) return fail(SLSF_ERR_INVALID, "cannot write " + tmp);
+    bool ok = std::fwrite(&r, sizeof(r), 1, f) == 1;
+    ok = ok && std::fwrite(p.jxy.data(), 8, p.jxy.size(), f) == p.jxy.size();
+    ok = ok && std::fwrite(p.jz.data(), 8, p.jz.size(), f) == p.jz.size();
+    ok = ok && (state.empty() || std::fwrite(state.data(), 1, state.size(), f) == state.size());
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok || std::rename(tmp.c_str(), path.c_str()) != 0) return fail(SLSF_ERR_INVALID, "cannot write " + path);
+    return SLSF_OK;
+}
+
+int read_request(const std::string& path, Pending* p) {
+    std::FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) return fail(SLSF_ERR_INVALID, "cannot read " + path);
+    RequestRecord r;
+    bool ok = std::fread(&r, sizeof(r), 1, f) == 1 && std::memcmp(r.magic, kRequestMagic, 8) == 0;
+    if (ok) {
+        std::memset(&p->req, 0, sizeof(p->req));
+        p->req.tag = r.tag, p->req.seed = r.seed;
+        p->req.lx = r.lx, p->req.ly = r.ly, p->req.lz = r.lz, p->req.wolff_steps = r.wolff_steps;
+        p->req.temperature = r.temperature, p->req.proposal_width = r.proposal_width;
+        p->req.sweeps = r.sweeps, p->req.thermalization = r.thermalization, p->req.n_bins = r.n_bins;
+        p->req.binsize = r.binsize;
+        p->jxy.resize(r.lz);
+        p->jz.resize(r.lz);
+        ok = std::fread(p->jxy.data(), 8, r.lz, f) == r.lz && std::fread(p->jz.data(), 8, r.lz, f) == r.lz;
+    }
+    if (ok && r.running) {
+        p->state.resize(r.state_bytes);
+        ok = r.state_bytes > 0 && std::fread(p->state.data(), 1, r.state_bytes, f) == r.state_bytes &&
+             r.plan_binsize > 0 && r.plan_n_bins > 0 && r.remaining <= r.sweeps;
+        p->plan_binsize = r.plan_binsize, p->plan_n_bins = r.plan_n_bins, p->remaining = r.remaining;
+        p->accepted = r.accepted, p->cluster_sites = r.cluster_sites;
+    }
+    ok = ok && std::fgetc(f) == EOF;
+    std::fclose(f);
+    if (!ok) return fail(SLSF_ERR_INVALID, "not a request checkpoint: " + path);
+    return SLSF_OK;
+}
+
+}  // namespace
+
+int slsf_server_checkpoint(slsf_server* s, const char* dir, size_t* n_saved) {
+    if (!s || !dir) return fail(SLSF_ERR_INVALID, "NULL argument");
+    if (s->running) return fail(SLSF_ERR_STATE, "the server's worker thread is running; stop it first");
+    std::error_code ec;
+    std::filesystem::create_directories(dir, ec);
+    if (ec) return fail(SLSF_ERR_INVALID, std::string("cannot create ") + dir);
+    std::lock_guard<std::mutex> lock(s->mu);
+    size_t n = 0;
+    for (const Active& a : s->active) {
+        if (s->cancel.count(a.p.req.tag)) continue;
+        if (int rc = write_request(dir, a.p, &a)) return rc;
+        ++n;
+    }
+    for (const Pending& p : s->queue) {
+        if (int rc = write_request(dir, p, nullptr)) return rc;
+        ++n;
+    }
+    if (n_saved) *n_saved = n;
+    return SLSF_OK;
+}
+
+int slsf_server_restore(slsf_server* s, const char* dir, size_t* n_restored) {
+    if (!s || !dir) return fail(SLSF_ERR_INVALID, "NULL argument");
+    std::vector<Pending> got;
+    std::error_code ec;
+    for (const auto& e : std::filesystem::directory_iterator(dir, ec)) {
+        const std::string name = e.path().filename().string();
+        if (name.rfind("request_", 0) != 0 || e.path().extension() != ".ckpt") continue;
+        Pending p;
+        if (int rc = read_request(e.path().string(), &p)) return rc;
+        got.push_back(std::move(p));
+    }
+    if (ec) return fail(SLSF_ERR_INVALID, std::string("cannot read ") + dir);
+    std::sort(got.begin(), got.end(), [](const Pending& a, const Pending& b) { return a.req.tag < b.req.tag; });
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (Pending& p : got) {
+        p.submit_s = now_s(s->t0);
+        s->stats.submitted++;
+        const std::string invalid = validate(p);
+        if (!invalid.empty()) {
+            s->results.push_back(make_result(p, SLSF_ERR_INVALID, invalid, p.submit_s));
+            s->stats.failed++;
+            continue;
+        }
+        s->queue.push_back(std::move(p));
+    }
+    s->cv.notify_all();
+    if (n_restored) *n_restored = got.size();
     return SLSF_OK;
 }
 

@@ -93,6 +93,7 @@ class JobConfig:
     checkpoint_time_s: int = 30 * 60
     job_name: str = "xy_theta_rust"
     output_dir: Optional[str] = None
+    checkpoint: bool = False
 
 
 def _u64(text: str, what: str, value: str) -> int:
@@ -178,6 +179,7 @@ def config_from_toml(text: str) -> JobConfig:
     if "name" in spec:
         cfg.job_name = spec["name"]
     cfg.output_dir = spec.get("output_dir")
+    cfg.checkpoint = bool(spec.get("checkpoint", False))
     if "run_time" in spec:
         try:
             cfg.run_time_s = parse_duration(spec["run_time"])
@@ -331,72 +333,204 @@ def _observables(est: dict, corr: Optional[dict] = None):
     return dict(sorted(out.items()))
 
 
-def _run_served(pkg, ctx, tasks, epoch_sweeps):
-    """Tasks without correlations through the server: {task index: estimates}."""
+class Stopped(Exception):
+    """The run time ran out; the checkpoint holds the unfinished work."""
+
+
+class Checkpoints:
+    """carlo-mc's run-time and checkpoint-time schedule (ThetaJobConfig
+    run_time / checkpoint_time, src/model.rs:140-156) over a checkpoint
+    directory: a checkpoint every `every_s` seconds, and at `run_time_s` a
+    last one and a stop.  With restart, work saved in the directory is
+    resumed instead of started again."""
+
+    def __init__(self, directory, restart=False, run_time_s=None, every_s=None):
+        import time
+
+        self.dir = str(directory)
+        self.restart = restart
+        self.t0 = self.last = time.monotonic()
+        self.run_time_s = float("inf") if run_time_s is None else float(run_time_s)
+        self.every_s = float("inf") if every_s is None else float(every_s)
+        os.makedirs(self.dir, exist_ok=True)
+
+    def wait_s(self):
+        import time
+
+        now = time.monotonic()
+        return min(365 * 86400.0, max(0.01, min(self.last + self.every_s, self.t0 + self.run_time_s) - now))
+
+    def due(self):
+        """None, "checkpoint" or "stop"."""
+        import time
+
+        now = time.monotonic()
+        if now >= self.t0 + self.run_time_s:
+            return "stop"
+        if now >= self.last + self.every_s:
+            return "checkpoint"
+        return None
+
+    def saved(self):
+        import time
+
+        self.last = time.monotonic()
+
+    def path(self, *parts):
+        return os.path.join(self.dir, *parts)
+
+
+def _swap_dir(new, old):
+    """Replaces directory `old` by `new` (a checkpoint is whole or absent)."""
+    import shutil
+
+    if os.path.isdir(old):
+        shutil.rmtree(old)
+    os.replace(new, old)
+
+
+def _est_to_json(est):
+    return {k: (list(v) if isinstance(v, tuple) else v) for k, v in est.items()}
+
+
+def _est_from_json(d):
+    return {k: (tuple(v) if isinstance(v, list) else v) for k, v in d.items()}
+
+
+def _run_served(pkg, ctx, tasks, epoch_sweeps, ck: Optional[Checkpoints] = None):
+    """Tasks without correlations through the server: {task index: estimates}.
+    With checkpoints the server is stopped at each one, its finished results
+    kept in served/finished.json and its unfinished requests written by
+    slsf_server_checkpoint to served/; a restart restores both."""
     names = {k: t["name"] for k, t in tasks}
     srv = pkg.Server(ctx, epoch_sweeps=epoch_sweeps)
     out = {}
-    try:
-        for k, t in tasks:
-            srv.submit(k, (t["l_x"], t["l_y"], t["l_z"]), t["temperature"], t["seed"], t["j_xy_array"],
-                       t["j_z_array"], t["thermalization"] + t["sweeps"], thermalization=t["thermalization"],
-                       proposal_width=t["proposal_width"], wolff_steps=t["wolff_steps"], binsize=t["binsize"])
-        srv.start()
-        srv.wait_idle(365 * 86400.0)
-        srv.stop()
+
+    def collect():
         for r in srv.poll(len(tasks) + 16):
             if r["status"] != pkg.OK:
                 raise pkg.SlsfError(r["status"], f"task {names[r['tag']]}: {r['message']}")
             out[r["tag"]] = r["est"]
+
+    try:
+        sdir = ck.path("served") if ck else None
+        if ck and ck.restart and os.path.isdir(sdir):
+            with open(os.path.join(sdir, "finished.json"), encoding="utf-8") as f:
+                out.update({int(k): _est_from_json(v) for k, v in json.load(f).items()})
+            srv.restore(sdir)
+        else:
+            for k, t in tasks:
+                srv.submit(k, (t["l_x"], t["l_y"], t["l_z"]), t["temperature"], t["seed"], t["j_xy_array"],
+                           t["j_z_array"], t["thermalization"] + t["sweeps"], thermalization=t["thermalization"],
+                           proposal_width=t["proposal_width"], wolff_steps=t["wolff_steps"], binsize=t["binsize"])
+        srv.start()
+        while True:
+            try:
+                srv.wait_idle(ck.wait_s() if ck else 365 * 86400.0)
+                break
+            except pkg.SlsfError as e:
+                if e.code != pkg.ERR_TIMEOUT or ck is None:
+                    raise
+            due = ck.due()
+            if due is None:
+                continue
+            srv.stop()
+            collect()
+            tmp = sdir + ".new"
+            os.makedirs(tmp, exist_ok=True)
+            with open(os.path.join(tmp, "finished.json"), "w", encoding="utf-8") as f:
+                json.dump({str(k): _est_to_json(v) for k, v in out.items()}, f)
+            srv.checkpoint(tmp)
+            _swap_dir(tmp, sdir)
+            ck.saved()
+            if due == "stop":
+                raise Stopped(out)
+            srv.start()
+        srv.stop()
+        collect()
+        if ck:
+            # all finished: the checkpoint keeps the results and no requests
+            tmp = sdir + ".new"
+            os.makedirs(tmp, exist_ok=True)
+            with open(os.path.join(tmp, "finished.json"), "w", encoding="utf-8") as f:
+                json.dump({str(k): _est_to_json(v) for k, v in out.items()}, f)
+            _swap_dir(tmp, sdir)
     finally:
         srv.close()
     return out
 
 
-def _run_correlated(pkg, ctx, group):
+def _run_correlated(pkg, ctx, group, ck: Optional[Checkpoints] = None, gdir: Optional[str] = None):
     """One group of tasks sharing (thermalization, sweeps, correlation_interval)
     through the batched kernels: thermalization, then per correlation
     measurement m (m % interval == 0) the sweeps up to it and one batched
     correlation launch that adds every task's values into its correlation bins
     on the device.  A correlation series is binned with the task's bin size
     (BinnedEstimate::from_samples); a series shorter than one bin forms one
-    bin."""
+    bin.  With checkpoints, every task's device state (slsf_task_state_save,
+    the acceptance count riding in its caller words) goes to `gdir` between
+    measurements when one is due; a restart loads them and continues."""
     import ctypes as C
 
+    if ck and ck.restart and os.path.exists(os.path.join(gdir, "finished.json")):
+        with open(os.path.join(gdir, "finished.json"), encoding="utf-8") as f:
+            saved = json.load(f)
+        return [(_est_from_json(e), {k: tuple(v) for k, v in c.items()}) for e, c in saved]
     t0 = group[0][1]
     therm, sweeps, interval = t0["thermalization"], t0["sweeps"], t0["correlation_interval"]
     n_corr = (sweeps + interval - 1) // interval
-    objs, radii, corr_bin = [], [], []
+    objs, radii = [], []
     try:
         for _, t in group:
             o = pkg.Task(ctx, (t["l_x"], t["l_y"], t["l_z"]), t["j_xy_array"], t["j_z_array"], t["temperature"],
                          proposal_width=t["proposal_width"], wolff_steps=t["wolff_steps"], seed=t["seed"],
                          thermalization=therm, binsize=t["binsize"], n_bins=t["sweeps"] // t["binsize"])
-            o.init_random()
             objs.append(o)
             radii.append((min(t["correlation_rmax_xy"], t["l_x"] // 2, t["l_y"] // 2),
                           min(t["correlation_rmax_z"], t["l_z"] // 2)))
             cb = min(t["binsize"], n_corr)
-            corr_bin.append(cb)
             o.corr_setup(*radii[-1], cb, n_corr // cb)
+        accepted = np.zeros(len(objs), dtype=np.uint64)
+        resumed = ck and ck.restart and os.path.isdir(gdir)
+        for i, o in enumerate(objs):
+            if resumed:
+                with open(os.path.join(gdir, f"task_{group[i][0]}.state"), "rb") as f:
+                    accepted[i] = o.load_state(f.read())[0]
+            else:
+                o.init_random()
         handles = ctx.handle_array(objs)
         measured = [o for o in objs if o.corr_n_values]
         corr_handles = ctx.handle_array(measured)
-        accepted = np.zeros(len(objs))
+        pos = objs[0].counters[0]
+        corr_done = measured[0].corr_bins(0)[1] if measured else 0
 
         def advance(n):
+            nonlocal pos
             if n:
                 for i, s in enumerate(ctx.batch_run(objs, n, handles)):
                     accepted[i] += s["accepted"]
+                pos += n
 
-        advance(therm)
-        done = 0
-        for m in range(0, sweeps, interval):
-            advance(m + 1 - done)
-            done = m + 1
+        def save(due):
+            tmp = gdir + ".new"
+            os.makedirs(tmp, exist_ok=True)
+            for i, o in enumerate(objs):
+                with open(os.path.join(tmp, f"task_{group[i][0]}.state"), "wb") as f:
+                    f.write(o.save_state(user=(int(accepted[i]), 0, 0, 0)))
+            _swap_dir(tmp, gdir)
+            ck.saved()
+            if due == "stop":
+                raise Stopped()
+
+        if pos < therm:
+            advance(therm - pos)
+        for m in range(corr_done * interval, sweeps, interval):
+            advance(therm + m + 1 - pos)
             if measured:
                 ctx.batch_correlations(measured, corr_handles)
-        advance(sweeps - done)
+            if ck and (due := ck.due()):
+                save(due)
+        advance(therm + sweeps - pos)
         host = pkg.load_host()
         out = []
         for i, ((_, t), o) in enumerate(zip(group, objs)):
@@ -408,7 +542,7 @@ def _run_correlated(pkg, ctx, group):
                                                          1.0 / t["temperature"], C.byref(e)))
             est = e.as_dict()
             est["measurements"] = meas
-            est["acceptance"] = accepted[i] / (volume * (therm + sweeps))
+            est["acceptance"] = float(accepted[i]) / (volume * (therm + sweeps))
             corr = {}
             if o.corr_n_values:
                 means, count = o.corr_bins()
@@ -418,32 +552,55 @@ def _run_correlated(pkg, ctx, group):
                     r = pkg.binned_estimate(means[:, j], 1)
                     corr[name] = (r["mean"], r["stderr"])
             out.append((est, corr))
+        if ck:
+            tmp = gdir + ".new"
+            os.makedirs(tmp, exist_ok=True)
+            with open(os.path.join(tmp, "finished.json"), "w", encoding="utf-8") as f:
+                json.dump([[_est_to_json(e), {k: list(v) for k, v in c.items()}] for e, c in out], f)
+            _swap_dir(tmp, gdir)
         return out
     finally:
         for o in objs:
             o.close()
 
 
-def run_job(ctx, cfg: JobConfig, rank: int = 0, world_size: int = 1, epoch_sweeps: int = 100, tasks=None,
-            group_size: int = 1024):
-    """A rank's share of the job; returns the ThetaJobResult record."""
+def run_job_checkpointed(ctx, cfg: JobConfig, rank: int = 0, world_size: int = 1, epoch_sweeps: int = 100,
+                         tasks=None, group_size: int = 1024, ck: Optional[Checkpoints] = None):
+    """A rank's share of the job; returns (ThetaJobResult record, summary).
+    Without `ck` every task runs to the end.  With it, the run stops once
+    its run time is spent, after a last checkpoint; the record then holds
+    the finished tasks only and the summary says stopped_early (JobRunSummary,
+    src/model.rs:108-115)."""
+    import time
+
     pkg = _package()
+    started = time.monotonic()
     tasks = tasks if tasks is not None else make_tasks(cfg)
     mine = [(k, tasks[k]) for k in selected(len(tasks), rank, world_size)]
     served = [(k, t) for k, t in mine if not measures_correlations(t)]
-    est = _run_served(pkg, ctx, served, epoch_sweeps) if served else {}
-    corr = {}
-    groups = {}
-    for k, t in mine:
-        if measures_correlations(t):
-            groups.setdefault((t["thermalization"], t["sweeps"], t["correlation_interval"]), []).append((k, t))
-    for members in groups.values():
-        for lo in range(0, len(members), group_size):
-            chunk = members[lo: lo + group_size]
-            for (k, _), (e, c) in zip(chunk, _run_correlated(pkg, ctx, chunk)):
-                est[k], corr[k] = e, c
+    est, corr = {}, {}
+    stopped = False
+    try:
+        if served:
+            est.update(_run_served(pkg, ctx, served, epoch_sweeps, ck))
+        groups = {}
+        for k, t in mine:
+            if measures_correlations(t):
+                groups.setdefault((t["thermalization"], t["sweeps"], t["correlation_interval"]), []).append((k, t))
+        for (therm, sweeps, interval), members in groups.items():
+            for lo in range(0, len(members), group_size):
+                chunk = members[lo: lo + group_size]
+                gdir = ck.path(f"group_{therm}_{sweeps}_{interval}_{lo // group_size}") if ck else None
+                for (k, _), (e, c) in zip(chunk, _run_correlated(pkg, ctx, chunk, ck, gdir)):
+                    est[k], corr[k] = e, c
+    except Stopped as s:
+        stopped = True
+        if s.args:
+            est.update(s.args[0])
     out = []
     for k, t in mine:
+        if k not in est:
+            continue
         e = est[k]
         rec = {"task": t}
         if k:
@@ -451,7 +608,39 @@ def run_job(ctx, cfg: JobConfig, rank: int = 0, world_size: int = 1, epoch_sweep
         rec.update(observables=_observables(e, corr.get(k)), acceptance=e["acceptance"],
                    measurements=int(e["measurements"]))
         out.append(rec)
-    return {"job_name": cfg.job_name, "rank": rank, "world_size": world_size, "tasks": out}
+    result = {"job_name": cfg.job_name, "rank": rank, "world_size": world_size, "tasks": out}
+    summary = {"task_count": len(out), "elapsed_seconds": time.monotonic() - started, "stopped_early": stopped,
+               "checkpoint_dir": ck.dir if ck else None}
+    return result, summary
+
+
+def run_job(ctx, cfg: JobConfig, rank: int = 0, world_size: int = 1, epoch_sweeps: int = 100, tasks=None,
+            group_size: int = 1024):
+    """A rank's share of the job, run to the end; returns the ThetaJobResult record."""
+    return run_job_checkpointed(ctx, cfg, rank, world_size, epoch_sweeps, tasks, group_size)[0]
+
+
+def merge_results(results):
+    """merge_theta_job_results (src/results.rs:246-273): one record of all
+    ranks' tasks, sorted by task name, rank 0."""
+    if not results:
+        raise JobError("at least one rank result is required for merge")
+    first = results[0]
+    tasks = list(first["tasks"])
+    for r in results[1:]:
+        if r["job_name"] != first["job_name"]:
+            raise JobError("cannot merge results from different jobs")
+        if r["world_size"] != first["world_size"]:
+            raise JobError("cannot merge results with different world sizes")
+        tasks.extend(r["tasks"])
+    tasks.sort(key=lambda t: t["task"]["name"])
+    merged = []
+    for i, t in enumerate(tasks):
+        t = dict(t)
+        if t.get("task_index", 0) == 0 and i:
+            t["task_index"] = i
+        merged.append(t)
+    return {"job_name": first["job_name"], "rank": 0, "world_size": first["world_size"], "tasks": merged}
 
 
 def result_path(cfg: JobConfig, rank: int, output_dir: Optional[str] = None) -> str:
@@ -463,6 +652,34 @@ def result_path(cfg: JobConfig, rank: int, output_dir: Optional[str] = None) -> 
     if not d:
         d = os.path.dirname(cfg.job_name) or "results"
     return os.path.join(d, f"{os.path.basename(cfg.job_name) or cfg.job_name}.rank{rank}.results.json")
+
+
+def merged_path(cfg: JobConfig, output_dir: Optional[str] = None) -> str:
+    """`<dir>/<file name of job_name>.results.json` (merged_result_path_with_options,
+    src/model.rs:960-967)."""
+    return result_path(cfg, 0, output_dir).replace(".rank0.results.json", ".results.json")
+
+
+def checkpoint_dir(cfg: JobConfig, output_dir: Optional[str] = None) -> str:
+    """`<dir>/<file name of job_name>.data/checkpoints`, beside the
+    measurement directory of default_measurement_dir_with_options
+    (src/model.rs:969-980)."""
+    return result_path(cfg, 0, output_dir).replace(".rank0.results.json", ".data/checkpoints")
+
+
+def status(cfg: JobConfig, world_size: int = 1, output_dir: Optional[str] = None) -> str:
+    """theta_job_status_with_carlo (src/results.rs:377-395)."""
+    completed = files = 0
+    for rank in range(world_size):
+        path = result_path(cfg, rank, output_dir)
+        if os.path.exists(path):
+            files += 1
+            try:
+                with open(path, encoding="utf-8") as f:
+                    completed += len(json.load(f)["tasks"])
+            except (OSError, ValueError, KeyError):
+                pass
+    return f"{completed} theta task(s) completed; {files} of {world_size} rank result file(s) present"
 
 
 def write_result(result: dict, path: str) -> str:
@@ -477,18 +694,39 @@ def main(argv=None):
 
     p = argparse.ArgumentParser(description="Run a theta job file (the reference's TOML schema) on the B200 path.")
     p.add_argument("job", help="TOML job file")
+    p.add_argument("command", nargs="?", default="run", choices=("run", "merge", "status"))
     p.add_argument("--output-dir")
     p.add_argument("--rank", type=int, default=int(os.environ.get("RANK", 0)))
     p.add_argument("--world-size", type=int, default=int(os.environ.get("WORLD_SIZE", 1)))
     p.add_argument("--device", type=int, default=int(os.environ.get("LOCAL_RANK", 0)))
     p.add_argument("--epoch-sweeps", type=int, default=100)
+    p.add_argument("--checkpoint-dir", help="checkpoint here (default with `checkpoint = true`: "
+                                             "<output>/<job>.data/checkpoints)")
+    p.add_argument("--restart", action="store_true", help="resume from the checkpoint directory")
     args = p.parse_args(argv)
     cfg = load_job(args.job)
+    if args.command == "status":
+        print(status(cfg, args.world_size, args.output_dir))
+        return 0
+    if args.command == "merge":
+        paths = [result_path(cfg, r, args.output_dir) for r in range(args.world_size)]
+        results = []
+        for path in paths:
+            with open(path, encoding="utf-8") as f:
+                results.append(json.load(f))
+        out = write_result(merge_results(results), merged_path(cfg, args.output_dir))
+        print(f"merged {len(paths)} rank file(s) -> {out}")
+        return 0
     pkg = _package()
+    ck = None
+    cdir = args.checkpoint_dir or (checkpoint_dir(cfg, args.output_dir) if cfg.checkpoint or args.restart else None)
+    if cdir:
+        ck = Checkpoints(os.path.join(cdir, f"rank{args.rank}"), args.restart, cfg.run_time_s, cfg.checkpoint_time_s)
     with pkg.Context(args.device) as ctx:
-        res = run_job(ctx, cfg, args.rank, args.world_size, args.epoch_sweeps)
+        res, summary = run_job_checkpointed(ctx, cfg, args.rank, args.world_size, args.epoch_sweeps, ck=ck)
     path = write_result(res, result_path(cfg, args.rank, args.output_dir))
-    print(f"{len(res['tasks'])} tasks -> {path}")
+    note = "; stopped early: restart with --restart" if summary["stopped_early"] else ""
+    print(f"{len(res['tasks'])} tasks -> {path} ({summary['elapsed_seconds']:.1f} s){note}")
     return 0
 
 

@@ -160,3 +160,69 @@ def test_command_line_writes_result(slsf, jobs, tmp_path):
     for name in ("Energy", "RhoXY", "RhoZ", "Magnetization", "CorrX_r1", "CorrZ_r1", "CorrXY_z1_r1"):
         assert np.isfinite(task["observables"][name]["mean"]), name
     assert task["task"]["name"] == "L2x2x2_T2.000000_dJxy0.000000_dJz0.000000_sample1"
+
+
+class StopAt:
+    """A checkpoint schedule that asks for a stop at its n-th check."""
+
+    def __init__(self, jobs, directory, n, restart=False):
+        self.inner = jobs.Checkpoints(directory, restart)
+        self.n = n
+        self.dir = self.inner.dir
+        self.restart = restart
+
+    def wait_s(self):
+        return 0.001
+
+    def due(self):
+        self.n -= 1
+        return "stop" if self.n <= 0 else None
+
+    def saved(self):
+        pass
+
+    def path(self, *parts):
+        return self.inner.path(*parts)
+
+
+LONG_SERVED = SERVED.replace("L = [4, 6]", "L = [16, 32]").replace("sweeps = 16", "sweeps = 3000")
+
+
+@pytest.mark.parametrize("text,n_stop", [(LONG_SERVED, 1), (CORRELATED, 2)])
+def test_stop_and_restart_equals_uninterrupted(slsf, ctx, jobs, tmp_path, text, n_stop):
+    cfg = jobs.config_from_toml(text)
+    whole = jobs.run_job(ctx, cfg, epoch_sweeps=50)
+    first, s1 = jobs.run_job_checkpointed(ctx, cfg, epoch_sweeps=50, ck=StopAt(jobs, tmp_path, n_stop))
+    assert s1["stopped_early"] and len(first["tasks"]) < len(whole["tasks"])
+    again, s2 = jobs.run_job_checkpointed(ctx, cfg, epoch_sweeps=50,
+                                          ck=jobs.Checkpoints(tmp_path, restart=True))
+    assert not s2["stopped_early"]
+    want = {r["task"]["name"]: r for r in whole["tasks"]}
+    got = {r["task"]["name"]: r for r in again["tasks"]}
+    assert sorted(got) == sorted(want)
+    for name, rec in got.items():
+        w = want[name]
+        assert rec["measurements"] == w["measurements"] and rec["acceptance"] == w["acceptance"]
+        assert sorted(rec["observables"]) == sorted(w["observables"])
+        for obs, v in rec["observables"].items():
+            assert v["mean"] == pytest.approx(w["observables"][obs]["mean"], rel=1e-12, abs=1e-15), (name, obs)
+    # a restart of a finished run reads the saved results back
+    third, s3 = jobs.run_job_checkpointed(ctx, cfg, epoch_sweeps=50, ck=jobs.Checkpoints(tmp_path, restart=True))
+    assert third["tasks"] == again["tasks"]
+
+
+def test_merge_and_status(slsf, ctx, jobs, tmp_path):
+    cfg = jobs.config_from_toml(SERVED)
+    parts = [jobs.run_job(ctx, cfg, rank=r, world_size=2) for r in range(2)]
+    for r, p in enumerate(parts):
+        jobs.write_result(p, jobs.result_path(cfg, r, str(tmp_path)))
+    assert jobs.status(cfg, 2, str(tmp_path)) == "8 theta task(s) completed; 2 of 2 rank result file(s) present"
+    job = tmp_path / "job.toml"
+    job.write_text(SERVED)
+    assert jobs.main([str(job), "merge", "--world-size", "2", "--output-dir", str(tmp_path)]) == 0
+    merged = json.loads((tmp_path / "served_unit.results.json").read_text())
+    assert merged["rank"] == 0 and len(merged["tasks"]) == 8
+    names = [t["task"]["name"] for t in merged["tasks"]]
+    assert names == sorted(names)
+    with pytest.raises(jobs.JobError):
+        jobs.merge_results([parts[0], dict(parts[1], job_name="other")])
