@@ -353,6 +353,41 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
         }
         __syncthreads();
     }
+    if (g.lx == 32) {
+        /* A row is a warp (lane = x).  Each warp walks columns of rows along
+         * y -- (z, y segment) units, round robin -- so the projection of the
+         * +y row is the next row's own: two sincos per site instead of three,
+         * and no per-site index division. */
+        const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+        const uint32_t nseg = (nwarps + g.lz - 1) / g.lz;
+        const uint32_t seg = (g.ly + nseg - 1) / nseg;
+        for (uint32_t u = warp; u < g.lz * nseg; u += nwarps) {
+            const uint32_t z = u / nseg, y_lo = (u % nseg) * seg, y_hi = min(g.ly, y_lo + seg);
+            if (y_lo >= y_hi) continue;
+            const uint32_t zp_off = (z + 1 == g.lz) ? 0u : (z + 1) * g.plane; /* base of the +z plane */
+            const float jx = s.jxy[z], jzz = s.jz[z];
+            const uint32_t zbase = z * g.plane;
+            float ri = proj_of(s.th[slot(g, zbase + y_lo * 32u + lane, (lane + y_lo + z) & 1u)], cphi, sphi);
+            for (uint32_t y = y_lo; y < y_hi; ++y) {
+                const uint32_t idx = zbase + y * 32u + lane;
+                const uint32_t y1 = (y + 1 == g.ly) ? 0u : y + 1;
+                const float ryp = proj_of(s.th[slot(g, zbase + y1 * 32u + lane, (lane + y1 + z) & 1u)], cphi, sphi);
+                const float rzp = proj_of(s.th[slot(g, zp_off + y * 32u + lane, (lane + y + z + 1) & 1u)], cphi, sphi);
+                const float rxp = __shfl_sync(0xffffffffu, ri, (lane + 1) & 31u);
+                const slsf_u32x4 b = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, idx);
+                const uint32_t bal_x = __ballot_sync(0xffffffffu, wolff_bond_active(jx, ri, rxp, m2b, b.x));
+                const uint32_t bal_y = __ballot_sync(0xffffffffu, wolff_bond_active(jx, ri, ryp, m2b, b.y));
+                const uint32_t bal_z = __ballot_sync(0xffffffffu, wolff_bond_active(jzz, ri, rzp, m2b, b.z));
+                if (lane == 0) {
+                    const uint32_t row = y + g.ly * z;
+                    s.bx[row] = bal_x;
+                    s.by[row] = bal_y;
+                    s.bz[row] = bal_z;
+                }
+                ri = ryp;
+            }
+        }
+    } else
     /* Bond activation, one thread per site, warp-aligned site ranges. */
     for (uint32_t i0 = (threadIdx.x & ~31u); i0 < g.volume; i0 += blockDim.x) {
         const uint32_t idx = i0 + lane;
@@ -422,11 +457,48 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
     const uint32_t bound = t.loop_limit ? min(t.loop_limit, g.volume) : g.volume;
     uint32_t pass = 0;
     bool converged = false;
-    for (; pass <= bound; ++pass)
-        if (!__syncthreads_or(grow_pass(g, s))) {
-            converged = true;
-            break;
+    if (g.rows <= blockDim.x) {
+        /* one row per thread: its neighbour rows and bond masks stay fixed
+         * during the growth, so they are read once */
+        const uint32_t r = threadIdx.x;
+        const bool has = r < g.rows;
+        uint32_t r_yp = 0, r_ym = 0, r_zp = 0, r_zm = 0, b_ym = 0, b_yp = 0, b_zm = 0, b_zp = 0, b_x = 0;
+        if (has) {
+            const uint32_t z = slsf_fastdiv_div(r, g.div_ly);
+            const uint32_t y = r - z * g.ly;
+            r_yp = (y + 1 == g.ly) ? r + 1 - g.ly : r + 1;
+            r_ym = (y == 0) ? r + g.ly - 1 : r - 1;
+            r_zp = (z + 1 == g.lz) ? r + g.ly - g.rows : r + g.ly;
+            r_zm = (z == 0) ? r + g.rows - g.ly : r - g.ly;
+            b_ym = s.by[r_ym];
+            b_yp = s.by[r];
+            b_zm = s.bz[r_zm];
+            b_zp = s.bz[r];
+            b_x = s.bx[r];
         }
+        for (; pass <= bound; ++pass) {
+            int changed = 0;
+            if (has) {
+                const uint32_t old = s.cl[r];
+                const uint32_t c = old | (s.cl[r_ym] & b_ym) | (s.cl[r_yp] & b_yp) | (s.cl[r_zm] & b_zm) |
+                                   (s.cl[r_zp] & b_zp);
+                if (c != old) {
+                    s.cl[r] = close_row(c, b_x, g.lx, g.xmask);
+                    changed = 1;
+                }
+            }
+            if (!__syncthreads_or(changed)) {
+                converged = true;
+                break;
+            }
+        }
+    } else {
+        for (; pass <= bound; ++pass)
+            if (!__syncthreads_or(grow_pass(g, s))) {
+                converged = true;
+                break;
+            }
+    }
     if (!converged && threadIdx.x == 0) atomicOr(&t.stats[kStatError], kErrGrowthLimit);
     SLSF_PHASE(3);
     SLSF_PHASE_COUNT(6, pass + 1);
