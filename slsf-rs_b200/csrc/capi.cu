@@ -705,21 +705,18 @@ int slsf_task_correlations(slsf_task* t, uint32_t rmax_xy, uint32_t rmax_z, doub
     slsf_ctx* ctx = t->ctx;
     const uint32_t nv = slsf::corr_values(t->lz, rmax_xy, rmax_z);
     const size_t np = slsf::corr_partial_doubles(t->lx, t->ly, t->lz, rmax_xy, rmax_z);
-    const size_t off_values = align256(8 * np), off_table = off_values + align256(8ull * nv);
-    const size_t bytes = off_table + align256(sizeof(slsf::CorrTask));
+    const size_t off_values = align256(8 * np);
+    const size_t bytes = off_values + align256(8ull * nv);
     void* dv = nullptr;
     cudaError_t e = ctx->pool.allocate(bytes, &dv);
     if (e != cudaSuccess) return cuda_error(e, "correlation scratch");
     char* d = static_cast<char*>(dv);
     slsf::CorrTask ct = {t->theta, t->lx, t->ly, t->lz, rmax_xy, rmax_z, 0, 1, 0,
                          reinterpret_cast<double*>(d), reinterpret_cast<double*>(d + off_values), nullptr, nullptr};
-    auto* table = reinterpret_cast<slsf::CorrTask*>(d + off_table);
     std::vector<double> h(nv);
-    e = cudaMemcpyAsync(table, &ct, sizeof(ct), cudaMemcpyHostToDevice, ctx->stream);
     const uint32_t items = slsf::corr_items(t->lx, t->ly, t->lz, rmax_xy, rmax_z);
-    if (e == cudaSuccess)
-        e = slsf::launch_corr(table, 1, items, slsf::corr_ext(t->lx, t->ly, t->lz, rmax_xy, rmax_z), ctx->sm_count,
-                              ctx->stream);
+    e = slsf::launch_corr(nullptr, &ct, 1, items, slsf::corr_ext(t->lx, t->ly, t->lz, rmax_xy, rmax_z), ctx->sm_count,
+                          ctx->stream);
     ctx->launches += items ? 2 : 1;
     if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), ct.values, 8ull * nv, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -846,7 +843,7 @@ int slsf_batch_correlations(slsf_ctx* ctx, slsf_task* const* tasks, size_t n) {
     SLSF_CUDA(cudaMemcpyAsync(ctx->d_corr, ctx->h_corr, sizeof(slsf::CorrTask) * n, cudaMemcpyHostToDevice,
                               ctx->stream));
     SLSF_CUDA(cudaEventRecord(ctx->corr_uploaded, ctx->stream));
-    SLSF_CUDA(slsf::launch_corr(ctx->d_corr, (uint32_t)n, items, max_ext, ctx->sm_count, ctx->stream));
+    SLSF_CUDA(slsf::launch_corr(ctx->d_corr, nullptr, (uint32_t)n, items, max_ext, ctx->sm_count, ctx->stream));
     ctx->launches += items ? 2 : 1;
     for (size_t i = 0; i < n; ++i) tasks[i]->corr_count += 1;
     return SLSF_OK;

@@ -103,9 +103,10 @@ uint32_t corr_values(uint32_t lz, uint32_t rxy, uint32_t rz);
 uint32_t corr_ext(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
 bool corr_supports(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
 /* tasks_dev: n_tasks entries in item order (item0 ascending, n_items in
- * all); max_ext: the largest corr_ext of them. */
-cudaError_t launch_corr(const CorrTask* tasks_dev, uint32_t n_tasks, uint32_t n_items, uint32_t max_ext,
-                        int sm_count, cudaStream_t s);
+ * all) in device memory; or, for one task, `one` on the host (passed to the
+ * kernels by value, no copy).  max_ext: the largest corr_ext of them. */
+cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t n_tasks, uint32_t n_items,
+                        uint32_t max_ext, int sm_count, cudaStream_t s);
 
 /* ---- batched persistent engine, one CTA per replica (kernel_resident.cu) ---- */
 bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);

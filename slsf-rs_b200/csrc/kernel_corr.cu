@@ -11,13 +11,16 @@
  * with periodic shifts, r = 1..R (R = rmax_xy clamped to Lx/2, Ly/2) and
  * r = 1..R_z (R_z = rmax_z clamped to Lz/2); s . s' = cos cos' + sin sin'.
  *
- * k_corr_lines: a persistent grid walks the work items of all tasks.  An
+ * k_corr_lines: one block per work item of all tasks (the hardware balances
+ * items of different lengths across the SMs).  An
  * item is up to 32 parallel lines of one task along one axis -- x lines: 32
  * consecutive rows y of one layer; y lines: 32 consecutive x of one layer;
  * z lines: 32 consecutive x of one row y -- staged as (cos, sin) pairs in a
- * shared tile [n + R][33] (the first R entries of each line repeated after
- * its end, so k + r needs no modulo; the 33-pair pitch keeps both the
- * row-wise and the transposed fill free of bank conflicts).  Lane c owns
+ * shared tile [n + R][pitch] (the first R entries of each line repeated
+ * after its end, so k + r needs no modulo).  y and z lines fill the tile
+ * row-wise with a 32-pair pitch (a warp's row read is two aligned 128-byte
+ * wavefronts); x lines fill it transposed with a 33-pair pitch, which keeps
+ * that fill free of bank conflicts.  Lane c owns
  * line c; warp w owns 8 consecutive lags and keeps their partners in a
  * register ring along k, one shared load per k for 8 products.  Products
  * are FP32 (fused multiply-add), summed in FP32 over runs of 32 k and the
@@ -42,7 +45,7 @@ namespace {
 
 constexpr int kCorrThreads = 256;
 constexpr uint32_t kCorrCols = 32;  /* lines per item */
-constexpr uint32_t kCorrPitch = 33; /* (cos, sin) pairs per tile row */
+constexpr uint32_t kCorrPitch = 33; /* (cos, sin) pairs per tile row, at most */
 constexpr uint32_t kCorrLags = 8;   /* lags per warp pass */
 constexpr uint32_t kCorrRun = 32;   /* k per FP32 run */
 constexpr size_t kCorrMaxTile = 200 * 1024;
@@ -64,19 +67,20 @@ __host__ __device__ inline CorrShape corr_shape(uint32_t lx, uint32_t ly, uint32
     return s;
 }
 
+/* `tasks` in device memory, or NULL and the single task `one` by value. */
 __global__ void __launch_bounds__(kCorrThreads)
-    k_corr_lines(const CorrTask* __restrict__ tasks, uint32_t n_tasks, uint32_t n_items) {
+    k_corr_lines(const CorrTask* __restrict__ tasks, CorrTask one, uint32_t n_tasks, uint32_t n_items) {
     extern __shared__ float2 tile[]; /* [n + R][kCorrPitch] */
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (uint32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
         /* the task: the last one whose first item is at or before `item` */
         uint32_t lo = 0, hi = n_tasks;
-        while (hi - lo > 1) {
+        while (tasks && hi - lo > 1) {
             const uint32_t mid = (lo + hi) >> 1;
             if (tasks[mid].item0 <= item) lo = mid;
             else hi = mid;
         }
-        const CorrTask& T = tasks[lo];
+        const CorrTask& T = tasks ? tasks[lo] : one;
         const uint32_t lx = T.lx, ly = T.ly, lz = T.lz, plane = lx * ly;
         const CorrShape sh = corr_shape(lx, ly, lz, T.rxy, T.rz);
         const uint32_t local = item - T.item0;
@@ -99,13 +103,14 @@ __global__ void __launch_bounds__(kCorrThreads)
         const float* __restrict__ theta = T.theta;
         const uint32_t ext = n + rmax;
         __syncthreads(); /* the previous item's tile is no longer read */
+        const uint32_t pitch = cstride == 1 ? kCorrCols : kCorrPitch;
         if (cstride == 1) {
             for (uint32_t e = threadIdx.x; e < ext * kCorrCols; e += blockDim.x) {
                 const uint32_t k = e / kCorrCols, c = e % kCorrCols;
                 const uint32_t kk = k < n ? k : k - n;
                 float sn = 0.0f, cn = 0.0f;
                 if (c < cols) __sincosf(theta[base + kk * stride + c], &sn, &cn);
-                tile[k * kCorrPitch + c] = make_float2(cn, sn);
+                tile[k * pitch + c] = make_float2(cn, sn);
             }
         } else {
             /* x lines: consecutive threads take consecutive sites of a row */
@@ -114,7 +119,7 @@ __global__ void __launch_bounds__(kCorrThreads)
                 const uint32_t kk = k < n ? k : k - n;
                 float sn = 0.0f, cn = 0.0f;
                 if (c < cols) __sincosf(theta[base + c * cstride + kk], &sn, &cn);
-                tile[k * kCorrPitch + c] = make_float2(cn, sn);
+                tile[k * pitch + c] = make_float2(cn, sn);
             }
         }
         __syncthreads();
@@ -123,7 +128,7 @@ __global__ void __launch_bounds__(kCorrThreads)
             /* w[j]: partner of lag r0 + j at the current k */
             float2 w[kCorrLags];
 #pragma unroll
-            for (uint32_t j = 0; j < kCorrLags; ++j) w[j] = tile[min(r0 + j, ext - 1) * kCorrPitch + lane];
+            for (uint32_t j = 0; j < kCorrLags; ++j) w[j] = tile[min(r0 + j, ext - 1) * pitch + lane];
             double tot[kCorrLags];
             float part[kCorrLags];
 #pragma unroll
@@ -138,13 +143,13 @@ __global__ void __launch_bounds__(kCorrThreads)
             for (uint32_t k0 = 0; k0 < n8; k0 += kCorrLags) {
 #pragma unroll
                 for (uint32_t kk = 0; kk < kCorrLags; ++kk) {
-                    const float2 a = tile[(k0 + kk) * kCorrPitch + lane];
+                    const float2 a = tile[(k0 + kk) * pitch + lane];
 #pragma unroll
                     for (uint32_t j = 0; j < kCorrLags; ++j) {
                         const float2 wj = w[(kk + j) % kCorrLags];
                         part[j] = __fmaf_rn(a.y, wj.y, __fmaf_rn(a.x, wj.x, part[j]));
                     }
-                    w[kk] = tile[min(k0 + kk + r0 + kCorrLags, ext - 1) * kCorrPitch + lane];
+                    w[kk] = tile[min(k0 + kk + r0 + kCorrLags, ext - 1) * pitch + lane];
                 }
                 if ((k0 + kCorrLags) % kCorrRun == 0) {
 #pragma unroll
@@ -157,13 +162,13 @@ __global__ void __launch_bounds__(kCorrThreads)
             /* the ring is aligned again (slot j = lag r0 + j); the last n % 8
              * values of k slide it */
             for (uint32_t k = n8; k < n; ++k) {
-                const float2 a = tile[k * kCorrPitch + lane];
+                const float2 a = tile[k * pitch + lane];
 #pragma unroll
                 for (uint32_t j = 0; j < kCorrLags; ++j)
                     part[j] = __fmaf_rn(a.y, w[j].y, __fmaf_rn(a.x, w[j].x, part[j]));
 #pragma unroll
                 for (uint32_t j = 0; j + 1 < kCorrLags; ++j) w[j] = w[j + 1];
-                w[kCorrLags - 1] = tile[min(k + kCorrLags + r0, ext - 1) * kCorrPitch + lane];
+                w[kCorrLags - 1] = tile[min(k + kCorrLags + r0, ext - 1) * pitch + lane];
             }
 #pragma unroll
             for (uint32_t j = 0; j < kCorrLags; ++j) {
@@ -176,8 +181,10 @@ __global__ void __launch_bounds__(kCorrThreads)
     }
 }
 
-__global__ void __launch_bounds__(128) k_corr_finalize(const CorrTask* __restrict__ tasks) {
-    const CorrTask& T = tasks[blockIdx.x];
+constexpr int kFinThreads = 1024;
+
+__global__ void __launch_bounds__(kFinThreads) k_corr_finalize(const CorrTask* __restrict__ tasks, CorrTask one) {
+    const CorrTask& T = tasks ? tasks[blockIdx.x] : one;
     const uint32_t R = T.rxy, Rz = T.rz, lz = T.lz;
     if (R == 0 && Rz == 0) return;
     const CorrShape sh = corr_shape(T.lx, T.ly, lz, R, Rz);
@@ -217,9 +224,30 @@ __global__ void __launch_bounds__(128) k_corr_finalize(const CorrTask* __restric
         emit(R + r, cy);
         emit(2 * R + r, (cx + cy) / 2.0);
     }
+    /* C_z: `parts` threads per lag each sum the z items p = part mod parts,
+     * then one thread adds the parts in order */
+    __shared__ double zpart[kFinThreads];
+    const uint32_t parts = Rz ? max(1u, blockDim.x / Rz) : 1u;
+    if (threadIdx.x < Rz * parts) {
+        const uint32_t r = threadIdx.x % Rz, q = threadIdx.x / Rz;
+        const double* col = part + (size_t)(sh.nx + sh.ny) * sh.rp + r;
+        /* in item order; 16 loads in flight before their adds */
+        double a = 0.0;
+        uint32_t p = q;
+        for (; p + 15 * parts < sh.nz; p += 16 * parts) {
+            double v[16];
+#pragma unroll
+            for (uint32_t j = 0; j < 16; ++j) v[j] = col[(size_t)(p + j * parts) * sh.rp];
+#pragma unroll
+            for (uint32_t j = 0; j < 16; ++j) a += v[j];
+        }
+        for (; p < sh.nz; p += parts) a += col[(size_t)p * sh.rp];
+        zpart[threadIdx.x] = a;
+    }
+    __syncthreads();
     for (uint32_t r = threadIdx.x; r < Rz; r += blockDim.x) {
         double sz = 0.0;
-        for (uint32_t p = 0; p < sh.nz; ++p) sz += part[(size_t)(sh.nx + sh.ny + p) * sh.rp + r];
+        for (uint32_t q = 0; q < parts; ++q) sz += zpart[q * Rz + r];
         emit(3 * R + lz * R + r, sz / volume);
     }
     __syncthreads();
@@ -251,24 +279,23 @@ bool corr_supports(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t
     return (size_t)corr_ext(lx, ly, lz, rxy, rz) * kCorrPitch * sizeof(float2) <= kCorrMaxTile;
 }
 
-cudaError_t launch_corr(const CorrTask* tasks_dev, uint32_t n_tasks, uint32_t n_items, uint32_t max_ext,
-                        int sm_count, cudaStream_t s) {
-    if (n_tasks == 0) return cudaSuccess;
+cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t n_tasks, uint32_t n_items,
+                        uint32_t max_ext, int sm_count, cudaStream_t s) {
+    (void)sm_count; /* one block per item: the hardware spreads them */
+    if (n_tasks == 0 || (!tasks_dev && (!one || n_tasks != 1))) return cudaErrorInvalidValue;
+    const CorrTask by_value = one ? *one : CorrTask{};
     if (n_items > 0) {
         const size_t smem = (size_t)max_ext * kCorrPitch * sizeof(float2);
         cudaError_t e = cudaSuccess;
         if (smem > 48 * 1024)
             e = cudaFuncSetAttribute(k_corr_lines, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_corr_lines, kCorrThreads, smem);
-        if (e != cudaSuccess) return e;
-        const uint32_t grid = std::min<uint32_t>(n_items, (uint32_t)std::max(1, per_sm) * (uint32_t)sm_count);
-        k_corr_lines<<<grid, kCorrThreads, smem, s>>>(tasks_dev, n_tasks, n_items);
+        const uint32_t grid = std::min<uint32_t>(n_items, 1u << 30);
+        k_corr_lines<<<grid, kCorrThreads, smem, s>>>(one ? nullptr : tasks_dev, by_value, n_tasks, n_items);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    k_corr_finalize<<<n_tasks, 128, 0, s>>>(tasks_dev);
+    k_corr_finalize<<<n_tasks, kFinThreads, 0, s>>>(one ? nullptr : tasks_dev, by_value);
     return cudaGetLastError();
 }
 
