@@ -420,6 +420,80 @@ __device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Sme
         __syncthreads();
     }
     const uint32_t base_idx = g.plane * g.z0;
+    bool walked = false;
+    if constexpr (sizeof(W) == 8) {
+      if (g.lx_two_warps) {
+        walked = true;
+        /* L_x = 64: a warp holds a whole row, lane j the sites x = j and
+         * x = j + 32, and walks columns of rows along y -- (plane, y
+         * segment) units, round robin -- so the projections of the +y row are
+         * the next row's own: two sincos per site instead of three. */
+        const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+        const uint32_t nseg = (nwarps + g.nz - 1) / g.nz;
+        const uint32_t seg = (g.ly + nseg - 1) / nseg;
+        const uint32_t nxt = (lane + 1u) & 31u;
+        for (uint32_t u = warp; u < g.nz * nseg; u += nwarps) {
+            const uint32_t zl = u / nseg, y_lo = (u % nseg) * seg, y_hi = min(g.ly, y_lo + seg);
+            if (y_lo >= y_hi) continue;
+            const float jx = s.jxy[g.z0 + zl], jzz = s.jz[g.z0 + zl];
+            const uint32_t pbase = zl * g.plane;
+            /* colour of (x = lane, y, zl); x + 32 has the same colour */
+            uint32_t col = colour_of(g, lane, y_lo, zl);
+            float ra = proj_of(s.th[col * g.tstride + ((pbase + y_lo * 64u + lane) >> 1)], cphi, sphi);
+            float rb = proj_of(s.th[col * g.tstride + ((pbase + y_lo * 64u + lane + 32u) >> 1)], cphi, sphi);
+            uint32_t* hx32 = reinterpret_cast<uint32_t*>(s.bx);
+            uint32_t* hy32 = reinterpret_cast<uint32_t*>(s.by);
+            uint32_t* hz32 = reinterpret_cast<uint32_t*>(s.bz);
+            for (uint32_t y = y_lo; y < y_hi; ++y) {
+                const uint32_t li = pbase + y * 64u + lane;
+                const uint32_t y1 = (y + 1 == g.ly) ? 0u : y + 1;
+                const uint32_t ocol = col ^ 1u; /* colour of the +y and +z partners */
+                const uint32_t li_y = pbase + y1 * 64u + lane;
+                const uint32_t row = y + g.ly * zl;
+                const bool top = zl + 1 == g.nz;
+                /* +x partners: x + 1 in the same half, across the halves at x = 31 and x = 63 */
+                const float b0 = __shfl_sync(0xffffffffu, rb, 0), a0 = __shfl_sync(0xffffffffu, ra, 0);
+                const float na = __shfl_sync(0xffffffffu, ra, nxt), nb = __shfl_sync(0xffffffffu, rb, nxt);
+                /* half 0: x = lane; each half is finished (bonds, ballots, 32-bit row-word half) in turn */
+                const float rya = proj_of(s.th[ocol * g.tstride + (li_y >> 1)], cphi, sphi);
+                {
+                    const float tz = top ? halo_theta(g, s, true, ocol, (lane + 64u * y) >> 1)
+                                         : s.th[ocol * g.tstride + ((li + g.plane) >> 1)];
+                    const float rz = proj_of(tz, cphi, sphi);
+                    const slsf_u32x4 bw = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, base_idx + li);
+                    const uint32_t bx = __ballot_sync(0xffffffffu, wolff_bond_active(jx, ra, lane < 31u ? na : b0, m2b, bw.x));
+                    const uint32_t by = __ballot_sync(0xffffffffu, wolff_bond_active(jx, ra, rya, m2b, bw.y));
+                    const uint32_t bz = __ballot_sync(0xffffffffu, wolff_bond_active(jzz, ra, rz, m2b, bw.z));
+                    if (lane == 0) {
+                        hx32[2 * row] = bx;
+                        hy32[2 * row] = by;
+                        hz32[2 * row] = bz;
+                    }
+                }
+                /* half 1: x = lane + 32 */
+                const float ryb = proj_of(s.th[ocol * g.tstride + ((li_y + 32u) >> 1)], cphi, sphi);
+                {
+                    const float tz = top ? halo_theta(g, s, true, ocol, (lane + 32u + 64u * y) >> 1)
+                                         : s.th[ocol * g.tstride + ((li + 32u + g.plane) >> 1)];
+                    const float rz = proj_of(tz, cphi, sphi);
+                    const slsf_u32x4 bw = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, base_idx + li + 32u);
+                    const uint32_t bx = __ballot_sync(0xffffffffu, wolff_bond_active(jx, rb, lane < 31u ? nb : a0, m2b, bw.x));
+                    const uint32_t by = __ballot_sync(0xffffffffu, wolff_bond_active(jx, rb, ryb, m2b, bw.y));
+                    const uint32_t bz = __ballot_sync(0xffffffffu, wolff_bond_active(jzz, rb, rz, m2b, bw.z));
+                    if (lane == 0) {
+                        hx32[2 * row + 1] = bx;
+                        hy32[2 * row + 1] = by;
+                        hz32[2 * row + 1] = bz;
+                    }
+                }
+                ra = rya;
+                rb = ryb;
+                col = ocol;
+            }
+        }
+      }
+    }
+    if (!walked)
     for (uint32_t i0 = (threadIdx.x & ~31u); i0 < g.vs; i0 += blockDim.x) {
         const uint32_t li = i0 + lane;
         const bool valid = li < g.vs;
