@@ -387,6 +387,49 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
                 ri = ryp;
             }
         }
+    } else if (g.lx_tiles_warp) {
+        /* L_x = 4, 8, 16: a warp holds G = 32 / L_x rows (lane = x + L_x sub), sub-group sub
+         * in plane z = G zb + sub; each warp walks columns of rows along y --
+         * (zb, y segment) units, round robin -- so the projection of the +y
+         * row is the next row's own: two sincos per site instead of three,
+         * and no per-site index division.  Sub-groups past the last plane
+         * (L_z not a multiple of G) compute on the last plane and keep
+         * nothing. */
+        const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+        const uint32_t gsz = 32u / g.lx, sub = lane / g.lx, x = lane - sub * g.lx;
+        const uint32_t nzb = (g.lz + gsz - 1) / gsz;
+        const uint32_t nseg = (nwarps + nzb - 1) / nzb;
+        const uint32_t seg = (g.ly + nseg - 1) / nseg;
+        const uint32_t xsrc = sub * g.lx + (x + 1 == g.lx ? 0u : x + 1);
+        for (uint32_t u = warp; u < nzb * nseg; u += nwarps) {
+            const uint32_t zb = u / nseg, y_lo = (u % nseg) * seg, y_hi = min(g.ly, y_lo + seg);
+            if (y_lo >= y_hi) continue;
+            const uint32_t zq = zb * gsz + sub;
+            const bool zvalid = zq < g.lz;
+            const uint32_t z = zvalid ? zq : g.lz - 1;
+            const uint32_t zp_off = (z + 1 == g.lz) ? 0u : (z + 1) * g.plane; /* base of the +z plane */
+            const float jx = s.jxy[z], jzz = s.jz[z];
+            const uint32_t zbase = z * g.plane;
+            float ri = proj_of(s.th[slot(g, zbase + y_lo * g.lx + x, (x + y_lo + z) & 1u)], cphi, sphi);
+            for (uint32_t y = y_lo; y < y_hi; ++y) {
+                const uint32_t idx = zbase + y * g.lx + x;
+                const uint32_t y1 = (y + 1 == g.ly) ? 0u : y + 1;
+                const float ryp = proj_of(s.th[slot(g, zbase + y1 * g.lx + x, (x + y1 + z) & 1u)], cphi, sphi);
+                const float rzp = proj_of(s.th[slot(g, zp_off + y * g.lx + x, (x + y + z + 1) & 1u)], cphi, sphi);
+                const float rxp = __shfl_sync(0xffffffffu, ri, xsrc);
+                const slsf_u32x4 b = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, idx);
+                const uint32_t bal_x = __ballot_sync(0xffffffffu, wolff_bond_active(jx, ri, rxp, m2b, b.x));
+                const uint32_t bal_y = __ballot_sync(0xffffffffu, wolff_bond_active(jx, ri, ryp, m2b, b.y));
+                const uint32_t bal_z = __ballot_sync(0xffffffffu, wolff_bond_active(jzz, ri, rzp, m2b, b.z));
+                if (x == 0 && zvalid) {
+                    const uint32_t row = y + g.ly * z;
+                    s.bx[row] = (bal_x >> lane) & g.xmask;
+                    s.by[row] = (bal_y >> lane) & g.xmask;
+                    s.bz[row] = (bal_z >> lane) & g.xmask;
+                }
+                ri = ryp;
+            }
+        }
     } else
     /* Bond activation, one thread per site, warp-aligned site ranges. */
     for (uint32_t i0 = (threadIdx.x & ~31u); i0 < g.volume; i0 += blockDim.x) {

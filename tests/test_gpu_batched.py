@@ -51,7 +51,9 @@ def batched_tasks(slsf, ctx, orc, specs):
 @pytest.mark.parametrize("dims,wolff", [((8, 8, 8), 0), ((8, 8, 8), 1), ((32, 32, 32), 1), ((16, 8, 12), 2),
                                         ((24, 24, 24), 1), ((32, 16, 8), 1), ((12, 10, 6), 1),
                                         ((32, 32, 48), 1), ((32, 32, 96), 1), ((20, 24, 16), 1),
-                                        ((48, 48, 48), 1), ((64, 64, 64), 1), ((40, 16, 8), 1), ((64, 8, 6), 1)])
+                                        ((48, 48, 48), 1), ((64, 64, 64), 1), ((40, 16, 8), 1), ((64, 8, 6), 1),
+                                        ((8, 6, 6), 1), ((4, 4, 10), 2), ((4, 2, 2), 1), ((16, 10, 2), 1),
+                                        ((64, 6, 10), 1)])
 def test_batched_equals_plain_bitwise(slsf, ctx, orc, dims, wolff):
     ref, _ = plain_run(slsf, ctx, orc, dims, 1.1, seed=42, sweeps=4, wolff=wolff)
     [t] = batched_tasks(slsf, ctx, orc, [(dims, 1.1, 42, wolff, 0, 1, 0, 1)])
