@@ -4,6 +4,8 @@ radii), validation messages, the rank split and the result path.  The
 known answers are the reference's own (src/tests.rs:448-566); nothing here
 launches a kernel."""
 import importlib
+import os
+import re
 import math
 
 import numpy as np
@@ -243,3 +245,26 @@ def test_couplings_equal_host_draw(jobs, slsf):
         jx, jz = slsf.task_couplings(d)
         assert np.array_equal(jx, t["j_xy_array"]) and np.array_equal(jz, t["j_z_array"])
         assert set(jx) <= {0.5, 1.5} and set(np.round(jz, 12)) <= {0.0, 0.2}
+
+
+REFERENCE_EXAMPLES = "/root/reference/examples"
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_EXAMPLES), reason="the reference's example job files are not here")
+def test_reference_example_job_files_parse_and_expand(jobs):
+    # Every job file the reference ships parses, and expands to one task per
+    # lattice x dJxy x dJz x T x sample with the reference's name format.
+    names = sorted(f for f in os.listdir(REFERENCE_EXAMPLES) if f.endswith(".toml"))
+    assert names
+    for name in names:
+        cfg = jobs.load_job(os.path.join(REFERENCE_EXAMPLES, name))
+        specs = jobs.lattice_specs(cfg)
+        expected = len(specs) * len(cfg.delta_j_xy) * len(cfg.delta_j_z) * len(cfg.temperatures) * cfg.samples
+        if expected > 5000:
+            cfg.samples = 1  # the production files hold up to 20000 tasks: expand one sample of each
+            expected = len(specs) * len(cfg.delta_j_xy) * len(cfg.delta_j_z) * len(cfg.temperatures)
+        tasks = jobs.make_tasks(cfg)
+        assert len(tasks) == expected, name
+        assert all(re.fullmatch(r"L\d+x\d+x\d+_T\d+\.\d{6}_dJxy\d+\.\d{6}_dJz\d+\.\d{6}_sample\d+", t["name"])
+                   for t in tasks), name
+        assert cfg.run_time_s > 0 and cfg.checkpoint_time_s > 0
