@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     p.add_argument("--no-serve", action="store_true", help="skip the served-stream side figure")
     p.add_argument("--no-large", action="store_true", help="skip the L=256 large-lattice side figure")
+    p.add_argument("--no-job", action="store_true", help="skip the job-file side figure")
     p.add_argument("--no-tune", action="store_true",
                    help="use the default kernel choice instead of the autotuner (profiling runs)")
     p.add_argument("--serve-tasks", type=int, default=4096, help="tasks of the served stream")
@@ -374,6 +375,72 @@ def served_stream(pkg, ctx, n_tasks, epoch_sweeps):
     return out
 
 
+def job_figure(pkg):
+    """Job files end to end (slsf-rs_b200/jobs.py): a bounded sample of the
+    reference's production job shape (L in {8, 16, 24, 32}, ten temperatures in
+    [1.1, 1.5], two-point J_xy = 1.5 +- 0.5, J_z = 0.1, no correlations: the
+    served path) and a default-correlation job (r_max = L/2 measured every
+    sweep: batched groups with one correlation launch pair per measurement).
+    Wall clock around run_job (task expansion, device set-up, runs, estimates);
+    synthetic tasks from the job schema, no files written."""
+    import time
+    import importlib
+
+    jobs = importlib.import_module("slsf_rs_b200.jobs")
+    out = {}
+    specs = {
+        "served": """
+name = "bench_served"
+[model]
+L = [8, 16, 24, 32]
+T = [1.1, 1.1444444444444444, 1.1888888888888889, 1.2333333333333334, 1.2777777777777777, 1.3222222222222222,
+     1.3666666666666667, 1.4111111111111112, 1.4555555555555555, 1.5]
+samples = 8
+base_seed = 20260710
+j_xy = 1.5
+delta_j_xy = [0.5]
+j_z = 0.1
+[run]
+sweeps = 2000
+thermalization = 500
+binsize = 100
+[measure]
+corr_rmax_xy = [0, 0, 0, 0]
+corr_rmax_z = [0, 0, 0, 0]
+""",
+        "correlated": """
+name = "bench_correlated"
+[model]
+L = [8, 16]
+T = [1.1, 1.2, 1.3, 1.4, 1.5]
+samples = 8
+base_seed = 20260710
+j_xy = 1.5
+delta_j_xy = [0.5]
+j_z = 0.1
+[run]
+sweeps = 1000
+thermalization = 200
+binsize = 50
+""",
+    }
+    with pkg.Context() as ctx:
+        for key, text in specs.items():
+            cfg = jobs.config_from_toml(text)
+            tasks = jobs.make_tasks(cfg)
+            t0 = time.perf_counter()
+            res = jobs.run_job(ctx, cfg, tasks=tasks)
+            wall = time.perf_counter() - t0
+            updates = sum(t["l_x"] * t["l_y"] * t["l_z"] * (t["thermalization"] + t["sweeps"]) for t in tasks)
+            out[key] = {"tasks": len(tasks), "wall_s": wall, "value": updates / wall, "unit": "site-updates/s",
+                        "completed": len(res["tasks"]),
+                        "job": f"L={cfg.l}, {len(cfg.temperatures)} T, {cfg.samples} samples, "
+                               f"{cfg.thermalization}+{cfg.sweeps} sweeps, "
+                               + ("no correlations" if key == "served" else
+                                  f"C_x, C_y, C_xy(z), C_z with r_max = L/2 every {cfg.correlation_interval} sweep")}
+    return out
+
+
 def serve_only(args):
     import torch
 
@@ -503,6 +570,8 @@ def main():
             extra["large"] = large_lattice(pkg, ctx, stream)
         if not args.no_serve:
             extra["served"] = served_stream(pkg, ctx, args.serve_tasks, args.serve_epoch)
+        if not args.no_job:
+            extra["job"] = job_figure(pkg)
         if not args.no_cpu:
             extra["cpu_baseline"] = cpu_baseline(L, list(np.linspace(1.1, 1.5, args.temperatures)), 2000,
                                                  args.cpu_seconds)

@@ -138,6 +138,13 @@ int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n
  * task's counters of this step, in the order of the tasks at open. */
 int slsf_batch_step(slsf_batch* b, slsf_sweep_stats* stats);
 int slsf_batch_close(slsf_batch* b);
+/* n_cycles times: the session's step followed by one correlation
+ * measurement of every task (slsf_batch_correlations; every task needs
+ * slsf_task_corr_setup), all queued back to back with the step counters
+ * summed on the device; waits once at the end.  stats (may be NULL) receives
+ * each task's counters summed over the cycles.  The loop of
+ * ThetaModel::measure with correlation_interval = the session's sweeps. */
+int slsf_batch_step_correlations(slsf_batch* b, uint32_t n_cycles, slsf_sweep_stats* stats);
 
 /* ---------------------------------------------------------------- tuning
  * How the batched entry points run each lattice shape: the one-CTA kernel
@@ -253,7 +260,10 @@ int slsf_task_corr_bins(const slsf_task* task, double* bin_means, size_t n_rows,
 /* One correlation measurement of every task (each set up with
  * slsf_task_corr_setup) in two launches for the whole batch, queued on the
  * context's stream after the work already queued there (a batched run's
- * sweeps included); does not wait for it.  Tasks may differ in size. */
+ * sweeps or a session step included); does not wait for it.  Tasks may
+ * differ in size and may belong to an open batch session (the measurement
+ * only reads their angles).  Repeating the same task list reuses the
+ * device task table. */
 int slsf_batch_correlations(slsf_ctx* ctx, slsf_task* const* tasks, size_t n_tasks);
 
 /* Per-task bin accumulators of the batched engine: n_bins rows of

@@ -122,6 +122,7 @@ SIGNATURES = {
     "slsf_batch_open": (C.c_int, [_P, C.POINTER(_P), C.c_size_t, C.c_uint32, C.POINTER(_P)]),
     "slsf_batch_step": (C.c_int, [_P, C.POINTER(SweepStats)]),
     "slsf_batch_close": (C.c_int, [_P]),
+    "slsf_batch_step_correlations": (C.c_int, [_P, C.c_uint32, C.POINTER(SweepStats)]),
     "slsf_tune_get": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KernelChoice)]),
     "slsf_tune_set": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KernelChoice)]),
     "slsf_autotune": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KernelChoice),
@@ -295,6 +296,15 @@ class BatchSession:
         st = (SweepStats * self.n)()
         check(load().slsf_batch_step(self.h, st))
         return [x.as_dict() for x in st]
+
+    def step_correlations(self, n_cycles, raw=None):
+        """n_cycles x (step + one correlation measurement of every task)
+        (slsf_batch_step_correlations).  Returns the summed stats as a
+        uint64 array [n_tasks, 4] (sweeps, accepted, wolff_clusters,
+        wolff_cluster_sites)."""
+        st = raw if raw is not None else (SweepStats * self.n)()
+        check(load().slsf_batch_step_correlations(self.h, n_cycles, st))
+        return np.ctypeslib.as_array(st).view(np.uint64).reshape(self.n, 4)
 
     def close(self):
         if getattr(self, "h", None):

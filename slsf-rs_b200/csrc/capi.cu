@@ -147,6 +147,12 @@ struct slsf_ctx {
     slsf::CorrTask* h_corr = nullptr; /* pinned */
     size_t corr_cap = 0;
     cudaEvent_t corr_uploaded = nullptr;
+    /* the task list (and set-up generations) the device table holds, so a
+     * repeated batch reuses it without an upload */
+    std::vector<const slsf_task*> corr_last;
+    std::vector<uint64_t> corr_last_gen;
+    uint32_t corr_last_items = 0, corr_last_ext = 0;
+    uint64_t corr_gen = 0; /* slsf_task_corr_setup calls so far */
 };
 
 struct slsf_task {
@@ -178,6 +184,7 @@ struct slsf_task {
     uint64_t corr_bytes = 0;
     uint32_t corr_rxy = 0, corr_rz = 0, corr_binsize = 1, corr_n_bins = 0;
     uint64_t corr_count = 0; /* host mirror of *corr_count_dev */
+    uint64_t corr_gen = 0;   /* the context's set-up count when this set-up was made */
     double* corr_partial = nullptr;
     double* corr_bins = nullptr;
     unsigned long long* corr_count_dev = nullptr;
@@ -761,6 +768,7 @@ int slsf_task_corr_setup(slsf_task* t, uint32_t rmax_xy, uint32_t rmax_z, uint32
     t->corr_rxy = t->corr_rz = t->corr_n_bins = 0;
     t->corr_binsize = 1;
     t->corr_count = 0;
+    t->corr_gen = ++ctx->corr_gen;
     if (n_values) *n_values = nv;
     if (!on) return SLSF_OK;
     if (ctx->used + bytes > ctx->budget)
@@ -807,44 +815,58 @@ int slsf_task_corr_bins(const slsf_task* t, double* bin_means, size_t n_rows, ui
 int slsf_batch_correlations(slsf_ctx* ctx, slsf_task* const* tasks, size_t n) {
     if (!ctx || (!tasks && n)) return set_error(SLSF_ERR_INVALID, "NULL argument");
     if (n == 0) return SLSF_OK;
-    std::unordered_set<const slsf_task*> seen;
+    /* Correlations read the angles and write only the correlation bins, so
+     * tasks held by an open batch session are accepted (their steps and this
+     * launch are ordered on the context's stream). */
+    bool same = ctx->corr_last.size() == n;
     for (size_t i = 0; i < n; ++i) {
         const slsf_task* t = tasks[i];
         if (!t || t->ctx != ctx) return set_error(SLSF_ERR_INVALID, "task does not belong to this context");
-        if (int rc = check_free(t)) return rc;
         if (!t->corr_block)
             return set_error(SLSF_ERR_STATE, "task has no correlation bins; call slsf_task_corr_setup first");
-        if (!seen.insert(t).second) return set_error(SLSF_ERR_INVALID, "a task appears twice in the batch");
+        if (same && (ctx->corr_last[i] != t || ctx->corr_last_gen[i] != t->corr_gen)) same = false;
     }
     if (int rc = bind_device(ctx)) return rc;
-    if (!ctx->corr_uploaded) SLSF_CUDA(cudaEventCreateWithFlags(&ctx->corr_uploaded, cudaEventDisableTiming));
-    /* the pinned table may still be the source of the last queued upload */
-    SLSF_CUDA(cudaEventSynchronize(ctx->corr_uploaded));
-    if (ctx->corr_cap < n) {
-        SLSF_CUDA(cudaStreamSynchronize(ctx->stream)); /* queued launches may still read the device table */
-        if (ctx->d_corr) cudaFree(ctx->d_corr);
-        if (ctx->h_corr) cudaFreeHost(ctx->h_corr);
-        ctx->d_corr = nullptr;
-        ctx->h_corr = nullptr;
-        ctx->corr_cap = 0;
-        SLSF_CUDA(cudaMalloc(&ctx->d_corr, sizeof(slsf::CorrTask) * n));
-        SLSF_CUDA(cudaHostAlloc(&ctx->h_corr, sizeof(slsf::CorrTask) * n, cudaHostAllocDefault));
-        ctx->corr_cap = n;
+    if (!same) {
+        std::unordered_set<const slsf_task*> seen;
+        for (size_t i = 0; i < n; ++i)
+            if (!seen.insert(tasks[i]).second) return set_error(SLSF_ERR_INVALID, "a task appears twice in the batch");
+        if (!ctx->corr_uploaded) SLSF_CUDA(cudaEventCreateWithFlags(&ctx->corr_uploaded, cudaEventDisableTiming));
+        /* the pinned table may still be the source of the last queued upload */
+        SLSF_CUDA(cudaEventSynchronize(ctx->corr_uploaded));
+        ctx->corr_last.clear();
+        ctx->corr_last_gen.clear();
+        if (ctx->corr_cap < n) {
+            SLSF_CUDA(cudaStreamSynchronize(ctx->stream)); /* queued launches may still read the device table */
+            if (ctx->d_corr) cudaFree(ctx->d_corr);
+            if (ctx->h_corr) cudaFreeHost(ctx->h_corr);
+            ctx->d_corr = nullptr;
+            ctx->h_corr = nullptr;
+            ctx->corr_cap = 0;
+            SLSF_CUDA(cudaMalloc(&ctx->d_corr, sizeof(slsf::CorrTask) * n));
+            SLSF_CUDA(cudaHostAlloc(&ctx->h_corr, sizeof(slsf::CorrTask) * n, cudaHostAllocDefault));
+            ctx->corr_cap = n;
+        }
+        uint32_t items = 0, max_ext = 0;
+        for (size_t i = 0; i < n; ++i) {
+            slsf_task* t = tasks[i];
+            ctx->h_corr[i] = slsf::CorrTask{t->theta, t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz, items,
+                                            t->corr_binsize, t->corr_n_bins, t->corr_partial, nullptr, t->corr_bins,
+                                            t->corr_count_dev};
+            items += slsf::corr_items(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz);
+            max_ext = std::max(max_ext, slsf::corr_ext(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz));
+        }
+        SLSF_CUDA(cudaMemcpyAsync(ctx->d_corr, ctx->h_corr, sizeof(slsf::CorrTask) * n, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+        SLSF_CUDA(cudaEventRecord(ctx->corr_uploaded, ctx->stream));
+        ctx->corr_last.assign(tasks, tasks + n);
+        for (size_t i = 0; i < n; ++i) ctx->corr_last_gen.push_back(tasks[i]->corr_gen);
+        ctx->corr_last_items = items;
+        ctx->corr_last_ext = max_ext;
     }
-    uint32_t items = 0, max_ext = 0;
-    for (size_t i = 0; i < n; ++i) {
-        slsf_task* t = tasks[i];
-        ctx->h_corr[i] = slsf::CorrTask{t->theta, t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz, items,
-                                        t->corr_binsize, t->corr_n_bins, t->corr_partial, nullptr, t->corr_bins,
-                                        t->corr_count_dev};
-        items += slsf::corr_items(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz);
-        max_ext = std::max(max_ext, slsf::corr_ext(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz));
-    }
-    SLSF_CUDA(cudaMemcpyAsync(ctx->d_corr, ctx->h_corr, sizeof(slsf::CorrTask) * n, cudaMemcpyHostToDevice,
-                              ctx->stream));
-    SLSF_CUDA(cudaEventRecord(ctx->corr_uploaded, ctx->stream));
-    SLSF_CUDA(slsf::launch_corr(ctx->d_corr, nullptr, (uint32_t)n, items, max_ext, ctx->sm_count, ctx->stream));
-    ctx->launches += items ? 2 : 1;
+    SLSF_CUDA(slsf::launch_corr(ctx->d_corr, nullptr, (uint32_t)n, ctx->corr_last_items, ctx->corr_last_ext,
+                                ctx->sm_count, ctx->stream));
+    ctx->launches += ctx->corr_last_items ? 2 : 1;
     for (size_t i = 0; i < n; ++i) tasks[i]->corr_count += 1;
     return SLSF_OK;
 }
@@ -1234,9 +1256,13 @@ struct slsf_batch {
     unsigned long long* d_counters = nullptr; /* [view][Metropolis, Wolff], advanced by the kernels */
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    unsigned long long* d_acc = nullptr; /* stats summed over the cycles of slsf_batch_step_correlations */
+    unsigned long long* h_acc = nullptr; /* pinned */
 };
 
 static void batch_free(slsf_batch* b) {
+    if (b->d_acc) cudaFree(b->d_acc);
+    if (b->h_acc) cudaFreeHost(b->h_acc);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     if (b->d_views) cudaFree(b->d_views);
@@ -1386,6 +1412,64 @@ int slsf_batch_step(slsf_batch* b, slsf_sweep_stats* stats) {
         if (s[slsf::kStatError]) rc = set_error(SLSF_ERR_TIMEOUT, "a bounded device loop hit its iteration limit");
         if (stats) stats[i] = slsf_sweep_stats{b->n_sweeps, s[slsf::kStatAccepted], s[slsf::kStatClusters],
                                                s[slsf::kStatClusterSites]};
+    }
+    return rc;
+}
+
+namespace {
+
+/* acc[i] += add[i], one thread per counter. */
+__global__ void k_stats_add(const unsigned long long* __restrict__ add, unsigned long long* __restrict__ acc,
+                            uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) acc[i] += add[i];
+}
+
+}  // namespace
+
+int slsf_batch_step_correlations(slsf_batch* b, uint32_t n_cycles, slsf_sweep_stats* stats) {
+    if (!b) return set_error(SLSF_ERR_INVALID, "session is NULL");
+    slsf_ctx* ctx = b->ctx;
+    const size_t n = b->tasks.size();
+    for (slsf_task* t : b->tasks)
+        if (!t->corr_block)
+            return set_error(SLSF_ERR_STATE, "task has no correlation bins; call slsf_task_corr_setup first");
+    if (n_cycles == 0) {
+        if (stats)
+            for (size_t i = 0; i < n; ++i) stats[i] = slsf_sweep_stats{0, 0, 0, 0};
+        return SLSF_OK;
+    }
+    if (int rc = bind_device(ctx)) return rc;
+    const size_t slots = slsf::kStatSlots * n;
+    if (!b->d_acc) {
+        SLSF_CUDA(cudaMalloc(&b->d_acc, 8 * slots));
+        SLSF_CUDA(cudaHostAlloc(&b->h_acc, 8 * slots, cudaHostAllocDefault));
+    }
+    SLSF_CUDA(cudaMemsetAsync(b->d_acc, 0, 8 * slots, ctx->stream));
+    for (uint32_t c = 0; c < n_cycles; ++c) {
+        /* the step's stats are reset inside its graph; they are summed here
+         * on the device, so the cycles need no host round trip */
+        SLSF_CUDA(cudaGraphLaunch(b->exec, ctx->stream));
+        k_stats_add<<<(uint32_t)((slots + 255) / 256), 256, 0, ctx->stream>>>(b->d_stats, b->d_acc, (uint32_t)slots);
+        SLSF_CUDA(cudaGetLastError());
+        if (int rc = slsf_batch_correlations(ctx, b->tasks.data(), n)) return rc;
+        ctx->launches += 2;
+    }
+    SLSF_CUDA(cudaMemcpyAsync(b->h_acc, b->d_acc, 8 * slots, cudaMemcpyDeviceToHost, ctx->stream));
+    SLSF_CUDA(cudaStreamSynchronize(ctx->stream));
+    const uint64_t sweeps = (uint64_t)n_cycles * b->n_sweeps;
+    int rc = SLSF_OK;
+    for (size_t i = 0; i < n; ++i) {
+        slsf_task* t = b->tasks[i];
+        const uint64_t before = t->metro_sweeps;
+        t->metro_sweeps += sweeps;
+        t->wolff_done += sweeps * t->wolff_steps;
+        const uint64_t lo = std::max<uint64_t>(before, t->thermalization);
+        if (t->metro_sweeps > lo && t->n_bins) t->measurements += t->metro_sweeps - lo;
+        const unsigned long long* a = &b->h_acc[i * slsf::kStatSlots];
+        if (a[slsf::kStatError]) rc = set_error(SLSF_ERR_TIMEOUT, "a bounded device loop hit its iteration limit");
+        if (stats) stats[i] = slsf_sweep_stats{sweeps, a[slsf::kStatAccepted], a[slsf::kStatClusters],
+                                               a[slsf::kStatClusterSites]};
     }
     return rc;
 }

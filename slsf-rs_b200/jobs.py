@@ -480,6 +480,7 @@ def _run_correlated(pkg, ctx, group, ck: Optional[Checkpoints] = None, gdir: Opt
     therm, sweeps, interval = t0["thermalization"], t0["sweeps"], t0["correlation_interval"]
     n_corr = (sweeps + interval - 1) // interval
     objs, radii = [], []
+    session = None
     try:
         for _, t in group:
             o = pkg.Task(ctx, (t["l_x"], t["l_y"], t["l_z"]), t["j_xy_array"], t["j_z_array"], t["temperature"],
@@ -505,13 +506,21 @@ def _run_correlated(pkg, ctx, group, ck: Optional[Checkpoints] = None, gdir: Opt
         corr_done = measured[0].corr_bins(0)[1] if measured else 0
 
         def advance(n):
-            nonlocal pos
-            if n:
-                for i, s in enumerate(ctx.batch_run(objs, n, handles)):
-                    accepted[i] += s["accepted"]
-                pos += n
+            # sweeps outside whole measurement cycles (thermalization, the
+            # first measurement's sweep, the tail): one batched call
+            nonlocal pos, session
+            if not n:
+                return
+            if session:
+                session.close()
+                session = False
+            for i, st in enumerate(ctx.batch_run(objs, n, handles)):
+                accepted[i] += st["accepted"]
+            pos += n
 
         def save(due):
+            if due == "stop" and session:
+                session.close()
             tmp = gdir + ".new"
             os.makedirs(tmp, exist_ok=True)
             for i, o in enumerate(objs):
@@ -524,13 +533,34 @@ def _run_correlated(pkg, ctx, group, ck: Optional[Checkpoints] = None, gdir: Opt
 
         if pos < therm:
             advance(therm - pos)
-        for m in range(corr_done * interval, sweeps, interval):
-            advance(therm + m + 1 - pos)
-            if measured:
-                ctx.batch_correlations(measured, corr_handles)
+        m_idx = corr_done
+        while m_idx < n_corr:
+            n = therm + m_idx * interval + 1 - pos
+            if n == interval and len(measured) == len(objs) and session is not False:
+                # whole cycles (interval sweeps + a correlation measurement)
+                # run in the library, up to 64 between checkpoint checks
+                if session is None:
+                    try:
+                        session = ctx.session(objs, interval)
+                    except pkg.SlsfError as e:
+                        if e.code != pkg.ERR_INVALID:
+                            raise
+                        session = False
+                        continue
+                k = min(64, n_corr - m_idx)
+                accepted += session.step_correlations(k)[:, 1]
+                pos += k * interval
+                m_idx += k
+            else:
+                advance(n)
+                if measured:
+                    ctx.batch_correlations(measured, corr_handles)
+                m_idx += 1
             if ck and (due := ck.due()):
                 save(due)
         advance(therm + sweeps - pos)
+        if session:
+            session.close()
         host = pkg.load_host()
         out = []
         for i, ((_, t), o) in enumerate(zip(group, objs)):
@@ -560,6 +590,8 @@ def _run_correlated(pkg, ctx, group, ck: Optional[Checkpoints] = None, gdir: Opt
             _swap_dir(tmp, gdir)
         return out
     finally:
+        if session:
+            session.close()
         for o in objs:
             o.close()
 

@@ -127,3 +127,37 @@ def test_budget_counts_correlation_bins(slsf, orc):
         assert e.value.code == slsf.ERR_BUDGET
         assert t.corr_setup(1, 1, 1, 1) > 0
         t.close()
+
+
+def test_session_cycles_equal_manual_cycles(slsf, ctx, orc):
+    # slsf_batch_step_correlations: k x (session step of `interval` sweeps +
+    # one correlation measurement) equals the same cycles done by hand.
+    shapes = [(8, 8, 8), (16, 12, 20), (32, 32, 32), (48, 48, 48), (12, 8, 6)]
+    interval, cycles = 3, 5
+
+    def make():
+        ts = []
+        for k, d in enumerate(shapes):
+            t = task(slsf, ctx, orc, d, 40 + k)
+            t.corr_setup(d[0] // 2, d[2] // 2, 2, 3)
+            ts.append(t)
+        return ts
+
+    a, b = make(), make()
+    with ctx.session(a, interval) as ses:
+        st = ses.step_correlations(cycles)
+    manual = np.zeros((len(b), 4), dtype=np.uint64)
+    for _ in range(cycles):
+        for i, s in enumerate(ctx.batch_run(b, interval)):
+            manual[i] += np.array([s["sweeps"], s["accepted"], s["wolff_clusters"], s["wolff_cluster_sites"]],
+                                  dtype=np.uint64)
+        ctx.batch_correlations(b)
+    assert np.array_equal(st, manual)
+    for x, y in zip(a, b):
+        assert x.counters == y.counters == (interval * cycles, interval * cycles)
+        assert np.array_equal(x.theta.view(np.uint32), y.theta.view(np.uint32))
+        cx, nx = x.corr_bins()
+        cy, ny = y.corr_bins()
+        assert nx == ny == cycles and np.array_equal(cx, cy)
+        x.close()
+        y.close()
