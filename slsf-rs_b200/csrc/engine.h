@@ -104,9 +104,12 @@ uint32_t corr_ext(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t 
 bool corr_supports(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
 /* tasks_dev: n_tasks entries in item order (item0 ascending, n_items in
  * all) in device memory; or, for one task, `one` on the host (passed to the
- * kernels by value, no copy).  max_ext: the largest corr_ext of them. */
+ * kernels by value, no copy).  max_ext, max_r, max_nz: the largest corr_ext,
+ * radius and corr_z_items of them (they size the launches). */
 cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t n_tasks, uint32_t n_items,
-                        uint32_t max_ext, int sm_count, cudaStream_t s);
+                        uint32_t max_ext, uint32_t max_r, uint32_t max_nz, int sm_count, cudaStream_t s);
+/* z-line work items of a task (0 without C_z). */
+uint32_t corr_z_items(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
 
 /* ---- batched persistent engine, one CTA per replica (kernel_resident.cu) ---- */
 bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);

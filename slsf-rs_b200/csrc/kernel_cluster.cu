@@ -277,16 +277,25 @@ __device__ __forceinline__ float halo_theta(const Geo& g, const Smem<W>& s, bool
 
 template <typename W>
 __device__ __forceinline__ void load_slab(const TaskView& t, const Geo& g, Smem<W>& s) {
-    const float4* src = reinterpret_cast<const float4*>(t.theta + (size_t)g.plane * g.z0);
-    for (uint32_t q = threadIdx.x; q < g.vs / 4; q += blockDim.x) {
-        const float4 v = src[q];
-        const Coords c = coords_of(g, 4 * q);
-        const uint32_t p = colour_of(g, 0, c.y, c.zl); /* x = 4q mod lx is even */
-        const uint32_t h = 2 * q;
-        s.th[p * g.tstride + h] = v.x;
-        s.th[(p ^ 1u) * g.tstride + h] = v.y;
-        s.th[p * g.tstride + h + 1] = v.z;
-        s.th[(p ^ 1u) * g.tstride + h + 1] = v.w;
+    if (g.lx % 4) {
+        /* L_x = 2 mod 4: four consecutive sites may span two rows; copy site by site */
+        const float* src = t.theta + (size_t)g.plane * g.z0;
+        for (uint32_t li = threadIdx.x; li < g.vs; li += blockDim.x) {
+            const Coords c = coords_of(g, li);
+            s.th[colour_of(g, c.x, c.y, c.zl) * g.tstride + (li >> 1)] = src[li];
+        }
+    } else {
+        const float4* src = reinterpret_cast<const float4*>(t.theta + (size_t)g.plane * g.z0);
+        for (uint32_t q = threadIdx.x; q < g.vs / 4; q += blockDim.x) {
+            const float4 v = src[q];
+            const Coords c = coords_of(g, 4 * q);
+            const uint32_t p = colour_of(g, 0, c.y, c.zl); /* x = 4q mod lx is even */
+            const uint32_t h = 2 * q;
+            s.th[p * g.tstride + h] = v.x;
+            s.th[(p ^ 1u) * g.tstride + h] = v.y;
+            s.th[p * g.tstride + h + 1] = v.z;
+            s.th[(p ^ 1u) * g.tstride + h + 1] = v.w;
+        }
     }
     for (uint32_t z = threadIdx.x; z < g.lz; z += blockDim.x) {
         s.jxy[z] = t.jxy[z];
@@ -296,6 +305,14 @@ __device__ __forceinline__ void load_slab(const TaskView& t, const Geo& g, Smem<
 
 template <typename W>
 __device__ __forceinline__ void store_slab(const TaskView& t, const Geo& g, const Smem<W>& s) {
+    if (g.lx % 4) {
+        float* dst = t.theta + (size_t)g.plane * g.z0;
+        for (uint32_t li = threadIdx.x; li < g.vs; li += blockDim.x) {
+            const Coords c = coords_of(g, li);
+            dst[li] = s.th[colour_of(g, c.x, c.y, c.zl) * g.tstride + (li >> 1)];
+        }
+        return;
+    }
     float4* dst = reinterpret_cast<float4*>(t.theta + (size_t)g.plane * g.z0);
     for (uint32_t q = threadIdx.x; q < g.vs / 4; q += blockDim.x) {
         const Coords c = coords_of(g, 4 * q);
@@ -1041,9 +1058,9 @@ cudaError_t launch_w(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, u
 }  // namespace
 
 bool cluster_feasible(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t c, int device) {
-    /* Row words hold L_x <= 64 bits; the float4 colour-split copy needs
-     * L_x % 4 == 0 so that four consecutive sites never span two rows. */
-    if (lx > kMaxRowBits || lx < 4 || lx % 4 || ly < 2 || ly % 2 || lz < 2 || lz % 2) return false;
+    /* Row words hold L_x <= 64 bits; the colour-split layout needs even
+     * dimensions (L_x = 2 mod 4 copies the state site by site). */
+    if (lx > kMaxRowBits || lx < 4 || lx % 2 || ly < 2 || ly % 2 || lz < 2 || lz % 2) return false;
     if (c < 1 || c > kMaxCluster || (c & (c - 1)) || lz % c) return false;
     const size_t word = lx > 32 ? 8 : 4;
     const uint32_t nz = lz / c;

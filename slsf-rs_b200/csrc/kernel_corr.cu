@@ -268,6 +268,10 @@ size_t corr_partial_doubles(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy,
 
 uint32_t corr_values(uint32_t lz, uint32_t rxy, uint32_t rz) { return 3 * rxy + lz * rxy + rz; }
 
+uint32_t corr_z_items(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
+    return corr_shape(lx, ly, lz, rxy, rz).nz;
+}
+
 uint32_t corr_ext(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
     uint32_t e = 0;
     if (rxy) e = std::max(lx, ly) + rxy;
@@ -280,8 +284,14 @@ bool corr_supports(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t
 }
 
 cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t n_tasks, uint32_t n_items,
-                        uint32_t max_ext, int sm_count, cudaStream_t s) {
+                        uint32_t max_ext, uint32_t max_r, uint32_t max_nz, int sm_count, cudaStream_t s) {
     (void)sm_count; /* one block per item: the hardware spreads them */
+    /* a warp takes 8 lags per pass: blocks of one or two warps for small
+     * radii, so that short lines do not hold idle warps */
+    const int line_threads = max_r <= 16 ? 64 : (max_r <= 32 ? 128 : kCorrThreads);
+    /* the finalize splits each C_z sum over its z items only when there are
+     * many; each lag needs a thread of its own (R_z <= 258 < kFinThreads) */
+    const int fin_threads = (max_nz > 64 || max_r > 128) ? kFinThreads : 128;
     if (n_tasks == 0 || (!tasks_dev && (!one || n_tasks != 1))) return cudaErrorInvalidValue;
     const CorrTask by_value = one ? *one : CorrTask{};
     if (n_items > 0) {
@@ -291,11 +301,11 @@ cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t
             e = cudaFuncSetAttribute(k_corr_lines, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         const uint32_t grid = std::min<uint32_t>(n_items, 1u << 30);
-        k_corr_lines<<<grid, kCorrThreads, smem, s>>>(one ? nullptr : tasks_dev, by_value, n_tasks, n_items);
+        k_corr_lines<<<grid, line_threads, smem, s>>>(one ? nullptr : tasks_dev, by_value, n_tasks, n_items);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    k_corr_finalize<<<n_tasks, kFinThreads, 0, s>>>(one ? nullptr : tasks_dev, by_value);
+    k_corr_finalize<<<n_tasks, fin_threads, 0, s>>>(one ? nullptr : tasks_dev, by_value);
     return cudaGetLastError();
 }
 

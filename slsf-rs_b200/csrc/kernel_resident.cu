@@ -183,16 +183,24 @@ __device__ __forceinline__ Smem carve(unsigned char* base, uint32_t max_volume, 
 /* ---- phases ---- */
 
 __device__ __forceinline__ void load_state(const TaskView& t, const Geo& g, Smem& s) {
-    const float4* src = reinterpret_cast<const float4*>(t.theta);
-    for (uint32_t q = threadIdx.x; q < g.volume / 4; q += blockDim.x) {
-        const float4 v = src[q];
-        const Coords c = coords_of(g, 4 * q);
-        const uint32_t p = (c.y + c.z) & 1u; /* colour of the even-x site */
-        const uint32_t h = 2 * q;
-        s.th[p * g.stride1 + h] = v.x;
-        s.th[(p ^ 1u) * g.stride1 + h] = v.y;
-        s.th[p * g.stride1 + h + 1] = v.z;
-        s.th[(p ^ 1u) * g.stride1 + h + 1] = v.w;
+    if (g.lx % 4) {
+        /* L_x = 2 mod 4: four consecutive sites may span two rows; copy site by site */
+        for (uint32_t i = threadIdx.x; i < g.volume; i += blockDim.x) {
+            const Coords c = coords_of(g, i);
+            s.th[slot(g, i, (c.x + c.y + c.z) & 1u)] = t.theta[i];
+        }
+    } else {
+        const float4* src = reinterpret_cast<const float4*>(t.theta);
+        for (uint32_t q = threadIdx.x; q < g.volume / 4; q += blockDim.x) {
+            const float4 v = src[q];
+            const Coords c = coords_of(g, 4 * q);
+            const uint32_t p = (c.y + c.z) & 1u; /* colour of the even-x site */
+            const uint32_t h = 2 * q;
+            s.th[p * g.stride1 + h] = v.x;
+            s.th[(p ^ 1u) * g.stride1 + h] = v.y;
+            s.th[p * g.stride1 + h + 1] = v.z;
+            s.th[(p ^ 1u) * g.stride1 + h + 1] = v.w;
+        }
     }
     for (uint32_t z = threadIdx.x; z < g.lz; z += blockDim.x) {
         s.jxy[z] = t.jxy[z];
@@ -201,6 +209,13 @@ __device__ __forceinline__ void load_state(const TaskView& t, const Geo& g, Smem
 }
 
 __device__ __forceinline__ void store_state(const TaskView& t, const Geo& g, const Smem& s) {
+    if (g.lx % 4) {
+        for (uint32_t i = threadIdx.x; i < g.volume; i += blockDim.x) {
+            const Coords c = coords_of(g, i);
+            t.theta[i] = s.th[slot(g, i, (c.x + c.y + c.z) & 1u)];
+        }
+        return;
+    }
     float4* dst = reinterpret_cast<float4*>(t.theta);
     for (uint32_t q = threadIdx.x; q < g.volume / 4; q += blockDim.x) {
         const Coords c = coords_of(g, 4 * q);
@@ -709,9 +724,9 @@ int max_dynamic_smem(int device) {
 }  // namespace
 
 bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
-    /* Row words hold L_x <= 32 bits; the float4 colour-split copy needs
-     * L_x % 4 == 0 so that four consecutive sites never span two rows. */
-    if (lx > kMaxRowBits || lx < 4 || lx % 4 || ly < 2 || ly % 2 || lz < 2 || lz % 2) return false;
+    /* Row words hold L_x <= 32 bits; the colour-split layout needs even
+     * dimensions (L_x = 2 mod 4 copies the state site by site). */
+    if (lx > kMaxRowBits || lx < 4 || lx % 2 || ly < 2 || ly % 2 || lz < 2 || lz % 2) return false;
     const uint64_t v = (uint64_t)lx * ly * lz;
     return smem_bytes((uint32_t)v, ly * lz, lz) <= (size_t)max_dynamic_smem(device);
 }

@@ -161,3 +161,20 @@ def test_session_cycles_equal_manual_cycles(slsf, ctx, orc):
         assert nx == ny == cycles and np.array_equal(cx, cy)
         x.close()
         y.close()
+
+
+@pytest.mark.parametrize("dims,rxy,rz", [((4, 4, 500), 2, 250), ((4, 2, 260), 1, 130), ((8, 8, 40), 4, 20)])
+def test_tall_lattices_many_lags(slsf, ctx, orc, dims, rxy, rz):
+    # radii beyond the small launch sizes, few z items: every lag is formed
+    t = task(slsf, ctx, orc, dims, 3)
+    t.sweep(1)
+    R, Rz = min(rxy, dims[0] // 2, dims[1] // 2), min(rz, dims[2] // 2)
+    got = t.correlations(rxy, rz)
+    ref = orc.correlations_f32(dims, t.theta, R, Rz)
+    assert np.allclose(got["corr_z"], ref["corr_z"], atol=2e-6)
+    assert np.allclose(got["corr_x"], ref["corr_x"], atol=2e-6)
+    t.corr_setup(rxy, rz, 1, 1)
+    ctx.batch_correlations([t])
+    means, _ = t.corr_bins()
+    assert np.array_equal(means[0], flat(got))
+    t.close()
