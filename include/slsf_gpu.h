@@ -254,6 +254,17 @@ int slsf_task_correlations(slsf_task* task, uint32_t rmax_xy, uint32_t rmax_z, d
  * them into row count / binsize (rows past n_bins are not kept). */
 int slsf_task_corr_setup(slsf_task* task, uint32_t rmax_xy, uint32_t rmax_z, uint32_t binsize, uint32_t n_bins,
                          size_t* n_values);
+/* Correlations measured inside the batched sweeps: with interval > 0,
+ * every batched run or session step of the task (one-CTA kernel: even
+ * L_x <= 32 and a replica that fits shared memory) measures the correlation
+ * functions of the state after each sweep whose measurement index
+ * m = sweep - thermalization is a multiple of `interval`, from the replica
+ * in shared memory, into the bins of slsf_task_corr_setup (ThetaModel::measure,
+ * src/model.rs:410, with correlation_interval = interval).  0 turns it off.
+ * Such a task refuses the separate measurements (slsf_batch_correlations,
+ * slsf_batch_step_correlations).  Values agree with the separate kernels to
+ * FP32 partial-sum rounding. */
+int slsf_task_corr_fuse(slsf_task* task, uint32_t interval);
 /* The first n_rows rows of bin means ([n_rows][n_values]) and the number of
  * correlation measurements taken (either output may be NULL).  Blocks. */
 int slsf_task_corr_bins(const slsf_task* task, double* bin_means, size_t n_rows, uint64_t* count);

@@ -108,6 +108,7 @@ SIGNATURES = {
     "slsf_task_get_bins": (C.c_int, [_P, _F64P, C.c_size_t, _U64P]),
     "slsf_task_corr_setup": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_size_t)]),
     "slsf_task_corr_bins": (C.c_int, [_P, _F64P, C.c_size_t, _U64P]),
+    "slsf_task_corr_fuse": (C.c_int, [_P, C.c_uint32]),
     "slsf_batch_correlations": (C.c_int, [_P, C.POINTER(_P), C.c_size_t]),
     "slsf_task_state_size": (C.c_int, [_P, C.POINTER(C.c_size_t)]),
     "slsf_task_state_save": (C.c_int, [_P, _U64P, _P, C.c_size_t]),
@@ -441,6 +442,11 @@ class Task:
         check(load().slsf_task_corr_setup(self.h, rmax_xy, rmax_z, binsize, n_bins, C.byref(nv)))
         self.corr_n_values, self.corr_n_bins = nv.value, n_bins
         return nv.value
+
+    def corr_fuse(self, interval):
+        """Measure the correlations inside the batched sweeps every `interval`
+        measurements (slsf_task_corr_fuse; 0: off)."""
+        check(load().slsf_task_corr_fuse(self.h, interval))
 
     def corr_bins(self, n_rows=None):
         """(bin means [n_rows][values], correlation measurements so far)."""

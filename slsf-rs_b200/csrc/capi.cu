@@ -61,6 +61,8 @@ const char* kErrTemperature = "temperature T must be positive and finite";
 const char* kErrWidth = "proposal_width must be nonnegative and finite";
 const char* kErrEven = "red-black Metropolis sweep requires even lattice dimensions";
 const char* kErrCorrLong = "correlation lines plus lags longer than 775 sites are not supported";
+const char* kErrFuse = "correlations inside the sweeps need the one-CTA kernel (even L_x <= 32, replica in shared memory)";
+const char* kErrFused = "task measures its correlations inside the batched sweeps (slsf_task_corr_fuse)";
 
 bool temperature_ok(double t) { return t > 0.0 && std::isfinite(t); }
 bool width_ok(double w) { return w >= 0.0 && std::isfinite(w); }
@@ -121,6 +123,8 @@ struct slsf_ctx {
     /* batched engine scratch */
     TaskView* d_views = nullptr;
     TaskView* h_views = nullptr; /* pinned */
+    slsf::ResidentCorr* d_rcorr = nullptr; /* fused correlations, parallel to d_views */
+    slsf::ResidentCorr* h_rcorr = nullptr; /* pinned */
     unsigned long long* d_batch_stats = nullptr;
     unsigned long long* h_batch_stats = nullptr; /* pinned */
     uint32_t views_cap = 0;
@@ -185,6 +189,7 @@ struct slsf_task {
     uint32_t corr_rxy = 0, corr_rz = 0, corr_binsize = 1, corr_n_bins = 0;
     uint64_t corr_count = 0; /* host mirror of *corr_count_dev */
     uint64_t corr_gen = 0;   /* the context's set-up count when this set-up was made */
+    uint32_t corr_interval = 0; /* slsf_task_corr_fuse: measured inside the batched sweeps every this many */
     double* corr_partial = nullptr;
     double* corr_bins = nullptr;
     unsigned long long* corr_count_dev = nullptr;
@@ -259,16 +264,22 @@ int ensure_batch_capacity(slsf_ctx* ctx, size_t n) {
     if (ctx->views_cap >= n) return SLSF_OK;
     if (ctx->d_views) cudaFree(ctx->d_views);
     if (ctx->h_views) cudaFreeHost(ctx->h_views);
+    if (ctx->d_rcorr) cudaFree(ctx->d_rcorr);
+    if (ctx->h_rcorr) cudaFreeHost(ctx->h_rcorr);
     if (ctx->d_batch_stats) cudaFree(ctx->d_batch_stats);
     if (ctx->h_batch_stats) cudaFreeHost(ctx->h_batch_stats);
     ctx->d_views = nullptr;
     ctx->h_views = nullptr;
+    ctx->d_rcorr = nullptr;
+    ctx->h_rcorr = nullptr;
     ctx->d_batch_stats = nullptr;
     ctx->h_batch_stats = nullptr;
     ctx->views_cap = 0;
     const size_t cap = std::max<size_t>(n, 64);
     SLSF_CUDA(cudaMalloc(&ctx->d_views, sizeof(TaskView) * cap));
     SLSF_CUDA(cudaHostAlloc(&ctx->h_views, sizeof(TaskView) * cap, cudaHostAllocDefault));
+    SLSF_CUDA(cudaMalloc(&ctx->d_rcorr, sizeof(slsf::ResidentCorr) * cap));
+    SLSF_CUDA(cudaHostAlloc(&ctx->h_rcorr, sizeof(slsf::ResidentCorr) * cap, cudaHostAllocDefault));
     SLSF_CUDA(cudaMalloc(&ctx->d_batch_stats, 8 * slsf::kStatSlots * cap));
     SLSF_CUDA(cudaHostAlloc(&ctx->h_batch_stats, 8 * slsf::kStatSlots * cap, cudaHostAllocDefault));
     ctx->views_cap = (uint32_t)cap;
@@ -381,11 +392,13 @@ int slsf_ctx_destroy(slsf_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     cudaStreamSynchronize(ctx->own_stream);
-    void* dev[] = {ctx->d_views, ctx->d_batch_stats, ctx->d_queue, (void*)ctx->d_bin_src, ctx->d_bin_out};
+    void* dev[] = {ctx->d_views, ctx->d_batch_stats, ctx->d_queue, (void*)ctx->d_bin_src, ctx->d_bin_out,
+                   ctx->d_rcorr};
     for (void* p : dev)
         if (p) cudaFree(p);
     if (ctx->d_corr) cudaFree(ctx->d_corr);
-    void* host[] = {ctx->h_views, ctx->h_batch_stats, (void*)ctx->h_bin_src, ctx->h_bin_out, ctx->h_corr};
+    void* host[] = {ctx->h_views, ctx->h_batch_stats, (void*)ctx->h_bin_src, ctx->h_bin_out, ctx->h_corr,
+                    ctx->h_rcorr};
     for (void* p : host)
         if (p) cudaFreeHost(p);
     if (ctx->corr_uploaded) cudaEventDestroy(ctx->corr_uploaded);
@@ -769,6 +782,7 @@ int slsf_task_corr_setup(slsf_task* t, uint32_t rmax_xy, uint32_t rmax_z, uint32
     t->corr_rxy = t->corr_rz = t->corr_n_bins = 0;
     t->corr_binsize = 1;
     t->corr_count = 0;
+    t->corr_interval = 0;
     t->corr_gen = ++ctx->corr_gen;
     if (n_values) *n_values = nv;
     if (!on) return SLSF_OK;
@@ -792,6 +806,17 @@ int slsf_task_corr_setup(slsf_task* t, uint32_t rmax_xy, uint32_t rmax_z, uint32
     t->corr_rz = rz;
     t->corr_binsize = binsize ? binsize : 1;
     t->corr_n_bins = n_bins;
+    return SLSF_OK;
+}
+
+int slsf_task_corr_fuse(slsf_task* t, uint32_t interval) {
+    if (!t) return set_error(SLSF_ERR_INVALID, "task is NULL");
+    if (int rc = check_free(t)) return rc;
+    if (interval && !t->corr_block)
+        return set_error(SLSF_ERR_STATE, "task has no correlation bins; call slsf_task_corr_setup first");
+    if (interval && !slsf::resident_supports(t->lx, t->ly, t->lz, t->ctx->device))
+        return set_error(SLSF_ERR_INVALID, kErrFuse);
+    t->corr_interval = interval;
     return SLSF_OK;
 }
 
@@ -825,6 +850,7 @@ int slsf_batch_correlations(slsf_ctx* ctx, slsf_task* const* tasks, size_t n) {
         if (!t || t->ctx != ctx) return set_error(SLSF_ERR_INVALID, "task does not belong to this context");
         if (!t->corr_block)
             return set_error(SLSF_ERR_STATE, "task has no correlation bins; call slsf_task_corr_setup first");
+        if (t->corr_interval) return set_error(SLSF_ERR_STATE, kErrFused);
         if (same && (ctx->corr_last[i] != t || ctx->corr_last_gen[i] != t->corr_gen)) same = false;
     }
     if (int rc = bind_device(ctx)) return rc;
@@ -1117,6 +1143,33 @@ int ensure_queue_capacity(slsf_ctx* ctx, uint32_t n) {
 /* Shared body of slsf_batch_run (every task n_sweeps), slsf_batch_run_v
  * (task i per_task[i] sweeps; tasks with 0 sweeps are left out of the
  * launch) and the autotuner (`force`: one kernel choice for every task). */
+/* The fused-correlation entry of a task's view (bins NULL without). */
+static slsf::ResidentCorr rcorr_of(const slsf_task* t) {
+    if (!t->corr_interval || !t->corr_block) return slsf::ResidentCorr{nullptr, nullptr, 0, 0, 1, 0, 1};
+    return slsf::ResidentCorr{t->corr_bins, t->corr_count_dev, t->corr_rxy, t->corr_rz,
+                              t->corr_binsize, t->corr_n_bins, t->corr_interval};
+}
+
+static uint32_t rcorr_doubles(const slsf_task* t) {
+    return t->corr_interval ? slsf::resident_corr_doubles(t->ly, t->lz, t->corr_rxy, t->corr_rz) : 0;
+}
+
+/* Host mirrors of a task's counters after `sweeps` batched sweeps: sweep and
+ * Wolff counters, measurements (every sweep past thermalization) and fused
+ * correlation measurements (measurement m = sweep - thermalization when m is
+ * a multiple of the interval). */
+static void advance_counters(slsf_task* t, uint64_t sweeps) {
+    const uint64_t before = t->metro_sweeps;
+    t->metro_sweeps += sweeps;
+    t->wolff_done += sweeps * t->wolff_steps;
+    const uint64_t lo = std::max<uint64_t>(before, t->thermalization);
+    if (t->metro_sweeps > lo && t->n_bins) t->measurements += t->metro_sweeps - lo;
+    if (t->corr_interval && t->metro_sweeps > lo) {
+        const uint64_t q = t->corr_interval, a = lo - t->thermalization, b = t->metro_sweeps - t->thermalization;
+        t->corr_count += (b + q - 1) / q - (a + q - 1) / q; /* multiples of q in [a, b) */
+    }
+}
+
 static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_all, uint32_t n_sweeps,
                           const uint32_t* per_task, slsf_sweep_stats* all_stats,
                           const slsf::KernelChoice* force = nullptr) {
@@ -1148,6 +1201,7 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
         ch[i] = force ? *force : choice_for(ctx, t->lx, t->ly, t->lz);
         if (!choice_feasible(ch[i], t->lx, t->ly, t->lz, ctx->device))
             return set_error(SLSF_ERR_INVALID, "the kernel choice does not hold this lattice");
+        if (t->corr_interval && ch[i].kind != slsf::kKernelResident) return set_error(SLSF_ERR_INVALID, kErrFuse);
     }
     if (int rc = ensure_batch_capacity(ctx, n)) return rc;
     /* Grouped by kernel choice (one persistent launch each; cluster groups
@@ -1157,7 +1211,8 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
     auto rank = [&](size_t i) {
         const slsf::KernelChoice& c = ch[i];
         const uint32_t k = c.kind == slsf::kKernelCluster ? 2u : (c.kind == slsf::kKernelResident ? 1u : 0u);
-        return ((uint64_t)k << 48) | ((uint64_t)c.cluster << 16) | c.threads;
+        const uint64_t fused = tasks[i]->corr_interval ? 1u : 0u;
+        return ((uint64_t)k << 48) | (fused << 40) | ((uint64_t)c.cluster << 16) | c.threads;
     };
     std::vector<size_t> order(n);
     for (size_t i = 0; i < n; ++i) order[i] = i;
@@ -1170,13 +1225,19 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
     for (size_t k = 0; k < n; ++k)
         if (k == 0 || rank(order[k]) != rank(order[k - 1])) ++n_groups;
     if (int rc = ensure_queue_capacity(ctx, n_groups)) return rc;
+    bool any_fused = false;
     for (size_t k = 0; k < n; ++k) {
         TaskView v = tasks[order[k]]->view();
         v.stats = ctx->d_batch_stats + slsf::kStatSlots * order[k];
         v.sweeps = sweeps_of[order[k]];
         ctx->h_views[k] = v;
+        ctx->h_rcorr[k] = rcorr_of(tasks[order[k]]);
+        any_fused |= tasks[order[k]]->corr_interval != 0;
     }
     SLSF_CUDA(cudaMemcpyAsync(ctx->d_views, ctx->h_views, sizeof(TaskView) * n, cudaMemcpyHostToDevice, ctx->stream));
+    if (any_fused)
+        SLSF_CUDA(cudaMemcpyAsync(ctx->d_rcorr, ctx->h_rcorr, sizeof(slsf::ResidentCorr) * n, cudaMemcpyHostToDevice,
+                                  ctx->stream));
     SLSF_CUDA(cudaMemsetAsync(ctx->d_batch_stats, 0, 8 * slsf::kStatSlots * n, ctx->stream));
     SLSF_CUDA(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned int) * n_groups, ctx->stream));
     /* Group g runs on ctx->stream (g == 0) or on a side stream, forked after
@@ -1193,9 +1254,10 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
         }
         size_t hi = lo;
         const uint32_t parts = c.kind == slsf::kKernelCluster ? c.cluster : 1;
-        uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0, max_lx = 0;
+        uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0, max_lx = 0, max_cd = 0;
         while (hi < n && rank(order[hi]) == key) {
             const slsf_task* t = tasks[order[hi]];
+            max_cd = std::max(max_cd, rcorr_doubles(t));
             max_vs = std::max(max_vs, t->volume / parts);
             max_rows = std::max(max_rows, t->ly * (t->lz / parts));
             max_lz = std::max(max_lz, t->lz);
@@ -1207,7 +1269,8 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
             for (size_t k = lo; k < hi; ++k) run_grid_task(ctx, tasks[order[k]], ctx->h_views[k], st);
         } else if (c.kind == slsf::kKernelResident) {
             SLSF_CUDA(slsf::launch_resident(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
-                                            ctx->device, st, max_vs, max_rows, max_lz, c.threads, nullptr));
+                                            ctx->device, st, max_vs, max_rows, max_lz, c.threads, nullptr,
+                                            max_cd ? ctx->d_rcorr + lo : nullptr, max_cd));
             ctx->launches += 1;
         } else {
             SLSF_CUDA(slsf::launch_batched(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
@@ -1228,12 +1291,7 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
     for (size_t i = 0; i < n; ++i) {
         slsf_task* t = tasks[i];
         const uint32_t sw = sweeps_of[i];
-        const uint64_t before = t->metro_sweeps;
-        t->metro_sweeps += sw;
-        t->wolff_done += (uint64_t)sw * t->wolff_steps;
-        /* Measurements happen after sweeps past the thermalization count. */
-        const uint64_t lo = std::max<uint64_t>(before, t->thermalization);
-        if (t->metro_sweeps > lo && t->n_bins) t->measurements += t->metro_sweeps - lo;
+        advance_counters(t, sw);
         const unsigned long long* s = &ctx->h_batch_stats[i * slsf::kStatSlots];
         if (s[slsf::kStatError]) rc = set_error(SLSF_ERR_TIMEOUT, "a bounded device loop hit its iteration limit");
         if (all_stats) {
@@ -1261,12 +1319,14 @@ struct slsf_batch {
     unsigned long long* d_counters = nullptr; /* [view][Metropolis, Wolff], advanced by the kernels */
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    slsf::ResidentCorr* d_rcorr = nullptr; /* fused correlations, parallel to d_views */
     unsigned long long* d_acc = nullptr; /* stats summed over the cycles of slsf_batch_step_correlations */
     unsigned long long* h_acc = nullptr; /* pinned */
 };
 
 static void batch_free(slsf_batch* b) {
     if (b->d_acc) cudaFree(b->d_acc);
+    if (b->d_rcorr) cudaFree(b->d_rcorr);
     if (b->h_acc) cudaFreeHost(b->h_acc);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
@@ -1296,10 +1356,13 @@ int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n
         if (ch[i].kind == slsf::kKernelGrid || !choice_feasible(ch[i], t->lx, t->ly, t->lz, ctx->device))
             return set_error(SLSF_ERR_INVALID,
                              "batch sessions hold lattices that fit one thread-block cluster's shared memory");
+        if (t->corr_interval && ch[i].kind != slsf::kKernelResident) return set_error(SLSF_ERR_INVALID, kErrFuse);
     }
     auto rank = [&](size_t i) {
         const slsf::KernelChoice& c = ch[i];
-        return ((uint64_t)(c.kind == slsf::kKernelCluster ? 2u : 1u) << 48) | ((uint64_t)c.cluster << 16) | c.threads;
+        const uint64_t fused = tasks[i]->corr_interval ? 1u : 0u;
+        return ((uint64_t)(c.kind == slsf::kKernelCluster ? 2u : 1u) << 48) | (fused << 40) |
+               ((uint64_t)c.cluster << 16) | c.threads;
     };
     std::vector<size_t> order(n);
     for (size_t i = 0; i < n; ++i) order[i] = i;
@@ -1334,6 +1397,17 @@ int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n
         views[k] = v;
     }
     if (e == cudaSuccess) e = cudaMemcpy(b->d_views, views.data(), sizeof(TaskView) * n, cudaMemcpyHostToDevice);
+    {
+        std::vector<slsf::ResidentCorr> rc(n);
+        bool any = false;
+        for (size_t k = 0; k < n; ++k) {
+            rc[k] = rcorr_of(tasks[order[k]]);
+            any |= tasks[order[k]]->corr_interval != 0;
+        }
+        if (any && e == cudaSuccess) e = cudaMalloc(&b->d_rcorr, sizeof(slsf::ResidentCorr) * n);
+        if (any && e == cudaSuccess)
+            e = cudaMemcpy(b->d_rcorr, rc.data(), sizeof(slsf::ResidentCorr) * n, cudaMemcpyHostToDevice);
+    }
     if (e != cudaSuccess) {
         batch_free(b);
         return cuda_error(e, "batch session set-up");
@@ -1356,9 +1430,10 @@ int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n
         }
         size_t hi = lo;
         const uint32_t parts = c.kind == slsf::kKernelCluster ? c.cluster : 1;
-        uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0, max_lx = 0;
+        uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0, max_lx = 0, max_cd = 0;
         while (hi < n && rank(order[hi]) == key) {
             const slsf_task* t = tasks[order[hi]];
+            max_cd = std::max(max_cd, rcorr_doubles(t));
             max_vs = std::max(max_vs, t->volume / parts);
             max_rows = std::max(max_rows, t->ly * (t->lz / parts));
             max_lz = std::max(max_lz, t->lz);
@@ -1369,7 +1444,8 @@ int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n
         if (e == cudaSuccess) {
             if (c.kind == slsf::kKernelResident)
                 e = slsf::launch_resident(b->d_views + lo, (uint32_t)(hi - lo), n_sweeps, b->d_queue + q, ctx->device,
-                                          st, max_vs, max_rows, max_lz, c.threads, b->d_counters + 2 * lo);
+                                          st, max_vs, max_rows, max_lz, c.threads, b->d_counters + 2 * lo,
+                                          max_cd ? b->d_rcorr + lo : nullptr, max_cd);
             else
                 e = slsf::launch_batched(b->d_views + lo, (uint32_t)(hi - lo), n_sweeps, b->d_queue + q, ctx->device,
                                          st, c.cluster, c.threads, max_vs, max_rows, max_lz, max_plane, max_lx,
@@ -1408,11 +1484,7 @@ int slsf_batch_step(slsf_batch* b, slsf_sweep_stats* stats) {
     int rc = SLSF_OK;
     for (size_t i = 0; i < b->tasks.size(); ++i) {
         slsf_task* t = b->tasks[i];
-        const uint64_t before = t->metro_sweeps;
-        t->metro_sweeps += b->n_sweeps;
-        t->wolff_done += (uint64_t)b->n_sweeps * t->wolff_steps;
-        const uint64_t lo = std::max<uint64_t>(before, t->thermalization);
-        if (t->metro_sweeps > lo && t->n_bins) t->measurements += t->metro_sweeps - lo;
+        advance_counters(t, b->n_sweeps);
         const unsigned long long* s = &b->h_stats[i * slsf::kStatSlots];
         if (s[slsf::kStatError]) rc = set_error(SLSF_ERR_TIMEOUT, "a bounded device loop hit its iteration limit");
         if (stats) stats[i] = slsf_sweep_stats{b->n_sweeps, s[slsf::kStatAccepted], s[slsf::kStatClusters],
@@ -1436,9 +1508,11 @@ int slsf_batch_step_correlations(slsf_batch* b, uint32_t n_cycles, slsf_sweep_st
     if (!b) return set_error(SLSF_ERR_INVALID, "session is NULL");
     slsf_ctx* ctx = b->ctx;
     const size_t n = b->tasks.size();
-    for (slsf_task* t : b->tasks)
+    for (slsf_task* t : b->tasks) {
         if (!t->corr_block)
             return set_error(SLSF_ERR_STATE, "task has no correlation bins; call slsf_task_corr_setup first");
+        if (t->corr_interval) return set_error(SLSF_ERR_STATE, kErrFused);
+    }
     if (n_cycles == 0) {
         if (stats)
             for (size_t i = 0; i < n; ++i) stats[i] = slsf_sweep_stats{0, 0, 0, 0};
@@ -1466,11 +1540,7 @@ int slsf_batch_step_correlations(slsf_batch* b, uint32_t n_cycles, slsf_sweep_st
     int rc = SLSF_OK;
     for (size_t i = 0; i < n; ++i) {
         slsf_task* t = b->tasks[i];
-        const uint64_t before = t->metro_sweeps;
-        t->metro_sweeps += sweeps;
-        t->wolff_done += sweeps * t->wolff_steps;
-        const uint64_t lo = std::max<uint64_t>(before, t->thermalization);
-        if (t->metro_sweeps > lo && t->n_bins) t->measurements += t->metro_sweeps - lo;
+        advance_counters(t, sweeps);
         const unsigned long long* a = &b->h_acc[i * slsf::kStatSlots];
         if (a[slsf::kStatError]) rc = set_error(SLSF_ERR_TIMEOUT, "a bounded device loop hit its iteration limit");
         if (stats) stats[i] = slsf_sweep_stats{sweeps, a[slsf::kStatAccepted], a[slsf::kStatClusters],

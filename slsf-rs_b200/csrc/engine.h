@@ -47,6 +47,15 @@ struct TaskView {
     unsigned long long* stats;
 };
 
+/* Correlations measured inside the sweeps of the one-CTA kernel
+ * (slsf_task_corr_fuse), one entry per task view of a launch; bins NULL for
+ * a task without them. */
+struct ResidentCorr {
+    double* bins;               /* [n_bins][values] sums */
+    unsigned long long* count;  /* correlation measurements so far */
+    uint32_t rxy, rz, binsize, n_bins, interval;
+};
+
 /* How a batched launch runs one lattice shape: which kernel, how many CTAs
  * hold a replica (cluster kernel) and how many threads a CTA has.  The
  * choice changes neither a task's trajectory nor its bins beyond FP32
@@ -120,7 +129,10 @@ bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);
  * count (Ly Lz) and Lz over the views. */
 cudaError_t launch_resident(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                             int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
-                            uint32_t threads, unsigned long long* counters);
+                            uint32_t threads, unsigned long long* counters, const ResidentCorr* corr_dev = nullptr,
+                            uint32_t corr_doubles = 0);
+/* Shared doubles the fused correlation measurement of one task needs (0 without). */
+uint32_t resident_corr_doubles(uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
 
 /* ---- batched persistent engine, one cluster per replica (kernel_cluster.cu) ---- */
 /* Whether a cluster of c CTAs (a power of two up to 16) holds one replica of

@@ -165,6 +165,7 @@ struct Smem {
     uint32_t* cl;
     float* jxy;
     float* jz;
+    double* corr; /* fused correlation scratch (resident_corr_doubles) */
 };
 
 __device__ __forceinline__ Smem carve(unsigned char* base, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz) {
@@ -177,6 +178,8 @@ __device__ __forceinline__ Smem carve(unsigned char* base, uint32_t max_volume, 
     s.cl = w + 3 * max_rows;
     s.jxy = reinterpret_cast<float*>(w + 4 * max_rows);
     s.jz = s.jxy + max_lz;
+    /* 8-byte aligned: the volume is even, the other arrays are whole words */
+    s.corr = reinterpret_cast<double*>(s.jz + max_lz);
     return s;
 }
 
@@ -579,6 +582,133 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
     SLSF_PHASE(4);
 }
 
+/* (cos, sin) of the site (x, y, z) of the resident state. */
+__device__ __forceinline__ float2 trig_at(const Geo& g, const Smem& s, uint32_t x, uint32_t y, uint32_t z) {
+    float sn, cn;
+    __sincosf(s.th[slot(g, x + g.lx * (y + g.ly * z), (x + y + z) & 1u)], &sn, &cn);
+    return make_float2(cn, sn);
+}
+
+/* FP64 sum over the warp's lanes (the same shuffle tree everywhere). */
+__device__ __forceinline__ double warp_total(double v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    return v;
+}
+
+/* Correlation functions of the resident state (measure_theta_correlations_with_scratch,
+ * src/observables.rs:165-270), measured between sweeps and added into row
+ * count / binsize of the task's correlation bins in ThetaModel::measure's
+ * order (C_x, C_y, C_xy, C_xy(z, r), C_z).  Per layer z a warp takes the x
+ * lines (lane = x; partners at x + r by shuffle within the row) and the y
+ * lines (lane = x; a register window of 8 partners slides along y); per row
+ * y a warp takes the z lines the same way along z.  Products are FP32 fused
+ * multiply-adds summed per lane over one line length (<= 32), lanes and
+ * layers in FP64 in a fixed order.  Scratch (shared): sx, sy [L_z][R] and the
+ * per-row z sums [L_y][R_z]. */
+__device__ __noinline__ void corr_measure(const ResidentCorr& c, const Geo& g, const Smem& s) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t R = c.rxy, Rz = c.rz, lx = g.lx, ly = g.ly, lz = g.lz;
+    double* sx = s.corr;
+    double* sy = sx + lz * R;
+    double* szr = sy + lz * R;
+    const bool xv = lane < lx;
+    const uint32_t x = xv ? lane : 0u;
+    for (uint32_t u = warp; u < lz + ly; u += nwarps) {
+        if (u < lz) {
+            const uint32_t z = u;
+            for (uint32_t r0 = 1; r0 <= R; r0 += 8) {
+                /* x lines: the partner of x at lag r is lane (x + r) mod L_x of the row */
+                uint32_t src[8];
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j) src[j] = (x + r0 + j) % lx;
+                float ax[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                float ay[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                /* y lines: w[j] = partner (x, k + r0 + j) of the current k */
+                float2 w[8];
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j) w[j] = trig_at(g, s, x, (r0 + j) % ly, z);
+                uint32_t nxt = (r0 + 8) % ly; /* y of the partner entering the window after k */
+                for (uint32_t k = 0; k < ly; ++k) {
+                    float2 a = trig_at(g, s, x, k, z);
+                    if (!xv) a = make_float2(0.0f, 0.0f);
+#pragma unroll
+                    for (uint32_t j = 0; j < 8; ++j) {
+                        const float pc = __shfl_sync(0xffffffffu, a.x, src[j]);
+                        const float ps = __shfl_sync(0xffffffffu, a.y, src[j]);
+                        ax[j] = __fmaf_rn(a.y, ps, __fmaf_rn(a.x, pc, ax[j]));
+                        ay[j] = __fmaf_rn(a.y, w[j].y, __fmaf_rn(a.x, w[j].x, ay[j]));
+                    }
+#pragma unroll
+                    for (uint32_t j = 0; j + 1 < 8; ++j) w[j] = w[j + 1];
+                    w[7] = trig_at(g, s, x, nxt, z);
+                    nxt = nxt + 1 == ly ? 0u : nxt + 1;
+                }
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j) {
+                    const double vx = warp_total((double)ax[j]), vy = warp_total((double)ay[j]);
+                    if (lane == 0 && r0 + j <= R) {
+                        sx[z * R + r0 + j - 1] = vx;
+                        sy[z * R + r0 + j - 1] = vy;
+                    }
+                }
+            }
+        } else {
+            const uint32_t y = u - lz;
+            for (uint32_t r0 = 1; r0 <= Rz; r0 += 8) {
+                /* z lines of row y: w[j] = partner (x, y, k + r0 + j) */
+                float az[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                float2 w[8];
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j) w[j] = trig_at(g, s, x, y, (r0 + j) % lz);
+                uint32_t nxt = (r0 + 8) % lz;
+                for (uint32_t k = 0; k < lz; ++k) {
+                    float2 a = trig_at(g, s, x, y, k);
+                    if (!xv) a = make_float2(0.0f, 0.0f);
+#pragma unroll
+                    for (uint32_t j = 0; j < 8; ++j) az[j] = __fmaf_rn(a.y, w[j].y, __fmaf_rn(a.x, w[j].x, az[j]));
+#pragma unroll
+                    for (uint32_t j = 0; j + 1 < 8; ++j) w[j] = w[j + 1];
+                    w[7] = trig_at(g, s, x, y, nxt);
+                    nxt = nxt + 1 == lz ? 0u : nxt + 1;
+                }
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j) {
+                    const double v = warp_total((double)az[j]);
+                    if (lane == 0 && r0 + j <= Rz) szr[y * Rz + r0 + j - 1] = v;
+                }
+            }
+        }
+    }
+    __shared__ unsigned long long s_row;
+    if (threadIdx.x == 0) s_row = *c.count / c.binsize;
+    __syncthreads();
+    if (s_row < c.n_bins) {
+        const uint32_t nv = 3 * R + lz * R + Rz;
+        double* bin = c.bins + s_row * nv;
+        const double volume = (double)g.volume, area = (double)g.plane;
+        for (uint32_t j = threadIdx.x; j < lz * R; j += blockDim.x) bin[3 * R + j] += (sx[j] + sy[j]) / (2.0 * area);
+        for (uint32_t r = threadIdx.x; r < R; r += blockDim.x) {
+            double a = 0.0, b = 0.0;
+            for (uint32_t z = 0; z < lz; ++z) {
+                a += sx[z * R + r];
+                b += sy[z * R + r];
+            }
+            const double cx = a / volume, cy = b / volume;
+            bin[r] += cx;
+            bin[R + r] += cy;
+            bin[2 * R + r] += (cx + cy) / 2.0;
+        }
+        for (uint32_t r = threadIdx.x; r < Rz; r += blockDim.x) {
+            double a = 0.0;
+            for (uint32_t y = 0; y < ly; ++y) a += szr[y * Rz + r];
+            bin[3 * R + lz * R + r] += a / volume;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *c.count += 1;
+}
+
 /* Fused observables of the resident state (src/observables.rs:99-141): mx,
  * my, cos xyz, sin xyz; FP64 sums of the FP32 bond terms, block total valid
  * in thread 0. */
@@ -623,9 +753,11 @@ __device__ __forceinline__ void measure(const Geo& g, const Smem& s, double (&ac
 }
 
 
+template <bool kCorr>
 __global__ void __launch_bounds__(kBThreads, 1)
     k_resident(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
-               uint32_t max_volume, uint32_t max_rows, uint32_t max_lz, unsigned long long* __restrict__ counters) {
+               uint32_t max_volume, uint32_t max_rows, uint32_t max_lz, unsigned long long* __restrict__ counters,
+               const ResidentCorr* __restrict__ corr) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[8 * 32];
     __shared__ double bin_acc[kBinCols];
@@ -681,6 +813,16 @@ __global__ void __launch_bounds__(kBThreads, 1)
             SLSF_PHASE(1);
             for (uint32_t k = 0; k < t.wolff_steps; ++k)
                 wolff_update(t, g, s, t.wolff_done + (uint64_t)sw * t.wolff_steps + k, &s_cluster);
+            /* ThetaModel::measure's correlations of the state after this sweep:
+             * measurement m = sweep - thermalization, every corr_interval-th */
+            if constexpr (kCorr) {
+                const ResidentCorr& c = corr[item];
+                if (c.bins && sweep >= t.thermalization && (sweep - t.thermalization) % c.interval == 0) {
+                    __syncthreads();
+                    corr_measure(c, g, s);
+                    __syncthreads();
+                }
+            }
         }
         const uint64_t last = t.metro_sweeps + sweeps;
         /* the counters advance on the device, so that a replayed launch
@@ -710,8 +852,28 @@ __global__ void __launch_bounds__(kBThreads, 1)
     }
 }
 
-size_t smem_bytes(uint32_t max_volume, uint32_t max_rows, uint32_t max_lz) {
-    return 4ull * (max_volume + 2 * kPad) + 16ull * max_rows + 8ull * max_lz;
+size_t smem_bytes(uint32_t max_volume, uint32_t max_rows, uint32_t max_lz, uint32_t corr_doubles = 0) {
+    return 4ull * (max_volume + 2 * kPad) + 16ull * max_rows + 8ull * max_lz + 8ull * corr_doubles;
+}
+
+template <bool kCorr>
+cudaError_t launch_resident_t(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
+                              int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
+                              uint32_t threads, unsigned long long* counters, const ResidentCorr* corr,
+                              uint32_t corr_doubles) {
+    const size_t smem = smem_bytes(max_volume, max_rows, max_lz, corr_doubles);
+    cudaError_t e = cudaFuncSetAttribute(k_resident<kCorr>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int sms = 0, per_sm = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resident<kCorr>, (int)threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const uint32_t grid = std::min<uint32_t>(n, (uint32_t)(sms * per_sm));
+    k_resident<kCorr><<<grid, threads, smem, s>>>(views_dev, n, n_sweeps, queue, max_volume, max_rows, max_lz,
+                                                  counters, corr);
+    return cudaGetLastError();
 }
 
 int max_dynamic_smem(int device) {
@@ -731,22 +893,22 @@ bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device) {
     return smem_bytes((uint32_t)v, ly * lz, lz) <= (size_t)max_dynamic_smem(device);
 }
 
+uint32_t resident_corr_doubles(uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
+    return (rxy || rz) ? 2 * lz * rxy + ly * rz : 0;
+}
+
 cudaError_t launch_resident(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                             int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
-                            uint32_t threads, unsigned long long* counters) {
+                            uint32_t threads, unsigned long long* counters, const ResidentCorr* corr_dev,
+                            uint32_t corr_doubles) {
     if (threads < 32 || threads > (uint32_t)kBThreads || threads % 32) return cudaErrorInvalidConfiguration;
-    const size_t smem = smem_bytes(max_volume, max_rows, max_lz);
-    cudaError_t e = cudaFuncSetAttribute(k_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    int sms = 0, per_sm = 0;
-    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resident, (int)threads, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    const uint32_t grid = std::min<uint32_t>(n, (uint32_t)(sms * per_sm));
-    k_resident<<<grid, threads, smem, s>>>(views_dev, n, n_sweeps, queue, max_volume, max_rows, max_lz, counters);
-    return cudaGetLastError();
+    /* the fused correlation measurement is compiled into its own instance, so
+     * groups without it run the kernel unchanged */
+    if (corr_dev && corr_doubles)
+        return launch_resident_t<true>(views_dev, n, n_sweeps, queue, device, s, max_volume, max_rows, max_lz,
+                                       threads, counters, corr_dev, corr_doubles);
+    return launch_resident_t<false>(views_dev, n, n_sweeps, queue, device, s, max_volume, max_rows, max_lz,
+                                    threads, counters, nullptr, 0);
 }
 
 }  // namespace slsf

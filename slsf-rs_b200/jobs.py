@@ -17,11 +17,12 @@ ThetaJob::selected_tasks, src/model.rs:60-68):
 * tasks without correlation measurements go to the continuous-batching
   server (batched persistent launches, bins kept on the device);
 * tasks that measure correlations (the reference's default: r_max = L/2) run
-  as groups through the batched kernels too, stopping every
-  `correlation_interval` measurements for one batched launch of the
-  correlation functions of every task of the group, binned on the device
-  (ThetaModel::measure, src/model.rs:402-442).  The trajectories are the
-  ones the single-task path produces.
+  as groups through the batched kernels too (ThetaModel::measure,
+  src/model.rs:402-442), binned on the device: replicas that fit the
+  one-CTA kernel measure them inside the sweeps (slsf_task_corr_fuse);
+  other groups stop every `correlation_interval` measurements for one
+  batched correlation launch.  The trajectories are the ones the single-task
+  path produces.
 
 The result has the reference's ThetaJobResult layout (src/model.rs:72-106:
 job_name, rank, world_size, tasks[] with task, observables{name: {mean,
@@ -467,7 +468,9 @@ def _run_correlated(pkg, ctx, group, ck: Optional[Checkpoints] = None, gdir: Opt
     correlation launch that adds every task's values into its correlation bins
     on the device.  A correlation series is binned with the task's bin size
     (BinnedEstimate::from_samples); a series shorter than one bin forms one
-    bin.  With checkpoints, every task's device state (slsf_task_state_save,
+    bin.  When every replica fits the one-CTA kernel the measurements happen
+    inside the sweeps instead (slsf_task_corr_fuse) and the run is plain
+    batched sweeps.  With checkpoints, every task's device state (slsf_task_state_save,
     the acceptance count riding in its caller words) goes to `gdir` between
     measurements when one is due; a restart loads them and continues."""
     import ctypes as C
@@ -531,9 +534,42 @@ def _run_correlated(pkg, ctx, group, ck: Optional[Checkpoints] = None, gdir: Opt
             if due == "stop":
                 raise Stopped()
 
+        # Replicas that fit the one-CTA kernel measure their correlations
+        # inside the sweeps (slsf_task_corr_fuse): the whole run is then
+        # batched sweeps, 100 per CUDA-graph replay, checkpoint checks between.
+        fused = len(measured) == len(objs)
+        if fused:
+            try:
+                for o in objs:
+                    o.corr_fuse(interval)
+            except pkg.SlsfError as e:
+                if e.code != pkg.ERR_INVALID:
+                    raise
+                for o in objs:
+                    o.corr_fuse(0)
+                fused = False
+        chunk = 100
+        while fused and pos < therm + sweeps:
+            n = min(chunk, therm + sweeps - pos)
+            if n == chunk and session is not False:
+                if session is None:
+                    try:
+                        session = ctx.session(objs, chunk)
+                    except pkg.SlsfError as e:
+                        if e.code != pkg.ERR_INVALID:
+                            raise
+                        session = False
+                        continue
+                for i, st in enumerate(session.step()):
+                    accepted[i] += st["accepted"]
+                pos += n
+            else:
+                advance(n)
+            if ck and (due := ck.due()):
+                save(due)
         if pos < therm:
             advance(therm - pos)
-        m_idx = corr_done
+        m_idx = n_corr if fused else corr_done
         while m_idx < n_corr:
             n = therm + m_idx * interval + 1 - pos
             if n == interval and len(measured) == len(objs) and session is not False:

@@ -178,3 +178,70 @@ def test_tall_lattices_many_lags(slsf, ctx, orc, dims, rxy, rz):
     means, _ = t.corr_bins()
     assert np.array_equal(means[0], flat(got))
     t.close()
+
+
+@pytest.mark.parametrize("interval", [1, 3])
+def test_fused_correlations_equal_separate(slsf, ctx, orc, interval):
+    # In-kernel measurement (one-CTA kernel, replica in shared memory) against
+    # the separate kernels on the same trajectory: same counts and bins to
+    # FP32 partial-sum rounding.
+    shapes = [(8, 8, 8), (16, 12, 20), (32, 32, 32), (6, 10, 4), (12, 8, 6), (4, 4, 12)]
+    therm, sweeps = 2, 9
+    n_corr = (sweeps + interval - 1) // interval
+
+    def make(fused):
+        ts = []
+        for k, d in enumerate(shapes):
+            jxy, jz = np.full(d[2], 1.0), orc.uniform_disorder(d[2], 0.5, 1.5, 60 + k)
+            t = slsf.Task(ctx, d, jxy, jz, 1.2, seed=60 + k, thermalization=therm, binsize=3, n_bins=3)
+            t.init_random()
+            t.corr_setup(d[0] // 2, d[2] // 2, 1, n_corr)
+            if fused:
+                t.corr_fuse(interval)
+            ts.append(t)
+        return ts
+
+    fused, sep = make(True), make(False)
+    ctx.batch_run(fused, therm + 4)
+    ctx.batch_run(fused, sweeps - 4)  # the measurement schedule continues across launches
+    ctx.batch_run(sep, therm)
+    done = 0
+    for m in range(0, sweeps, interval):
+        ctx.batch_run(sep, m + 1 - done)
+        done = m + 1
+        ctx.batch_correlations(sep)
+    ctx.batch_run(sep, sweeps - done)
+    for a, b in zip(fused, sep):
+        assert np.array_equal(a.theta.view(np.uint32), b.theta.view(np.uint32))
+        ma, na = a.corr_bins()
+        mb, nb = b.corr_bins()
+        assert na == nb == n_corr
+        assert np.allclose(ma, mb, rtol=0, atol=2e-6), a.dims
+        a.close()
+        b.close()
+
+
+def test_fused_in_sessions_and_refusals(slsf, ctx, orc):
+    t = task(slsf, ctx, orc, (16, 16, 16), 70)
+    with pytest.raises(slsf.SlsfError) as e:
+        t.corr_fuse(1)
+    assert e.value.code == slsf.ERR_STATE  # no bins yet
+    t.corr_setup(8, 8, 2, 4)
+    t.corr_fuse(1)
+    with pytest.raises(slsf.SlsfError) as e:
+        ctx.batch_correlations([t])
+    assert e.value.code == slsf.ERR_STATE and "inside the batched sweeps" in str(e.value)
+    with ctx.session([t], 4) as ses:
+        ses.step()
+        ses.step()
+        with pytest.raises(slsf.SlsfError):
+            ses.step_correlations(1)
+    _, n = t.corr_bins()
+    assert n == 8
+    big = task(slsf, ctx, orc, (48, 48, 48), 71)
+    big.corr_setup(4, 4, 1, 1)
+    with pytest.raises(slsf.SlsfError) as e:
+        big.corr_fuse(1)
+    assert "one-CTA kernel" in str(e.value)
+    t.close()
+    big.close()

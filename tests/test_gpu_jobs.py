@@ -122,9 +122,11 @@ def test_correlated_job_equals_single_task_path(slsf, ctx, jobs):
         names = jobs.corr_names(t["l_z"], t["correlation_rmax_xy"], t["correlation_rmax_z"])
         assert sorted(n for n in rec["observables"] if n.startswith("Corr")) == sorted(names)
         for j, name in enumerate(names):
-            # same trajectory, same correlation kernel: the series agree bit for bit
+            # same trajectory; measured inside the sweeps (the job's lattices fit
+            # the one-CTA kernel) against the separate kernels: FP32 partial sums
             ref = slsf.binned_estimate(corr[:, j], 3)
-            assert rec["observables"][name] == {"mean": ref["mean"], "error": ref["stderr"]}, name
+            got = rec["observables"][name]
+            assert abs(got["mean"] - ref["mean"]) < 2e-6 and abs(got["error"] - ref["stderr"]) < 2e-6, name
         for name in slsf.BIN_NAMES + slsf.DERIVED:
             # batched bins reduce in FP32 per site, the grid measure in FP64
             x, y = rec["observables"][name]["mean"], est[name][0]
@@ -186,9 +188,11 @@ class StopAt:
 
 
 LONG_SERVED = SERVED.replace("L = [4, 6]", "L = [16, 32]").replace("sweeps = 16", "sweeps = 3000")
+# 243 sweeps: three CUDA-graph replays of at most 100 sweeps, checkpoint checks between them
+LONG_CORRELATED = CORRELATED.replace("sweeps = 12", "sweeps = 240")
 
 
-@pytest.mark.parametrize("text,n_stop", [(LONG_SERVED, 1), (CORRELATED, 2)])
+@pytest.mark.parametrize("text,n_stop", [(LONG_SERVED, 1), (LONG_CORRELATED, 2)])
 def test_stop_and_restart_equals_uninterrupted(slsf, ctx, jobs, tmp_path, text, n_stop):
     cfg = jobs.config_from_toml(text)
     whole = jobs.run_job(ctx, cfg, epoch_sweeps=50)
