@@ -380,7 +380,7 @@ def job_figure(pkg):
     reference's production job shape (L in {8, 16, 24, 32}, ten temperatures in
     [1.1, 1.5], two-point J_xy = 1.5 +- 0.5, J_z = 0.1, no correlations: the
     served path) and a default-correlation job (r_max = L/2 measured every
-    sweep: batched groups with one correlation launch pair per measurement).
+    sweep, measured inside the one-CTA kernel's sweeps).
     Wall clock around run_job (task expansion, device set-up, runs, estimates);
     synthetic tasks from the job schema, no files written."""
     import time
@@ -412,8 +412,8 @@ corr_rmax_z = [0, 0, 0, 0]
 name = "bench_correlated"
 [model]
 L = [8, 16]
-T = [1.1, 1.2, 1.3, 1.4, 1.5]
-samples = 8
+T = [1.1, 1.15, 1.2, 1.25, 1.3, 1.35, 1.4, 1.45, 1.5, 1.55]
+samples = 16
 base_seed = 20260710
 j_xy = 1.5
 delta_j_xy = [0.5]
@@ -566,6 +566,9 @@ def main():
         if not args.no_plain:
             extra["plain"] = plain_rate(pkg, ctx)
             extra["plain"]["batched_over_plain"] = value / extra["plain"]["value"]
+            # the same single-task path on the headline's replica size, for context
+            same = plain_rate(pkg, ctx, L=L, T=1.3, sweeps=500)
+            extra["plain"]["same_L"] = {"value": same["value"], "L": L, "batched_over_plain": value / same["value"]}
         if not args.no_large:
             extra["large"] = large_lattice(pkg, ctx, stream)
         if not args.no_serve:
