@@ -70,7 +70,7 @@ __host__ __device__ inline CorrShape corr_shape(uint32_t lx, uint32_t ly, uint32
 /* `tasks` in device memory, or NULL and the single task `one` by value. */
 __global__ void __launch_bounds__(kCorrThreads)
     k_corr_lines(const CorrTask* __restrict__ tasks, CorrTask one, uint32_t n_tasks, uint32_t n_items) {
-    extern __shared__ float2 tile[]; /* [n + R][kCorrPitch] */
+    extern __shared__ float2 tile[]; /* [n + R + kCorrLags][pitch] */
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (uint32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
         /* the task: the last one whose first item is at or before `item` */
@@ -124,11 +124,13 @@ __global__ void __launch_bounds__(kCorrThreads)
         }
         __syncthreads();
         double* out = T.partial + (size_t)local * sh.rp;
+        /* The window reads rows up to ext + 7 (k <= n - 1, r0 <= R): the tile has kCorrLags
+         * rows past ext, left unset; they meet only lags beyond R, which are dropped. */
         for (uint32_t r0 = 1 + warp * kCorrLags; r0 <= rmax; r0 += nwarps * kCorrLags) {
             /* w[j]: partner of lag r0 + j at the current k */
             float2 w[kCorrLags];
 #pragma unroll
-            for (uint32_t j = 0; j < kCorrLags; ++j) w[j] = tile[min(r0 + j, ext - 1) * pitch + lane];
+            for (uint32_t j = 0; j < kCorrLags; ++j) w[j] = tile[(r0 + j) * pitch + lane];
             double tot[kCorrLags];
             float part[kCorrLags];
 #pragma unroll
@@ -149,7 +151,7 @@ __global__ void __launch_bounds__(kCorrThreads)
                         const float2 wj = w[(kk + j) % kCorrLags];
                         part[j] = __fmaf_rn(a.y, wj.y, __fmaf_rn(a.x, wj.x, part[j]));
                     }
-                    w[kk] = tile[min(k0 + kk + r0 + kCorrLags, ext - 1) * pitch + lane];
+                    w[kk] = tile[(k0 + kk + r0 + kCorrLags) * pitch + lane];
                 }
                 if ((k0 + kCorrLags) % kCorrRun == 0) {
 #pragma unroll
@@ -168,7 +170,7 @@ __global__ void __launch_bounds__(kCorrThreads)
                     part[j] = __fmaf_rn(a.y, w[j].y, __fmaf_rn(a.x, w[j].x, part[j]));
 #pragma unroll
                 for (uint32_t j = 0; j + 1 < kCorrLags; ++j) w[j] = w[j + 1];
-                w[kCorrLags - 1] = tile[min(k + kCorrLags + r0, ext - 1) * pitch + lane];
+                w[kCorrLags - 1] = tile[(k + kCorrLags + r0) * pitch + lane];
             }
 #pragma unroll
             for (uint32_t j = 0; j < kCorrLags; ++j) {
@@ -295,7 +297,7 @@ cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t
     if (n_tasks == 0 || (!tasks_dev && (!one || n_tasks != 1))) return cudaErrorInvalidValue;
     const CorrTask by_value = one ? *one : CorrTask{};
     if (n_items > 0) {
-        const size_t smem = (size_t)max_ext * kCorrPitch * sizeof(float2);
+        const size_t smem = (size_t)(max_ext + kCorrLags) * kCorrPitch * sizeof(float2);
         cudaError_t e = cudaSuccess;
         if (smem > 48 * 1024)
             e = cudaFuncSetAttribute(k_corr_lines, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
