@@ -814,7 +814,9 @@ int slsf_task_corr_fuse(slsf_task* t, uint32_t interval) {
     if (int rc = check_free(t)) return rc;
     if (interval && !t->corr_block)
         return set_error(SLSF_ERR_STATE, "task has no correlation bins; call slsf_task_corr_setup first");
-    if (interval && !slsf::resident_supports(t->lx, t->ly, t->lz, t->ctx->device))
+    /* the context's kernel choice for this shape (default or tuned) must be the one-CTA kernel */
+    slsf_kernel_choice kc = {};
+    if (interval && (slsf_tune_get(t->ctx, t->lx, t->ly, t->lz, &kc) != SLSF_OK || kc.kind != SLSF_KERNEL_RESIDENT))
         return set_error(SLSF_ERR_INVALID, kErrFuse);
     t->corr_interval = interval;
     return SLSF_OK;

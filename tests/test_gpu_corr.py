@@ -243,5 +243,15 @@ def test_fused_in_sessions_and_refusals(slsf, ctx, orc):
     with pytest.raises(slsf.SlsfError) as e:
         big.corr_fuse(1)
     assert "one-CTA kernel" in str(e.value)
+    # a shape that fits the one-CTA kernel but is tuned to the cluster kernel
+    small = task(slsf, ctx, orc, (12, 12, 12), 72)
+    small.corr_setup(6, 6, 1, 1)
+    ctx.tune_set((12, 12, 12), "cluster", 1, 512)
+    with pytest.raises(slsf.SlsfError) as e:
+        small.corr_fuse(1)
+    assert "one-CTA kernel" in str(e.value)
+    ctx.tune_set((12, 12, 12), "resident", 1, 128)
+    small.corr_fuse(1)
     t.close()
     big.close()
+    small.close()
