@@ -240,3 +240,52 @@ def test_server_admits_while_submissions_continue(slsf, ctx, orc):
     [alone] = one.poll()
     one.close()
     assert alone["est"]["Energy"] == res[reqs[4][0]]["est"]["Energy"]
+
+
+def test_served_stream_passes_two_sigma(slsf, ctx, orc):
+    """Served results are statistically those of the reference algorithm.  A
+    mixed stream of 24 requests (L = 8, 12, 16; T ~ U[1.0, 1.6]; J_z drawn per
+    request) is served in one pass; each request runs again on the oracle's
+    reference-order CPU path (FastRng streams, independent of the device's
+    Philox streams) with the same couplings.  Per request and observable,
+    z = (device - oracle) / sqrt(err_device^2 + err_oracle^2) over 20-sweep
+    bins.  A request passes 2 sigma when its Energy and MagnetizationSquared
+    both do; the latencies of passing requests are reported."""
+    rng = np.random.default_rng(20260710)
+    therm, measured, binsize = 100, 800, 20
+    srv = slsf.Server(ctx, epoch_sweeps=50)
+    reqs = []
+    for tag in range(1, 25):
+        L, T, seed = int(rng.choice([8, 12, 16])), float(rng.uniform(1.0, 1.6)), 7000 + tag
+        jxy, jz = couplings(orc, L, seed)
+        reqs.append((tag, L, T, jxy, jz))
+        srv.submit(tag, (L, L, L), T, seed, jxy, jz, therm + measured, thermalization=therm, binsize=binsize)
+    drain(srv)
+    res = {r["tag"]: r for r in srv.poll()}
+    srv.close()
+    assert sorted(res) == [r[0] for r in reqs]
+    zs, passing = [], []
+    n_bins = measured // binsize
+    for tag, L, T, jxy, jz in reqs:
+        got = res[tag]
+        assert got["status"] == slsf.OK, got["message"]
+        assert got["est"]["measurements"] == measured and got["est"]["n_bins"] == n_bins
+        m = orc.Model(L, L, L, jxy, jz, T, wolff_steps=1, seed=90000 + tag)
+        m.init()
+        series, _ = m.run_series(therm, measured)
+        bins = series.reshape(n_bins, binsize, slsf.BIN_COLS).mean(axis=1)
+        c_mean, c_err = bins.mean(axis=0), bins.std(axis=0, ddof=1) / np.sqrt(n_bins)
+        z = {}
+        for k, name in enumerate(slsf.BIN_NAMES):
+            g_mean, g_err = got["est"][name]
+            z[name] = (g_mean - c_mean[k]) / np.hypot(g_err, c_err[k])
+        zs.extend(z.values())
+        if abs(z["Energy"]) < 2 and abs(z["MagnetizationSquared"]) < 2:
+            passing.append(got["finish_s"] - got["submit_s"])
+    zs = np.array(zs)
+    print(f"served 2-sigma: {len(passing)} of {len(reqs)} pass; mean z^2 {np.mean(zs ** 2):.2f}; "
+          f"max |z| {np.abs(zs).max():.2f}; latency of passing requests p50 {np.percentile(passing, 50):.3f} s, "
+          f"p99 {np.percentile(passing, 99):.3f} s")
+    # |z| < 2 holds for about 91% of requests when both observables are unbiased
+    assert len(passing) >= 0.7 * len(reqs)
+    assert np.mean(zs ** 2) < 2.0 and np.abs(zs).max() < 5.0
