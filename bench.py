@@ -198,6 +198,23 @@ def cpu_baseline(L, temps, sweeps_hint, seconds, threads=None):
             "seconds": sec}
 
 
+def cpu_plain(L=64, T=1.3, sweeps_hint=1000, seconds=8.0):
+    """c1 on the CPU: the oracle's reference-order path driving one L^3 task on
+    one thread (the reference runs one task per process), on a bounded sample
+    of the 1000-sweep run sized to about `seconds`."""
+    import oracle
+
+    jxy = np.full(L, 1.2)
+    jz = oracle.uniform_disorder(L, 0.5, 1.5, BASE_SEED)
+    t1, _ = oracle.bench_tasks((L, L, L), jxy, jz, [T], math.pi, 1, [BASE_SEED], 2, 1)
+    sweeps = max(2, min(sweeps_hint, int(seconds / max(t1 / 2, 1e-9))))
+    sec, _ = oracle.bench_tasks((L, L, L), jxy, jz, [T], math.pi, 1, [BASE_SEED], sweeps, 1)
+    return {"value": sweeps * L ** 3 / sec, "unit": "site-updates/s", "cores": 1, "kind": "port",
+            "sample": f"c1 single replica L={L}, T={T}, {sweeps} of its {sweeps_hint} sweeps (Metropolis + 1 Wolff + "
+                      "measure each), 1 thread, FP64 C++ restatement of SLSF-rs (not the Rust binary)",
+            "seconds": sec}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -579,6 +596,10 @@ def main():
             extra["cpu_baseline"] = cpu_baseline(L, list(np.linspace(1.1, 1.5, args.temperatures)), 2000,
                                                  args.cpu_seconds)
             extra["cpu_baseline"]["gpu_over_cpu"] = value / extra["cpu_baseline"]["value"]
+            c1 = cpu_plain()
+            if "plain" in extra:
+                c1["plain_gpu_over_cpu"] = extra["plain"]["value"] / c1["value"]
+            extra["cpu_baseline"]["c1"] = c1
 
     if rank == 0:
         line = {
