@@ -262,6 +262,7 @@ int bind_device(const slsf_ctx* ctx) {
 /* Grows the batched-engine scratch to hold n views. */
 int ensure_batch_capacity(slsf_ctx* ctx, size_t n) {
     if (ctx->views_cap >= n) return SLSF_OK;
+    if (ctx->d_views) SLSF_CUDA(cudaStreamSynchronize(ctx->stream)); /* queued launches may still read them */
     if (ctx->d_views) cudaFree(ctx->d_views);
     if (ctx->h_views) cudaFreeHost(ctx->h_views);
     if (ctx->d_rcorr) cudaFree(ctx->d_rcorr);
