@@ -164,6 +164,40 @@ def test_command_line_writes_result(slsf, jobs, tmp_path):
     assert task["task"]["name"] == "L2x2x2_T2.000000_dJxy0.000000_dJz0.000000_sample1"
 
 
+# TINY_CONFIG of theta_model_runs_through_carlo_runner (src/model.rs:484-498)
+TINY = """
+name = "tiny"
+[model]
+l = [2]
+temperatures = [2.0]
+samples = 1
+j_xy = 1.0
+j_z_mean = 0.1
+delta_j_xy = [0.0]
+delta_j_z = [0.0]
+[run]
+sweeps = 4
+thermalization = 2
+binsize = 2
+wolff_steps = 1
+"""
+
+
+def test_theta_model_runs_through_runner(slsf, ctx, jobs):
+    # theta_model_runs_through_carlo_runner (src/model.rs:500-515): one task,
+    # not stopped early, completed, with Energy and MagnetizationSquared.
+    cfg = jobs.config_from_toml(TINY)
+    tasks = jobs.make_tasks(cfg)
+    assert len(tasks) == 1
+    res, summary = jobs.run_job_checkpointed(ctx, cfg, tasks=tasks)
+    assert not summary["stopped_early"]
+    assert len(res["tasks"]) == 1
+    [rec] = res["tasks"]
+    assert rec["measurements"] == 4  # completed: every post-thermalization sweep measured
+    assert "Energy" in rec["observables"] and "MagnetizationSquared" in rec["observables"]
+    assert all(np.isfinite(v["mean"]) for v in rec["observables"].values())
+
+
 class StopAt:
     """A checkpoint schedule that asks for a stop at its n-th check."""
 

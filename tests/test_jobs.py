@@ -268,3 +268,15 @@ def test_reference_example_job_files_parse_and_expand(jobs):
         assert all(re.fullmatch(r"L\d+x\d+x\d+_T\d+\.\d{6}_dJxy\d+\.\d{6}_dJz\d+\.\d{6}_sample\d+", t["name"])
                    for t in tasks), name
         assert cfg.run_time_s > 0 and cfg.checkpoint_time_s > 0
+
+
+def test_tiny_config_builds_one_task(jobs):
+    # the parse half of theta_model_runs_through_carlo_runner (src/model.rs:500-504);
+    # the run half is in test_gpu_jobs.py
+    from test_gpu_jobs import TINY
+
+    [t] = jobs.make_tasks(jobs.config_from_toml(TINY))
+    assert t["name"] == "L2x2x2_T2.000000_dJxy0.000000_dJz0.000000_sample1"
+    assert (t["l_x"], t["l_y"], t["l_z"], t["temperature"]) == (2, 2, 2, 2.0)
+    assert t["j_xy_array"] == [1.0, 1.0] and t["j_z_array"] == [0.1, 0.1]
+    assert (t["sweeps"], t["thermalization"], t["binsize"], t["wolff_steps"]) == (4, 2, 2, 1)
