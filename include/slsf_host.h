@@ -99,6 +99,8 @@ typedef struct slsf_server_config {
     uint32_t epoch_sweeps; /* sweeps per launch: the admission granularity (default 100) */
     uint32_t max_active;   /* tasks on the device at once (0: only the budget limits) */
     uint64_t budget_bytes; /* device bytes for task state (0: the context's budget) */
+    uint32_t keep_bins;    /* nonzero: keep each completed request's bin means for
+                              slsf_server_take_bins */
 } slsf_server_config;
 
 /* One request: a task, its sweep count and measurement plan. */
@@ -162,6 +164,14 @@ int slsf_server_wait_idle(slsf_server* s, double timeout_s);
 /* Moves up to `max` finished results to `out` (thread-safe). */
 int slsf_server_poll(slsf_server* s, slsf_result* out, size_t max, size_t* n);
 int slsf_server_stats_get(slsf_server* s, slsf_server_stats* out);
+/* The complete bins of a finished request, kept when the server was created
+ * with keep_bins (the measurement_bins of ThetaTaskResult,
+ * src/model.rs:81, that src/results.rs:55-105 writes to .meas.h5): bin means
+ * [n_rows][SLSF_BIN_COLS], one row per `binsize` measured sweeps.  *n_rows
+ * receives the row count; with out != NULL and max_rows >= *n_rows the rows
+ * are copied and released.  SLSF_ERR_INVALID when nothing is kept for the
+ * tag (not finished, failed, cancelled, already taken, or keep_bins off). */
+int slsf_server_take_bins(slsf_server* s, uint64_t tag, double* out, size_t max_rows, size_t* n_rows);
 /* Checkpoint of the serving loop (carlo-mc's checkpoint directory and
  * restart, src/results.rs:211-239): with the worker stopped, writes one file
  * per unfinished request to `dir` -- queued ones as submitted, running ones

@@ -566,7 +566,8 @@ class ThetaTaskDesc(C.Structure):
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("epoch_sweeps", C.c_uint32), ("max_active", C.c_uint32), ("budget_bytes", C.c_uint64)]
+    _fields_ = [("epoch_sweeps", C.c_uint32), ("max_active", C.c_uint32), ("budget_bytes", C.c_uint64),
+                ("keep_bins", C.c_uint32)]
 
 
 class Request(C.Structure):
@@ -615,6 +616,7 @@ HOST_SIGNATURES = {
     "slsf_server_wait_idle": (C.c_int, [_P, C.c_double]),
     "slsf_server_poll": (C.c_int, [_P, C.POINTER(Result), C.c_size_t, C.POINTER(C.c_size_t)]),
     "slsf_server_stats_get": (C.c_int, [_P, C.POINTER(ServerStats)]),
+    "slsf_server_take_bins": (C.c_int, [_P, C.c_uint64, _F64P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "slsf_server_checkpoint": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_size_t)]),
     "slsf_server_restore": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_size_t)]),
 }
@@ -700,9 +702,10 @@ def model_run(ctx, desc, batched=True):
 class Server:
     """Continuous-batching server (slsf_server_*)."""
 
-    def __init__(self, ctx, epoch_sweeps=100, max_active=0, budget_bytes=0):
+    def __init__(self, ctx, epoch_sweeps=100, max_active=0, budget_bytes=0, keep_bins=False):
         h = _P()
-        cfg = ServerConfig(epoch_sweeps=epoch_sweeps, max_active=max_active, budget_bytes=budget_bytes)
+        cfg = ServerConfig(epoch_sweeps=epoch_sweeps, max_active=max_active, budget_bytes=budget_bytes,
+                           keep_bins=int(bool(keep_bins)))
         host_check(load_host().slsf_server_create(ctx.h, C.byref(cfg), C.byref(h)))
         self.h = h
         self.ctx = ctx
@@ -752,6 +755,14 @@ class Server:
         n = C.c_size_t()
         host_check(load_host().slsf_server_poll(self.h, buf, max_results, C.byref(n)))
         return [buf[i].as_dict() for i in range(n.value)]
+
+    def take_bins(self, tag):
+        """Bin means [n_rows, BIN_COLS] of a finished request (server created with keep_bins)."""
+        n = C.c_size_t()
+        host_check(load_host().slsf_server_take_bins(self.h, tag, None, 0, C.byref(n)))
+        out = np.empty((n.value, BIN_COLS), dtype=np.float64)
+        host_check(load_host().slsf_server_take_bins(self.h, tag, _ptr(out, C.c_double), n.value, C.byref(n)))
+        return out
 
     def checkpoint(self, directory):
         """Writes every unfinished request to `directory` (worker stopped); returns the count."""

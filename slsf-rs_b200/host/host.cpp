@@ -21,6 +21,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <unordered_set>
 #include <vector>
 
@@ -290,6 +291,7 @@ struct Active {
 struct slsf_server {
     slsf_ctx* ctx = nullptr;
     slsf_server_config cfg = {};
+    std::unordered_map<uint64_t, std::vector<double>> kept_bins; /* guarded by mu */
     std::chrono::steady_clock::time_point t0;
     std::mutex mu;                /* guards queue, results, cancel set, stats */
     std::condition_variable cv;   /* new work or stop */
@@ -524,6 +526,7 @@ int retire(slsf_server* s) {
         }
     }
     std::vector<slsf_result> out;
+    std::vector<std::pair<uint64_t, std::vector<double>>> kept;
     size_t k = 0;
     const double t = now_s(s->t0);
     for (size_t i : done) {
@@ -540,6 +543,10 @@ int retire(slsf_server* s) {
             const double vol = (double)a.p.req.lx * a.p.req.ly * a.p.req.lz;
             const uint32_t full = (uint32_t)std::min<uint64_t>(a.n_bins, meas[k] / a.binsize);
             if (full > 0) slsf_estimates_from_bins(per[k].data(), full, vol, 1.0 / a.p.req.temperature, &r.est);
+            if (s->cfg.keep_bins && full > 0) {
+                per[k].resize((size_t)full * SLSF_BIN_COLS);
+                kept.emplace_back(r.tag, std::move(per[k]));
+            }
             r.est.measurements = meas[k];
             r.est.acceptance = (double)a.accepted / (vol * (double)std::max<uint64_t>(1, r.sweeps));
             ++k;
@@ -550,6 +557,7 @@ int retire(slsf_server* s) {
     }
     std::lock_guard<std::mutex> lock(s->mu);
     for (auto it = done.rbegin(); it != done.rend(); ++it) s->active.erase(s->active.begin() + *it);
+    for (auto& kb : kept) s->kept_bins[kb.first] = std::move(kb.second);
     for (auto& r : out) {
         if (r.status == SLSF_OK)
             s->stats.completed++;
@@ -739,6 +747,20 @@ int slsf_server_wait_idle(slsf_server* s, double timeout_s) {
     });
     if (!s->worker_error.empty()) return fail(SLSF_ERR_CUDA, "server worker stopped: " + s->worker_error);
     return ok ? SLSF_OK : fail(SLSF_ERR_TIMEOUT, "server still has queued or running requests");
+}
+
+int slsf_server_take_bins(slsf_server* s, uint64_t tag, double* out, size_t max_rows, size_t* n_rows) {
+    if (!s || !n_rows) return fail(SLSF_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->kept_bins.find(tag);
+    if (it == s->kept_bins.end()) return fail(SLSF_ERR_INVALID, "no bins kept for this tag");
+    const size_t rows = it->second.size() / SLSF_BIN_COLS;
+    *n_rows = rows;
+    if (out && max_rows >= rows) {
+        std::copy(it->second.begin(), it->second.end(), out);
+        s->kept_bins.erase(it);
+    }
+    return SLSF_OK;
 }
 
 int slsf_server_poll(slsf_server* s, slsf_result* out, size_t max, size_t* n) {

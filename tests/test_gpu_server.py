@@ -289,3 +289,37 @@ def test_served_stream_passes_two_sigma(slsf, ctx, orc):
     # |z| < 2 holds for about 91% of requests when both observables are unbiased
     assert len(passing) >= 0.7 * len(reqs)
     assert np.mean(zs ** 2) < 2.0 and np.abs(zs).max() < 5.0
+
+
+def test_server_keeps_bins_for_take_bins(slsf, ctx, orc):
+    # keep_bins: each completed request's bin means stay until taken once; they
+    # are the bins its estimates came from
+    import ctypes
+
+    srv = slsf.Server(ctx, epoch_sweeps=5, keep_bins=True)
+    reqs = [(1, (8, 8, 8), 1.0, 11, 40, 5, 5), (2, (16, 16, 16), 1.3, 12, 55, 10, 9), (3, (6, 6, 4), 1.1, 14, 25, 5, 2)]
+    for r in reqs:
+        submit(srv, orc, r)
+    drain(srv)
+    res = {r["tag"]: r for r in srv.poll()}
+    for tag, dims, T, _, _, _, n_bins in reqs:
+        bins = srv.take_bins(tag)
+        assert bins.shape == (n_bins, slsf.BIN_COLS)
+        e = slsf.Estimates()
+        b = np.ascontiguousarray(bins)
+        slsf.host_check(slsf.load_host().slsf_estimates_from_bins(
+            b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(b), float(np.prod(dims)), 1.0 / T,
+            ctypes.byref(e)))
+        for name in slsf.BIN_NAMES + slsf.DERIVED:
+            assert e.as_dict()[name] == res[tag]["est"][name], (tag, name)
+        with pytest.raises(slsf.SlsfError) as err:
+            srv.take_bins(tag)  # released by the first take
+        assert "no bins kept" in str(err.value)
+    srv.close()
+    plain = slsf.Server(ctx, epoch_sweeps=5)
+    submit(plain, orc, reqs[0])
+    drain(plain)
+    plain.poll()
+    with pytest.raises(slsf.SlsfError):
+        plain.take_bins(1)
+    plain.close()
