@@ -404,14 +404,18 @@ def _run_served(pkg, ctx, tasks, epoch_sweeps, ck: Optional[Checkpoints] = None)
     kept in served/finished.json and its unfinished requests written by
     slsf_server_checkpoint to served/; a restart restores both."""
     names = {k: t["name"] for k, t in tasks}
-    srv = pkg.Server(ctx, epoch_sweeps=epoch_sweeps)
+    binsizes = {k: t["binsize"] for k, t in tasks}
+    srv = pkg.Server(ctx, epoch_sweeps=epoch_sweeps, keep_bins=True)
     out = {}
 
     def collect():
         for r in srv.poll(len(tasks) + 16):
             if r["status"] != pkg.OK:
                 raise pkg.SlsfError(r["status"], f"task {names[r['tag']]}: {r['message']}")
-            out[r["tag"]] = r["est"]
+            est = r["est"]
+            rows = srv.take_bins(r["tag"]).tolist() if est["n_bins"] else []  # no complete bin: nothing kept
+            est["_bins"] = {"binsize": binsizes[r["tag"]], "rows": rows}
+            out[r["tag"]] = est
 
     try:
         sdir = ck.path("served") if ck else None
@@ -609,14 +613,17 @@ def _run_correlated(pkg, ctx, group, ck: Optional[Checkpoints] = None, gdir: Opt
             est = e.as_dict()
             est["measurements"] = meas
             est["acceptance"] = float(accepted[i]) / (volume * (therm + sweeps))
+            est["_bins"] = {"binsize": t["binsize"], "rows": b.tolist()}
             corr = {}
             if o.corr_n_values:
                 means, count = o.corr_bins()
                 assert count == n_corr
-                for j, name in enumerate(corr_names(t["l_z"], *radii[i])):
+                names = corr_names(t["l_z"], *radii[i])
+                for j, name in enumerate(names):
                     # bins of one mean each: the mean of the bin means and their standard error
                     r = pkg.binned_estimate(means[:, j], 1)
                     corr[name] = (r["mean"], r["stderr"])
+                est["_corr_bins"] = {"binsize": min(t["binsize"], n_corr), "names": names, "rows": means.tolist()}
             out.append((est, corr))
         if ck:
             tmp = gdir + ".new"
@@ -630,6 +637,27 @@ def _run_correlated(pkg, ctx, group, ck: Optional[Checkpoints] = None, gdir: Opt
             session.close()
         for o in objs:
             o.close()
+
+
+def measurement_bins(est: dict) -> dict:
+    """A task's measurement_bins (ThetaTaskResult, src/model.rs:81) from its
+    estimates: {observable: (internal bin length, bin means)} for the twelve
+    per-sweep observables and, when measured, every correlation observable.
+    The reference's two per-sweep timing series (_ll_sweep_time,
+    _ll_measure_time, src/model.rs:438-439) have no counterpart in batched
+    sweeps and are left out."""
+    out = {}
+    b = est.get("_bins")
+    if b and b["rows"]:
+        rows = np.asarray(b["rows"], dtype=np.float64)
+        for j, name in enumerate(_package().BIN_NAMES):
+            out[name] = (b["binsize"], rows[:, j])
+    c = est.get("_corr_bins")
+    if c and c["rows"]:
+        rows = np.asarray(c["rows"], dtype=np.float64)
+        for j, name in enumerate(c["names"]):
+            out[name] = (c["binsize"], rows[:, j])
+    return out
 
 
 def run_job_checkpointed(ctx, cfg: JobConfig, rank: int = 0, world_size: int = 1, epoch_sweeps: int = 100,
@@ -665,11 +693,12 @@ def run_job_checkpointed(ctx, cfg: JobConfig, rank: int = 0, world_size: int = 1
         stopped = True
         if s.args:
             est.update(s.args[0])
-    out = []
+    out, bins = [], {}
     for k, t in mine:
         if k not in est:
             continue
         e = est[k]
+        bins[k] = measurement_bins(e)
         rec = {"task": t}
         if k:
             rec["task_index"] = k  # omitted when zero, as the reference's serializer does
@@ -678,7 +707,7 @@ def run_job_checkpointed(ctx, cfg: JobConfig, rank: int = 0, world_size: int = 1
         out.append(rec)
     result = {"job_name": cfg.job_name, "rank": rank, "world_size": world_size, "tasks": out}
     summary = {"task_count": len(out), "elapsed_seconds": time.monotonic() - started, "stopped_early": stopped,
-               "checkpoint_dir": ck.dir if ck else None}
+               "checkpoint_dir": ck.dir if ck else None, "measurement_bins": bins}
     return result, summary
 
 
@@ -720,6 +749,12 @@ def result_path(cfg: JobConfig, rank: int, output_dir: Optional[str] = None) -> 
     if not d:
         d = os.path.dirname(cfg.job_name) or "results"
     return os.path.join(d, f"{os.path.basename(cfg.job_name) or cfg.job_name}.rank{rank}.results.json")
+
+
+def measurement_dir(cfg: JobConfig, output_dir: Optional[str] = None) -> str:
+    """`<dir>/<file name of job_name>.data` (default_measurement_dir_with_options,
+    src/model.rs:970-980), the directory of the per-task .meas.h5 files."""
+    return result_path(cfg, 0, output_dir).replace(".rank0.results.json", ".data")
 
 
 def merged_path(cfg: JobConfig, output_dir: Optional[str] = None) -> str:
@@ -771,6 +806,7 @@ def main(argv=None):
     p.add_argument("--checkpoint-dir", help="checkpoint here (default with `checkpoint = true`: "
                                              "<output>/<job>.data/checkpoints)")
     p.add_argument("--restart", action="store_true", help="resume from the checkpoint directory")
+    p.add_argument("--measurement-dir", help="per-task .meas.h5 files here (default <output>/<job>.data)")
     args = p.parse_args(argv)
     cfg = load_job(args.job)
     if args.command == "status":
@@ -792,6 +828,10 @@ def main(argv=None):
         ck = Checkpoints(os.path.join(cdir, f"rank{args.rank}"), args.restart, cfg.run_time_s, cfg.checkpoint_time_s)
     with pkg.Context(args.device) as ctx:
         res, summary = run_job_checkpointed(ctx, cfg, args.rank, args.world_size, args.epoch_sweeps, ck=ck)
+    # finish_theta_job_run (src/results.rs:130-150): measurement files, then the result record
+    meas_h5 = importlib.import_module(_package().__name__ + ".meas_h5")
+    meas_h5.write_job_measurements(res["tasks"], summary["measurement_bins"],
+                                   args.measurement_dir or measurement_dir(cfg, args.output_dir))
     path = write_result(res, result_path(cfg, args.rank, args.output_dir))
     note = "; stopped early: restart with --restart" if summary["stopped_early"] else ""
     print(f"{len(res['tasks'])} tasks -> {path} ({summary['elapsed_seconds']:.1f} s){note}")

@@ -162,6 +162,42 @@ def test_command_line_writes_result(slsf, jobs, tmp_path):
     for name in ("Energy", "RhoXY", "RhoZ", "Magnetization", "CorrX_r1", "CorrZ_r1", "CorrXY_z1_r1"):
         assert np.isfinite(task["observables"][name]["mean"]), name
     assert task["task"]["name"] == "L2x2x2_T2.000000_dJxy0.000000_dJz0.000000_sample1"
+    # the measurement file beside it (src/tests.rs:606): bins of every measured observable
+    h5 = tmp_path / "out" / "carlo_unit.data" / "task0001" / "run0001.meas.h5"
+    assert h5.exists()
+    check_meas_h5(slsf, h5, task, n_plain_bins=2, corr_bin_len=2, n_corr_bins=2)
+
+
+def check_meas_h5(slsf, path, rec, n_plain_bins, corr_bin_len=None, n_corr_bins=None):
+    """The .meas.h5 of one task read back with the specification reader: each
+    measured observable's bins, whose mean is the record's estimate."""
+    import h5read
+
+    r = h5read.read(str(path))
+    names = sorted(k.split("/")[2] for k in r if k.count("/") == 2 and k.startswith("/observables/"))
+    corr = sorted(n for n in rec["observables"] if n.startswith("Corr"))
+    assert names == sorted(list(slsf.BIN_NAMES) + corr)
+    for name in names:
+        bl = int(r[f"/observables/{name}/bin_length"].value)
+        s = r[f"/observables/{name}/samples"].value
+        if name.startswith("Corr"):
+            assert (bl, len(s)) == (corr_bin_len, n_corr_bins), name
+        else:
+            assert (bl, len(s)) == (rec["task"]["binsize"], n_plain_bins), name
+        assert s.mean() == pytest.approx(rec["observables"][name]["mean"], rel=1e-12, abs=1e-15), name
+    assert r["/version/mc_package"].value == "SLSF.XYCarlo"
+
+
+def test_served_job_writes_measurement_files(slsf, jobs, tmp_path):
+    job = tmp_path / "served_unit.toml"
+    job.write_text(SERVED)
+    assert jobs.main([str(job), "--output-dir", str(tmp_path / "out")]) == 0
+    out = json.loads((tmp_path / "out" / "served_unit.rank0.results.json").read_text())
+    assert len(out["tasks"]) == 8
+    for rec in out["tasks"]:
+        k = rec.get("task_index", 0)
+        check_meas_h5(slsf, tmp_path / "out" / "served_unit.data" / f"task{k + 1:04d}" / "run0001.meas.h5", rec,
+                      n_plain_bins=16 // 4)
 
 
 # TINY_CONFIG of theta_model_runs_through_carlo_runner (src/model.rs:484-498)
