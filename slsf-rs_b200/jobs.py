@@ -40,6 +40,7 @@ import math
 import os
 import re
 import sys
+from collections.abc import Mapping
 from typing import Optional
 
 import numpy as np
@@ -390,8 +391,16 @@ def _swap_dir(new, old):
     os.replace(new, old)
 
 
+def _jsonable(v):
+    if isinstance(v, np.ndarray):
+        return v.tolist()
+    if isinstance(v, dict):
+        return {k: _jsonable(x) for k, x in v.items()}
+    return v
+
+
 def _est_to_json(est):
-    return {k: (list(v) if isinstance(v, tuple) else v) for k, v in est.items()}
+    return {k: (list(v) if isinstance(v, tuple) else _jsonable(v)) for k, v in est.items()}
 
 
 def _est_from_json(d):
@@ -413,7 +422,7 @@ def _run_served(pkg, ctx, tasks, epoch_sweeps, ck: Optional[Checkpoints] = None)
             if r["status"] != pkg.OK:
                 raise pkg.SlsfError(r["status"], f"task {names[r['tag']]}: {r['message']}")
             est = r["est"]
-            rows = srv.take_bins(r["tag"]).tolist() if est["n_bins"] else []  # no complete bin: nothing kept
+            rows = srv.take_bins(r["tag"]) if est["n_bins"] else np.zeros((0, pkg.BIN_COLS))  # none kept
             est["_bins"] = {"binsize": binsizes[r["tag"]], "rows": rows}
             out[r["tag"]] = est
 
@@ -613,7 +622,7 @@ def _run_correlated(pkg, ctx, group, ck: Optional[Checkpoints] = None, gdir: Opt
             est = e.as_dict()
             est["measurements"] = meas
             est["acceptance"] = float(accepted[i]) / (volume * (therm + sweeps))
-            est["_bins"] = {"binsize": t["binsize"], "rows": b.tolist()}
+            est["_bins"] = {"binsize": t["binsize"], "rows": b}
             corr = {}
             if o.corr_n_values:
                 means, count = o.corr_bins()
@@ -623,7 +632,7 @@ def _run_correlated(pkg, ctx, group, ck: Optional[Checkpoints] = None, gdir: Opt
                     # bins of one mean each: the mean of the bin means and their standard error
                     r = pkg.binned_estimate(means[:, j], 1)
                     corr[name] = (r["mean"], r["stderr"])
-                est["_corr_bins"] = {"binsize": min(t["binsize"], n_corr), "names": names, "rows": means.tolist()}
+                est["_corr_bins"] = {"binsize": min(t["binsize"], n_corr), "names": names, "rows": means}
             out.append((est, corr))
         if ck:
             tmp = gdir + ".new"
@@ -648,16 +657,30 @@ def measurement_bins(est: dict) -> dict:
     sweeps and are left out."""
     out = {}
     b = est.get("_bins")
-    if b and b["rows"]:
-        rows = np.asarray(b["rows"], dtype=np.float64)
-        for j, name in enumerate(_package().BIN_NAMES):
-            out[name] = (b["binsize"], rows[:, j])
+    if b is not None and len(b["rows"]):
+        cols = np.asarray(b["rows"], dtype=np.float64).T
+        out.update(zip(_package().BIN_NAMES, ((b["binsize"], col) for col in cols)))
     c = est.get("_corr_bins")
-    if c and c["rows"]:
-        rows = np.asarray(c["rows"], dtype=np.float64)
-        for j, name in enumerate(c["names"]):
-            out[name] = (c["binsize"], rows[:, j])
+    if c is not None and len(c["rows"]):
+        cols = np.asarray(c["rows"], dtype=np.float64).T
+        out.update(zip(c["names"], ((c["binsize"], col) for col in cols)))
     return out
+
+
+class _TaskBins(Mapping):
+    """{task index: measurement_bins} over a run's estimates, built when read."""
+
+    def __init__(self, estimates):
+        self._est = estimates
+
+    def __getitem__(self, k):
+        return measurement_bins(self._est[k])
+
+    def __iter__(self):
+        return iter(self._est)
+
+    def __len__(self):
+        return len(self._est)
 
 
 def run_job_checkpointed(ctx, cfg: JobConfig, rank: int = 0, world_size: int = 1, epoch_sweeps: int = 100,
@@ -693,12 +716,11 @@ def run_job_checkpointed(ctx, cfg: JobConfig, rank: int = 0, world_size: int = 1
         stopped = True
         if s.args:
             est.update(s.args[0])
-    out, bins = [], {}
+    out = []
     for k, t in mine:
         if k not in est:
             continue
         e = est[k]
-        bins[k] = measurement_bins(e)
         rec = {"task": t}
         if k:
             rec["task_index"] = k  # omitted when zero, as the reference's serializer does
@@ -707,7 +729,8 @@ def run_job_checkpointed(ctx, cfg: JobConfig, rank: int = 0, world_size: int = 1
         out.append(rec)
     result = {"job_name": cfg.job_name, "rank": rank, "world_size": world_size, "tasks": out}
     summary = {"task_count": len(out), "elapsed_seconds": time.monotonic() - started, "stopped_early": stopped,
-               "checkpoint_dir": ck.dir if ck else None, "measurement_bins": bins}
+               "checkpoint_dir": ck.dir if ck else None,
+               "measurement_bins": _TaskBins({k: est[k] for k, _ in mine if k in est})}
     return result, summary
 
 

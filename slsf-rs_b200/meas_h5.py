@@ -245,11 +245,12 @@ def write_job_measurements(records, bins_by_index: dict, output_dir) -> list:
     paths = []
     for rec in records:
         k = rec.get("task_index", 0)
-        if not bins_by_index.get(k):
+        bins = bins_by_index.get(k)
+        if not bins:
             raise MeasH5Error("theta task result does not contain measurement bins")
-        for name in bins_by_index[k]:
+        for name in bins:
             if name not in rec.get("observables", {}):
                 raise MeasH5Error(f"missing observable estimate for {name}")
         path = os.path.join(os.fspath(output_dir), f"task{k + 1:04d}", "run0001.meas.h5")
-        paths.append(write_meas_h5(path, bins_by_index[k]))
+        paths.append(write_meas_h5(path, bins))
     return paths
