@@ -248,11 +248,21 @@ __global__ void __launch_bounds__(kThreads)
     __syncthreads();
     bool ok = true;
     for (uint32_t l = threadIdx.x; l < kTileSites; l += blockDim.x) {
-        const uint32_t bits = lbits[l];
-        if (!bits) continue;
+        /* a warp holds one row (lane = x); a y or z bond whose left neighbour's
+         * bond joins the same two x-runs adds nothing, so only the first bond of
+         * each such stretch unions */
+        const uint32_t lane = l % kTileX, bits = lbits[l];
         const uint32_t ay = (l / kTileX) % kTileY, az = l / (kTileX * kTileY);
-        if ((bits & 2u) && ay + 1 < ey) ok &= tile_union(lpar, l, l + kTileX, bu);
-        if ((bits & 4u) && az + 1 < ez) ok &= tile_union(lpar, l, l + kTileX * kTileY, bu);
+        const bool yin = ay + 1 < ey, zin = az + 1 < ez; /* warp-uniform */
+        const bool xin = lane + 1 < ex;
+        const unsigned own = __ballot_sync(0xffffffffu, (bits & 1u) && xin);
+        const unsigned yb = __ballot_sync(0xffffffffu, (bits & 2u) && yin);
+        const unsigned zb = __ballot_sync(0xffffffffu, (bits & 4u) && zin);
+        const unsigned yrow = yin ? __ballot_sync(0xffffffffu, (lbits[l + kTileX] & 1u) && xin) : 0u;
+        const unsigned zrow = zin ? __ballot_sync(0xffffffffu, (lbits[l + kTileX * kTileY] & 1u) && xin) : 0u;
+        const unsigned ylead = yb & ~((yb & own & yrow) << 1), zlead = zb & ~((zb & own & zrow) << 1);
+        if ((ylead >> lane) & 1u) ok &= tile_union(lpar, l, l + kTileX, bu);
+        if ((zlead >> lane) & 1u) ok &= tile_union(lpar, l, l + kTileX * kTileY, bu);
     }
     __syncthreads();
     for (uint32_t l = threadIdx.x; l < kTileSites; l += blockDim.x) {
