@@ -277,41 +277,52 @@ __global__ void __launch_bounds__(kThreads)
     if (!ok) atomicOr(&stats[kStatError], kErrUnionFindLimit);
 }
 
-/* The active bonds that leave a tile (the tile's last x, y or z, periodic
- * wraps included), joined in the global union-find over the tile roots.  The
- * bonds of one direction that a warp holds mostly join the same two tile
- * components (a tile face crosses one or two components), so the lanes group
- * them by their (tile root, tile root) pair and one lane per pair joins. */
+/* The active bonds that leave a tile (its last x, y or z; periodic wraps
+ * included), joined in the global union-find over the tile roots.  A warp
+ * takes one face row of one tile: the 8 x 4 bonds of the +x face (lane =
+ * y + 8 z), one of the 4 rows of the +y face or one of the 8 rows of the +z
+ * face (lane = x).  The bonds of a face row mostly join the same few pairs of
+ * tile roots, so the lanes group them by (root, root) pair and one lane per
+ * pair joins. */
+constexpr uint32_t kFaceRows = 1 + kTileZ + kTileY;
+static_assert(kTileY * kTileZ == 32, "an x face is one warp");
+
 __global__ void __launch_bounds__(kThreads)
-    k_wolff_boundary(const uint8_t* __restrict__ bonds, uint32_t lx, uint32_t ly, uint32_t lz,
+    k_wolff_boundary(const uint8_t* __restrict__ bonds, uint32_t lx, uint32_t ly, uint32_t lz, uint32_t n_tiles,
                      uint32_t* parent, unsigned long long* stats, uint32_t limit) {
-    const uint32_t volume = lx * ly * lz;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool in = i < volume;
-    const uint32_t bits = in ? bonds[i] : 0u;
-    const uint32_t ii = in ? i : 0u;
-    const uint32_t x = ii % lx, row = ii / lx, y = row % ly, z = row / ly;
-    const uint32_t plane = lx * ly;
-    const bool cross[3] = {(x % kTileX == kTileX - 1) || (x + 1 == lx), (y % kTileY == kTileY - 1) || (y + 1 == ly),
-                           (z % kTileZ == kTileZ - 1) || (z + 1 == lz)};
-    const uint32_t nb[3] = {(x + 1 == lx) ? ii + 1 - lx : ii + 1, (y + 1 == ly) ? ii + lx - plane : ii + lx,
-                            (z + 1 == lz) ? ii + plane - volume : ii + plane};
-    const UfBounds bd = uf_bounds(volume, limit);
     const uint32_t lane = threadIdx.x & 31u;
-    bool ok = true;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const bool act = in && cross[d] && (bits & (1u << d));
-        if (!__any_sync(0xffffffffu, act)) continue;
-        uint32_t a = 0, b = 0;
-        if (act) {
-            a = parent[ii];
-            b = parent[nb[d]];
-        }
-        const unsigned long long key = act ? (((unsigned long long)a << 32) | b) : ~0ull;
-        const unsigned grp = __match_any_sync(0xffffffffu, key);
-        if (act && lane == (uint32_t)(__ffs(grp) - 1) && a != b) ok &= uf_union(parent, a, b, bd);
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t tile = w / kFaceRows, item = w - tile * kFaceRows;
+    if (tile >= n_tiles) return; /* whole warps */
+    const uint32_t ntx = (lx + kTileX - 1) / kTileX, nty = (ly + kTileY - 1) / kTileY;
+    const uint32_t tx = tile % ntx, rest = tile / ntx, ty = rest % nty, tz = rest / nty;
+    const uint32_t x0 = tx * kTileX, y0 = ty * kTileY, z0 = tz * kTileZ;
+    const uint32_t ex = min(kTileX, lx - x0), ey = min(kTileY, ly - y0), ez = min(kTileZ, lz - z0);
+    const uint32_t plane = lx * ly, volume = plane * lz;
+    uint32_t ax, ay, az, d;
+    if (item == 0) {
+        d = 0, ax = ex - 1, ay = lane % kTileY, az = lane / kTileY;
+    } else if (item <= kTileZ) {
+        d = 1, ax = lane, ay = ey - 1, az = item - 1;
+    } else {
+        d = 2, ax = lane, ay = item - 1 - kTileZ, az = ez - 1;
     }
+    const bool in = ax < ex && ay < ey && az < ez;
+    const uint32_t x = x0 + ax, y = y0 + ay, z = z0 + az;
+    const uint32_t i = in ? x + lx * (y + ly * z) : 0u;
+    const bool act = in && (bonds[i] & (1u << d));
+    uint32_t a = 0, b = 0;
+    if (act) {
+        const uint32_t nb = d == 0   ? ((x + 1 == lx) ? i + 1 - lx : i + 1)
+                            : d == 1 ? ((y + 1 == ly) ? i + lx - plane : i + lx)
+                                     : ((z + 1 == lz) ? i + plane - volume : i + plane);
+        a = parent[i];
+        b = parent[nb];
+    }
+    const unsigned long long key = act ? (((unsigned long long)a << 32) | b) : ~0ull;
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    bool ok = true;
+    if (act && lane == (uint32_t)(__ffs(grp) - 1) && a != b) ok = uf_union(parent, a, b, uf_bounds(volume, limit));
     if (!ok) atomicOr(&stats[kStatError], kErrUnionFindLimit);
 }
 
@@ -474,7 +485,8 @@ void launch_wolff(const TaskView& t, uint64_t counter, uint8_t* bonds, uint32_t*
                            ((t.lz + kTileZ - 1) / kTileZ);
     k_wolff_tiles<<<tiles, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, -2.0f * t.beta, phi,
                                              t.seed, counter, bonds, parent, t.stats, t.loop_limit);
-    k_wolff_boundary<<<grid, kThreads, 0, s>>>(bonds, t.lx, t.ly, t.lz, parent, t.stats, t.loop_limit);
+    k_wolff_boundary<<<blocks_for((uint64_t)tiles * kFaceRows * 32, kThreads), kThreads, 0, s>>>(
+        bonds, t.lx, t.ly, t.lz, tiles, parent, t.stats, t.loop_limit);
     k_wolff_compress<<<grid, kThreads, 0, s>>>(bonds, volume, parent, t.stats, t.loop_limit);
     k_wolff_flip<<<grid, kThreads, 0, s>>>(t.theta, volume, parent, seed_idx, phi, t.stats, cluster_out);
     if (phi_out) *phi_out = phi;
