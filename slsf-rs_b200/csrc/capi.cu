@@ -109,6 +109,8 @@ TaskLayout layout_of(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t n_bins) {
 
 }  // namespace
 
+constexpr size_t kSmallReadBack = 256; /* bytes */
+
 struct slsf_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
@@ -127,6 +129,9 @@ struct slsf_ctx {
     slsf::ResidentCorr* h_rcorr = nullptr; /* pinned */
     unsigned long long* d_batch_stats = nullptr;
     unsigned long long* h_batch_stats = nullptr; /* pinned */
+    /* pinned landing area of the single-task calls' small read-backs (stats,
+     * observables): a pageable destination would be staged by the driver */
+    double* h_small = nullptr;
     uint32_t views_cap = 0;
     unsigned int* d_queue = nullptr; /* one counter per kernel group */
     uint32_t queue_cap = 0;
@@ -241,9 +246,11 @@ int check_free(const slsf_task* t) {
 }
 
 int read_stats(slsf_task* t, unsigned long long out[slsf::kStatSlots]) {
-    SLSF_CUDA(cudaMemcpyAsync(out, t->stats, sizeof(unsigned long long) * slsf::kStatSlots,
+    static_assert(sizeof(unsigned long long) * slsf::kStatSlots <= kSmallReadBack, "stats fit the landing area");
+    SLSF_CUDA(cudaMemcpyAsync(t->ctx->h_small, t->stats, sizeof(unsigned long long) * slsf::kStatSlots,
                               cudaMemcpyDeviceToHost, t->ctx->stream));
     SLSF_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    std::memcpy(out, t->ctx->h_small, sizeof(unsigned long long) * slsf::kStatSlots);
     if (out[slsf::kStatError])
         return set_error(SLSF_ERR_TIMEOUT, "a bounded device loop hit its iteration limit");
     return SLSF_OK;
@@ -372,6 +379,7 @@ int slsf_ctx_create(int device, uint64_t budget_bytes, uint32_t flags, slsf_ctx*
     ctx->budget = budget_bytes ? budget_bytes : (uint64_t)(0.9 * (double)free_b);
     e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaHostAlloc(&ctx->h_small, kSmallReadBack, cudaHostAllocDefault);
     for (int q = 0; q < kSideStreams && e == cudaSuccess; ++q) {
         e = cudaStreamCreateWithFlags(&ctx->side[q], cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join[q], cudaEventDisableTiming);
@@ -379,6 +387,7 @@ int slsf_ctx_create(int device, uint64_t budget_bytes, uint32_t flags, slsf_ctx*
     if (e != cudaSuccess) {
         destroy_streams(ctx);
         if (ctx->d_queue) cudaFree(ctx->d_queue);
+        if (ctx->h_small) cudaFreeHost(ctx->h_small);
         delete ctx;
         return cuda_error(e, "context set-up");
     }
@@ -399,7 +408,7 @@ int slsf_ctx_destroy(slsf_ctx* ctx) {
         if (p) cudaFree(p);
     if (ctx->d_corr) cudaFree(ctx->d_corr);
     void* host[] = {ctx->h_views, ctx->h_batch_stats, (void*)ctx->h_bin_src, ctx->h_bin_out, ctx->h_corr,
-                    ctx->h_rcorr};
+                    ctx->h_rcorr, ctx->h_small};
     for (void* p : host)
         if (p) cudaFreeHost(p);
     if (ctx->corr_uploaded) cudaEventDestroy(ctx->corr_uploaded);
@@ -699,8 +708,9 @@ int slsf_task_measure(slsf_task* t, slsf_observables* out) {
     t->ctx->launches += 1;
     SLSF_CUDA(cudaGetLastError());
     double r[8];
-    SLSF_CUDA(cudaMemcpyAsync(r, t->result, sizeof(r), cudaMemcpyDeviceToHost, t->ctx->stream));
+    SLSF_CUDA(cudaMemcpyAsync(t->ctx->h_small, t->result, sizeof(r), cudaMemcpyDeviceToHost, t->ctx->stream));
     SLSF_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    std::memcpy(r, t->ctx->h_small, sizeof(r));
     const double v = (double)t->volume;
     /* energy_sum = -(sum of the J cos terms) (src/observables.rs:129-138). */
     out->energy = -(r[2] + r[3] + r[4]) / v;
