@@ -280,3 +280,28 @@ def test_tiny_config_builds_one_task(jobs):
     assert (t["l_x"], t["l_y"], t["l_z"], t["temperature"]) == (2, 2, 2, 2.0)
     assert t["j_xy_array"] == [1.0, 1.0] and t["j_z_array"] == [0.1, 0.1]
     assert (t["sweeps"], t["thermalization"], t["binsize"], t["wolff_steps"]) == (4, 2, 2, 1)
+
+
+def test_measurement_bins_mapping_and_checkpoint_round_trip(jobs, slsf):
+    # a task's measurement_bins (src/model.rs:81) from its estimates: the
+    # twelve per-sweep columns and the correlation columns, each with its own
+    # bin length; they survive the JSON form the checkpoints keep
+    rows = np.arange(3 * slsf.BIN_COLS, dtype=np.float64).reshape(3, slsf.BIN_COLS)
+    corr = np.array([[0.5, 0.25], [0.75, 0.125]])
+    est = {"Energy": (1.0, 0.1), "n_bins": 3, "_bins": {"binsize": 4, "rows": rows},
+           "_corr_bins": {"binsize": 2, "names": ["CorrX_r1", "CorrZ_r1"], "rows": corr}}
+    bins = jobs.measurement_bins(est)
+    assert sorted(bins) == sorted(list(slsf.BIN_NAMES) + ["CorrX_r1", "CorrZ_r1"])
+    for j, name in enumerate(slsf.BIN_NAMES):
+        assert bins[name][0] == 4 and np.array_equal(bins[name][1], rows[:, j])
+    assert bins["CorrZ_r1"][0] == 2 and np.array_equal(bins["CorrZ_r1"][1], corr[:, 1])
+    import json
+
+    back = jobs._est_from_json(json.loads(json.dumps(jobs._est_to_json(est))))
+    assert back["Energy"] == (1.0, 0.1)
+    again = jobs.measurement_bins(back)
+    assert sorted(again) == sorted(bins)
+    for name in bins:
+        assert again[name][0] == bins[name][0] and np.array_equal(again[name][1], bins[name][1])
+    # a served task without a complete bin keeps no bins
+    assert jobs.measurement_bins({"_bins": {"binsize": 4, "rows": np.zeros((0, slsf.BIN_COLS))}}) == {}
