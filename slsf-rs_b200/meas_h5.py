@@ -11,7 +11,7 @@ through the hdf5-pure 0.21 crate; the dataframe tool of the reference reads
 them back.  This module writes the same objects in the HDF5 file format
 (HDF5 File Format Specification): a version 0 superblock, version 1 object
 headers, groups as symbol tables (a version 1 B-tree of symbol table nodes
-over a local heap of names, one or two B-tree levels), and datasets with a
+over a local heap of names, as many B-tree levels as a group needs), and datasets with a
 version 1 dataspace, a version 1 datatype, a version 1 fill value message and
 a version 2 contiguous layout.  The one difference from the reference's
 files: `samples` is stored contiguously, without the chunking (1000) and
@@ -159,24 +159,24 @@ class _Writer:
         return self.alloc(bytes(node))
 
     def btree(self, snods) -> int:
+        """A group B-tree over its symbol table nodes, as many levels as the
+        name count needs; the nodes of one level carry sibling addresses."""
         cap = 2 * INTERNAL_K
-        if len(snods) <= cap:
-            return self.btree_node(0, snods, 0, UNDEF, UNDEF)
-        if len(snods) > cap * cap:
-            raise MeasH5Error("group too large for a two-level B-tree")
-        parts = [snods[lo:lo + cap] for lo in range(0, len(snods), cap)]
-        # level-0 nodes, with sibling addresses: reserve their space first
         node_size = 24 + 8 * (2 * cap + 1)
-        base = len(self.buf)
-        addrs = [base + k * node_size for k in range(len(parts))]
-        leaves = []
-        for k, part in enumerate(parts):
-            left_key = 0 if k == 0 else parts[k - 1][-1][1]
-            a = self.btree_node(0, part, left_key, addrs[k - 1] if k else UNDEF,
-                                addrs[k + 1] if k + 1 < len(parts) else UNDEF)
-            assert a == addrs[k]
-            leaves.append((a, part[-1][1]))
-        return self.btree_node(1, leaves, 0, UNDEF, UNDEF)
+        children, level = snods, 0
+        while len(children) > cap:
+            parts = [children[lo:lo + cap] for lo in range(0, len(children), cap)]
+            base = len(self.buf)  # this level's nodes are laid out back to back
+            addrs = [base + k * node_size for k in range(len(parts))]
+            nodes = []
+            for k, part in enumerate(parts):
+                left_key = 0 if k == 0 else parts[k - 1][-1][1]
+                a = self.btree_node(level, part, left_key, addrs[k - 1] if k else UNDEF,
+                                    addrs[k + 1] if k + 1 < len(parts) else UNDEF)
+                assert a == addrs[k]
+                nodes.append((a, part[-1][1]))
+            children, level = nodes, level + 1
+        return self.btree_node(level, children, 0, UNDEF, UNDEF)
 
     def finish(self, root) -> bytes:
         header, btree, heap = root

@@ -75,9 +75,11 @@ def test_round_trip(slsf, meas, tmp_path, monkeypatch):
     assert (f.base, f.leaf_k, f.internal_k, f.eof) == (0, 4, 16, len(data))
 
 
-def test_large_group_needs_two_btree_levels(slsf, meas, tmp_path):
-    # L = 64 with r_max = 32 measures over 2000 correlation observables
-    bins = sample_bins(slsf, n_corr_z=700)
+@pytest.mark.parametrize("n_corr_z", [700, 8460])
+def test_large_groups_take_more_btree_levels(slsf, meas, tmp_path, n_corr_z):
+    # L = 64 with r_max = 32 measures over 2000 correlation observables (two
+    # B-tree levels), L = 128 with r_max = 64 over 8400 (three)
+    bins = sample_bins(slsf, n_corr_z=n_corr_z)
     path = meas.write_meas_h5(tmp_path / "big.meas.h5", bins)
     check(h5read.read(path), bins)
 
