@@ -22,6 +22,7 @@
 #include <algorithm>
 
 #include "engine.h"
+#include "fastdiv.h"
 #include "xy_device.cuh"
 
 namespace slsf {
@@ -61,8 +62,8 @@ template <bool kRecord>
 __global__ void __launch_bounds__(kThreads)
     k_metro_colour(float* __restrict__ theta, const float* __restrict__ jxy,
                    const float* __restrict__ jz, uint32_t lx, uint32_t ly, uint32_t lz, float beta,
-                   float width, uint64_t seed, uint64_t sweep, uint32_t colour,
-                   unsigned long long* __restrict__ stats, uint8_t* __restrict__ record) {
+                   float width, uint64_t seed, uint64_t sweep, uint32_t colour, slsf_fastdiv div_hx,
+                   slsf_fastdiv div_ly, unsigned long long* __restrict__ stats, uint8_t* __restrict__ record) {
     const uint32_t volume = lx * ly * lz;
     const uint32_t half = volume >> 1;
     const uint32_t npairs = (half + 1) >> 1;
@@ -74,7 +75,14 @@ __global__ void __launch_bounds__(kThreads)
         for (uint32_t lane = 0; lane < 2; ++lane) {
             const uint32_t h = 2 * p + lane;
             if (h >= half) break;
-            const SiteXYZ s = decode_colour_site(h, colour, lx, ly);
+            /* the h-th site of this colour: row = h / (L_x / 2) (x + L_x row = site index),
+             * x = 2 (h mod L_x / 2) + (colour + y + z) mod 2; divisions as multiply-shifts */
+            SiteXYZ s;
+            const uint32_t row = slsf_fastdiv_div(h, div_hx), k = h - row * div_hx.d;
+            s.z = slsf_fastdiv_div(row, div_ly);
+            s.y = row - s.z * ly;
+            s.x = 2u * k + ((colour + s.y + s.z) & 1u);
+            s.idx = s.x + lx * row;
             uint32_t nb[6];
             neighbour_indices(s, lx, ly, lz, nb);
             float ns[6], nc[6];
@@ -374,8 +382,8 @@ constexpr int kMeasureThreads = 256;
 
 __global__ void __launch_bounds__(kMeasureThreads)
     k_measure(const float* __restrict__ theta, const float* __restrict__ jxy,
-              const float* __restrict__ jz, uint32_t lx, uint32_t ly, uint32_t lz,
-              double* __restrict__ partials, unsigned int* __restrict__ done,
+              const float* __restrict__ jz, uint32_t lx, uint32_t ly, uint32_t lz, slsf_fastdiv div_lx,
+              slsf_fastdiv div_ly, double* __restrict__ partials, unsigned int* __restrict__ done,
               double* __restrict__ result, double* __restrict__ bin_row) {
     __shared__ double scratch[8 * 32];
     __shared__ bool last;
@@ -383,7 +391,8 @@ __global__ void __launch_bounds__(kMeasureThreads)
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < volume; i += stride) {
-        const uint32_t x = i % lx, row = i / lx, y = row % ly, z = row / ly;
+        const uint32_t row = slsf_fastdiv_div(i, div_lx), z = slsf_fastdiv_div(row, div_ly);
+        const uint32_t x = i - row * lx, y = row - z * ly;
         const uint32_t ix = (x + 1 == lx) ? i + 1 - lx : i + 1;
         const uint32_t iy = (y + 1 == ly) ? i + lx - plane : i + lx;
         const uint32_t iz = (z + 1 == lz) ? i + plane - volume : i + plane;
@@ -463,12 +472,13 @@ void launch_metro_colour(const TaskView& t, uint64_t sweep, uint32_t colour, uin
     const uint32_t volume = t.lx * t.ly * t.lz;
     const uint32_t npairs = ((volume >> 1) + 1) >> 1;
     const uint32_t grid = blocks_for(npairs, kThreads);
+    const slsf_fastdiv dhx = slsf_fastdiv_make(t.lx / 2), dly = slsf_fastdiv_make(t.ly);
     if (record)
-        k_metro_colour<true><<<grid, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, t.beta,
-                                                       t.width, t.seed, sweep, colour, t.stats, record);
+        k_metro_colour<true><<<grid, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, t.beta, t.width,
+                                                       t.seed, sweep, colour, dhx, dly, t.stats, record);
     else
-        k_metro_colour<false><<<grid, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, t.beta,
-                                                        t.width, t.seed, sweep, colour, t.stats, nullptr);
+        k_metro_colour<false><<<grid, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, t.beta, t.width,
+                                                        t.seed, sweep, colour, dhx, dly, t.stats, nullptr);
 }
 
 void launch_wolff(const TaskView& t, uint64_t counter, uint8_t* bonds, uint32_t* parent,
@@ -504,15 +514,17 @@ int measure_partial_blocks(uint32_t volume) {
 void launch_measure(const TaskView& t, double* partials, unsigned int* done, double* result,
                     cudaStream_t s) {
     const uint32_t volume = t.lx * t.ly * t.lz;
-    k_measure<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly,
-                                                                         t.lz, partials, done, result, nullptr);
+    k_measure<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(
+        t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, slsf_fastdiv_make(t.lx), slsf_fastdiv_make(t.ly), partials, done,
+        result, nullptr);
 }
 
 void launch_measure_into_bin(const TaskView& t, double* partials, unsigned int* done, double* result,
                              double* bin_row, cudaStream_t s) {
     const uint32_t volume = t.lx * t.ly * t.lz;
-    k_measure<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly,
-                                                                         t.lz, partials, done, result, bin_row);
+    k_measure<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(
+        t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, slsf_fastdiv_make(t.lx), slsf_fastdiv_make(t.ly), partials, done,
+        result, bin_row);
 }
 
 }  // namespace slsf

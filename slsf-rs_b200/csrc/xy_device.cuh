@@ -24,19 +24,6 @@ struct SiteXYZ {
     uint32_t x, y, z, idx;
 };
 
-__device__ __forceinline__ SiteXYZ decode_colour_site(uint32_t h, uint32_t colour, uint32_t lx,
-                                                      uint32_t ly) {
-    const uint32_t hx = lx >> 1;
-    const uint32_t row = h / hx;
-    const uint32_t k = h - row * hx;
-    SiteXYZ s;
-    s.y = row % ly;
-    s.z = row / ly;
-    s.x = 2u * k + ((colour + s.y + s.z) & 1u);
-    s.idx = s.x + lx * row;
-    return s;
-}
-
 /* Neighbour indices in the order +x, -x, +y, -y, +z, -z (the neighbors!
  * macro of src/updates.rs:131-167). */
 __device__ __forceinline__ void neighbour_indices(const SiteXYZ& s, uint32_t lx, uint32_t ly,
