@@ -70,7 +70,7 @@ __host__ __device__ inline CorrShape corr_shape(uint32_t lx, uint32_t ly, uint32
 /* `tasks` in device memory, or NULL and the single task `one` by value. */
 __global__ void __launch_bounds__(kCorrThreads)
     k_corr_lines(const CorrTask* __restrict__ tasks, CorrTask one, uint32_t n_tasks, uint32_t n_items) {
-    extern __shared__ float2 tile[]; /* [n + R + kCorrLags][pitch] */
+    extern __shared__ float2 tile[]; /* [n][pitch]: one period of each line */
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (uint32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
         /* the task: the last one whose first item is at or before `item` */
@@ -101,36 +101,36 @@ __global__ void __launch_bounds__(kCorrThreads)
             rmax = T.rz;
         }
         const float* __restrict__ theta = T.theta;
-        const uint32_t ext = n + rmax;
         __syncthreads(); /* the previous item's tile is no longer read */
         const uint32_t pitch = cstride == 1 ? kCorrCols : kCorrPitch;
         if (cstride == 1) {
-            for (uint32_t e = threadIdx.x; e < ext * kCorrCols; e += blockDim.x) {
+            for (uint32_t e = threadIdx.x; e < n * kCorrCols; e += blockDim.x) {
                 const uint32_t k = e / kCorrCols, c = e % kCorrCols;
-                const uint32_t kk = k < n ? k : k - n;
                 float sn = 0.0f, cn = 0.0f;
-                if (c < cols) __sincosf(theta[base + kk * stride + c], &sn, &cn);
+                if (c < cols) __sincosf(theta[base + k * stride + c], &sn, &cn);
                 tile[k * pitch + c] = make_float2(cn, sn);
             }
         } else {
             /* x lines: consecutive threads take consecutive sites of a row */
-            for (uint32_t e = threadIdx.x; e < ext * kCorrCols; e += blockDim.x) {
-                const uint32_t c = e / ext, k = e % ext;
-                const uint32_t kk = k < n ? k : k - n;
+            for (uint32_t e = threadIdx.x; e < n * kCorrCols; e += blockDim.x) {
+                const uint32_t c = e / n, k = e % n;
                 float sn = 0.0f, cn = 0.0f;
-                if (c < cols) __sincosf(theta[base + c * cstride + kk], &sn, &cn);
+                if (c < cols) __sincosf(theta[base + c * cstride + k], &sn, &cn);
                 tile[k * pitch + c] = make_float2(cn, sn);
             }
         }
         __syncthreads();
         double* out = T.partial + (size_t)local * sh.rp;
-        /* The window reads rows up to ext + 7 (k <= n - 1, r0 <= R): the tile has kCorrLags
-         * rows past ext, left unset; they meet only lags beyond R, which are dropped. */
+        /* The tile holds one period of each line: the partner of site k at lag
+         * r is row (k + r) mod n.  Lags past R in the last group of 8 are
+         * computed and dropped. */
         for (uint32_t r0 = 1 + warp * kCorrLags; r0 <= rmax; r0 += nwarps * kCorrLags) {
             /* w[j]: partner of lag r0 + j at the current k */
             float2 w[kCorrLags];
 #pragma unroll
-            for (uint32_t j = 0; j < kCorrLags; ++j) w[j] = tile[(r0 + j) * pitch + lane];
+            for (uint32_t j = 0; j < kCorrLags; ++j) w[j] = tile[((r0 + j) % n) * pitch + lane];
+            /* row of the next partner to load, (k + r0 + 8) mod n, advanced by one per k */
+            uint32_t q = (r0 + kCorrLags) % n;
             double tot[kCorrLags];
             float part[kCorrLags];
 #pragma unroll
@@ -151,7 +151,8 @@ __global__ void __launch_bounds__(kCorrThreads)
                         const float2 wj = w[(kk + j) % kCorrLags];
                         part[j] = __fmaf_rn(a.y, wj.y, __fmaf_rn(a.x, wj.x, part[j]));
                     }
-                    w[kk] = tile[(k0 + kk + r0 + kCorrLags) * pitch + lane];
+                    w[kk] = tile[q * pitch + lane];
+                    q = q + 1 == n ? 0u : q + 1;
                 }
                 if ((k0 + kCorrLags) % kCorrRun == 0) {
 #pragma unroll
@@ -170,7 +171,8 @@ __global__ void __launch_bounds__(kCorrThreads)
                     part[j] = __fmaf_rn(a.y, w[j].y, __fmaf_rn(a.x, w[j].x, part[j]));
 #pragma unroll
                 for (uint32_t j = 0; j + 1 < kCorrLags; ++j) w[j] = w[j + 1];
-                w[kCorrLags - 1] = tile[(k + kCorrLags + r0) * pitch + lane];
+                w[kCorrLags - 1] = tile[q * pitch + lane];
+                q = q + 1 == n ? 0u : q + 1;
             }
 #pragma unroll
             for (uint32_t j = 0; j < kCorrLags; ++j) {
@@ -274,6 +276,13 @@ uint32_t corr_z_items(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint3
     return corr_shape(lx, ly, lz, rxy, rz).nz;
 }
 
+uint32_t corr_len(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
+    uint32_t n = 0;
+    if (rxy) n = std::max(lx, ly);
+    if (rz) n = std::max(n, lz);
+    return n;
+}
+
 uint32_t corr_ext(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
     uint32_t e = 0;
     if (rxy) e = std::max(lx, ly) + rxy;
@@ -286,7 +295,7 @@ bool corr_supports(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t
 }
 
 cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t n_tasks, uint32_t n_items,
-                        uint32_t max_ext, uint32_t max_r, uint32_t max_nz, int sm_count, cudaStream_t s) {
+                        uint32_t max_len, uint32_t max_r, uint32_t max_nz, int sm_count, cudaStream_t s) {
     (void)sm_count; /* one block per item: the hardware spreads them */
     /* a warp takes 8 lags per pass: blocks of one or two warps for small
      * radii, so that short lines do not hold idle warps */
@@ -297,7 +306,7 @@ cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t
     if (n_tasks == 0 || (!tasks_dev && (!one || n_tasks != 1))) return cudaErrorInvalidValue;
     const CorrTask by_value = one ? *one : CorrTask{};
     if (n_items > 0) {
-        const size_t smem = (size_t)(max_ext + kCorrLags) * kCorrPitch * sizeof(float2);
+        const size_t smem = (size_t)max_len * kCorrPitch * sizeof(float2);
         cudaError_t e = cudaSuccess;
         if (smem > 48 * 1024)
             e = cudaFuncSetAttribute(k_corr_lines, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
