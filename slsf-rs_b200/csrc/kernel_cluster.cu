@@ -140,7 +140,7 @@ struct Geo {
     uint32_t tstride;             /* colour-1 offset of theta */
     uint32_t hp;                  /* sites of one colour in one plane */
     bool lx_tiles_warp;           /* 32 % lx == 0 */
-    bool lx_two_warps;            /* lx == 64 */
+    bool lx_two_warps;            /* 32 < lx <= 64: a warp holds a row, lanes j and j + 32 */
     slsf_fastdiv div_hx, div_ly, div_lx;
 };
 
@@ -161,7 +161,7 @@ __device__ __forceinline__ Geo make_geo(const TaskView& t, uint32_t rank, uint32
     g.tstride = g.half_s + kPad;
     g.hp = g.plane >> 1;
     g.lx_tiles_warp = t.lx <= 32 && (32u % t.lx) == 0;
-    g.lx_two_warps = t.lx == 64;
+    g.lx_two_warps = t.lx > 32 && t.lx <= 64;
     g.div_hx = slsf_fastdiv_make(t.lx >> 1);
     g.div_ly = slsf_fastdiv_make(t.ly);
     g.div_lx = slsf_fastdiv_make(t.lx);
@@ -441,40 +441,49 @@ __device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Sme
     if constexpr (sizeof(W) == 8) {
       if (g.lx_two_warps) {
         walked = true;
-        /* L_x = 64: a warp holds a whole row, lane j the sites x = j and
-         * x = j + 32, and walks columns of rows along y -- (plane, y
-         * segment) units, round robin -- so the projections of the +y row are
-         * the next row's own: two sincos per site instead of three. */
+        /* 32 < L_x <= 64: a warp holds a whole row, lane j the sites x = j and
+         * x = j + 32 (lanes past the row's end repeat x = j, whose colour is the
+         * same, and keep no bits).  Each warp walks an equal run of the slab's
+         * rows in order (y fastest), so the projections of the +y row are the
+         * next row's own -- two sincos per site instead of three -- except at
+         * the first row of its run and of each plane. */
         const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-        const uint32_t nseg = (nwarps + g.nz - 1) / g.nz;
-        const uint32_t seg = (g.ly + nseg - 1) / nseg;
+        const uint32_t nrows = g.nz * g.ly;
+        const uint32_t r_lo = (uint32_t)((uint64_t)warp * nrows / nwarps);
+        const uint32_t r_hi = (uint32_t)((uint64_t)(warp + 1) * nrows / nwarps);
         const uint32_t nxt = (lane + 1u) & 31u;
-        for (uint32_t u = warp; u < g.nz * nseg; u += nwarps) {
-            const uint32_t zl = u / nseg, y_lo = (u % nseg) * seg, y_hi = min(g.ly, y_lo + seg);
-            if (y_lo >= y_hi) continue;
+        const uint32_t lx = g.lx;
+        const uint32_t xb = lane + 32u < lx ? lane + 32u : lane; /* this lane's site of half 1 */
+        const uint32_t mb = lx == 64u ? 0xffffffffu : ((1u << (lx - 32u)) - 1u);
+        const bool wrap_b = lane + 33u >= lx; /* half 1's +x partner is x = 0 */
+        uint32_t* hx32 = reinterpret_cast<uint32_t*>(s.bx);
+        uint32_t* hy32 = reinterpret_cast<uint32_t*>(s.by);
+        uint32_t* hz32 = reinterpret_cast<uint32_t*>(s.bz);
+        uint32_t zl = slsf_fastdiv_div(r_lo, g.div_ly), y = r_lo - zl * g.ly;
+        uint32_t col = 0;
+        float ra = 0.0f, rb = 0.0f;
+        for (uint32_t row = r_lo; row < r_hi; ++row) {
             const float jx = s.jxy[g.z0 + zl], jzz = s.jz[g.z0 + zl];
             const uint32_t pbase = zl * g.plane;
-            /* colour of (x = lane, y, zl); x + 32 has the same colour */
-            uint32_t col = colour_of(g, lane, y_lo, zl);
-            float ra = proj_of(s.th[col * g.tstride + ((pbase + y_lo * 64u + lane) >> 1)], cphi, sphi);
-            float rb = proj_of(s.th[col * g.tstride + ((pbase + y_lo * 64u + lane + 32u) >> 1)], cphi, sphi);
-            uint32_t* hx32 = reinterpret_cast<uint32_t*>(s.bx);
-            uint32_t* hy32 = reinterpret_cast<uint32_t*>(s.by);
-            uint32_t* hz32 = reinterpret_cast<uint32_t*>(s.bz);
-            for (uint32_t y = y_lo; y < y_hi; ++y) {
-                const uint32_t li = pbase + y * 64u + lane;
+            if (row == r_lo || y == 0) {
+                /* colour of (x = lane, y, zl); x + 32 has the same colour */
+                col = colour_of(g, lane, y, zl);
+                ra = proj_of(s.th[col * g.tstride + ((pbase + y * lx + lane) >> 1)], cphi, sphi);
+                rb = proj_of(s.th[col * g.tstride + ((pbase + y * lx + xb) >> 1)], cphi, sphi);
+            }
+            {
+                const uint32_t li = pbase + y * lx + lane, lib = pbase + y * lx + xb;
                 const uint32_t y1 = (y + 1 == g.ly) ? 0u : y + 1;
                 const uint32_t ocol = col ^ 1u; /* colour of the +y and +z partners */
-                const uint32_t li_y = pbase + y1 * 64u + lane;
-                const uint32_t row = y + g.ly * zl;
+                const uint32_t li_y = pbase + y1 * lx + lane, lib_y = pbase + y1 * lx + xb;
                 const bool top = zl + 1 == g.nz;
-                /* +x partners: x + 1 in the same half, across the halves at x = 31 and x = 63 */
+                /* +x partners: x + 1 in the same half, across the halves at x = 31 and x = L_x - 1 */
                 const float b0 = __shfl_sync(0xffffffffu, rb, 0), a0 = __shfl_sync(0xffffffffu, ra, 0);
                 const float na = __shfl_sync(0xffffffffu, ra, nxt), nb = __shfl_sync(0xffffffffu, rb, nxt);
                 /* half 0: x = lane; each half is finished (bonds, ballots, 32-bit row-word half) in turn */
                 const float rya = proj_of(s.th[ocol * g.tstride + (li_y >> 1)], cphi, sphi);
                 {
-                    const float tz = top ? halo_theta(g, s, true, ocol, (lane + 64u * y) >> 1)
+                    const float tz = top ? halo_theta(g, s, true, ocol, (lane + lx * y) >> 1)
                                          : s.th[ocol * g.tstride + ((li + g.plane) >> 1)];
                     const float rz = proj_of(tz, cphi, sphi);
                     const slsf_u32x4 bw = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, base_idx + li);
@@ -488,24 +497,28 @@ __device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Sme
                     }
                 }
                 /* half 1: x = lane + 32 */
-                const float ryb = proj_of(s.th[ocol * g.tstride + ((li_y + 32u) >> 1)], cphi, sphi);
+                const float ryb = proj_of(s.th[ocol * g.tstride + (lib_y >> 1)], cphi, sphi);
                 {
-                    const float tz = top ? halo_theta(g, s, true, ocol, (lane + 32u + 64u * y) >> 1)
-                                         : s.th[ocol * g.tstride + ((li + 32u + g.plane) >> 1)];
+                    const float tz = top ? halo_theta(g, s, true, ocol, (xb + lx * y) >> 1)
+                                         : s.th[ocol * g.tstride + ((lib + g.plane) >> 1)];
                     const float rz = proj_of(tz, cphi, sphi);
-                    const slsf_u32x4 bw = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, base_idx + li + 32u);
-                    const uint32_t bx = __ballot_sync(0xffffffffu, wolff_bond_active(jx, rb, lane < 31u ? nb : a0, m2b, bw.x));
+                    const slsf_u32x4 bw = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, base_idx + lib);
+                    const uint32_t bx = __ballot_sync(0xffffffffu, wolff_bond_active(jx, rb, wrap_b ? a0 : nb, m2b, bw.x));
                     const uint32_t by = __ballot_sync(0xffffffffu, wolff_bond_active(jx, rb, ryb, m2b, bw.y));
                     const uint32_t bz = __ballot_sync(0xffffffffu, wolff_bond_active(jzz, rb, rz, m2b, bw.z));
                     if (lane == 0) {
-                        hx32[2 * row + 1] = bx;
-                        hy32[2 * row + 1] = by;
-                        hz32[2 * row + 1] = bz;
+                        hx32[2 * row + 1] = bx & mb;
+                        hy32[2 * row + 1] = by & mb;
+                        hz32[2 * row + 1] = bz & mb;
                     }
                 }
                 ra = rya;
                 rb = ryb;
                 col = ocol;
+            }
+            if (++y == g.ly) {
+                y = 0;
+                ++zl;
             }
         }
       }
@@ -543,22 +556,12 @@ __device__ __forceinline__ void wolff_bonds(const TaskView& t, const Geo& g, Sme
             const uint32_t bal_x = __ballot_sync(0xffffffffu, ax);
             const uint32_t bal_y = __ballot_sync(0xffffffffu, ay);
             const uint32_t bal_z = __ballot_sync(0xffffffffu, az);
-            if (g.lx_tiles_warp) {
-                if (valid && c.x == 0) {
-                    const W m = (W)((g.lx >= 32) ? 0xffffffffu : ((1u << g.lx) - 1u));
-                    s.bx[c.row] = (W)(bal_x >> lane) & m;
-                    s.by[c.row] = (W)(bal_y >> lane) & m;
-                    s.bz[c.row] = (W)(bal_z >> lane) & m;
-                }
-            } else if (valid && lane == 0) {
-                /* lx == 64: this warp holds half a row; write its 32-bit half */
-                uint32_t* hx32 = reinterpret_cast<uint32_t*>(s.bx);
-                uint32_t* hy32 = reinterpret_cast<uint32_t*>(s.by);
-                uint32_t* hz32 = reinterpret_cast<uint32_t*>(s.bz);
-                const uint32_t half = c.x >> 5;
-                hx32[2 * c.row + half] = bal_x;
-                hy32[2 * c.row + half] = bal_y;
-                hz32[2 * c.row + half] = bal_z;
+            /* L_x dividing 32 (rows of 32 < L_x <= 64 are walked above) */
+            if (valid && c.x == 0) {
+                const W m = (W)((g.lx >= 32) ? 0xffffffffu : ((1u << g.lx) - 1u));
+                s.bx[c.row] = (W)(bal_x >> lane) & m;
+                s.by[c.row] = (W)(bal_y >> lane) & m;
+                s.bz[c.row] = (W)(bal_z >> lane) & m;
             }
         } else {
             /* The warp's 32 consecutive sites cover pieces of a few rows; the
