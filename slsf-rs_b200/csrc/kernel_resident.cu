@@ -363,7 +363,7 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
     __sincosf(phi, &sphi, &cphi);
     const float m2b = __fmul_rn(-2.0f, t.beta);
 
-    if (!g.lx_tiles_warp) {
+    if (!g.lx_tiles_warp && g.lx < 24) { /* the general path below ORs into the rows */
         for (uint32_t r = threadIdx.x; r < g.rows; r += blockDim.x) {
             s.bx[r] = 0;
             s.by[r] = 0;
@@ -403,6 +403,51 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
                     s.bz[row] = bal_z;
                 }
                 ri = ryp;
+            }
+        }
+    } else if (g.lx >= 24) {
+        /* 24 <= L_x < 32: a row is a warp (lane = x; lanes past the row read
+         * the row's first site and keep no bits).  Each warp walks an equal run
+         * of the replica's rows in order (y fastest), so the projection of the
+         * +y row is the next row's own -- two sincos per site instead of
+         * three, and no per-site index division -- except at the first row of
+         * its run and of each plane.  (Narrower rows would leave too many
+         * lanes idle: they take the general path below.) */
+        const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+        const uint32_t nrows = g.rows;
+        const uint32_t r_lo = (uint32_t)((uint64_t)warp * nrows / nwarps);
+        const uint32_t r_hi = (uint32_t)((uint64_t)(warp + 1) * nrows / nwarps);
+        const uint32_t xl = lane < g.lx ? lane : 0u;
+        const uint32_t xsrc = lane + 1u < g.lx ? lane + 1u : 0u;
+        uint32_t z = slsf_fastdiv_div(r_lo, g.div_ly), y = r_lo - z * g.ly;
+        uint32_t zbase = 0, zp_off = 0;
+        float ri = 0.0f, jx = 0.0f, jzz = 0.0f;
+        for (uint32_t row = r_lo; row < r_hi; ++row) {
+            if (row == r_lo || y == 0) { /* a new plane: its couplings, offsets and first row */
+                zbase = z * g.plane;
+                zp_off = (z + 1 == g.lz) ? 0u : (z + 1) * g.plane; /* base of the +z plane */
+                jx = s.jxy[z];
+                jzz = s.jz[z];
+                ri = proj_of(s.th[slot(g, zbase + y * g.lx + xl, (xl + y + z) & 1u)], cphi, sphi);
+            }
+            const uint32_t idx = zbase + y * g.lx + xl;
+            const uint32_t y1 = (y + 1 == g.ly) ? 0u : y + 1;
+            const float ryp = proj_of(s.th[slot(g, zbase + y1 * g.lx + xl, (xl + y1 + z) & 1u)], cphi, sphi);
+            const float rzp = proj_of(s.th[slot(g, zp_off + y * g.lx + xl, (xl + y + z + 1) & 1u)], cphi, sphi);
+            const float rxp = __shfl_sync(0xffffffffu, ri, xsrc);
+            const slsf_u32x4 b = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, idx);
+            const uint32_t bal_x = __ballot_sync(0xffffffffu, wolff_bond_active(jx, ri, rxp, m2b, b.x));
+            const uint32_t bal_y = __ballot_sync(0xffffffffu, wolff_bond_active(jx, ri, ryp, m2b, b.y));
+            const uint32_t bal_z = __ballot_sync(0xffffffffu, wolff_bond_active(jzz, ri, rzp, m2b, b.z));
+            if (lane == 0) {
+                s.bx[row] = bal_x & g.xmask;
+                s.by[row] = bal_y & g.xmask;
+                s.bz[row] = bal_z & g.xmask;
+            }
+            ri = ryp;
+            if (++y == g.ly) {
+                y = 0;
+                ++z;
             }
         }
     } else if (g.lx_tiles_warp) {
