@@ -54,7 +54,8 @@ def batched_tasks(slsf, ctx, orc, specs):
                                         ((48, 48, 48), 1), ((64, 64, 64), 1), ((40, 16, 8), 1), ((64, 8, 6), 1),
                                         ((8, 6, 6), 1), ((4, 4, 10), 2), ((4, 2, 2), 1), ((16, 10, 2), 1),
                                         ((64, 6, 10), 1), ((6, 6, 6), 1), ((10, 10, 10), 2), ((14, 6, 8), 1),
-                                        ((18, 18, 18), 1), ((30, 8, 4), 1), ((34, 34, 34), 1), ((50, 10, 8), 1)])
+                                        ((18, 18, 18), 1), ((30, 8, 4), 1), ((34, 34, 34), 1), ((50, 10, 8), 1),
+                                        ((26, 12, 6), 1), ((28, 6, 10), 2)])
 def test_batched_equals_plain_bitwise(slsf, ctx, orc, dims, wolff):
     ref, _ = plain_run(slsf, ctx, orc, dims, 1.1, seed=42, sweeps=4, wolff=wolff)
     [t] = batched_tasks(slsf, ctx, orc, [(dims, 1.1, 42, wolff, 0, 1, 0, 1)])
