@@ -144,6 +144,8 @@ def lib():
         "or_measure_f32": (None, [_SZ, _SZ, _SZ, _F, _F, _F, C.POINTER(Obs)]),
         "or_correlations_f32": (None, [_SZ, _SZ, _SZ, _F, _SZ, _SZ, _D, _D, _D, _D]),
         "or_bench_tasks": (C.c_int, [_SZ, _SZ, _SZ, _SZ, _D, _D, _D, C.c_double, _SZ, _U64, _SZ, C.c_int, _D, _D]),
+        "or_series_tasks": (C.c_int, [_SZ, _SZ, _SZ, _SZ, _D, _D, _D, C.c_double, _SZ, _U64, _SZ, _SZ, _SZ, C.c_int,
+                                      _D]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -496,3 +498,21 @@ def bench_tasks(dims, jxy, jz, temperatures, width, wolff_steps, seeds, sweeps, 
     _check(lib().or_bench_tasks(n, lx, ly, lz, dptr(a), dptr(b), dptr(t), width, wolff_steps, ptr(s, C.c_uint64),
                                 sweeps, threads, C.byref(sec), C.byref(chk)))
     return sec.value, chk.value
+
+
+def series_tasks(dims, jxy, jz, temperatures, seeds, thermalization, sweeps, n_bins, width=np.pi, wolff_steps=1,
+                 threads=None):
+    """Independent reference-order tasks (FastRng streams) on host threads;
+    returns bin means [n_tasks][n_bins][SERIES_COLS] of each task's measured
+    series (`sweeps` a multiple of `n_bins`).  jxy/jz are [n_tasks][lz]."""
+    lx, ly, lz = dims
+    n = len(temperatures)
+    a = np.ascontiguousarray(jxy, np.float64).reshape(n, lz)
+    b = np.ascontiguousarray(jz, np.float64).reshape(n, lz)
+    t = np.ascontiguousarray(temperatures, np.float64)
+    s = np.ascontiguousarray(seeds, np.uint64)
+    out = np.zeros((n, n_bins, SERIES_COLS))
+    threads = threads or os.cpu_count() or 1
+    _check(lib().or_series_tasks(n, lx, ly, lz, dptr(a), dptr(b), dptr(t), width, wolff_steps, ptr(s, C.c_uint64),
+                                 thermalization, sweeps, n_bins, threads, dptr(out)))
+    return out

@@ -1103,4 +1103,50 @@ int or_bench_tasks(size_t n_tasks, size_t lx, size_t ly, size_t lz, const double
     return status.load();
 }
 
+/* ---- independent reference-order tasks with binned series (2-sigma checks) ---- */
+int or_series_tasks(size_t n_tasks, size_t lx, size_t ly, size_t lz, const double* jxy,
+                    const double* jz, const double* temperature, double width, size_t wolff_steps,
+                    const uint64_t* seeds, size_t thermalization, size_t sweeps, size_t n_bins,
+                    int threads, double* bin_means) {
+    /* Each task is ThetaModel::new + init + the Runner's loop of sweep and
+     * measure (src/model.rs:314-442), its measurement stream cut into n_bins
+     * bins of equal length (carlo's bins, pinned by src/tests.rs:436-446). */
+    if (n_bins == 0 || sweeps % n_bins != 0) return fail("sweeps must be a positive multiple of n_bins");
+    if (threads < 1) threads = 1;
+    const size_t binsize = sweeps / n_bins;
+    std::atomic<size_t> next{0};
+    std::atomic<int> status{0};
+    auto worker = [&]() {
+        std::vector<double> series(sweeps * OR_SERIES_COLS);
+        for (;;) {
+            const size_t t = next.fetch_add(1);
+            if (t >= n_tasks || status.load()) return;
+            or_model* m = nullptr;
+            if (or_model_new(lx, ly, lz, jxy + t * lz, lz, jz + t * lz, lz, temperature[t], width,
+                             wolff_steps, seeds[t], &m)) {
+                status = 1;
+                return;
+            }
+            or_model_init(m, 0);
+            if (or_model_run_series(m, thermalization, sweeps, host_batch8(), series.data(), nullptr)) {
+                status = 1;
+                or_model_free(m);
+                return;
+            }
+            or_model_free(m);
+            double* out = bin_means + t * n_bins * OR_SERIES_COLS;
+            for (size_t b = 0; b < n_bins; ++b)
+                for (int c = 0; c < OR_SERIES_COLS; ++c) {
+                    double acc = 0;
+                    for (size_t i = 0; i < binsize; ++i) acc += series[(b * binsize + i) * OR_SERIES_COLS + c];
+                    out[b * OR_SERIES_COLS + c] = acc / (double)binsize;
+                }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int k = 0; k < threads; ++k) pool.emplace_back(worker);
+    for (auto& th : pool) th.join();
+    return status.load();
+}
+
 }  // extern "C"

@@ -191,6 +191,15 @@ int or_bench_tasks(size_t n_tasks, size_t lx, size_t ly, size_t lz, const double
                    size_t wolff_steps, const uint64_t* seeds, size_t sweeps, int threads,
                    double* seconds, double* checksum);
 
+/* Independent tasks in the reference's order (FastRng streams), each run
+ * for `thermalization` + `sweeps` sweeps with a measurement after every
+ * measured sweep; bin_means is [n_tasks][n_bins][OR_SERIES_COLS], n_bins
+ * equal bins of the measured series (sweeps must be a multiple of n_bins). */
+int or_series_tasks(size_t n_tasks, size_t lx, size_t ly, size_t lz, const double* jxy,
+                    const double* jz, const double* temperature, double proposal_width,
+                    size_t wolff_steps, const uint64_t* seeds, size_t thermalization, size_t sweeps,
+                    size_t n_bins, int threads, double* bin_means);
+
 #ifdef __cplusplus
 }
 #endif

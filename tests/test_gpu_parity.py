@@ -1,6 +1,6 @@
 """GPU parity against the oracle through the C ABI (marked gpu).
 
-Bars (also stated in DESIGN.md):
+Bars:
   - initial angles, proposals, reflections: bit-exact FP32 (shared Philox
     streams and explicitly rounded FP32 operations);
   - Metropolis decisions: identical on every site whose accept probability
@@ -147,6 +147,55 @@ def test_wolff_cluster_bit_exact(slsf, ctx, orc, dims, T):
             assert np.array_equal(after.view(np.uint32), expect.view(np.uint32))
         assert np.array_equal(after[~members], before[~members])
         assert 1 <= dbg["size"] <= t.volume
+
+
+def test_large_lattice_near_transition_decisions_and_cluster(slsf, ctx, orc):
+    """Large lattice near the transition (L = 256, 16.8M sites, J_xy = 1.2,
+    J_z ~ U[0.5, 1.5], T = 1.22), where Wolff clusters span the lattice: from
+    the cold state and 20 device sweeps (Metropolis + Wolff), both colour
+    half-sweeps' accept decisions equal the oracle's outside the tie band, and
+    two Wolff updates' bonds equal the oracle's outside their tie band with
+    the cluster bit-exact against the oracle's DFS of the device bonds
+    (src/updates.rs:238-271, :551-620)."""
+    L, T, seed = 256, 1.22, 4242
+    dims = (L, L, L)
+    t, jxy, jz = make_task(slsf, ctx, orc, dims, T, seed=seed)
+    t.init_cold()
+    t.sweep(20)
+    beta = np.float32(1.0 / T)
+    jx32, jz32 = jxy.astype(np.float32), jz.astype(np.float32)
+    sweep = t.counters[0]
+    ties = 0
+    for colour in (0, 1):
+        before = t.theta
+        acc, mask = t.metropolis_color(colour)
+        ref = orc.keyed_metro_half(dims, before, jx32, jz32, beta, np.float32(math.pi), seed, sweep, colour,
+                                   EPS_METRO)
+        sure = (ref["decision"] >= 0) & (ref["tie"] == 0)
+        assert np.array_equal(mask[sure], ref["decision"][sure].astype(np.uint8))
+        assert acc == int(mask.sum())
+        ties += int(ref["tie"].sum())
+    assert ties <= 4 * EPS_METRO * t.volume, ties
+    fractions = []
+    w0 = t.counters[1]
+    for step in range(2):
+        t.counters = (sweep, w0 + step)  # a Wolff update's randoms are keyed by the Wolff counter
+        before = t.theta
+        dbg = t.wolff_step_debug()
+        ref = orc.keyed_wolff(dims, before, jx32, jz32, beta, seed, w0 + step, 0, EPS_WOLFF)
+        phi, site = orc.keyed_wolff_pick(dims, seed, w0 + step, 0)
+        assert dbg["phi"] == phi and dbg["seed_site"] == site
+        tie_bits = (ref["bonds"] >> 3) & 7
+        differ = (dbg["bonds"] ^ ref["bonds"]) & 7
+        assert np.all((differ & ~tie_bits) == 0)
+        seed_idx = site[0] + L * (site[1] + L * site[2])
+        cl, size = orc.cluster_from_bonds(dims, dbg["bonds"], seed_idx)
+        assert size == dbg["size"]
+        assert np.array_equal(cl, dbg["cluster"])
+        members = dbg["cluster"] == 1
+        assert np.array_equal(t.theta[~members], before[~members])
+        fractions.append(size / t.volume)
+    print(f"L=256 T=1.22: {ties} Metropolis tie sites, Wolff cluster fractions {fractions}")
 
 
 @pytest.mark.parametrize("dims", [(8, 8, 8), (16, 8, 4), (64, 64, 64), (30, 14, 22)])

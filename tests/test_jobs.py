@@ -247,10 +247,13 @@ def test_couplings_equal_host_draw(jobs, slsf):
         assert set(jx) <= {0.5, 1.5} and set(np.round(jz, 12)) <= {0.0, 0.2}
 
 
-REFERENCE_EXAMPLES = "/root/reference/examples"
+# Directory of the reference's example job files (its `examples/`), given by
+# the environment; the test is skipped where it is not set.
+REFERENCE_EXAMPLES = os.environ.get("SLSF_REFERENCE_EXAMPLES", "")
 
 
-@pytest.mark.skipif(not os.path.isdir(REFERENCE_EXAMPLES), reason="the reference's example job files are not here")
+@pytest.mark.skipif(not REFERENCE_EXAMPLES or not os.path.isdir(REFERENCE_EXAMPLES),
+                    reason="SLSF_REFERENCE_EXAMPLES does not name the reference's example job files")
 def test_reference_example_job_files_parse_and_expand(jobs):
     # Every job file the reference ships parses, and expands to one task per
     # lattice x dJxy x dJz x T x sample with the reference's name format.
