@@ -14,8 +14,9 @@ whole 2000-sweep job.  The state (512 MiB FP32) is larger than L2.
 
 Under torchrun (N > 1) every rank runs its own 4096 replicas (weak scaling,
 no data-path collective); the time is the max over ranks of the CUDA-event
-time.  `--impl reference` times the CPU restatement of the reference path on
-the host cores instead (rank 0 only).
+time.  `--impl reference` times the CPU restatement of the reference path
+(its vectorised Metropolis batches on glibc's vector math library) on the
+host cores instead (rank 0 only).
 """
 import argparse
 import json
@@ -174,8 +175,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def host_description():
+    """CPU model, logical CPUs, physical cores and the baseline build in use."""
+    import oracle
+
+    cpu = oracle.host_cpu()
+    return {"cpu_model": cpu["model"], "logical_cpus": cpu["logical_cpus"], "physical_cores": cpu["physical_cores"],
+            "build": oracle.baseline_lib().name + (" (8-lane AVX-512 batches)" if cpu["avx512f"] else
+                                                   " (4-lane AVX2 batches)")}
+
+
+BASELINE_LABEL = ("FP64 C++ restatement of SLSF-rs in the reference's order, Metropolis batches on glibc's vector "
+                  "sincos/exp as the reference's on sleef's (not the Rust binary)")
+
+
 def cpu_baseline(L, temps, sweeps_hint, seconds, threads=None):
-    """Time the oracle's reference-order CPU path on all host threads on a
+    """Time the reference-order CPU path with the reference's vectorised
+    Metropolis batches (oracle/baseline_simd.cpp) on all host threads on a
     bounded sample of the workload: one L^3 replica per thread (rank-per-task,
     src/model.rs:680-685), sized to run about `seconds`."""
     import oracle
@@ -184,18 +200,20 @@ def cpu_baseline(L, temps, sweeps_hint, seconds, threads=None):
     jxy = np.full(L, 1.2)
     jz = oracle.uniform_disorder(L, 0.5, 1.5, BASE_SEED)
     # calibrate with one replica x 2 sweeps on one thread
-    t1, _ = oracle.bench_tasks((L, L, L), jxy, jz, [temps[0]], math.pi, 1, [1], 2, 1)
+    t1, _ = oracle.bench_tasks((L, L, L), jxy, jz, [temps[0]], math.pi, 1, [1], 2, 1, simd=True)
     per_sweep = t1 / 2
     sweeps = max(2, min(sweeps_hint, int(seconds / max(per_sweep, 1e-9))))
     n = threads
     tt = [temps[i % len(temps)] for i in range(n)]
     sec, chk = oracle.bench_tasks((L, L, L), np.tile(jxy, n), np.tile(jz, n), tt, math.pi, 1,
-                                  [BASE_SEED + i for i in range(n)], sweeps, threads)
+                                  [BASE_SEED + i for i in range(n)], sweeps, threads, simd=True)
     updates = n * sweeps * L ** 3
-    return {"value": updates / sec, "unit": "site-updates/s", "cores": threads, "kind": "port",
-            "sample": f"{n} replicas of L={L} x {sweeps} sweeps (Metropolis + 1 Wolff + measure each), "
-                      f"{threads} threads, FP64 C++ restatement of SLSF-rs (not the Rust binary)",
-            "seconds": sec}
+    out = {"value": updates / sec, "unit": "site-updates/s", "cores": threads, "kind": "port",
+           "sample": f"{n} replicas of L={L} x {sweeps} sweeps (Metropolis + 1 Wolff + measure each), "
+                     f"{threads} threads, {BASELINE_LABEL}",
+           "seconds": sec}
+    out.update(host_description())
+    return out
 
 
 def cpu_plain(L=64, T=1.3, sweeps_hint=1000, seconds=8.0):
@@ -206,12 +224,12 @@ def cpu_plain(L=64, T=1.3, sweeps_hint=1000, seconds=8.0):
 
     jxy = np.full(L, 1.2)
     jz = oracle.uniform_disorder(L, 0.5, 1.5, BASE_SEED)
-    t1, _ = oracle.bench_tasks((L, L, L), jxy, jz, [T], math.pi, 1, [BASE_SEED], 2, 1)
+    t1, _ = oracle.bench_tasks((L, L, L), jxy, jz, [T], math.pi, 1, [BASE_SEED], 2, 1, simd=True)
     sweeps = max(2, min(sweeps_hint, int(seconds / max(t1 / 2, 1e-9))))
-    sec, _ = oracle.bench_tasks((L, L, L), jxy, jz, [T], math.pi, 1, [BASE_SEED], sweeps, 1)
+    sec, _ = oracle.bench_tasks((L, L, L), jxy, jz, [T], math.pi, 1, [BASE_SEED], sweeps, 1, simd=True)
     return {"value": sweeps * L ** 3 / sec, "unit": "site-updates/s", "cores": 1, "kind": "port",
             "sample": f"c1 single replica L={L}, T={T}, {sweeps} of its {sweeps_hint} sweeps (Metropolis + 1 Wolff + "
-                      "measure each), 1 thread, FP64 C++ restatement of SLSF-rs (not the Rust binary)",
+                      f"measure each), 1 thread, {BASELINE_LABEL}",
             "seconds": sec}
 
 
@@ -237,8 +255,8 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"c2 batched replicas: L={L}, J_xy=1.2, J_z~U[0.5,1.5], T in [1.1,1.5], "
                                "Metropolis + 1 Wolff + measure per sweep", "L": L},
-        "cpu_baseline": {"value": value, "unit": "site-updates/s", "cores": threads, "kind": "port",
-                         "sample": r["sample"]},
+        "cpu_baseline": dict({"value": value, "unit": "site-updates/s", "cores": threads, "kind": "port",
+                              "sample": r["sample"]}, **host_description()),
         "e2e": {"value": value, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

@@ -72,7 +72,8 @@ class OracleError(RuntimeError):
 
 
 def build(force: bool = False) -> str:
-    if force or not os.path.exists(LIB_PATH):
+    if force or not all(os.path.exists(os.path.join(HERE, "_build", n))
+                        for n in ("liboracle.so", "libbaseline_v4.so", "libbaseline_v3.so")):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 
@@ -486,8 +487,65 @@ def correlations_f32(dims, theta, rmax_xy, rmax_z):
             "corr_z": cz[:rmax_z]}
 
 
-def bench_tasks(dims, jxy, jz, temperatures, width, wolff_steps, seeds, sweeps, threads):
-    """Time independent tasks on `threads` host threads (the CPU baseline)."""
+def host_cpu():
+    """The host CPU: model name, logical CPUs, physical cores and AVX-512F support (/proc/cpuinfo)."""
+    model, flags, cores = "unknown", set(), set()
+    phys = core = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                key, _, val = line.partition(":")
+                key, val = key.strip(), val.strip()
+                if key == "model name":
+                    model = val
+                elif key == "flags" and not flags:
+                    flags = set(val.split())
+                elif key == "physical id":
+                    phys = val
+                elif key == "core id":
+                    core = val
+                elif not key and phys is not None:
+                    cores.add((phys, core))
+                    phys = core = None
+        if phys is not None:
+            cores.add((phys, core))
+    except OSError:
+        pass
+    logical = os.cpu_count() or 1
+    return {"model": model, "logical_cpus": logical, "physical_cores": len(cores) or logical,
+            "avx512f": "avx512f" in flags}
+
+
+_baseline = None
+
+
+def baseline_lib():
+    """The timed CPU baseline (baseline_simd.cpp): the AVX-512 build on hosts with AVX-512F, else the AVX2 build."""
+    global _baseline
+    if _baseline is not None:
+        return _baseline
+    build()
+    name = "libbaseline_v4.so" if host_cpu()["avx512f"] else "libbaseline_v3.so"
+    L = C.CDLL(os.path.join(HERE, "_build", name))
+    L.or_bench_tasks.restype = C.c_int
+    L.or_bench_tasks.argtypes = [_SZ, _SZ, _SZ, _SZ, _D, _D, _D, C.c_double, _SZ, _U64, _SZ, C.c_int, _D, _D]
+    L.or_series_tasks.restype = C.c_int
+    L.or_series_tasks.argtypes = [_SZ, _SZ, _SZ, _SZ, _D, _D, _D, C.c_double, _SZ, _U64, _SZ, _SZ, _SZ, C.c_int, _D]
+    L.or_last_error.restype = C.c_char_p
+    L.or_last_error.argtypes = []
+    L.name = name
+    _baseline = L
+    return L
+
+
+def _check_lib(L, code):
+    if code != 0:
+        raise OracleError(L.or_last_error().decode("utf-8"))
+
+
+def bench_tasks(dims, jxy, jz, temperatures, width, wolff_steps, seeds, sweeps, threads, simd=False):
+    """Time independent tasks on `threads` host threads (the CPU baseline).  simd=True runs the
+    SIMD build (the reference's vectorised Metropolis batches), else the scalar oracle."""
     lx, ly, lz = dims
     n = len(temperatures)
     a = np.ascontiguousarray(jxy, np.float64).reshape(n, lz)
@@ -495,13 +553,14 @@ def bench_tasks(dims, jxy, jz, temperatures, width, wolff_steps, seeds, sweeps, 
     t = np.ascontiguousarray(temperatures, np.float64)
     s = np.ascontiguousarray(seeds, np.uint64)
     sec, chk = C.c_double(), C.c_double()
-    _check(lib().or_bench_tasks(n, lx, ly, lz, dptr(a), dptr(b), dptr(t), width, wolff_steps, ptr(s, C.c_uint64),
-                                sweeps, threads, C.byref(sec), C.byref(chk)))
+    L = baseline_lib() if simd else lib()
+    _check_lib(L, L.or_bench_tasks(n, lx, ly, lz, dptr(a), dptr(b), dptr(t), width, wolff_steps,
+                                   ptr(s, C.c_uint64), sweeps, threads, C.byref(sec), C.byref(chk)))
     return sec.value, chk.value
 
 
 def series_tasks(dims, jxy, jz, temperatures, seeds, thermalization, sweeps, n_bins, width=np.pi, wolff_steps=1,
-                 threads=None):
+                 threads=None, simd=False):
     """Independent reference-order tasks (FastRng streams) on host threads;
     returns bin means [n_tasks][n_bins][SERIES_COLS] of each task's measured
     series (`sweeps` a multiple of `n_bins`).  jxy/jz are [n_tasks][lz]."""
@@ -513,6 +572,7 @@ def series_tasks(dims, jxy, jz, temperatures, seeds, thermalization, sweeps, n_b
     s = np.ascontiguousarray(seeds, np.uint64)
     out = np.zeros((n, n_bins, SERIES_COLS))
     threads = threads or os.cpu_count() or 1
-    _check(lib().or_series_tasks(n, lx, ly, lz, dptr(a), dptr(b), dptr(t), width, wolff_steps, ptr(s, C.c_uint64),
-                                 thermalization, sweeps, n_bins, threads, dptr(out)))
+    L = baseline_lib() if simd else lib()
+    _check_lib(L, L.or_series_tasks(n, lx, ly, lz, dptr(a), dptr(b), dptr(t), width, wolff_steps,
+                                    ptr(s, C.c_uint64), thermalization, sweeps, n_bins, threads, dptr(out)))
     return out

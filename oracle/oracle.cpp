@@ -164,6 +164,52 @@ bool step_at(or_model& m, double width, double beta, size_t idx, size_t x, size_
     return false;
 }
 
+/* The batched transcendental functions of the 8- and 4-lane Metropolis
+ * batches (src/fast_math.rs:3-25).  The oracle evaluates them lane by lane
+ * with glibc's scalar sin, cos and exp.  The timed CPU baseline compiles this
+ * file a second time with OR_SIMD_BASELINE (baseline_simd.cpp), which
+ * supplies the same three functions on glibc's vector math library, as the
+ * reference calls sleef's vector functions there. */
+#ifndef OR_SIMD_BASELINE
+template <int LANES>
+inline void batch_sincos(const double* x, double* s, double* c) {
+    for (int lane = 0; lane < LANES; ++lane) {
+        s[lane] = std::sin(x[lane]);
+        c[lane] = std::cos(x[lane]);
+    }
+}
+template <int LANES>
+inline void batch_exp(const double* x, double* y) {
+    for (int lane = 0; lane < LANES; ++lane) y[lane] = std::exp(x[lane]);
+}
+#endif
+
+/* metropolis_accept_probabilities (src/updates.rs:21-53): the uphill lanes'
+ * arguments are packed; with at least 3 of 8 (2 of 4) uphill lanes the packed
+ * exp runs, otherwise the scalar exp per uphill lane. */
+template <int LANES>
+inline void accept_probabilities(const double* de, double beta, double* prob) {
+    double arg[LANES] = {0};
+    int lane_of[LANES];
+    int uphill = 0;
+    for (int lane = 0; lane < LANES; ++lane) {
+        prob[lane] = 1.0;
+        if (de[lane] > 0.0) {
+            arg[uphill] = -de[lane] * beta;
+            lane_of[uphill] = lane;
+            ++uphill;
+        }
+    }
+    const int min_uphill = LANES == 8 ? 3 : (LANES == 4 ? 2 : LANES);
+    if (uphill >= min_uphill) {
+        double packed[LANES];
+        batch_exp<LANES>(arg, packed);
+        for (int k = 0; k < uphill; ++k) prob[lane_of[k]] = packed[k];
+    } else {
+        for (int k = 0; k < uphill; ++k) prob[lane_of[k]] = std::exp(arg[k]);
+    }
+}
+
 /* local_metropolis_step_x_batch (src/updates.rs:302-356): proposals for all
  * lanes first, then the accept draws in lane order, each only when the lane
  * is uphill (the `||` short-circuit at :349). */
@@ -179,15 +225,10 @@ size_t step_batch(or_model& m, double width, double beta, size_t x0, size_t y, s
         local_field(m, idx, x, y, z, hx[lane], hy[lane]);
         old_e[lane] = -(m.cos_t[idx] * hx[lane] + m.sin_t[idx] * hy[lane]);
     }
-    for (int lane = 0; lane < LANES; ++lane) {
-        ns[lane] = std::sin(nw[lane]);
-        nc[lane] = std::cos(nw[lane]);
-        de[lane] = -(nc[lane] * hx[lane] + ns[lane] * hy[lane]) - old_e[lane];
-    }
-    /* metropolis_accept_probabilities (:22-53): the packed and scalar exp are
-     * the same function here (sleef packed == scalar to 1e-14). */
+    batch_sincos<LANES>(nw, ns, nc);
+    for (int lane = 0; lane < LANES; ++lane) de[lane] = -(nc[lane] * hx[lane] + ns[lane] * hy[lane]) - old_e[lane];
     double prob[LANES];
-    for (int lane = 0; lane < LANES; ++lane) prob[lane] = de[lane] > 0.0 ? std::exp(-de[lane] * beta) : 1.0;
+    accept_probabilities<LANES>(de, beta, prob);
     size_t accepted = 0;
     for (int lane = 0; lane < LANES; ++lane) {
         if (de[lane] <= 0.0 || rng_f64(&m.rng) < prob[lane]) {
