@@ -646,9 +646,8 @@ int slsf_task_wolff_step_debug(slsf_task* t, uint8_t* bonds, uint8_t* cluster, f
     }
     float phi_h = 0;
     uint32_t site[3] = {0, 0, 0};
-    slsf::launch_wolff(t->view(), t->wolff_done, t->bonds, t->parent, (uint8_t*)d_cluster, t->ctx->stream, &phi_h,
-                       site);
-    t->ctx->launches += 4;
+    t->ctx->launches += slsf::launch_wolff(t->view(), t->wolff_done, t->bonds, t->parent, (uint8_t*)d_cluster,
+                                           t->ctx->stream, &phi_h, site, bonds != nullptr);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && bonds)
         e = cudaMemcpyAsync(bonds, t->bonds, t->volume, cudaMemcpyDeviceToHost, t->ctx->stream);
@@ -684,9 +683,9 @@ int slsf_task_sweep(slsf_task* t, uint32_t n_sweeps, slsf_sweep_stats* stats) {
         t->metro_sweeps += 1;
         t->ctx->launches += 2;
         for (uint32_t k = 0; k < t->wolff_steps; ++k) {
-            slsf::launch_wolff(v, t->wolff_done, t->bonds, t->parent, nullptr, t->ctx->stream, nullptr, nullptr);
+            t->ctx->launches +=
+                slsf::launch_wolff(v, t->wolff_done, t->bonds, t->parent, nullptr, t->ctx->stream, nullptr, nullptr);
             t->wolff_done += 1;
-            t->ctx->launches += 4;
         }
     }
     SLSF_CUDA(cudaGetLastError());
@@ -1078,9 +1077,8 @@ static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v, 
         slsf::launch_metro_colour(v, sweep, 1, nullptr, st);
         ctx->launches += 2;
         for (uint32_t k = 0; k < t->wolff_steps; ++k) {
-            slsf::launch_wolff(v, t->wolff_done + (uint64_t)sw * t->wolff_steps + k, t->bonds, t->parent, nullptr,
-                               st, nullptr, nullptr);
-            ctx->launches += 4;
+            ctx->launches += slsf::launch_wolff(v, t->wolff_done + (uint64_t)sw * t->wolff_steps + k, t->bonds,
+                                                t->parent, nullptr, st, nullptr, nullptr);
         }
         const uint64_t done = sweep + 1;
         if (done > t->thermalization && t->n_bins) {

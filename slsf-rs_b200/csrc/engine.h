@@ -75,8 +75,20 @@ int report_error(int code, const std::string& message);
 void launch_init_random(float* theta, uint32_t volume, uint64_t seed, cudaStream_t s);
 void launch_metro_colour(const TaskView& t, uint64_t sweep, uint32_t colour, uint8_t* record,
                          cudaStream_t s);
-void launch_wolff(const TaskView& t, uint64_t wolff_counter, uint8_t* bonds, uint32_t* parent,
-                  uint8_t* cluster_out, cudaStream_t s, float* phi_out, uint32_t seed_site[3]);
+/* One Wolff update; returns the number of kernels launched.  bonds [V] and
+ * parent [V] are the task's scratch; with record_bonds the per-site bond
+ * bits (+x, +y, +z in bits 0-2) are left in `bonds`. */
+int launch_wolff(const TaskView& t, uint64_t wolff_counter, uint8_t* bonds, uint32_t* parent,
+                 uint8_t* cluster_out, cudaStream_t s, float* phi_out, uint32_t seed_site[3],
+                 bool record_bonds = false);
+/* ---- Wolff on bit-packed bonds, the seed's cluster only (kernel_wolff_bits.cu) ---- */
+/* Sides that are multiples of 32 (regions of 32^3 sites). */
+bool wolff_bits_supports(uint32_t lx, uint32_t ly, uint32_t lz);
+uint64_t wolff_bits_scratch_bytes(uint32_t lx, uint32_t ly, uint32_t lz);
+/* `scratch` holds wolff_bits_scratch_bytes(); bond_bytes (or NULL) receives
+ * the per-site bond bits, cluster_out (or NULL) the cluster mask. */
+int launch_wolff_bits(const TaskView& t, uint64_t counter, void* scratch, uint8_t* bond_bytes, uint8_t* cluster_out,
+                      cudaStream_t s, float* phi_out, uint32_t seed_site[3]);
 /* Fused observables: writes 8 FP64 sums (mx, my, cos xyz, sin xyz) to result. */
 void launch_measure(const TaskView& t, double* partials, unsigned int* done, double* result,
                     cudaStream_t s);

@@ -1,0 +1,509 @@
+/*
+ * Single-task Wolff update on bit-packed bonds: grows the seed's cluster
+ * only, for lattices whose three sides are multiples of 32 (the large
+ * single-replica lattices: L = 64 ... 256 and more).
+ *
+ * Replaces, for those shapes, the whole-lattice union-find labelling of
+ * kernels_plain.cu.  The reference grows one cluster from a random seed by
+ * depth-first search (wolff_cluster_step_with_theta_scratch,
+ * src/updates.rs:551-620); with one counter-based random per bond, that
+ * cluster is the seed's connected component over the active bonds, and only
+ * it is needed.
+ *
+ *   k_wb_bonds   per-site +x/+y/+z bond activation (try_add_wolff_neighbor,
+ *                src/updates.rs:537-548) into three bit planes: bit i of the
+ *                flat bitmap is site i (site index x + Lx (y + Ly z), so a
+ *                32-bit word is 32 consecutive sites of one row); clears the
+ *                cluster bitmap and sets the seed's bit, and queues the
+ *                seed's region.
+ *   k_wb_grow    the cluster over the active bonds.  The lattice is cut into
+ *                regions of 32 x 32 x 32 sites (one word wide, 32 rows, 32
+ *                planes).  A CTA takes a region from a work queue, reads its
+ *                cluster and bond words into shared memory with the bits that
+ *                enter through the region's faces, closes the region in
+ *                passes (each pass a full warp scan along y -- lane = y -- or
+ *                along z -- lane = z, the shared array read transposed --
+ *                one step along the other axis, and the closure along x
+ *                inside each word), ORs the result back and queues every
+ *                neighbour region its bits can enter.  Regions are processed
+ *                as they are queued, with no grid-wide barrier: CTAs only
+ *                wait for work that running CTAs hold, so the kernel needs
+ *                no co-residency.  Bits only ever get set, so the fixed point
+ *                is the seed's component whatever the order.
+ *   k_wb_flip    reflection of the cluster's sites (src/updates.rs:602-617)
+ *                and its size.
+ *
+ * Every wait and loop is bounded; past a bound the kernel sets
+ * kErrGrowthLimit in the task's error word and returns.
+ */
+#include <algorithm>
+
+#include "engine.h"
+#include "xy_device.cuh"
+
+namespace slsf {
+
+namespace {
+
+constexpr uint32_t kRegion = 32; /* region edge in sites along y and z; one word along x */
+constexpr uint32_t kGrowThreads = kRegion * kRegion;
+constexpr int kBondThreads = 256;
+constexpr int kFlipThreads = 256;
+constexpr uint32_t kEmpty = 0;
+
+/* Scratch of one update, carved from the task's union-find array. */
+struct WolffBits {
+    uint32_t* bx;      /* bond bit planes, one bit per site */
+    uint32_t* by;
+    uint32_t* bz;
+    uint32_t* cl;      /* cluster bitmap */
+    uint32_t* queued;  /* [regions] 1 while the region is in the queue */
+    uint32_t* ring;    /* [cap] region + 1, or 0 */
+    uint32_t* ctl;     /* head, tail, pending (queued or in flight), abort */
+    uint32_t regions, cap;
+};
+
+__host__ __device__ inline uint64_t round256(uint64_t b) { return (b + 255) & ~255ull; }
+
+/* Periodic rotations of a 32-bit row word (L_x == 32: the row is one word). */
+__device__ __forceinline__ uint32_t rotl32(uint32_t w, uint32_t s) { return __funnelshift_l(w, w, s); }
+__device__ __forceinline__ uint32_t rotr32(uint32_t w, uint32_t s) { return __funnelshift_r(w, w, s); }
+
+/* Closure of the cluster bits c of one word along x through its bonds b
+ * (bit j: bond j -- j+1), by doubling in both directions.  periodic: the
+ * word is a whole row (L_x == 32) and bit 31 bonds to bit 0; otherwise the
+ * word is open at both ends (bits crossing words enter between passes). */
+__device__ __forceinline__ uint32_t close_word(uint32_t c, uint32_t b, bool periodic) {
+    if (periodic) {
+        uint32_t gr = c, pr = b, gl = c, pl = rotl32(b, 1);
+#pragma unroll
+        for (uint32_t s = 1; s < 32; s <<= 1) {
+            gr |= rotl32(gr & pr, s);
+            pr &= rotr32(pr, s);
+            gl |= rotr32(gl & pl, s);
+            pl &= rotl32(pl, s);
+        }
+        return gr | gl;
+    }
+    /* open word: bond bit 31 leads out of the word and is not used here */
+    const uint32_t bi = b & 0x7fffffffu;
+    uint32_t gr = c, pr = bi, gl = c, pl = bi << 1;
+#pragma unroll
+    for (uint32_t s = 1; s < 32; s <<= 1) {
+        gr |= (gr & pr) << s;
+        pr &= pr >> s;
+        gl |= (gl & pl) >> s;
+        pl &= pl << s;
+    }
+    return gr | gl;
+}
+
+/* Closure along a line of 32 words held one per lane (lane = position):
+ * bit x of lane i passes to lane i+1 when bit x of p (the lane's bond to the
+ * next position) is set.  Doubling in both directions; periodic lines wrap
+ * from lane 31 to lane 0. */
+__device__ __forceinline__ uint32_t close_line(uint32_t c, uint32_t p, bool periodic) {
+    const uint32_t lane = threadIdx.x & 31u;
+    /* upward: G(i) |= P(i) & G(i - s), P(i) = bonds i-1 -> i over the span */
+    uint32_t g = c;
+    uint32_t q = __shfl_sync(0xffffffffu, p, (lane + 31u) & 31u);
+    if (!periodic && lane == 0) q = 0;
+#pragma unroll
+    for (uint32_t s = 1; s < 32; s <<= 1) {
+        const uint32_t src = (lane - s) & 31u;
+        const uint32_t gs = __shfl_sync(0xffffffffu, g, src);
+        const uint32_t qs = __shfl_sync(0xffffffffu, q, src);
+        if (periodic || lane >= s) {
+            g |= q & gs;
+            q &= qs;
+        }
+    }
+    /* downward: H(i) |= R(i) & H(i + s), R(i) = bonds i -> i+1 over the span */
+    uint32_t h = c;
+    uint32_t r = p;
+    if (!periodic && lane == 31) r = 0;
+#pragma unroll
+    for (uint32_t s = 1; s < 32; s <<= 1) {
+        const uint32_t src = (lane + s) & 31u;
+        const uint32_t hs = __shfl_sync(0xffffffffu, h, src);
+        const uint32_t rs = __shfl_sync(0xffffffffu, r, src);
+        if (periodic || lane + s < 32) {
+            h |= r & hs;
+            r &= rs;
+        }
+    }
+    return g | h;
+}
+
+__device__ __forceinline__ float proj_at(const float* __restrict__ theta, uint32_t i, float cphi, float sphi) {
+    float sn, cn;
+    __sincosf(theta[i], &sn, &cn);
+    return wolff_projection(cn, sn, cphi, sphi);
+}
+
+/* Bond activation.  A warp owns word k of plane z for a run of rows y
+ * (lane = bit = x - 32 k) and walks it along y, so the projection of the +y
+ * row is the next row's own: two sincos per site.  The seed word gets its
+ * bit; the seed's region is queued. */
+__global__ void __launch_bounds__(kBondThreads)
+    k_wb_bonds(const float* __restrict__ theta, const float* __restrict__ jxy, const float* __restrict__ jz,
+               uint32_t lx, uint32_t ly, uint32_t lz, float minus_two_beta, float phi, uint64_t seed,
+               uint64_t counter, WolffBits wb, uint32_t seed_idx, uint32_t seg, uint8_t* __restrict__ bond_bytes) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t words = lx >> 5, nseg = ly / seg;
+    const uint32_t k = wid % words, rest = wid / words;
+    const uint32_t sg = rest % nseg, z = rest / nseg;
+    if (z >= lz) return; /* whole warps */
+    float sphi, cphi;
+    __sincosf(phi, &sphi, &cphi);
+    const uint32_t plane = lx * ly;
+    const uint32_t x = 32u * k + lane;
+    const uint32_t xn = (k + 1 == words) ? 0u : 32u * (k + 1); /* first site of the next word, periodic */
+    const uint32_t zbase = z * plane, zp_base = (z + 1 == lz) ? 0u : (z + 1) * plane;
+    const float jx = jxy[z], jzz = jz[z];
+    const uint32_t y0 = sg * seg;
+    float ri = proj_at(theta, zbase + y0 * lx + x, cphi, sphi);
+    for (uint32_t y = y0; y < y0 + seg; ++y) {
+        const uint32_t row = zbase + y * lx;
+        const uint32_t i = row + x;
+        const uint32_t y1 = (y + 1 == ly) ? 0u : y + 1;
+        const float ryp = proj_at(theta, zbase + y1 * lx + x, cphi, sphi);
+        const float rzp = proj_at(theta, zp_base + y * lx + x, cphi, sphi);
+        const float rnext = proj_at(theta, row + xn, cphi, sphi);
+        float rxp = __shfl_sync(0xffffffffu, ri, (lane + 1u) & 31u);
+        if (lane == 31) rxp = rnext;
+        const slsf_u32x4 b = slsf_stream(seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, i);
+        const bool ax = wolff_bond_active(jx, ri, rxp, minus_two_beta, b.x);
+        const bool ay = wolff_bond_active(jx, ri, ryp, minus_two_beta, b.y);
+        const bool az = wolff_bond_active(jzz, ri, rzp, minus_two_beta, b.z);
+        const uint32_t wx = __ballot_sync(0xffffffffu, ax);
+        const uint32_t wy = __ballot_sync(0xffffffffu, ay);
+        const uint32_t wz = __ballot_sync(0xffffffffu, az);
+        const uint32_t w = i >> 5;
+        if (lane == 0) wb.bx[w] = wx;
+        if (lane == 1) wb.by[w] = wy;
+        if (lane == 2) wb.bz[w] = wz;
+        if (lane == 3) wb.cl[w] = (w == (seed_idx >> 5)) ? (1u << (seed_idx & 31u)) : 0u;
+        if (bond_bytes) bond_bytes[i] = (uint8_t)((ax ? 1u : 0u) | (ay ? 2u : 0u) | (az ? 4u : 0u));
+        ri = ryp;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        /* the seed's region is the first queue entry (the scratch was zeroed) */
+        const uint32_t sx = seed_idx % lx, srow = seed_idx / lx, sy = srow % ly, sz = srow / ly;
+        const uint32_t r = (sx >> 5) + words * ((sy / kRegion) + (ly / kRegion) * (sz / kRegion));
+        wb.queued[r] = 1;
+        wb.ring[0] = r + 1;
+        wb.ctl[1] = 1; /* tail */
+        wb.ctl[2] = 1; /* pending */
+    }
+}
+
+struct GrowGeo {
+    uint32_t lx, ly, lz, words, ry_n, rz_n;
+    bool px, py, pz; /* the region spans the whole period along x (one-word rows), y, z */
+};
+
+/* Queues region r unless it is queued already. */
+__device__ __forceinline__ void push_region(const WolffBits& wb, uint32_t r) {
+    if (atomicExch(&wb.queued[r], 1u) != 0u) return;
+    atomicAdd(&wb.ctl[2], 1u); /* pending before the entry is visible */
+    const uint32_t slot = atomicAdd(&wb.ctl[1], 1u);
+    __threadfence();
+    atomicExch(&wb.ring[slot & (wb.cap - 1)], r + 1);
+}
+
+__device__ __forceinline__ uint32_t region_of(const GrowGeo& g, uint32_t k, uint32_t ry, uint32_t rz) {
+    return k + g.words * (ry + g.ry_n * rz);
+}
+
+/* One region: load with the bits entering through its faces, close in
+ * shared memory, OR back, queue the neighbours its bits can enter.  Returns
+ * false if a pass bound was hit. */
+__device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, uint32_t (*C)[kRegion + 1],
+                            uint32_t (*BY)[kRegion + 1], uint32_t (*BZ)[kRegion + 1], uint32_t (*BX)[kRegion + 1]) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t k = r % g.words, rest = r / g.words, ry = rest % g.ry_n, rz = rest / g.ry_n;
+    const uint32_t rowlen = g.words; /* words per row */
+    const uint32_t gy = ry * kRegion + lane, gz = rz * kRegion + warp;
+    auto word = [&](uint32_t kk, uint32_t yy, uint32_t zz) { return kk + rowlen * (yy + g.ly * zz); };
+    const uint32_t w = word(k, gy, gz);
+    const uint32_t c0 = __ldcg(&wb.cl[w]);
+    const uint32_t bxw = wb.bx[w], byw = wb.by[w], bzw = wb.bz[w];
+    uint32_t c = c0;
+    /* bits entering through the faces */
+    const uint32_t kl = k == 0 ? g.words - 1 : k - 1, kr = k + 1 == g.words ? 0 : k + 1;
+    const uint32_t ym = gy == 0 ? g.ly - 1 : gy - 1, yp = gy + 1 == g.ly ? 0 : gy + 1;
+    const uint32_t zm = gz == 0 ? g.lz - 1 : gz - 1, zp = gz + 1 == g.lz ? 0 : gz + 1;
+    if (!g.px) {
+        const uint32_t wl = word(kl, gy, gz), wr = word(kr, gy, gz);
+        c |= (__ldcg(&wb.cl[wl]) >> 31) & (wb.bx[wl] >> 31);
+        c |= ((__ldcg(&wb.cl[wr]) & 1u) & (bxw >> 31)) << 31;
+    }
+    if (!g.py) {
+        if (lane == 0) {
+            const uint32_t wm = word(k, ym, gz);
+            c |= __ldcg(&wb.cl[wm]) & wb.by[wm];
+        }
+        if (lane == kRegion - 1) c |= __ldcg(&wb.cl[word(k, yp, gz)]) & byw;
+    }
+    if (!g.pz) {
+        if (warp == 0) {
+            const uint32_t wm = word(k, gy, zm);
+            c |= __ldcg(&wb.cl[wm]) & wb.bz[wm];
+        }
+        if (warp == kRegion - 1) c |= __ldcg(&wb.cl[word(k, gy, zp)]) & bzw;
+    }
+    c = close_word(c, bxw, g.px);
+    C[warp][lane] = c;
+    BX[warp][lane] = bxw;
+    BY[warp][lane] = byw;
+    BZ[warp][lane] = bzw;
+    __syncthreads();
+    /* passes: even ones scan y (lane = y, warp = z), odd ones scan z (lane =
+     * z, warp = y); each also takes one step along the other axis and closes
+     * x.  A pass that changes nothing means the region is closed. */
+    bool ok = false;
+    /* every pass that changes something sets a bit: at most 32^3 of them */
+    for (uint32_t pass = 0; pass <= kRegion * kGrowThreads; ++pass) {
+        int changed = 0;
+        if ((pass & 1u) == 0) {
+            const uint32_t z = warp, y = lane;
+            const uint32_t old = C[z][y];
+            uint32_t v = close_line(old, BY[z][y], g.py);
+            if (z > 0) v |= C[z - 1][y] & BZ[z - 1][y];
+            else if (g.pz) v |= C[kRegion - 1][y] & BZ[kRegion - 1][y];
+            if (z + 1 < kRegion) v |= C[z + 1][y] & BZ[z][y];
+            else if (g.pz) v |= C[0][y] & BZ[z][y];
+            v = close_word(v, BX[z][y], g.px);
+            if (v != old) {
+                C[z][y] = v;
+                changed = 1;
+            }
+        } else {
+            const uint32_t z = lane, y = warp;
+            const uint32_t old = C[z][y];
+            uint32_t v = close_line(old, BZ[z][y], g.pz);
+            if (y > 0) v |= C[z][y - 1] & BY[z][y - 1];
+            else if (g.py) v |= C[z][kRegion - 1] & BY[z][kRegion - 1];
+            if (y + 1 < kRegion) v |= C[z][y + 1] & BY[z][y];
+            else if (g.py) v |= C[z][0] & BY[z][y];
+            v = close_word(v, BX[z][y], g.px);
+            if (v != old) {
+                C[z][y] = v;
+                changed = 1;
+            }
+        }
+        if (!__syncthreads_or(changed)) {
+            ok = true;
+            break;
+        }
+    }
+    c = C[warp][lane];
+    if (c != c0) atomicOr(&wb.cl[w], c);
+    __threadfence();
+    /* neighbours that the region's bits can enter */
+    if (!g.px) {
+        const uint32_t wl = word(kl, gy, gz), wr = word(kr, gy, gz);
+        if ((c & 1u) && (wb.bx[wl] >> 31) && !(__ldcg(&wb.cl[wl]) >> 31)) push_region(wb, region_of(g, kl, ry, rz));
+        if ((c >> 31) && (bxw >> 31) && !(__ldcg(&wb.cl[wr]) & 1u)) push_region(wb, region_of(g, kr, ry, rz));
+    }
+    if (!g.py) {
+        if (lane == 0) {
+            const uint32_t wm = word(k, ym, gz);
+            if (c & wb.by[wm] & ~__ldcg(&wb.cl[wm])) push_region(wb, region_of(g, k, ry == 0 ? g.ry_n - 1 : ry - 1, rz));
+        }
+        if (lane == kRegion - 1 && (c & byw & ~__ldcg(&wb.cl[word(k, yp, gz)])))
+            push_region(wb, region_of(g, k, ry + 1 == g.ry_n ? 0 : ry + 1, rz));
+    }
+    if (!g.pz) {
+        if (warp == 0) {
+            const uint32_t wm = word(k, gy, zm);
+            if (c & wb.bz[wm] & ~__ldcg(&wb.cl[wm])) push_region(wb, region_of(g, k, ry, rz == 0 ? g.rz_n - 1 : rz - 1));
+        }
+        if (warp == kRegion - 1 && (c & bzw & ~__ldcg(&wb.cl[word(k, gy, zp)])))
+            push_region(wb, region_of(g, k, ry, rz + 1 == g.rz_n ? 0 : rz + 1));
+    }
+    return ok;
+}
+
+__global__ void __launch_bounds__(kGrowThreads, 1)
+    k_wb_grow(WolffBits wb, GrowGeo g, uint32_t max_items, unsigned long long* __restrict__ stats) {
+    __shared__ uint32_t C[kRegion][kRegion + 1];
+    __shared__ uint32_t BY[kRegion][kRegion + 1];
+    __shared__ uint32_t BZ[kRegion][kRegion + 1];
+    __shared__ uint32_t BX[kRegion][kRegion + 1];
+    __shared__ uint32_t s_item;
+    /* Each CTA pops regions until the queue is empty and no region is in
+     * flight.  A popped entry may still be being written by its producer
+     * (slot claimed, entry not yet stored): the CTA waits for it, bounded. */
+    constexpr uint32_t kSpin = 1u << 24;
+    bool ok = true;
+    for (uint32_t item = 0; item < max_items; ++item) {
+        if (threadIdx.x == 0) {
+            uint32_t got = 0xfffffffeu; /* gave up, unless set below */
+            for (uint32_t spin = 0; spin < kSpin; ++spin) {
+                volatile uint32_t* ctl = wb.ctl;
+                const uint32_t head = ctl[0], tail = ctl[1];
+                if (head < tail) {
+                    if (atomicCAS(&wb.ctl[0], head, head + 1) != head) continue;
+                    volatile uint32_t* slot = &wb.ring[head & (wb.cap - 1)];
+                    uint32_t v = kEmpty;
+                    for (uint32_t s2 = 0; s2 < kSpin && (v = *slot) == kEmpty; ++s2) __nanosleep(32);
+                    if (v != kEmpty) {
+                        *slot = kEmpty;
+                        got = v - 1;
+                    }
+                    break;
+                }
+                if (ctl[2] == 0 || ctl[3] != 0) { /* nothing queued and nothing in flight, or aborted */
+                    got = 0xffffffffu;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            if (got < wb.regions) atomicExch(&wb.queued[got], 0u); /* re-queueable from here on */
+            __threadfence();
+            s_item = got;
+        }
+        __syncthreads();
+        const uint32_t r = s_item;
+        __syncthreads();
+        if (r == 0xffffffffu) break;
+        if (r >= wb.regions) {
+            ok = false;
+            break;
+        }
+        ok &= grow_region(wb, g, r, C, BY, BZ, BX);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicSub(&wb.ctl[2], 1u);
+        }
+        if (item + 1 == max_items) ok = false;
+    }
+    if (!ok && threadIdx.x == 0) {
+        atomicOr(&stats[kStatError], kErrGrowthLimit);
+        atomicExch(&wb.ctl[3], 1u); /* the other CTAs stop at their next pop */
+    }
+}
+
+/* Reflect the cluster's sites, count them; optional byte mask. */
+__global__ void __launch_bounds__(kFlipThreads)
+    k_wb_flip(float* __restrict__ theta, uint32_t volume, const uint32_t* __restrict__ cl, float phi,
+              unsigned long long* __restrict__ stats, uint8_t* __restrict__ cluster_out) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; /* four sites */
+    uint32_t n = 0;
+    if (4ull * q < volume) {
+        const uint32_t i = 4 * q;
+        const uint32_t m = (__ldcg(&cl[i >> 5]) >> (i & 31u)) & 0xfu;
+        if (m) {
+            float4 v = reinterpret_cast<float4*>(theta)[q];
+            if (m & 1u) v.x = slsf_reflect(v.x, phi);
+            if (m & 2u) v.y = slsf_reflect(v.y, phi);
+            if (m & 4u) v.z = slsf_reflect(v.z, phi);
+            if (m & 8u) v.w = slsf_reflect(v.w, phi);
+            reinterpret_cast<float4*>(theta)[q] = v;
+        }
+        n = __popc(m);
+        if (cluster_out) {
+            uchar4 o = make_uchar4(m & 1u, (m >> 1) & 1u, (m >> 2) & 1u, (m >> 3) & 1u);
+            reinterpret_cast<uchar4*>(cluster_out)[q] = o;
+        }
+    }
+    __shared__ unsigned int s_sum;
+    if (threadIdx.x == 0) s_sum = 0;
+    __syncthreads();
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) n += __shfl_down_sync(0xffffffffu, n, off);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(&s_sum, n);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_sum) atomicAdd(&stats[kStatClusterSites], (unsigned long long)s_sum);
+}
+
+uint32_t pow2_at_least(uint32_t n) {
+    uint32_t p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+}  // namespace
+
+bool wolff_bits_supports(uint32_t lx, uint32_t ly, uint32_t lz) {
+    return lx % 32 == 0 && ly % kRegion == 0 && lz % kRegion == 0 && lx > 0 && ly > 0 && lz > 0 &&
+           (uint64_t)lx * ly * lz < (1ull << 31);
+}
+
+uint64_t wolff_bits_scratch_bytes(uint32_t lx, uint32_t ly, uint32_t lz) {
+    const uint64_t words = (uint64_t)lx * ly * lz / 32;
+    const uint64_t regions = words / (kRegion * kRegion);
+    const uint64_t cap = pow2_at_least((uint32_t)(2 * regions + 2));
+    return 4 * round256(4 * words) + round256(4 * regions) + round256(4 * cap) + 256;
+}
+
+int launch_wolff_bits(const TaskView& t, uint64_t counter, void* scratch, uint8_t* bond_bytes, uint8_t* cluster_out,
+                      cudaStream_t s, float* phi_out, uint32_t seed_site[3]) {
+    /* The reflection axis and seed site (src/updates.rs:564-568) from the
+     * WOLFF_PICK block, computed on the host from the shared header. */
+    const slsf_u32x4 pick = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_PICK, 0, 0);
+    const float phi = slsf_angle_from_word(pick.x);
+    const uint32_t x0 = slsf_range(pick.y, t.lx), y0 = slsf_range(pick.z, t.ly), z0 = slsf_range(pick.w, t.lz);
+    const uint32_t volume = t.lx * t.ly * t.lz;
+    const uint32_t seed_idx = x0 + t.lx * (y0 + t.ly * z0);
+    const uint64_t words = volume / 32;
+    WolffBits wb;
+    unsigned char* p = static_cast<unsigned char*>(scratch);
+    wb.bx = reinterpret_cast<uint32_t*>(p);
+    p += round256(4 * words);
+    wb.by = reinterpret_cast<uint32_t*>(p);
+    p += round256(4 * words);
+    wb.bz = reinterpret_cast<uint32_t*>(p);
+    p += round256(4 * words);
+    wb.cl = reinterpret_cast<uint32_t*>(p);
+    p += round256(4 * words);
+    wb.regions = (uint32_t)(words / (kRegion * kRegion));
+    wb.cap = pow2_at_least(2 * wb.regions + 2);
+    unsigned char* control = p;
+    wb.queued = reinterpret_cast<uint32_t*>(p);
+    p += round256(4ull * wb.regions);
+    wb.ring = reinterpret_cast<uint32_t*>(p);
+    p += round256(4ull * wb.cap);
+    wb.ctl = reinterpret_cast<uint32_t*>(p);
+    p += 256;
+    cudaMemsetAsync(control, 0, (size_t)(p - control), s);
+    /* bond kernel: warps walk runs of `seg` rows */
+    const uint32_t seg = 16; /* L_y is a multiple of 32 */
+    const uint64_t warps = (uint64_t)(t.lx / 32) * (t.ly / seg) * t.lz;
+    const uint32_t bond_blocks = (uint32_t)((warps * 32 + kBondThreads - 1) / kBondThreads);
+    k_wb_bonds<<<bond_blocks, kBondThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, -2.0f * t.beta, phi,
+                                                    t.seed, counter, wb, seed_idx, seg, bond_bytes);
+    GrowGeo g;
+    g.lx = t.lx;
+    g.ly = t.ly;
+    g.lz = t.lz;
+    g.words = t.lx / 32;
+    g.ry_n = t.ly / kRegion;
+    g.rz_n = t.lz / kRegion;
+    g.px = g.words == 1;
+    g.py = g.ry_n == 1;
+    g.pz = g.rz_n == 1;
+    int device = 0, sms = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const uint32_t grid = std::min<uint32_t>(wb.regions, (uint32_t)sms);
+    /* every region is processed at most once per bit it gains */
+    const uint32_t max_items = t.loop_limit ? t.loop_limit : std::max<uint32_t>(64, volume / 32);
+    k_wb_grow<<<grid, kGrowThreads, 0, s>>>(wb, g, max_items, t.stats);
+    const uint32_t quads = volume / 4;
+    k_wb_flip<<<(quads + kFlipThreads - 1) / kFlipThreads, kFlipThreads, 0, s>>>(t.theta, volume, wb.cl, phi,
+                                                                                 t.stats, cluster_out);
+    if (phi_out) *phi_out = phi;
+    if (seed_site) {
+        seed_site[0] = x0;
+        seed_site[1] = y0;
+        seed_site[2] = z0;
+    }
+    return 3;
+}
+
+}  // namespace slsf

@@ -481,8 +481,14 @@ void launch_metro_colour(const TaskView& t, uint64_t sweep, uint32_t colour, uin
                                                         t.seed, sweep, colour, dhx, dly, t.stats, nullptr);
 }
 
-void launch_wolff(const TaskView& t, uint64_t counter, uint8_t* bonds, uint32_t* parent,
-                  uint8_t* cluster_out, cudaStream_t s, float* phi_out, uint32_t seed_site[3]) {
+int launch_wolff(const TaskView& t, uint64_t counter, uint8_t* bonds, uint32_t* parent,
+                 uint8_t* cluster_out, cudaStream_t s, float* phi_out, uint32_t seed_site[3], bool record_bonds) {
+    /* Lattices with sides that are multiples of 32 grow the seed's cluster
+     * on bit-packed bonds (kernel_wolff_bits.cu), in the union-find array. */
+    if (wolff_bits_supports(t.lx, t.ly, t.lz) &&
+        wolff_bits_scratch_bytes(t.lx, t.ly, t.lz) <= 4ull * t.lx * t.ly * t.lz)
+        return launch_wolff_bits(t, counter, parent, record_bonds ? bonds : nullptr, cluster_out, s, phi_out,
+                                 seed_site);
     /* The reflection axis and seed site (src/updates.rs:564-568) come from
      * the WOLFF_PICK block, computed here on the host from the same header. */
     const slsf_u32x4 pick = slsf_stream(t.seed, counter, SLSF_PURPOSE_WOLFF_PICK, 0, 0);
@@ -505,6 +511,7 @@ void launch_wolff(const TaskView& t, uint64_t counter, uint8_t* bonds, uint32_t*
         seed_site[1] = y0;
         seed_site[2] = z0;
     }
+    return 4;
 }
 
 int measure_partial_blocks(uint32_t volume) {

@@ -110,11 +110,21 @@ def test_metropolis_width_zero_and_wrap(slsf, ctx, orc):
     assert np.array_equal(t3.theta.view(np.uint32)[same], ref["theta"].view(np.uint32)[same])
 
 
-@pytest.mark.parametrize("dims,T", [((8, 8, 8), 1.1), ((12, 6, 8), 0.9), ((64, 64, 64), 1.3), ((32, 32, 32), 3.0),
-                                    ((40, 12, 6), 1.0), ((96, 16, 10), 0.8), ((128, 24, 10), 1.2)])
-def test_wolff_cluster_bit_exact(slsf, ctx, orc, dims, T):
+@pytest.mark.parametrize("dims,T,cold", [((8, 8, 8), 1.1, False), ((12, 6, 8), 0.9, False), ((64, 64, 64), 1.3, False),
+                                         ((32, 32, 32), 3.0, False), ((40, 12, 6), 1.0, False),
+                                         ((96, 16, 10), 0.8, False), ((128, 24, 10), 1.2, False),
+                                         ((32, 32, 32), 1.1, True), ((64, 64, 64), 1.22, True),
+                                         ((96, 32, 64), 1.5, False), ((128, 64, 32), 1.22, True),
+                                         ((64, 32, 96), 1.3, True)])
+def test_wolff_cluster_bit_exact(slsf, ctx, orc, dims, T, cold):
+    # Sides that are multiples of 32 grow the seed's cluster on bit-packed
+    # bonds; the others label the whole lattice by union-find.  Cold starts
+    # give clusters that span the lattice and cross every region face.
     t, jxy, jz = make_task(slsf, ctx, orc, dims, T, seed=31)
-    t.init_random()
+    if cold:
+        t.init_cold()
+    else:
+        t.init_random()
     for _ in range(2):
         t.metropolis_sweep()
     beta = np.float32(1.0 / T)
