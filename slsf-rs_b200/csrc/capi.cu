@@ -269,7 +269,13 @@ int bind_device(const slsf_ctx* ctx) {
 /* Grows the batched-engine scratch to hold n views. */
 int ensure_batch_capacity(slsf_ctx* ctx, size_t n) {
     if (ctx->views_cap >= n) return SLSF_OK;
-    if (ctx->d_views) SLSF_CUDA(cudaStreamSynchronize(ctx->stream)); /* queued launches may still read them */
+    if (ctx->d_views) {
+        /* queued launches may still read them, on the main stream or on a
+         * side stream that an earlier failed call left unjoined */
+        SLSF_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int k = 0; k < kSideStreams; ++k)
+            if (ctx->side[k]) SLSF_CUDA(cudaStreamSynchronize(ctx->side[k]));
+    }
     if (ctx->d_views) cudaFree(ctx->d_views);
     if (ctx->h_views) cudaFreeHost(ctx->h_views);
     if (ctx->d_rcorr) cudaFree(ctx->d_rcorr);

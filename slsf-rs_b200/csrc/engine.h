@@ -96,6 +96,9 @@ void launch_measure(const TaskView& t, double* partials, unsigned int* done, dou
  * bin_row (a task's bin sums row). */
 void launch_measure_into_bin(const TaskView& t, double* partials, unsigned int* done, double* result,
                              double* bin_row, cudaStream_t s);
+/* Blocks of a measurement launch: one per 256 sites, at most kMeasureMaxBlocks
+ * (148 SMs x 8), so its per-block partial sums fit kMeasureMaxBlocks rows. */
+constexpr int kMeasureMaxBlocks = 148 * 8;
 int measure_partial_blocks(uint32_t volume);
 /* dst[i * per + k] = src[i][k] for i < n, k < per. */
 void launch_gather(const double* const* src, uint32_t n, uint32_t per, double* dst, cudaStream_t s);

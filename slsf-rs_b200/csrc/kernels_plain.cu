@@ -515,7 +515,7 @@ int launch_wolff(const TaskView& t, uint64_t counter, uint8_t* bonds, uint32_t* 
 }
 
 int measure_partial_blocks(uint32_t volume) {
-    return (int)std::max<uint32_t>(1, std::min<uint32_t>(blocks_for(volume, kMeasureThreads), 148 * 8));
+    return (int)std::max<uint32_t>(1, std::min<uint32_t>(blocks_for(volume, kMeasureThreads), kMeasureMaxBlocks));
 }
 
 void launch_measure(const TaskView& t, double* partials, unsigned int* done, double* result,

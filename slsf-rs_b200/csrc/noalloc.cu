@@ -16,11 +16,12 @@
  * left, and calls whose kernels overlap on the GPU (different streams, or
  * different host threads, on the same device) race on it.  Serialise them.
  *
- * The first call on a device does a one-time set-up on that device: it
- * takes the array's device address with cudaGetSymbolAddress (the host-side
- * name of a __device__ array is only a stand-in, not a device address) and
- * zeroes the last-block counter.  Make that first call before any stream
- * capture.
+ * Every call takes the array's device address with cudaGetSymbolAddress on
+ * the current device (the host-side name of a __device__ array is only a
+ * stand-in, not a device address; the lookup allocates nothing).  The first
+ * call on a device -- and the first after the device's context was rebuilt,
+ * which moves the array -- also zeroes the last-block counter and waits for
+ * that: make such a first call before any stream capture.
  */
 #include <cuda_runtime.h>
 
@@ -32,8 +33,9 @@
 
 namespace {
 
-/* Partial-sum rows: the measurement grid never exceeds 148 * 8 blocks. */
-constexpr int kNoAllocMaxBlocks = 148 * 8;
+/* Partial-sum rows: one per block of the measurement grid, whose size the
+ * measurement launcher bounds by the same constant. */
+constexpr int kNoAllocMaxBlocks = slsf::kMeasureMaxBlocks;
 constexpr int kNoAllocMaxDevices = 64;
 
 struct NoAllocScratch {
@@ -45,21 +47,23 @@ struct NoAllocScratch {
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
 std::mutex g_setup_mutex;
+/* The array's address on each device when its counter was last zeroed. */
 NoAllocScratch* g_scratch_ptr[kNoAllocMaxDevices] = {};
 
 }  // namespace
 
-/* Set-up on the current device: the array's device address, counter zeroed. */
+/* The array's device address on the current device; its counter is zeroed
+ * whenever that address is new (first use, or a rebuilt context). */
 static int noalloc_scratch(int device, cudaStream_t stream, NoAllocScratch** out, std::string* err) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+        *err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+        return SLSF_ERR_CUDA;
+    }
+    NoAllocScratch* s = static_cast<NoAllocScratch*>(p);
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) {
-            *err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
-            return SLSF_ERR_CUDA;
-        }
-        NoAllocScratch* s = static_cast<NoAllocScratch*>(p);
+    if (g_scratch_ptr[device] != s) {
         e = cudaMemsetAsync(&s->done, 0, sizeof(unsigned int), stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) {
@@ -68,7 +72,7 @@ static int noalloc_scratch(int device, cudaStream_t stream, NoAllocScratch** out
         }
         g_scratch_ptr[device] = s;
     }
-    *out = g_scratch_ptr[device];
+    *out = s;
     return SLSF_OK;
 }
 
@@ -83,8 +87,7 @@ extern "C" int slsf_measure_noalloc(const float* theta, const float* j_xy, const
     const uint64_t volume = (uint64_t)lx * ly * lz;
     if (volume > SLSF_NOALLOC_MAX_SITES)
         return fail(SLSF_ERR_INVALID, "lattice volume exceeds the no-allocation measurement limit of 2^31 - 1 sites");
-    if (slsf::measure_partial_blocks((uint32_t)volume) > kNoAllocMaxBlocks)
-        return fail(SLSF_ERR_INVALID, "measurement grid exceeds the no-allocation scratch array");
+    /* measure_partial_blocks never exceeds kMeasureMaxBlocks, the rows of the array */
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return fail(SLSF_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));

@@ -15,7 +15,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def test_noalloc_measure_matches_task_measure(slsf):
+def test_noalloc_measure_matches_task_measure(slsf, orc):
     import torch
 
     slsf.build()
@@ -37,7 +37,12 @@ def test_noalloc_measure_matches_task_measure(slsf):
         jz_d = torch.from_numpy(jz.astype(np.float32)).to(dev)
         torch.cuda.synchronize(dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
-        for _ in range(2):  # two calls in a row share the static scratch
+        exact = orc.measure_f32(dims, theta, jxy.astype(np.float32), jz.astype(np.float32))
+        free_before = None
+        for call in range(2):  # two calls in a row share the static scratch
+            if call == 1:
+                torch.cuda.synchronize(dev)
+                free_before = torch.cuda.mem_get_info(dev)[0]
             out = slsf.Observables()
             rc = lib.slsf_measure_noalloc(C.c_void_p(th_d.data_ptr()), C.c_void_p(jxy_d.data_ptr()),
                                           C.c_void_p(jz_d.data_ptr()), L, L, L, C.c_void_p(stream), C.byref(out))
@@ -48,6 +53,14 @@ def test_noalloc_measure_matches_task_measure(slsf):
             assert abs(got["magnetization_squared"] - ref["magnetization_squared"]) < 1e-5
             for k in ("cos_x", "cos_y", "cos_z", "sin_x", "sin_y", "sin_z"):
                 assert abs(got[k] - ref[k]) < 2e-5 * v + 1e-5, (k, got[k], ref[k])
+            # and against the oracle's FP64 evaluation of the same FP32 state
+            assert abs(got["energy"] - exact["energy"]) < 2e-5
+            assert abs(got["magnetization_squared"] - exact["magnetization_squared"]) < 1e-5
+            for k in ("cos_x", "cos_y", "cos_z", "sin_x", "sin_y", "sin_z"):
+                assert abs(got[k] - exact[k]) < 2e-5 * v + 1e-5, (k, got[k], exact[k])
+        # the second call took no device memory
+        torch.cuda.synchronize(dev)
+        assert torch.cuda.mem_get_info(dev)[0] == free_before
         task.close()
 
 
