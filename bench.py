@@ -111,13 +111,34 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_site():
-    """DRAM bytes per replica site per launch from the committed ncu summary, if any."""
+def resident_profile():
+    """Per-site figures of the committed k_resident ncu capture (DRAM bytes per replica site per
+    launch, warp instructions per site-update), or {}."""
     path = os.path.join(ROOT, "profiles", "k_resident_c2_traffic.json")
     if os.path.exists(path):
         with open(path) as f:
-            return float(json.load(f)["dram_bytes_per_site_per_launch"])
-    return None
+            return json.load(f)
+    return {}
+
+
+def traffic_per_site():
+    v = resident_profile().get("dram_bytes_per_site_per_launch")
+    return float(v) if v is not None else None
+
+
+def issue_roofline(value, sm_mhz, sms=148):
+    """The bound that does bind the one-CTA kernel: instruction issue.  Achieved warp
+    instructions per second (site-updates/s x the committed ncu count of warp instructions per
+    site-update) against 4 schedulers x SMs x the SM clock sampled in the timed region."""
+    ipsu = resident_profile().get("warp_instructions_per_site_update")
+    if ipsu is None or not sm_mhz:
+        return None
+    achieved = value * ipsu
+    peak = 4 * sms * sm_mhz * 1e6
+    return {"bound": "issue", "warp_instructions_per_site_update": ipsu, "achieved": achieved, "peak": peak,
+            "unit": "warp instructions/s", "frac": achieved / peak,
+            "source": "instructions per site-update from profiles/k_resident_c2_traffic.json (ncu), peak = "
+                      "4 issue slots x 148 SMs x median SM clock of the timed region"}
 
 
 class ClockSampler:
@@ -635,6 +656,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "site-updates/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps},
             "roofline": roofline,
+            "issue_roofline": issue_roofline(value / world, clk.get("sm_mhz")) if choice["kind"] == "resident" else None,
             "step_ms": step_ms,
         }
         line.update(extra)

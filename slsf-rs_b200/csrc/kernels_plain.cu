@@ -15,7 +15,9 @@
  *                        the seed's component
  *   k_measure            measure_theta_observables_with_scratch
  *                        (src/observables.rs:80-154), FP64 block sums, fixed
- *                        summation order (last block reduces the partials)
+ *                        summation order (last block reduces the partials);
+ *   k_measure_rows       the same with warps walking rows (L_x a multiple of
+ *                        32): two sincos per site instead of four
  *
  * (The correlation functions are in kernel_corr.cu, batched over tasks.)
  */
@@ -443,6 +445,88 @@ __global__ void __launch_bounds__(kMeasureThreads)
     }
 }
 
+/* The same measurement for L_x a multiple of 32 and L_y a multiple of 16:
+ * a warp owns word k (lane = x - 32 k) of plane z for a run of 16 rows and
+ * walks it along y, so each site's own trig is the previous row's +y trig:
+ * two sincos per site (+y, +z) instead of four, the +x neighbour by shuffle.
+ * Identical FP32 bond terms; FP64 sums in another order. */
+constexpr uint32_t kMeasureSeg = 16;
+
+__global__ void __launch_bounds__(kMeasureThreads)
+    k_measure_rows(const float* __restrict__ theta, const float* __restrict__ jxy,
+                   const float* __restrict__ jz, uint32_t lx, uint32_t ly, uint32_t lz,
+                   double* __restrict__ partials, unsigned int* __restrict__ done,
+                   double* __restrict__ result, double* __restrict__ bin_row) {
+    __shared__ double scratch[8 * 32];
+    __shared__ bool last;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t words = lx >> 5, nseg = ly / kMeasureSeg, plane = lx * ly, volume = plane * lz;
+    const uint32_t units = words * nseg * lz;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < units; u += nwarps) {
+        const uint32_t k = u % words, rest = u / words, sg = rest % nseg, z = rest / nseg;
+        const uint32_t x = 32u * k + lane, xn = (k + 1 == words) ? 0u : 32u * (k + 1);
+        const uint32_t zbase = z * plane, zp_base = (z + 1 == lz) ? 0u : (z + 1) * plane;
+        const float jx = jxy[z], jzz = jz[z];
+        const uint32_t y0 = sg * kMeasureSeg;
+        float si, ci;
+        __sincosf(theta[zbase + y0 * lx + x], &si, &ci);
+        for (uint32_t y = y0; y < y0 + kMeasureSeg; ++y) {
+            const uint32_t row = zbase + y * lx;
+            const uint32_t y1 = (y + 1 == ly) ? 0u : y + 1;
+            float sx, cx, sy, cy, sz, cz, sn, cn;
+            __sincosf(theta[zbase + y1 * lx + x], &sy, &cy);
+            __sincosf(theta[zp_base + y * lx + x], &sz, &cz);
+            __sincosf(theta[row + xn], &sn, &cn);
+            sx = __shfl_sync(0xffffffffu, si, (lane + 1u) & 31u);
+            cx = __shfl_sync(0xffffffffu, ci, (lane + 1u) & 31u);
+            if (lane == 31) {
+                sx = sn;
+                cx = cn;
+            }
+            acc[0] += ci;
+            acc[1] += si;
+            acc[2] += bond_cos(jx, ci, si, cx, sx);
+            acc[3] += bond_cos(jx, ci, si, cy, sy);
+            acc[4] += bond_cos(jzz, ci, si, cz, sz);
+            acc[5] += bond_sin(jx, ci, si, cx, sx);
+            acc[6] += bond_sin(jx, ci, si, cy, sy);
+            acc[7] += bond_sin(jzz, ci, si, cz, sz);
+            si = sy;
+            ci = cy;
+        }
+    }
+    block_sum<8>(acc, scratch);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 8; ++k) partials[blockIdx.x * 8 + k] = acc[k];
+        __threadfence();
+        last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+        for (int k = 0; k < 8; ++k) tot[k] += ((volatile double*)partials)[b * 8 + k];
+    block_sum<8>(tot, scratch);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 8; ++k) result[k] = tot[k];
+        if (bin_row) {
+            const double v = (double)volume;
+            const double e = -(tot[2] + tot[3] + tot[4]) / v;
+            const double vals[kBinCols] = {e,      e * e,  (tot[0] * tot[0] + tot[1] * tot[1]) / (v * v),
+                                           tot[2], tot[3], tot[4],
+                                           tot[5], tot[6], tot[7],
+                                           tot[5] * tot[5], tot[6] * tot[6], tot[7] * tot[7]};
+            for (int q = 0; q < kBinCols; ++q) bin_row[q] += vals[q];
+        }
+        *done = 0;
+    }
+}
+
+inline bool measure_rows_supported(uint32_t lx, uint32_t ly) { return lx % 32 == 0 && ly % kMeasureSeg == 0; }
+
 inline uint32_t blocks_for(uint64_t n, int threads) { return (uint32_t)((n + threads - 1) / threads); }
 
 }  // namespace
@@ -521,6 +605,11 @@ int measure_partial_blocks(uint32_t volume) {
 void launch_measure(const TaskView& t, double* partials, unsigned int* done, double* result,
                     cudaStream_t s) {
     const uint32_t volume = t.lx * t.ly * t.lz;
+    if (measure_rows_supported(t.lx, t.ly)) {
+        k_measure_rows<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly,
+                                                                                  t.lz, partials, done, result, nullptr);
+        return;
+    }
     k_measure<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(
         t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, slsf_fastdiv_make(t.lx), slsf_fastdiv_make(t.ly), partials, done,
         result, nullptr);
@@ -529,6 +618,11 @@ void launch_measure(const TaskView& t, double* partials, unsigned int* done, dou
 void launch_measure_into_bin(const TaskView& t, double* partials, unsigned int* done, double* result,
                              double* bin_row, cudaStream_t s) {
     const uint32_t volume = t.lx * t.ly * t.lz;
+    if (measure_rows_supported(t.lx, t.ly)) {
+        k_measure_rows<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly,
+                                                                                  t.lz, partials, done, result, bin_row);
+        return;
+    }
     k_measure<<<measure_partial_blocks(volume), kMeasureThreads, 0, s>>>(
         t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, slsf_fastdiv_make(t.lx), slsf_fastdiv_make(t.ly), partials, done,
         result, bin_row);
