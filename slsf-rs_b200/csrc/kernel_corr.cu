@@ -27,6 +27,18 @@
  * runs in FP64; the item's per-lag sums (FP64, over its lines) go to the
  * task's scratch.
  *
+ * z lines whose length is 32, 64, 128 or 256 take a shorter route
+ * (k_corr_zfft, launched beside k_corr_lines, which skips those items):
+ * the circular correlation of a line is the inverse transform of its power
+ * spectrum, sum_k s_k . s_{k+r} = Re (1/n) sum_q |A(q)|^2 e^{2 pi i q r / n}
+ * with A the discrete Fourier transform of cos + i sin along the line.  A
+ * warp transforms one line at a time in FP64 (lane t holds elements t + 32 j:
+ * a radix-(n/32) DFT in registers, twiddles, then a 32-point decimation-in-
+ * frequency FFT across the lanes), the item sums |A|^2 over its lines in a
+ * fixed order, and one thread per lag forms the item's per-lag sum from the
+ * spectrum.  O(n log n) per line instead of O(n R); the FP32 products of the
+ * direct form become FP64 transforms of the same FP32 trig values.
+ *
  * k_corr_finalize: one block per task sums the item partials in a fixed
  * order (per layer for x and y, over everything for z), forms the values in
  * ThetaModel::measure's order (src/model.rs:420-437) -- C_x, C_y, C_xy,
@@ -67,6 +79,136 @@ __host__ __device__ inline CorrShape corr_shape(uint32_t lx, uint32_t ly, uint32
     return s;
 }
 
+constexpr uint32_t kFftMax = 256; /* longest z line of the spectral route */
+
+/* z lines of length n = 32 N1 (N1 = 1, 2, 4, 8) take the spectral route. */
+__host__ __device__ inline bool corr_fft_len(uint32_t n) { return n == 32 || n == 64 || n == 128 || n == 256; }
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+/* The spectral route for one item of z lines: tile [n][kCorrPitch] holds
+ * (cos, sin) of `cols` lines (zero past them), tw[q] = exp(-2 pi i q / n),
+ * P[n] receives the item's summed power spectrum.  Writes out[r - 1] for
+ * r = 1..rmax. */
+template <uint32_t N1>
+__device__ void corr_z_spectral(const float2* __restrict__ tile, const double2* __restrict__ tw, double* P,
+                                uint32_t cols, uint32_t rmax, double* __restrict__ out) {
+    constexpr uint32_t n = 32 * N1;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    double pw[N1];
+#pragma unroll
+    for (uint32_t m = 0; m < N1; ++m) pw[m] = 0.0;
+    for (uint32_t c = warp; c < cols; c += nwarps) {
+        double2 x[N1];
+#pragma unroll
+        for (uint32_t j = 0; j < N1; ++j) {
+            const float2 v = tile[(lane + 32 * j) * kCorrPitch + c];
+            x[j] = make_double2((double)v.x, (double)v.y);
+        }
+        /* radix-N1 DFT over j (elements lane + 32 j), then the twiddle w_n^(lane m) */
+        double2 X[N1];
+#pragma unroll
+        for (uint32_t m = 0; m < N1; ++m) {
+            double2 acc = x[0];
+#pragma unroll
+            for (uint32_t j = 1; j < N1; ++j) {
+                const double2 w = tw[((j * m) % N1) * 32];
+                acc.x += x[j].x * w.x - x[j].y * w.y;
+                acc.y += x[j].x * w.y + x[j].y * w.x;
+            }
+            X[m] = m ? cmul(acc, tw[(lane * m) % n]) : acc;
+        }
+        /* 32-point decimation-in-frequency FFT across the lanes; lane t ends
+         * with frequency index bitrev5(t) of each m */
+#pragma unroll
+        for (uint32_t h = 16; h > 0; h >>= 1) {
+            const bool upper = lane & h;
+            const double2 w = tw[(lane & (h - 1)) * (n / (2 * h))];
+#pragma unroll
+            for (uint32_t m = 0; m < N1; ++m) {
+                const double yx = __shfl_xor_sync(0xffffffffu, X[m].x, h);
+                const double yy = __shfl_xor_sync(0xffffffffu, X[m].y, h);
+                if (!upper) {
+                    X[m] = make_double2(X[m].x + yx, X[m].y + yy);
+                } else {
+                    X[m] = cmul(make_double2(yx - X[m].x, yy - X[m].y), w);
+                }
+            }
+        }
+#pragma unroll
+        for (uint32_t m = 0; m < N1; ++m) pw[m] += X[m].x * X[m].x + X[m].y * X[m].y;
+    }
+    /* the item's spectrum: warps add theirs in order */
+    const uint32_t s = __brev(lane) >> 27;
+    for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) P[q] = 0.0;
+    for (uint32_t w = 0; w < nwarps; ++w) {
+        __syncthreads();
+        if (warp == w) {
+#pragma unroll
+            for (uint32_t m = 0; m < N1; ++m) P[m + N1 * s] += pw[m];
+        }
+    }
+    __syncthreads();
+    /* per-lag sums: (1/n) sum_q P(q) cos(2 pi q r / n) */
+    for (uint32_t r = threadIdx.x + 1; r <= rmax; r += blockDim.x) {
+        double a = 0.0;
+        for (uint32_t q = 0; q < n; ++q) a += P[q] * tw[(q * r) % n].x;
+        out[r - 1] = a / (double)n;
+    }
+}
+
+/* The task of a work item: the last one whose first item is at or before it. */
+__device__ __forceinline__ const CorrTask& item_task(const CorrTask* __restrict__ tasks, const CorrTask& one,
+                                                    uint32_t n_tasks, uint32_t item) {
+    uint32_t lo = 0, hi = n_tasks;
+    while (tasks && hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (tasks[mid].item0 <= item) lo = mid;
+        else hi = mid;
+    }
+    return tasks ? tasks[lo] : one;
+}
+
+/* The spectral route for z items (one block per item; other items return). */
+__global__ void __launch_bounds__(kCorrThreads)
+    k_corr_zfft(const CorrTask* __restrict__ tasks, CorrTask one, uint32_t n_tasks, uint32_t n_items) {
+    extern __shared__ float2 tile[]; /* [n][kCorrPitch] */
+    __shared__ double2 tw[kFftMax];
+    __shared__ double spec[kFftMax];
+    for (uint32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+        const CorrTask& T = item_task(tasks, one, n_tasks, item);
+        const CorrShape sh = corr_shape(T.lx, T.ly, T.lz, T.rxy, T.rz);
+        const uint32_t local = item - T.item0;
+        const uint32_t n = T.lz;
+        if (local < sh.nx + sh.ny || !corr_fft_len(n)) continue; /* block-uniform */
+        const uint32_t plane = T.lx * T.ly;
+        const uint32_t q = local - sh.nx - sh.ny, y = q / sh.cy, x0 = (q % sh.cy) * kCorrCols;
+        const uint32_t cols = min(kCorrCols, T.lx - x0), base = y * T.lx + x0;
+        __syncthreads(); /* the previous item's tile and spectrum are no longer read */
+        for (uint32_t e = threadIdx.x; e < n * kCorrCols; e += blockDim.x) {
+            const uint32_t k = e / kCorrCols, c = e % kCorrCols;
+            float sn = 0.0f, cn = 0.0f;
+            if (c < cols) __sincosf(T.theta[base + k * plane + c], &sn, &cn);
+            tile[k * kCorrPitch + c] = make_float2(cn, sn);
+        }
+        for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+            double sn, cn;
+            sincospi(-2.0 * (double)k / (double)n, &sn, &cn);
+            tw[k] = make_double2(cn, sn);
+        }
+        __syncthreads();
+        double* out = T.partial + (size_t)local * sh.rp;
+        switch (n) {
+            case 32: corr_z_spectral<1>(tile, tw, spec, cols, T.rz, out); break;
+            case 64: corr_z_spectral<2>(tile, tw, spec, cols, T.rz, out); break;
+            case 128: corr_z_spectral<4>(tile, tw, spec, cols, T.rz, out); break;
+            default: corr_z_spectral<8>(tile, tw, spec, cols, T.rz, out); break;
+        }
+    }
+}
+
 /* `tasks` in device memory, or NULL and the single task `one` by value. */
 __global__ void __launch_bounds__(kCorrThreads)
     k_corr_lines(const CorrTask* __restrict__ tasks, CorrTask one, uint32_t n_tasks, uint32_t n_items) {
@@ -101,6 +243,7 @@ __global__ void __launch_bounds__(kCorrThreads)
             rmax = T.rz;
         }
         const float* __restrict__ theta = T.theta;
+        if (local >= sh.nx + sh.ny && corr_fft_len(n)) continue; /* k_corr_zfft's item (block-uniform) */
         __syncthreads(); /* the previous item's tile is no longer read */
         const uint32_t pitch = cstride == 1 ? kCorrCols : kCorrPitch;
         if (cstride == 1) {
@@ -315,6 +458,15 @@ cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t
         k_corr_lines<<<grid, line_threads, smem, s>>>(one ? nullptr : tasks_dev, by_value, n_tasks, n_items);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
+        if (max_nz > 0) {
+            /* z items of lines of 32..256 sites: the spectral route */
+            const size_t zsmem = (size_t)kFftMax * kCorrPitch * sizeof(float2);
+            e = cudaFuncSetAttribute(k_corr_zfft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem);
+            if (e != cudaSuccess) return e;
+            k_corr_zfft<<<grid, kCorrThreads, zsmem, s>>>(one ? nullptr : tasks_dev, by_value, n_tasks, n_items);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+        }
     }
     k_corr_finalize<<<n_tasks, fin_threads, 0, s>>>(one ? nullptr : tasks_dev, by_value);
     return cudaGetLastError();

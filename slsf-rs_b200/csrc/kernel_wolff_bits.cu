@@ -51,6 +51,20 @@ constexpr int kBondThreads = 256;
 constexpr int kFlipThreads = 256;
 constexpr uint32_t kEmpty = 0;
 
+/* Optional counters (build with -DSLSF_WB_STATS): regions processed, growth
+ * passes, grow launches, and region loads that changed nothing. */
+#ifdef SLSF_WB_STATS
+__device__ unsigned long long g_wb_stats[4];
+#define SLSF_WB_COUNT(k, n)                                                          \
+    do {                                                                             \
+        if (threadIdx.x == 0) atomicAdd(&g_wb_stats[k], (unsigned long long)(n));    \
+    } while (0)
+#else
+#define SLSF_WB_COUNT(k, n) \
+    do {                    \
+    } while (0)
+#endif
+
 /* Scratch of one update, carved from the task's union-find array. */
 struct WolffBits {
     uint32_t* bx;      /* bond bit planes, one bit per site */
@@ -296,6 +310,8 @@ __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, u
         }
         if (!__syncthreads_or(changed)) {
             ok = true;
+            SLSF_WB_COUNT(1, pass + 1);
+            if (pass == 0) SLSF_WB_COUNT(3, 1);
             break;
         }
     }
@@ -375,6 +391,7 @@ __global__ void __launch_bounds__(kGrowThreads, 1)
             break;
         }
         ok &= grow_region(wb, g, r, C, BY, BZ, BX);
+        SLSF_WB_COUNT(0, 1);
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();
@@ -507,3 +524,14 @@ int launch_wolff_bits(const TaskView& t, uint64_t counter, void* scratch, uint8_
 }
 
 }  // namespace slsf
+
+#ifdef SLSF_WB_STATS
+extern "C" int slsf_debug_wb_stats(unsigned long long out[4], int reset) {
+    cudaError_t e = cudaMemcpyFromSymbol(out, slsf::g_wb_stats, sizeof(unsigned long long) * 4);
+    if (e == cudaSuccess && reset) {
+        const unsigned long long zero[4] = {0, 0, 0, 0};
+        e = cudaMemcpyToSymbol(slsf::g_wb_stats, zero, sizeof(zero));
+    }
+    return e == cudaSuccess ? 0 : 1;
+}
+#endif
