@@ -14,8 +14,8 @@
  *                src/updates.rs:537-548) into three bit planes: bit i of the
  *                flat bitmap is site i (site index x + Lx (y + Ly z), so a
  *                32-bit word is 32 consecutive sites of one row); clears the
- *                cluster bitmap and sets the seed's bit, and queues the
- *                seed's region.
+ *                cluster bitmap and queues the seed's region, whose first
+ *                processing adds the seed's bit.
  *   k_wb_grow    the cluster over the active bonds.  The lattice is cut into
  *                regions of 32 x 32 x 32 sites (one word wide, 32 rows, 32
  *                planes).  A CTA takes a region from a work queue, reads its
@@ -73,7 +73,7 @@ struct WolffBits {
     uint32_t* cl;      /* cluster bitmap */
     uint32_t* queued;  /* [regions] 1 while the region is in the queue */
     uint32_t* ring;    /* [cap] region + 1, or 0 */
-    uint32_t* ctl;     /* head, tail, pending (queued or in flight), abort */
+    uint32_t* ctl;     /* head, tail, pending (queued or in flight), abort, seed site + 1 */
     uint32_t regions, cap;
 };
 
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(kBondThreads)
         if (lane == 0) wb.bx[w] = wx;
         if (lane == 1) wb.by[w] = wy;
         if (lane == 2) wb.bz[w] = wz;
-        if (lane == 3) wb.cl[w] = (w == (seed_idx >> 5)) ? (1u << (seed_idx & 31u)) : 0u;
+        if (lane == 3) wb.cl[w] = 0u;
         if (bond_bytes) bond_bytes[i] = (uint8_t)((ax ? 1u : 0u) | (ay ? 2u : 0u) | (az ? 4u : 0u));
         ri = ryp;
     }
@@ -210,6 +210,7 @@ __global__ void __launch_bounds__(kBondThreads)
         wb.ring[0] = r + 1;
         wb.ctl[1] = 1; /* tail */
         wb.ctl[2] = 1; /* pending */
+        wb.ctl[4] = seed_idx + 1; /* the seed's bit enters its region like a face bit */
     }
 }
 
@@ -234,8 +235,9 @@ __device__ __forceinline__ uint32_t region_of(const GrowGeo& g, uint32_t k, uint
 /* One region: load with the bits entering through its faces, close in
  * shared memory, OR back, queue the neighbours its bits can enter.  Returns
  * false if a pass bound was hit. */
-__device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, uint32_t (*C)[kRegion + 1],
-                            uint32_t (*BY)[kRegion + 1], uint32_t (*BZ)[kRegion + 1], uint32_t (*BX)[kRegion + 1]) {
+__device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, uint32_t seed_site,
+                            uint32_t (*C)[kRegion + 1], uint32_t (*BY)[kRegion + 1], uint32_t (*BZ)[kRegion + 1],
+                            uint32_t (*BX)[kRegion + 1]) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t k = r % g.words, rest = r / g.words, ry = rest % g.ry_n, rz = rest / g.ry_n;
     const uint32_t rowlen = g.words; /* words per row */
@@ -268,7 +270,13 @@ __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, u
         }
         if (warp == kRegion - 1) c |= __ldcg(&wb.cl[word(k, gy, zp)]) & bzw;
     }
+    if (w == seed_site >> 5) c |= 1u << (seed_site & 31u);
     c = close_word(c, bxw, g.px);
+    /* the stored region is closed already: without new bits nothing changes */
+    if (!__syncthreads_or(c != c0)) {
+        SLSF_WB_COUNT(3, 1);
+        return true;
+    }
     C[warp][lane] = c;
     BX[warp][lane] = bxw;
     BY[warp][lane] = byw;
@@ -284,12 +292,15 @@ __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, u
         if ((pass & 1u) == 0) {
             const uint32_t z = warp, y = lane;
             const uint32_t old = C[z][y];
-            uint32_t v = close_line(old, BY[z][y], g.py);
+            const uint32_t by_ = BY[z][y];
+            /* a warp scans only if some bit of it sits on a bond along the line */
+            const uint32_t by_in = __shfl_sync(0xffffffffu, by_, (lane + 31u) & 31u);
+            uint32_t v = __any_sync(0xffffffffu, (old & (by_ | by_in)) != 0u) ? close_line(old, by_, g.py) : old;
             if (z > 0) v |= C[z - 1][y] & BZ[z - 1][y];
             else if (g.pz) v |= C[kRegion - 1][y] & BZ[kRegion - 1][y];
             if (z + 1 < kRegion) v |= C[z + 1][y] & BZ[z][y];
             else if (g.pz) v |= C[0][y] & BZ[z][y];
-            v = close_word(v, BX[z][y], g.px);
+            if (__any_sync(0xffffffffu, v != old)) v = close_word(v, BX[z][y], g.px);
             if (v != old) {
                 C[z][y] = v;
                 changed = 1;
@@ -297,12 +308,14 @@ __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, u
         } else {
             const uint32_t z = lane, y = warp;
             const uint32_t old = C[z][y];
-            uint32_t v = close_line(old, BZ[z][y], g.pz);
+            const uint32_t bz_ = BZ[z][y];
+            const uint32_t bz_in = __shfl_sync(0xffffffffu, bz_, (lane + 31u) & 31u);
+            uint32_t v = __any_sync(0xffffffffu, (old & (bz_ | bz_in)) != 0u) ? close_line(old, bz_, g.pz) : old;
             if (y > 0) v |= C[z][y - 1] & BY[z][y - 1];
             else if (g.py) v |= C[z][kRegion - 1] & BY[z][kRegion - 1];
             if (y + 1 < kRegion) v |= C[z][y + 1] & BY[z][y];
             else if (g.py) v |= C[z][0] & BY[z][y];
-            v = close_word(v, BX[z][y], g.px);
+            if (__any_sync(0xffffffffu, v != old)) v = close_word(v, BX[z][y], g.px);
             if (v != old) {
                 C[z][y] = v;
                 changed = 1;
@@ -311,7 +324,6 @@ __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, u
         if (!__syncthreads_or(changed)) {
             ok = true;
             SLSF_WB_COUNT(1, pass + 1);
-            if (pass == 0) SLSF_WB_COUNT(3, 1);
             break;
         }
     }
@@ -354,6 +366,7 @@ __global__ void __launch_bounds__(kGrowThreads, 1)
      * flight.  A popped entry may still be being written by its producer
      * (slot claimed, entry not yet stored): the CTA waits for it, bounded. */
     constexpr uint32_t kSpin = 1u << 24;
+    const uint32_t seed_site = __ldcg(&wb.ctl[4]) - 1;
     bool ok = true;
     for (uint32_t item = 0; item < max_items; ++item) {
         if (threadIdx.x == 0) {
@@ -390,7 +403,7 @@ __global__ void __launch_bounds__(kGrowThreads, 1)
             ok = false;
             break;
         }
-        ok &= grow_region(wb, g, r, C, BY, BZ, BX);
+        ok &= grow_region(wb, g, r, seed_site, C, BY, BZ, BX);
         SLSF_WB_COUNT(0, 1);
         __syncthreads();
         if (threadIdx.x == 0) {
