@@ -329,6 +329,8 @@ __global__ void __launch_bounds__(kCorrThreads)
 }
 
 constexpr int kFinThreads = 1024;
+constexpr uint32_t kZParts = 8;     /* interleaved partial sums per C_z lag */
+constexpr uint32_t kMaxZLags = 400; /* R_z <= corr_ext - L_z < 775 / 2 */
 
 __global__ void __launch_bounds__(kFinThreads) k_corr_finalize(const CorrTask* __restrict__ tasks, CorrTask one) {
     const CorrTask& T = tasks ? tasks[blockIdx.x] : one;
@@ -371,30 +373,31 @@ __global__ void __launch_bounds__(kFinThreads) k_corr_finalize(const CorrTask* _
         emit(R + r, cy);
         emit(2 * R + r, (cx + cy) / 2.0);
     }
-    /* C_z: `parts` threads per lag each sum the z items p = part mod parts,
-     * then one thread adds the parts in order */
-    __shared__ double zpart[kFinThreads];
-    const uint32_t parts = Rz ? max(1u, blockDim.x / Rz) : 1u;
-    if (threadIdx.x < Rz * parts) {
-        const uint32_t r = threadIdx.x % Rz, q = threadIdx.x / Rz;
+    /* C_z: each lag's sum over the z items in kZParts interleaved partial
+     * sums (items p = q mod kZParts, in order), then the partial sums in
+     * order -- the same order whatever the block size, so every launch of a
+     * task gives the same bits */
+    __shared__ double zpart[kZParts * kMaxZLags];
+    for (uint32_t idx = threadIdx.x; idx < Rz * kZParts; idx += blockDim.x) {
+        const uint32_t r = idx % Rz, q = idx / Rz;
         const double* col = part + (size_t)(sh.nx + sh.ny) * sh.rp + r;
         /* in item order; 16 loads in flight before their adds */
         double a = 0.0;
         uint32_t p = q;
-        for (; p + 15 * parts < sh.nz; p += 16 * parts) {
+        for (; p + 15 * kZParts < sh.nz; p += 16 * kZParts) {
             double v[16];
 #pragma unroll
-            for (uint32_t j = 0; j < 16; ++j) v[j] = col[(size_t)(p + j * parts) * sh.rp];
+            for (uint32_t j = 0; j < 16; ++j) v[j] = col[(size_t)(p + j * kZParts) * sh.rp];
 #pragma unroll
             for (uint32_t j = 0; j < 16; ++j) a += v[j];
         }
-        for (; p < sh.nz; p += parts) a += col[(size_t)p * sh.rp];
-        zpart[threadIdx.x] = a;
+        for (; p < sh.nz; p += kZParts) a += col[(size_t)p * sh.rp];
+        zpart[idx] = a;
     }
     __syncthreads();
     for (uint32_t r = threadIdx.x; r < Rz; r += blockDim.x) {
         double sz = 0.0;
-        for (uint32_t q = 0; q < parts; ++q) sz += zpart[q * Rz + r];
+        for (uint32_t q = 0; q < kZParts; ++q) sz += zpart[q * Rz + r];
         emit(3 * R + lz * R + r, sz / volume);
     }
     __syncthreads();
