@@ -50,6 +50,7 @@ constexpr uint32_t kGrowThreads = kRegion * kRegion;
 constexpr int kBondThreads = 256;
 constexpr int kFlipThreads = 256;
 constexpr uint32_t kEmpty = 0;
+constexpr uint32_t kNoRegion = 0xffffffffu;
 
 /* Optional counters (build with -DSLSF_WB_STATS): regions processed, growth
  * passes, grow launches, and region loads that changed nothing. */
@@ -178,13 +179,26 @@ __global__ void __launch_bounds__(kBondThreads)
     const float jx = jxy[z], jzz = jz[z];
     const uint32_t y0 = sg * seg;
     float ri = proj_at(theta, zbase + y0 * lx + x, cphi, sphi);
+    /* the angles of the next row's loads, one row ahead */
+    auto yrow = [&](uint32_t y) { return (y + 1 == ly) ? 0u : y + 1; };
+    float t_yp = theta[zbase + yrow(y0) * lx + x], t_zp = theta[zp_base + y0 * lx + x];
+    float t_xn = theta[zbase + y0 * lx + xn];
     for (uint32_t y = y0; y < y0 + seg; ++y) {
         const uint32_t row = zbase + y * lx;
         const uint32_t i = row + x;
-        const uint32_t y1 = (y + 1 == ly) ? 0u : y + 1;
-        const float ryp = proj_at(theta, zbase + y1 * lx + x, cphi, sphi);
-        const float rzp = proj_at(theta, zp_base + y * lx + x, cphi, sphi);
-        const float rnext = proj_at(theta, row + xn, cphi, sphi);
+        const float a_yp = t_yp, a_zp = t_zp, a_xn = t_xn;
+        if (y + 1 < y0 + seg) {
+            t_yp = theta[zbase + yrow(y + 1) * lx + x];
+            t_zp = theta[zp_base + (y + 1) * lx + x];
+            t_xn = theta[row + lx + xn];
+        }
+        float sn, cn;
+        __sincosf(a_yp, &sn, &cn);
+        const float ryp = wolff_projection(cn, sn, cphi, sphi);
+        __sincosf(a_zp, &sn, &cn);
+        const float rzp = wolff_projection(cn, sn, cphi, sphi);
+        __sincosf(a_xn, &sn, &cn);
+        const float rnext = wolff_projection(cn, sn, cphi, sphi);
         float rxp = __shfl_sync(0xffffffffu, ri, (lane + 1u) & 31u);
         if (lane == 31) rxp = rnext;
         const slsf_u32x4 b = slsf_stream(seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, i);
@@ -219,10 +233,13 @@ struct GrowGeo {
     bool px, py, pz; /* the region spans the whole period along x (one-word rows), y, z */
 };
 
-/* Queues region r unless it is queued already. */
-__device__ __forceinline__ void push_region(const WolffBits& wb, uint32_t r) {
+/* Claims region r for processing unless it is claimed already (queued or
+ * kept): the first neighbour a CTA claims it keeps in *keep and processes
+ * next itself, the others go to the queue. */
+__device__ __forceinline__ void push_region(const WolffBits& wb, uint32_t r, uint32_t* keep) {
     if (atomicExch(&wb.queued[r], 1u) != 0u) return;
-    atomicAdd(&wb.ctl[2], 1u); /* pending before the entry is visible */
+    atomicAdd(&wb.ctl[2], 1u); /* pending before the region can be taken */
+    if (atomicCAS(keep, kNoRegion, r) == kNoRegion) return;
     const uint32_t slot = atomicAdd(&wb.ctl[1], 1u);
     __threadfence();
     atomicExch(&wb.ring[slot & (wb.cap - 1)], r + 1);
@@ -237,7 +254,7 @@ __device__ __forceinline__ uint32_t region_of(const GrowGeo& g, uint32_t k, uint
  * false if a pass bound was hit. */
 __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, uint32_t seed_site,
                             uint32_t (*C)[kRegion + 1], uint32_t (*BY)[kRegion + 1], uint32_t (*BZ)[kRegion + 1],
-                            uint32_t (*BX)[kRegion + 1]) {
+                            uint32_t (*BX)[kRegion + 1], uint32_t* keep) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t k = r % g.words, rest = r / g.words, ry = rest % g.ry_n, rz = rest / g.ry_n;
     const uint32_t rowlen = g.words; /* words per row */
@@ -333,24 +350,24 @@ __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, u
     /* neighbours that the region's bits can enter */
     if (!g.px) {
         const uint32_t wl = word(kl, gy, gz), wr = word(kr, gy, gz);
-        if ((c & 1u) && (wb.bx[wl] >> 31) && !(__ldcg(&wb.cl[wl]) >> 31)) push_region(wb, region_of(g, kl, ry, rz));
-        if ((c >> 31) && (bxw >> 31) && !(__ldcg(&wb.cl[wr]) & 1u)) push_region(wb, region_of(g, kr, ry, rz));
+        if ((c & 1u) && (wb.bx[wl] >> 31) && !(__ldcg(&wb.cl[wl]) >> 31)) push_region(wb, region_of(g, kl, ry, rz), keep);
+        if ((c >> 31) && (bxw >> 31) && !(__ldcg(&wb.cl[wr]) & 1u)) push_region(wb, region_of(g, kr, ry, rz), keep);
     }
     if (!g.py) {
         if (lane == 0) {
             const uint32_t wm = word(k, ym, gz);
-            if (c & wb.by[wm] & ~__ldcg(&wb.cl[wm])) push_region(wb, region_of(g, k, ry == 0 ? g.ry_n - 1 : ry - 1, rz));
+            if (c & wb.by[wm] & ~__ldcg(&wb.cl[wm])) push_region(wb, region_of(g, k, ry == 0 ? g.ry_n - 1 : ry - 1, rz), keep);
         }
         if (lane == kRegion - 1 && (c & byw & ~__ldcg(&wb.cl[word(k, yp, gz)])))
-            push_region(wb, region_of(g, k, ry + 1 == g.ry_n ? 0 : ry + 1, rz));
+            push_region(wb, region_of(g, k, ry + 1 == g.ry_n ? 0 : ry + 1, rz), keep);
     }
     if (!g.pz) {
         if (warp == 0) {
             const uint32_t wm = word(k, gy, zm);
-            if (c & wb.bz[wm] & ~__ldcg(&wb.cl[wm])) push_region(wb, region_of(g, k, ry, rz == 0 ? g.rz_n - 1 : rz - 1));
+            if (c & wb.bz[wm] & ~__ldcg(&wb.cl[wm])) push_region(wb, region_of(g, k, ry, rz == 0 ? g.rz_n - 1 : rz - 1), keep);
         }
         if (warp == kRegion - 1 && (c & bzw & ~__ldcg(&wb.cl[word(k, gy, zp)])))
-            push_region(wb, region_of(g, k, ry, rz + 1 == g.rz_n ? 0 : rz + 1));
+            push_region(wb, region_of(g, k, ry, rz + 1 == g.rz_n ? 0 : rz + 1), keep);
     }
     return ok;
 }
@@ -362,48 +379,52 @@ __global__ void __launch_bounds__(kGrowThreads, 1)
     __shared__ uint32_t BZ[kRegion][kRegion + 1];
     __shared__ uint32_t BX[kRegion][kRegion + 1];
     __shared__ uint32_t s_item;
-    /* Each CTA pops regions until the queue is empty and no region is in
-     * flight.  A popped entry may still be being written by its producer
-     * (slot claimed, entry not yet stored): the CTA waits for it, bounded. */
+    __shared__ uint32_t s_keep;
+    /* Each CTA takes regions until nothing is queued or in flight: the
+     * neighbour it claimed while processing the last one (no queue round
+     * trip), else the queue entry of its ticket (one atomic; the producer
+     * may not have filled it yet, the CTA waits for it, bounded).  A ticket
+     * whose entry never comes is given up when nothing is pending. */
     constexpr uint32_t kSpin = 1u << 24;
     const uint32_t seed_site = __ldcg(&wb.ctl[4]) - 1;
     bool ok = true;
+    if (threadIdx.x == 0) s_keep = kNoRegion;
+    __syncthreads();
     for (uint32_t item = 0; item < max_items; ++item) {
         if (threadIdx.x == 0) {
-            uint32_t got = 0xfffffffeu; /* gave up, unless set below */
-            for (uint32_t spin = 0; spin < kSpin; ++spin) {
+            uint32_t got = s_keep;
+            if (got == kNoRegion) {
+                got = 0xfffffffeu; /* gave up, unless set below */
+                const uint32_t ticket = atomicAdd(&wb.ctl[0], 1u);
+                volatile uint32_t* slot = &wb.ring[ticket & (wb.cap - 1)];
                 volatile uint32_t* ctl = wb.ctl;
-                const uint32_t head = ctl[0], tail = ctl[1];
-                if (head < tail) {
-                    if (atomicCAS(&wb.ctl[0], head, head + 1) != head) continue;
-                    volatile uint32_t* slot = &wb.ring[head & (wb.cap - 1)];
-                    uint32_t v = kEmpty;
-                    for (uint32_t s2 = 0; s2 < kSpin && (v = *slot) == kEmpty; ++s2) __nanosleep(32);
+                for (uint32_t spin = 0; spin < kSpin; ++spin) {
+                    const uint32_t v = *slot;
                     if (v != kEmpty) {
                         *slot = kEmpty;
                         got = v - 1;
+                        break;
                     }
-                    break;
+                    if (ctl[2] == 0 || ctl[3] != 0) { /* nothing queued or in flight, or aborted */
+                        got = 0xffffffffu;
+                        break;
+                    }
+                    __nanosleep(32);
                 }
-                if (ctl[2] == 0 || ctl[3] != 0) { /* nothing queued and nothing in flight, or aborted */
-                    got = 0xffffffffu;
-                    break;
-                }
-                __nanosleep(64);
             }
-            if (got < wb.regions) atomicExch(&wb.queued[got], 0u); /* re-queueable from here on */
+            s_keep = kNoRegion;
+            if (got < wb.regions) wb.queued[got] = 0u; /* claimable again from here on */
             __threadfence();
             s_item = got;
         }
         __syncthreads();
         const uint32_t r = s_item;
-        __syncthreads();
         if (r == 0xffffffffu) break;
         if (r >= wb.regions) {
             ok = false;
             break;
         }
-        ok &= grow_region(wb, g, r, seed_site, C, BY, BZ, BX);
+        ok &= grow_region(wb, g, r, seed_site, C, BY, BZ, BX, &s_keep);
         SLSF_WB_COUNT(0, 1);
         __syncthreads();
         if (threadIdx.x == 0) {
