@@ -101,60 +101,74 @@ __device__ void corr_z_spectral(const float2* __restrict__ tile, const double2* 
 #pragma unroll
     for (uint32_t m = 0; m < N1; ++m) pw[m] = 0.0;
     for (uint32_t c = warp; c < cols; c += nwarps) {
-        double2 x[N1];
+        double2 X[N1];
 #pragma unroll
         for (uint32_t j = 0; j < N1; ++j) {
             const float2 v = tile[(lane + 32 * j) * kCorrPitch + c];
-            x[j] = make_double2((double)v.x, (double)v.y);
+            X[j] = make_double2((double)v.x, (double)v.y);
         }
-        /* radix-N1 DFT over j (elements lane + 32 j), then the twiddle w_n^(lane m) */
-        double2 X[N1];
+        /* radix-2 decimation in frequency over j in registers (N1-point DFT of
+         * the elements lane + 32 j); slot j ends with frequency bitrev(j) */
 #pragma unroll
-        for (uint32_t m = 0; m < N1; ++m) {
-            double2 acc = x[0];
+        for (uint32_t h = N1 / 2; h > 0; h >>= 1) {
 #pragma unroll
-            for (uint32_t j = 1; j < N1; ++j) {
-                const double2 w = tw[((j * m) % N1) * 32];
-                acc.x += x[j].x * w.x - x[j].y * w.y;
-                acc.y += x[j].x * w.y + x[j].y * w.x;
+            for (uint32_t j = 0; j < N1; ++j) {
+                if (j & h) continue;
+                const double2 a = X[j], b = X[j + h];
+                const double2 w = tw[(j & (h - 1)) * (n / (2 * h))];
+                X[j] = make_double2(a.x + b.x, a.y + b.y);
+                X[j + h] = cmul(make_double2(a.x - b.x, a.y - b.y), w);
             }
-            X[m] = m ? cmul(acc, tw[(lane * m) % n]) : acc;
+        }
+        /* the twiddle w_n^(lane m) of slot j, m = bitrev(j) */
+#pragma unroll
+        for (uint32_t j = 1; j < N1; ++j) {
+            const uint32_t m = (__brev(j) >> (32 - __ffs(N1) + 1)) & (N1 - 1);
+            X[j] = cmul(X[j], tw[(lane * m) & (n - 1)]);
         }
         /* 32-point decimation-in-frequency FFT across the lanes; lane t ends
-         * with frequency index bitrev5(t) of each m */
+         * with frequency index bitrev5(t) */
 #pragma unroll
         for (uint32_t h = 16; h > 0; h >>= 1) {
             const bool upper = lane & h;
             const double2 w = tw[(lane & (h - 1)) * (n / (2 * h))];
 #pragma unroll
-            for (uint32_t m = 0; m < N1; ++m) {
-                const double yx = __shfl_xor_sync(0xffffffffu, X[m].x, h);
-                const double yy = __shfl_xor_sync(0xffffffffu, X[m].y, h);
+            for (uint32_t j = 0; j < N1; ++j) {
+                const double yx = __shfl_xor_sync(0xffffffffu, X[j].x, h);
+                const double yy = __shfl_xor_sync(0xffffffffu, X[j].y, h);
                 if (!upper) {
-                    X[m] = make_double2(X[m].x + yx, X[m].y + yy);
+                    X[j] = make_double2(X[j].x + yx, X[j].y + yy);
                 } else {
-                    X[m] = cmul(make_double2(yx - X[m].x, yy - X[m].y), w);
+                    X[j] = cmul(make_double2(yx - X[j].x, yy - X[j].y), w);
                 }
             }
         }
 #pragma unroll
-        for (uint32_t m = 0; m < N1; ++m) pw[m] += X[m].x * X[m].x + X[m].y * X[m].y;
+        for (uint32_t j = 0; j < N1; ++j) pw[j] += X[j].x * X[j].x + X[j].y * X[j].y;
     }
-    /* the item's spectrum: warps add theirs in order */
+    /* the item's spectrum: warps add theirs in order; slot j of lane t is
+     * frequency m + N1 s with m = bitrev(j), s = bitrev5(t) */
     const uint32_t s = __brev(lane) >> 27;
     for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) P[q] = 0.0;
     for (uint32_t w = 0; w < nwarps; ++w) {
         __syncthreads();
         if (warp == w) {
 #pragma unroll
-            for (uint32_t m = 0; m < N1; ++m) P[m + N1 * s] += pw[m];
+            for (uint32_t j = 0; j < N1; ++j) {
+                const uint32_t m = N1 == 1 ? 0u : (__brev(j) >> (32 - __ffs(N1) + 1)) & (N1 - 1);
+                P[m + N1 * s] += pw[j];
+            }
         }
     }
     __syncthreads();
     /* per-lag sums: (1/n) sum_q P(q) cos(2 pi q r / n) */
     for (uint32_t r = threadIdx.x + 1; r <= rmax; r += blockDim.x) {
         double a = 0.0;
-        for (uint32_t q = 0; q < n; ++q) a += P[q] * tw[(q * r) % n].x;
+        uint32_t idx = 0;
+        for (uint32_t q = 0; q < n; ++q) {
+            a += P[q] * tw[idx].x;
+            idx = (idx + r) & (n - 1);
+        }
         out[r - 1] = a / (double)n;
     }
 }
@@ -172,7 +186,7 @@ __device__ __forceinline__ const CorrTask& item_task(const CorrTask* __restrict_
 }
 
 /* The spectral route for z items (one block per item; other items return). */
-__global__ void __launch_bounds__(kCorrThreads)
+__global__ void __launch_bounds__(kCorrThreads, 2)
     k_corr_zfft(const CorrTask* __restrict__ tasks, CorrTask one, uint32_t n_tasks, uint32_t n_items) {
     extern __shared__ float2 tile[]; /* [n][kCorrPitch] */
     __shared__ double2 tw[kFftMax];
