@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kThreads)
 /* Smallest lattice whose Wolff update grows the seed's cluster on bit-packed
  * bonds instead of labelling 32x8x4 tiles (measured crossover on B200). */
 #ifndef SLSF_WOLFF_BITS_MIN_SITES
-#define SLSF_WOLFF_BITS_MIN_SITES (1u << 21)
+#define SLSF_WOLFF_BITS_MIN_SITES (1u << 22)
 #endif
 constexpr uint64_t kWolffBitsMinSites = SLSF_WOLFF_BITS_MIN_SITES;
 

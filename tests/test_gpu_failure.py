@@ -15,7 +15,7 @@ def task(slsf, ctx, dims, T=0.5, seed=3):
     return t
 
 
-@pytest.mark.parametrize("dims,path", [((64, 64, 64), "single"), ((32, 32, 32), "batched"),
+@pytest.mark.parametrize("dims,path", [((64, 64, 64), "single"), ((256, 128, 128), "single"), ((32, 32, 32), "batched"),
                                        ((48, 48, 48), "batched"), ((128, 8, 8), "batched")])
 def test_bounded_loop_reports_timeout_and_context_recovers(slsf, dims, path):
     ctx = slsf.Context()

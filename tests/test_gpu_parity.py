@@ -115,11 +115,13 @@ def test_metropolis_width_zero_and_wrap(slsf, ctx, orc):
                                          ((96, 16, 10), 0.8, False), ((128, 24, 10), 1.2, False),
                                          ((32, 32, 32), 1.1, True), ((64, 64, 64), 1.22, True),
                                          ((96, 32, 64), 1.5, False), ((128, 64, 32), 1.22, True),
-                                         ((64, 32, 96), 1.3, True)])
+                                         ((64, 32, 96), 1.3, True), ((256, 128, 128), 1.22, True),
+                                         ((128, 256, 128), 1.5, False)])
 def test_wolff_cluster_bit_exact(slsf, ctx, orc, dims, T, cold):
-    # Sides that are multiples of 32 grow the seed's cluster on bit-packed
-    # bonds; the others label the whole lattice by union-find.  Cold starts
-    # give clusters that span the lattice and cross every region face.
+    # Lattices of 2^22 sites and more whose sides are multiples of 32 grow
+    # the seed's cluster on bit-packed bonds; the others label 32x8x4 tiles by
+    # union-find.  Cold starts give clusters that span the lattice and cross
+    # every region face.
     t, jxy, jz = make_task(slsf, ctx, orc, dims, T, seed=31)
     if cold:
         t.init_cold()
