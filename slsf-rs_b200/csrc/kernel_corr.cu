@@ -80,6 +80,7 @@ __host__ __device__ inline CorrShape corr_shape(uint32_t lx, uint32_t ly, uint32
 }
 
 constexpr uint32_t kFftMax = 256; /* longest z line of the spectral route */
+constexpr uint32_t kFftMaxN1 = kFftMax / 32;
 
 /* z lines of length n = 32 N1 (N1 = 1, 2, 4, 8) take the spectral route. */
 __host__ __device__ inline bool corr_fft_len(uint32_t n) { return n == 32 || n == 64 || n == 128 || n == 256; }
@@ -88,14 +89,47 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
+/* Twiddles of the spectral route, laid out so that a warp reads 32
+ * consecutive entries: stage[k][t] = w_(2h)^(t mod h) for the lane stage of
+ * half-size h = 16 >> k, slot[j][t] = w_n^(t bitrev(j)) for register slot j,
+ * reg[q] = w_n^q for q < n (the register stages and the inverse transform),
+ * with w_N = exp(-2 pi i / N). */
+struct FftTables {
+    double2 stage[5][32];
+    double2 slot[kFftMaxN1][32];
+    double2 reg[kFftMax];
+};
+
+__device__ __forceinline__ uint32_t bitrev_bits(uint32_t j, uint32_t bits) {
+    return bits ? (__brev(j) >> (32 - bits)) : 0u;
+}
+
+__device__ void fft_tables(FftTables& T, uint32_t n) {
+    const uint32_t n1 = n / 32, bits = __ffs(n1) - 1;
+    auto w = [&](uint32_t q) {
+        double sn, cn;
+        sincospi(-2.0 * (double)(q & (n - 1)) / (double)n, &sn, &cn);
+        return make_double2(cn, sn);
+    };
+    for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) T.reg[q] = w(q);
+    for (uint32_t e = threadIdx.x; e < 5 * 32; e += blockDim.x) {
+        const uint32_t k = e / 32, t = e % 32, h = 16u >> k;
+        T.stage[k][t] = w((t & (h - 1)) * (n / (2 * h)));
+    }
+    for (uint32_t e = threadIdx.x; e < n1 * 32; e += blockDim.x) {
+        const uint32_t j = e / 32, t = e % 32;
+        T.slot[j][t] = w(t * bitrev_bits(j, bits));
+    }
+}
+
 /* The spectral route for one item of z lines: tile [n][kCorrPitch] holds
- * (cos, sin) of `cols` lines (zero past them), tw[q] = exp(-2 pi i q / n),
- * P[n] receives the item's summed power spectrum.  Writes out[r - 1] for
- * r = 1..rmax. */
+ * (cos, sin) of `cols` lines (zero past them); P[n] receives the item's
+ * summed power spectrum.  Writes out[r - 1] for r = 1..rmax. */
 template <uint32_t N1>
-__device__ void corr_z_spectral(const float2* __restrict__ tile, const double2* __restrict__ tw, double* P,
-                                uint32_t cols, uint32_t rmax, double* __restrict__ out) {
+__device__ void corr_z_spectral(const float2* __restrict__ tile, const FftTables& T, double* P, uint32_t cols,
+                                uint32_t rmax, double* __restrict__ out) {
     constexpr uint32_t n = 32 * N1;
+    constexpr uint32_t bits = N1 == 1 ? 0 : (N1 == 2 ? 1 : (N1 == 4 ? 2 : 3));
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     double pw[N1];
 #pragma unroll
@@ -115,23 +149,20 @@ __device__ void corr_z_spectral(const float2* __restrict__ tile, const double2* 
             for (uint32_t j = 0; j < N1; ++j) {
                 if (j & h) continue;
                 const double2 a = X[j], b = X[j + h];
-                const double2 w = tw[(j & (h - 1)) * (n / (2 * h))];
+                const double2 w = T.reg[(j & (h - 1)) * (n / (2 * h))]; /* same entry across the warp */
                 X[j] = make_double2(a.x + b.x, a.y + b.y);
                 X[j + h] = cmul(make_double2(a.x - b.x, a.y - b.y), w);
             }
         }
-        /* the twiddle w_n^(lane m) of slot j, m = bitrev(j) */
 #pragma unroll
-        for (uint32_t j = 1; j < N1; ++j) {
-            const uint32_t m = (__brev(j) >> (32 - __ffs(N1) + 1)) & (N1 - 1);
-            X[j] = cmul(X[j], tw[(lane * m) & (n - 1)]);
-        }
+        for (uint32_t j = 1; j < N1; ++j) X[j] = cmul(X[j], T.slot[j][lane]);
         /* 32-point decimation-in-frequency FFT across the lanes; lane t ends
          * with frequency index bitrev5(t) */
 #pragma unroll
-        for (uint32_t h = 16; h > 0; h >>= 1) {
+        for (uint32_t k = 0; k < 5; ++k) {
+            const uint32_t h = 16u >> k;
             const bool upper = lane & h;
-            const double2 w = tw[(lane & (h - 1)) * (n / (2 * h))];
+            const double2 w = T.stage[k][lane];
 #pragma unroll
             for (uint32_t j = 0; j < N1; ++j) {
                 const double yx = __shfl_xor_sync(0xffffffffu, X[j].x, h);
@@ -147,27 +178,27 @@ __device__ void corr_z_spectral(const float2* __restrict__ tile, const double2* 
         for (uint32_t j = 0; j < N1; ++j) pw[j] += X[j].x * X[j].x + X[j].y * X[j].y;
     }
     /* the item's spectrum: warps add theirs in order; slot j of lane t is
-     * frequency m + N1 s with m = bitrev(j), s = bitrev5(t) */
+     * frequency bitrev(j) + N1 bitrev5(t) */
     const uint32_t s = __brev(lane) >> 27;
     for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) P[q] = 0.0;
     for (uint32_t w = 0; w < nwarps; ++w) {
         __syncthreads();
         if (warp == w) {
 #pragma unroll
-            for (uint32_t j = 0; j < N1; ++j) {
-                const uint32_t m = N1 == 1 ? 0u : (__brev(j) >> (32 - __ffs(N1) + 1)) & (N1 - 1);
-                P[m + N1 * s] += pw[j];
-            }
+            for (uint32_t j = 0; j < N1; ++j) P[bitrev_bits(j, bits) + N1 * s] += pw[j];
         }
     }
     __syncthreads();
-    /* per-lag sums: (1/n) sum_q P(q) cos(2 pi q r / n) */
+    /* per-lag sums (1/n) sum_q P(q) cos(2 pi q r / n): the phase advances by
+     * a rotation per q (FP64; the rotation error over n steps is ~n ulp) */
     for (uint32_t r = threadIdx.x + 1; r <= rmax; r += blockDim.x) {
-        double a = 0.0;
-        uint32_t idx = 0;
+        const double2 rot = T.reg[r];
+        double a = 0.0, cq = 1.0, sq = 0.0;
         for (uint32_t q = 0; q < n; ++q) {
-            a += P[q] * tw[idx].x;
-            idx = (idx + r) & (n - 1);
+            a = fma(P[q], cq, a);
+            const double c2 = cq * rot.x - sq * rot.y;
+            sq = cq * rot.y + sq * rot.x;
+            cq = c2;
         }
         out[r - 1] = a / (double)n;
     }
@@ -189,8 +220,9 @@ __device__ __forceinline__ const CorrTask& item_task(const CorrTask* __restrict_
 __global__ void __launch_bounds__(kCorrThreads, 2)
     k_corr_zfft(const CorrTask* __restrict__ tasks, CorrTask one, uint32_t n_tasks, uint32_t n_items) {
     extern __shared__ float2 tile[]; /* [n][kCorrPitch] */
-    __shared__ double2 tw[kFftMax];
+    __shared__ FftTables tabs;
     __shared__ double spec[kFftMax];
+    uint32_t tab_n = 0; /* the line length the tables hold */
     for (uint32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
         const CorrTask& T = item_task(tasks, one, n_tasks, item);
         const CorrShape sh = corr_shape(T.lx, T.ly, T.lz, T.rxy, T.rz);
@@ -207,18 +239,17 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
             if (c < cols) __sincosf(T.theta[base + k * plane + c], &sn, &cn);
             tile[k * kCorrPitch + c] = make_float2(cn, sn);
         }
-        for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
-            double sn, cn;
-            sincospi(-2.0 * (double)k / (double)n, &sn, &cn);
-            tw[k] = make_double2(cn, sn);
+        if (n != tab_n) {
+            fft_tables(tabs, n);
+            tab_n = n;
         }
         __syncthreads();
         double* out = T.partial + (size_t)local * sh.rp;
         switch (n) {
-            case 32: corr_z_spectral<1>(tile, tw, spec, cols, T.rz, out); break;
-            case 64: corr_z_spectral<2>(tile, tw, spec, cols, T.rz, out); break;
-            case 128: corr_z_spectral<4>(tile, tw, spec, cols, T.rz, out); break;
-            default: corr_z_spectral<8>(tile, tw, spec, cols, T.rz, out); break;
+            case 32: corr_z_spectral<1>(tile, tabs, spec, cols, T.rz, out); break;
+            case 64: corr_z_spectral<2>(tile, tabs, spec, cols, T.rz, out); break;
+            case 128: corr_z_spectral<4>(tile, tabs, spec, cols, T.rz, out); break;
+            default: corr_z_spectral<8>(tile, tabs, spec, cols, T.rz, out); break;
         }
     }
 }
