@@ -204,6 +204,32 @@ __device__ void corr_z_spectral(const float2* __restrict__ tile, const FftTables
     }
 }
 
+/* Stages n rows of `cols` consecutive angles (row k at base + k * stride) as
+ * (cos, sin) pairs into tile[k * pitch + c], zero past `cols`.  Eight loads
+ * per thread are issued before their trig, so the block keeps many loads in
+ * flight. */
+__device__ __forceinline__ void stage_rows(float2* __restrict__ tile, uint32_t pitch, const float* __restrict__ theta,
+                                           uint32_t base, uint32_t stride, uint32_t n, uint32_t cols) {
+    constexpr uint32_t kU = 8;
+    const uint32_t total = n * kCorrCols;
+    for (uint32_t e0 = threadIdx.x; e0 < total; e0 += kU * blockDim.x) {
+        float v[kU];
+#pragma unroll
+        for (uint32_t u = 0; u < kU; ++u) {
+            const uint32_t e = e0 + u * blockDim.x, k = e / kCorrCols, c = e % kCorrCols;
+            v[u] = (e < total && c < cols) ? theta[base + k * stride + c] : 0.0f;
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < kU; ++u) {
+            const uint32_t e = e0 + u * blockDim.x, k = e / kCorrCols, c = e % kCorrCols;
+            if (e >= total) break;
+            float sn = 0.0f, cn = 0.0f;
+            if (c < cols) __sincosf(v[u], &sn, &cn);
+            tile[k * pitch + c] = make_float2(cn, sn);
+        }
+    }
+}
+
 /* The task of a work item: the last one whose first item is at or before it. */
 __device__ __forceinline__ const CorrTask& item_task(const CorrTask* __restrict__ tasks, const CorrTask& one,
                                                     uint32_t n_tasks, uint32_t item) {
@@ -233,12 +259,7 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
         const uint32_t q = local - sh.nx - sh.ny, y = q / sh.cy, x0 = (q % sh.cy) * kCorrCols;
         const uint32_t cols = min(kCorrCols, T.lx - x0), base = y * T.lx + x0;
         __syncthreads(); /* the previous item's tile and spectrum are no longer read */
-        for (uint32_t e = threadIdx.x; e < n * kCorrCols; e += blockDim.x) {
-            const uint32_t k = e / kCorrCols, c = e % kCorrCols;
-            float sn = 0.0f, cn = 0.0f;
-            if (c < cols) __sincosf(T.theta[base + k * plane + c], &sn, &cn);
-            tile[k * kCorrPitch + c] = make_float2(cn, sn);
-        }
+        stage_rows(tile, kCorrPitch, T.theta, base, plane, n, cols);
         if (n != tab_n) {
             fft_tables(tabs, n);
             tab_n = n;
@@ -292,12 +313,7 @@ __global__ void __launch_bounds__(kCorrThreads)
         __syncthreads(); /* the previous item's tile is no longer read */
         const uint32_t pitch = cstride == 1 ? kCorrCols : kCorrPitch;
         if (cstride == 1) {
-            for (uint32_t e = threadIdx.x; e < n * kCorrCols; e += blockDim.x) {
-                const uint32_t k = e / kCorrCols, c = e % kCorrCols;
-                float sn = 0.0f, cn = 0.0f;
-                if (c < cols) __sincosf(theta[base + k * stride + c], &sn, &cn);
-                tile[k * pitch + c] = make_float2(cn, sn);
-            }
+            stage_rows(tile, pitch, theta, base, stride, n, cols);
         } else {
             /* x lines: consecutive threads take consecutive sites of a row */
             for (uint32_t e = threadIdx.x; e < n * kCorrCols; e += blockDim.x) {
