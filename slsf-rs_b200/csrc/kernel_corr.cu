@@ -62,10 +62,17 @@ constexpr uint32_t kCorrLags = 8;   /* lags per warp pass */
 constexpr uint32_t kCorrRun = 32;   /* k per FP32 run */
 constexpr size_t kCorrMaxTile = 200 * 1024;
 
+constexpr uint32_t kFftMax = 256; /* longest z line of the spectral route */
+constexpr uint32_t kFftMaxN1 = kFftMax / 32;
+
+/* z lines of length n = 32 N1 (N1 = 1, 2, 4, 8) take the spectral route. */
+__host__ __device__ inline bool corr_fft_len(uint32_t n) { return n == 32 || n == 64 || n == 128 || n == 256; }
+
 struct CorrShape {
     uint32_t cx, cy;     /* items per layer: x lines (chunks of rows), y or z lines (chunks of x) */
     uint32_t nx, ny, nz; /* items along x, y, z */
-    uint32_t rp;         /* partial row pitch: max(R, R_z) */
+    uint32_t rp;         /* partial row pitch: max(R, R_z), and L_z / 2 + 1 on the spectral route */
+    bool spectral;       /* z items store folded power spectra */
 };
 
 __host__ __device__ inline CorrShape corr_shape(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
@@ -76,14 +83,11 @@ __host__ __device__ inline CorrShape corr_shape(uint32_t lx, uint32_t ly, uint32
     s.ny = rxy ? lz * s.cy : 0;
     s.nz = rz ? ly * s.cy : 0;
     s.rp = rxy > rz ? rxy : rz;
+    s.spectral = rz > 0 && corr_fft_len(lz);
+    if (s.spectral && s.rp < lz / 2 + 1) s.rp = lz / 2 + 1;
     return s;
 }
 
-constexpr uint32_t kFftMax = 256; /* longest z line of the spectral route */
-constexpr uint32_t kFftMaxN1 = kFftMax / 32;
-
-/* z lines of length n = 32 N1 (N1 = 1, 2, 4, 8) take the spectral route. */
-__host__ __device__ inline bool corr_fft_len(uint32_t n) { return n == 32 || n == 64 || n == 128 || n == 256; }
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -124,10 +128,10 @@ __device__ void fft_tables(FftTables& T, uint32_t n) {
 
 /* The spectral route for one item of z lines: tile [n][kCorrPitch] holds
  * (cos, sin) of `cols` lines (zero past them); P[n] receives the item's
- * summed power spectrum.  Writes out[r - 1] for r = 1..rmax. */
+ * summed power spectrum, out[0 .. n/2] its folded form. */
 template <uint32_t N1>
 __device__ void corr_z_spectral(const float2* __restrict__ tile, const FftTables& T, double* P, uint32_t cols,
-                                uint32_t rmax, double* __restrict__ out) {
+                                double* __restrict__ out) {
     constexpr uint32_t n = 32 * N1;
     constexpr uint32_t bits = N1 == 1 ? 0 : (N1 == 2 ? 1 : (N1 == 4 ? 2 : 3));
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -189,19 +193,11 @@ __device__ void corr_z_spectral(const float2* __restrict__ tile, const FftTables
         }
     }
     __syncthreads();
-    /* per-lag sums (1/n) sum_q P(q) cos(2 pi q r / n): the phase advances by
-     * a rotation per q (FP64; the rotation error over n steps is ~n ulp) */
-    for (uint32_t r = threadIdx.x + 1; r <= rmax; r += blockDim.x) {
-        const double2 rot = T.reg[r];
-        double a = 0.0, cq = 1.0, sq = 0.0;
-        for (uint32_t q = 0; q < n; ++q) {
-            a = fma(P[q], cq, a);
-            const double c2 = cq * rot.x - sq * rot.y;
-            sq = cq * rot.y + sq * rot.x;
-            cq = c2;
-        }
-        out[r - 1] = a / (double)n;
-    }
+    /* the folded spectrum F(0) = P(0), F(q) = P(q) + P(n - q), F(n/2) = P(n/2):
+     * the item's lag sums are (1/n) sum_q F(q) cos(2 pi q r / n), formed once
+     * per task by the finalize from the items' summed F */
+    for (uint32_t q = threadIdx.x; q <= n / 2; q += blockDim.x)
+        out[q] = (q == 0 || q == n / 2) ? P[q] : P[q] + P[n - q];
 }
 
 /* Stages n rows of `cols` consecutive angles (row k at base + k * stride) as
@@ -267,10 +263,10 @@ __global__ void __launch_bounds__(kCorrThreads, 2)
         __syncthreads();
         double* out = T.partial + (size_t)local * sh.rp;
         switch (n) {
-            case 32: corr_z_spectral<1>(tile, tabs, spec, cols, T.rz, out); break;
-            case 64: corr_z_spectral<2>(tile, tabs, spec, cols, T.rz, out); break;
-            case 128: corr_z_spectral<4>(tile, tabs, spec, cols, T.rz, out); break;
-            default: corr_z_spectral<8>(tile, tabs, spec, cols, T.rz, out); break;
+            case 32: corr_z_spectral<1>(tile, tabs, spec, cols, out); break;
+            case 64: corr_z_spectral<2>(tile, tabs, spec, cols, out); break;
+            case 128: corr_z_spectral<4>(tile, tabs, spec, cols, out); break;
+            default: corr_z_spectral<8>(tile, tabs, spec, cols, out); break;
         }
     }
 }
@@ -434,13 +430,15 @@ __global__ void __launch_bounds__(kFinThreads) k_corr_finalize(const CorrTask* _
         emit(R + r, cy);
         emit(2 * R + r, (cx + cy) / 2.0);
     }
-    /* C_z: each lag's sum over the z items in kZParts interleaved partial
-     * sums (items p = q mod kZParts, in order), then the partial sums in
-     * order -- the same order whatever the block size, so every launch of a
-     * task gives the same bits */
+    /* C_z: each column of the z items' rows (a lag, or on the spectral route
+     * a frequency of the folded spectrum) summed over the items in kZParts
+     * interleaved partial sums (items p = q mod kZParts, in order), then the
+     * partial sums in order -- the same order whatever the block size, so
+     * every launch of a task gives the same bits */
     __shared__ double zpart[kZParts * kMaxZLags];
-    for (uint32_t idx = threadIdx.x; idx < Rz * kZParts; idx += blockDim.x) {
-        const uint32_t r = idx % Rz, q = idx / Rz;
+    const uint32_t zc = sh.spectral ? lz / 2 + 1 : Rz; /* columns */
+    for (uint32_t idx = threadIdx.x; idx < zc * kZParts; idx += blockDim.x) {
+        const uint32_t r = idx % zc, q = idx / zc;
         const double* col = part + (size_t)(sh.nx + sh.ny) * sh.rp + r;
         /* in item order; 16 loads in flight before their adds */
         double a = 0.0;
@@ -456,9 +454,22 @@ __global__ void __launch_bounds__(kFinThreads) k_corr_finalize(const CorrTask* _
         zpart[idx] = a;
     }
     __syncthreads();
-    for (uint32_t r = threadIdx.x; r < Rz; r += blockDim.x) {
+    __shared__ double zcol[kMaxZLags];
+    for (uint32_t r = threadIdx.x; r < zc; r += blockDim.x) {
         double sz = 0.0;
-        for (uint32_t q = 0; q < kZParts; ++q) sz += zpart[q * Rz + r];
+        for (uint32_t q = 0; q < kZParts; ++q) sz += zpart[q * zc + r];
+        zcol[r] = sz;
+    }
+    __syncthreads();
+    for (uint32_t r = threadIdx.x; r < Rz; r += blockDim.x) {
+        double sz = zcol[r];
+        if (sh.spectral) {
+            /* lag r + 1 from the summed folded spectrum, in frequency order */
+            const uint32_t n = lz, lag = r + 1;
+            sz = 0.0;
+            for (uint32_t q = 0; q <= n / 2; ++q) sz += zcol[q] * cospi(2.0 * (double)((q * lag) % n) / (double)n);
+            sz /= (double)n;
+        }
         emit(3 * R + lz * R + r, sz / volume);
     }
     __syncthreads();
