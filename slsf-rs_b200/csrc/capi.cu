@@ -61,13 +61,18 @@ const char* kErrTemperature = "temperature T must be positive and finite";
 const char* kErrWidth = "proposal_width must be nonnegative and finite";
 const char* kErrEven = "red-black Metropolis sweep requires even lattice dimensions";
 const char* kErrCorrLong = "correlation lines plus lags longer than 775 sites are not supported";
-const char* kErrFuse = "correlations inside the sweeps need the one-CTA kernel (even L_x <= 32, replica in shared memory)";
+const char* kErrFuse =
+    "correlations inside the sweeps need the one-CTA kernel (even L_x <= 32, replica in shared memory) or the grid-wide kernels";
 const char* kErrFused = "task measures its correlations inside the batched sweeps (slsf_task_corr_fuse)";
 
 bool temperature_ok(double t) { return t > 0.0 && std::isfinite(t); }
 bool width_ok(double w) { return w >= 0.0 && std::isfinite(w); }
 
 uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
+
+/* Kernels of one correlation measurement (launch_corr): the line items, the
+ * spectral z items when there are z items, and the finalize. */
+uint32_t corr_launch_count(uint32_t items, uint32_t z_items) { return items ? (z_items ? 3u : 2u) : 1u; }
 
 /* Side streams for the kernel groups of a batch after the first (group g
  * runs on side[(g - 1) % kSideStreams]); each group has its own work-queue
@@ -754,7 +759,7 @@ int slsf_task_correlations(slsf_task* t, uint32_t rmax_xy, uint32_t rmax_z, doub
     e = slsf::launch_corr(nullptr, &ct, 1, items, slsf::corr_len(t->lx, t->ly, t->lz, rmax_xy, rmax_z),
                           std::max(rmax_xy, rmax_z), slsf::corr_z_items(t->lx, t->ly, t->lz, rmax_xy, rmax_z),
                           ctx->sm_count, ctx->stream);
-    ctx->launches += items ? 2 : 1;
+    ctx->launches += corr_launch_count(items, slsf::corr_z_items(t->lx, t->ly, t->lz, rmax_xy, rmax_z));
     if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), ct.values, 8ull * nv, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     ctx->pool.free(dv, bytes);
@@ -830,9 +835,12 @@ int slsf_task_corr_fuse(slsf_task* t, uint32_t interval) {
     if (int rc = check_free(t)) return rc;
     if (interval && !t->corr_block)
         return set_error(SLSF_ERR_STATE, "task has no correlation bins; call slsf_task_corr_setup first");
-    /* the context's kernel choice for this shape (default or tuned) must be the one-CTA kernel */
+    /* the context's kernel choice for this shape (default or tuned) must be the
+     * one-CTA kernel (correlations from the replica in shared memory) or the
+     * grid-wide kernels (the correlation launches queued after the sweep) */
     slsf_kernel_choice kc = {};
-    if (interval && (slsf_tune_get(t->ctx, t->lx, t->ly, t->lz, &kc) != SLSF_OK || kc.kind != SLSF_KERNEL_RESIDENT))
+    if (interval && (slsf_tune_get(t->ctx, t->lx, t->ly, t->lz, &kc) != SLSF_OK ||
+                     (kc.kind != SLSF_KERNEL_RESIDENT && kc.kind != SLSF_KERNEL_GRID)))
         return set_error(SLSF_ERR_INVALID, kErrFuse);
     t->corr_interval = interval;
     return SLSF_OK;
@@ -915,7 +923,7 @@ int slsf_batch_correlations(slsf_ctx* ctx, slsf_task* const* tasks, size_t n) {
     }
     SLSF_CUDA(slsf::launch_corr(ctx->d_corr, nullptr, (uint32_t)n, ctx->corr_last_items, ctx->corr_last_len,
                                 ctx->corr_last_r, ctx->corr_last_nz, ctx->sm_count, ctx->stream));
-    ctx->launches += ctx->corr_last_items ? 2 : 1;
+    ctx->launches += corr_launch_count(ctx->corr_last_items, ctx->corr_last_nz);
     for (size_t i = 0; i < n; ++i) tasks[i]->corr_count += 1;
     return SLSF_OK;
 }
@@ -1095,6 +1103,22 @@ static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v, 
                 ctx->launches += 1;
             }
         }
+        /* ThetaModel::measure's correlations of the state after this sweep
+         * (slsf_task_corr_fuse), as the one-CTA kernel takes them: measurement
+         * m = sweep - thermalization, every corr_interval-th, into the bins */
+        if (t->corr_interval && t->corr_block && sweep >= t->thermalization &&
+            (sweep - t->thermalization) % t->corr_interval == 0) {
+            const slsf::CorrTask ct = {t->theta,         t->lx,         t->ly,          t->lz,
+                                       t->corr_rxy,      t->corr_rz,    0,              t->corr_binsize,
+                                       t->corr_n_bins,   t->corr_partial, nullptr,      t->corr_bins,
+                                       t->corr_count_dev};
+            const uint32_t items = slsf::corr_items(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz);
+            slsf::launch_corr(nullptr, &ct, 1, items, slsf::corr_len(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz),
+                              std::max(t->corr_rxy, t->corr_rz),
+                              slsf::corr_z_items(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz), ctx->sm_count, st);
+            ctx->launches +=
+                corr_launch_count(items, slsf::corr_z_items(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz));
+        }
     }
 }
 
@@ -1218,7 +1242,7 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
         ch[i] = force ? *force : choice_for(ctx, t->lx, t->ly, t->lz);
         if (!choice_feasible(ch[i], t->lx, t->ly, t->lz, ctx->device))
             return set_error(SLSF_ERR_INVALID, "the kernel choice does not hold this lattice");
-        if (t->corr_interval && ch[i].kind != slsf::kKernelResident) return set_error(SLSF_ERR_INVALID, kErrFuse);
+        if (t->corr_interval && ch[i].kind == slsf::kKernelCluster) return set_error(SLSF_ERR_INVALID, kErrFuse);
     }
     if (int rc = ensure_batch_capacity(ctx, n)) return rc;
     /* Grouped by kernel choice (one persistent launch each; cluster groups
@@ -1373,7 +1397,7 @@ int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n
         if (ch[i].kind == slsf::kKernelGrid || !choice_feasible(ch[i], t->lx, t->ly, t->lz, ctx->device))
             return set_error(SLSF_ERR_INVALID,
                              "batch sessions hold lattices that fit one thread-block cluster's shared memory");
-        if (t->corr_interval && ch[i].kind != slsf::kKernelResident) return set_error(SLSF_ERR_INVALID, kErrFuse);
+        if (t->corr_interval && ch[i].kind == slsf::kKernelCluster) return set_error(SLSF_ERR_INVALID, kErrFuse);
     }
     auto rank = [&](size_t i) {
         const slsf::KernelChoice& c = ch[i];

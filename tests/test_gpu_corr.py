@@ -221,6 +221,45 @@ def test_fused_correlations_equal_separate(slsf, ctx, orc, interval):
         b.close()
 
 
+def test_fused_correlations_on_the_grid_path_equal_separate(slsf, ctx, orc):
+    # A lattice too large for one cluster's shared memory runs through the
+    # grid-wide kernels; with slsf_task_corr_fuse its correlations are launched
+    # after every interval-th sweep inside the same batched call, with no host
+    # round trip per sweep: the same kernels as the separate measurement, so
+    # the same bits.
+    d, therm, sweeps, interval = (128, 32, 32), 1, 5, 2
+    n_corr = (sweeps - therm + interval - 1) // interval
+    jxy, jz = np.full(d[2], 1.2), orc.uniform_disorder(d[2], 0.5, 1.5, 80)
+
+    def make():
+        t = slsf.Task(ctx, d, jxy, jz, 1.3, seed=80, thermalization=therm, binsize=2, n_bins=2)
+        t.init_random()
+        t.corr_setup(8, d[2] // 2, 1, n_corr)
+        return t
+
+    ctx.tune_set(d, "grid", 1, 256)
+    fused, sep = make(), make()
+    fused.corr_fuse(interval)
+    ctx.batch_run([fused], sweeps)
+    ctx.batch_run([sep], therm)
+    done = therm
+    for m in range(0, sweeps - therm, interval):
+        ctx.batch_run([sep], therm + m + 1 - done)
+        done = therm + m + 1
+        ctx.batch_correlations([sep])
+    ctx.batch_run([sep], sweeps - done)
+    assert np.array_equal(fused.theta.view(np.uint32), sep.theta.view(np.uint32))
+    ma, na = fused.corr_bins()
+    mb, nb = sep.corr_bins()
+    assert na == nb == n_corr
+    assert np.array_equal(ma, mb)
+    ba, _ = fused.bins()
+    bb, _ = sep.bins()
+    assert np.array_equal(ba, bb)
+    fused.close()
+    sep.close()
+
+
 def test_fused_in_sessions_and_refusals(slsf, ctx, orc):
     t = task(slsf, ctx, orc, (16, 16, 16), 70)
     with pytest.raises(slsf.SlsfError) as e:
@@ -238,11 +277,11 @@ def test_fused_in_sessions_and_refusals(slsf, ctx, orc):
             ses.step_correlations(1)
     _, n = t.corr_bins()
     assert n == 8
-    big = task(slsf, ctx, orc, (48, 48, 48), 71)
+    big = task(slsf, ctx, orc, (48, 48, 48), 71)  # the cluster kernel by default
     big.corr_setup(4, 4, 1, 1)
     with pytest.raises(slsf.SlsfError) as e:
         big.corr_fuse(1)
-    assert "one-CTA kernel" in str(e.value)
+    assert "one-CTA kernel" in str(e.value) and "grid-wide kernels" in str(e.value)
     # a shape that fits the one-CTA kernel but is tuned to the cluster kernel
     small = task(slsf, ctx, orc, (12, 12, 12), 72)
     small.corr_setup(6, 6, 1, 1)
