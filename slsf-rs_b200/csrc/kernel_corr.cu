@@ -89,23 +89,24 @@ __host__ __device__ inline CorrShape corr_shape(uint32_t lx, uint32_t ly, uint32
 }
 
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
 
-/* Twiddles of the spectral route, laid out so that a warp reads 32
+/* Twiddles of the spectral route (FP32), laid out so that a warp reads 32
  * consecutive entries: stage[k][t] = w_(2h)^(t mod h) for the lane stage of
  * half-size h = 16 >> k, slot[j][t] = w_n^(t bitrev(j)) for register slot j,
- * reg[q] = w_n^q for q < n (the register stages and the inverse transform),
- * with w_N = exp(-2 pi i / N). */
+ * reg[q] = w_n^q for q < n (the register stages), with w_N = exp(-2 pi i / N)
+ * evaluated in FP64 and rounded. */
 struct FftTables {
-    double2 stage[5][32];
-    double2 slot[kFftMaxN1][32];
-    double2 reg[kFftMax];
+    float2 stage[5][32];
+    float2 slot[kFftMaxN1][32];
+    float2 reg[kFftMax];
 };
 
 __device__ __forceinline__ uint32_t bitrev_bits(uint32_t j, uint32_t bits) {
     return bits ? (__brev(j) >> (32 - bits)) : 0u;
+}
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
 __device__ void fft_tables(FftTables& T, uint32_t n) {
@@ -113,7 +114,7 @@ __device__ void fft_tables(FftTables& T, uint32_t n) {
     auto w = [&](uint32_t q) {
         double sn, cn;
         sincospi(-2.0 * (double)(q & (n - 1)) / (double)n, &sn, &cn);
-        return make_double2(cn, sn);
+        return make_float2((float)cn, (float)sn);
     };
     for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) T.reg[q] = w(q);
     for (uint32_t e = threadIdx.x; e < 5 * 32; e += blockDim.x) {
@@ -128,7 +129,10 @@ __device__ void fft_tables(FftTables& T, uint32_t n) {
 
 /* The spectral route for one item of z lines: tile [n][kCorrPitch] holds
  * (cos, sin) of `cols` lines (zero past them); P[n] receives the item's
- * summed power spectrum, out[0 .. n/2] its folded form. */
+ * summed power spectrum (FP64), out[0 .. n/2] its folded form.  The
+ * transforms run in FP32: their rounding moves C_z by about 1e-8 on
+ * ordered-phase lines, against the 2e-6 agreement held with the FP64
+ * oracle. */
 template <uint32_t N1>
 __device__ void corr_z_spectral(const float2* __restrict__ tile, const FftTables& T, double* P, uint32_t cols,
                                 double* __restrict__ out) {
@@ -139,12 +143,9 @@ __device__ void corr_z_spectral(const float2* __restrict__ tile, const FftTables
 #pragma unroll
     for (uint32_t m = 0; m < N1; ++m) pw[m] = 0.0;
     for (uint32_t c = warp; c < cols; c += nwarps) {
-        double2 X[N1];
+        float2 X[N1];
 #pragma unroll
-        for (uint32_t j = 0; j < N1; ++j) {
-            const float2 v = tile[(lane + 32 * j) * kCorrPitch + c];
-            X[j] = make_double2((double)v.x, (double)v.y);
-        }
+        for (uint32_t j = 0; j < N1; ++j) X[j] = tile[(lane + 32 * j) * kCorrPitch + c];
         /* radix-2 decimation in frequency over j in registers (N1-point DFT of
          * the elements lane + 32 j); slot j ends with frequency bitrev(j) */
 #pragma unroll
@@ -152,34 +153,35 @@ __device__ void corr_z_spectral(const float2* __restrict__ tile, const FftTables
 #pragma unroll
             for (uint32_t j = 0; j < N1; ++j) {
                 if (j & h) continue;
-                const double2 a = X[j], b = X[j + h];
-                const double2 w = T.reg[(j & (h - 1)) * (n / (2 * h))]; /* same entry across the warp */
-                X[j] = make_double2(a.x + b.x, a.y + b.y);
-                X[j + h] = cmul(make_double2(a.x - b.x, a.y - b.y), w);
+                const float2 a = X[j], b = X[j + h];
+                const float2 w = T.reg[(j & (h - 1)) * (n / (2 * h))]; /* same entry across the warp */
+                X[j] = make_float2(a.x + b.x, a.y + b.y);
+                X[j + h] = cmulf(make_float2(a.x - b.x, a.y - b.y), w);
             }
         }
 #pragma unroll
-        for (uint32_t j = 1; j < N1; ++j) X[j] = cmul(X[j], T.slot[j][lane]);
+        for (uint32_t j = 1; j < N1; ++j) X[j] = cmulf(X[j], T.slot[j][lane]);
         /* 32-point decimation-in-frequency FFT across the lanes; lane t ends
          * with frequency index bitrev5(t) */
 #pragma unroll
         for (uint32_t k = 0; k < 5; ++k) {
             const uint32_t h = 16u >> k;
             const bool upper = lane & h;
-            const double2 w = T.stage[k][lane];
+            const float2 w = T.stage[k][lane];
 #pragma unroll
             for (uint32_t j = 0; j < N1; ++j) {
-                const double yx = __shfl_xor_sync(0xffffffffu, X[j].x, h);
-                const double yy = __shfl_xor_sync(0xffffffffu, X[j].y, h);
-                if (!upper) {
-                    X[j] = make_double2(X[j].x + yx, X[j].y + yy);
-                } else {
-                    X[j] = cmul(make_double2(yx - X[j].x, yy - X[j].y), w);
-                }
+                const float yx = __shfl_xor_sync(0xffffffffu, X[j].x, h);
+                const float yy = __shfl_xor_sync(0xffffffffu, X[j].y, h);
+                const float2 sum = make_float2(X[j].x + yx, X[j].y + yy);
+                const float2 dif = cmulf(make_float2(yx - X[j].x, yy - X[j].y), w);
+                X[j] = upper ? dif : sum;
             }
         }
 #pragma unroll
-        for (uint32_t j = 0; j < N1; ++j) pw[j] += X[j].x * X[j].x + X[j].y * X[j].y;
+        for (uint32_t j = 0; j < N1; ++j) {
+            const double re = (double)X[j].x, im = (double)X[j].y;
+            pw[j] += re * re + im * im;
+        }
     }
     /* the item's spectrum: warps add theirs in order; slot j of lane t is
      * frequency bitrev(j) + N1 bitrev5(t) */
@@ -239,7 +241,7 @@ __device__ __forceinline__ const CorrTask& item_task(const CorrTask* __restrict_
 }
 
 /* The spectral route for z items (one block per item; other items return). */
-__global__ void __launch_bounds__(kCorrThreads, 2)
+__global__ void __launch_bounds__(kCorrThreads, 3)
     k_corr_zfft(const CorrTask* __restrict__ tasks, CorrTask one, uint32_t n_tasks, uint32_t n_items) {
     extern __shared__ float2 tile[]; /* [n][kCorrPitch] */
     __shared__ FftTables tabs;
