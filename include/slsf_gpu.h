@@ -255,12 +255,15 @@ int slsf_task_correlations(slsf_task* task, uint32_t rmax_xy, uint32_t rmax_z, d
 int slsf_task_corr_setup(slsf_task* task, uint32_t rmax_xy, uint32_t rmax_z, uint32_t binsize, uint32_t n_bins,
                          size_t* n_values);
 /* Correlations measured inside the batched sweeps: with interval > 0,
- * every batched run or session step of the task (one-CTA kernel: even
- * L_x <= 32 and a replica that fits shared memory) measures the correlation
+ * every batched run or session step of the task measures the correlation
  * functions of the state after each sweep whose measurement index
- * m = sweep - thermalization is a multiple of `interval`, from the replica
- * in shared memory, into the bins of slsf_task_corr_setup (ThetaModel::measure,
- * src/model.rs:410, with correlation_interval = interval).  0 turns it off.
+ * m = sweep - thermalization is a multiple of `interval` into the bins of
+ * slsf_task_corr_setup (ThetaModel::measure, src/model.rs:410, with
+ * correlation_interval = interval): from the replica in shared memory on the
+ * one-CTA kernel (even L_x <= 32 and a replica that fits shared memory), or
+ * by the correlation kernels queued after those sweeps on the grid-wide
+ * kernels (lattices too large for one cluster; not in sessions).  Tasks on
+ * the cluster kernel are refused.  0 turns it off.
  * Such a task refuses the separate measurements (slsf_batch_correlations,
  * slsf_batch_step_correlations).  Values agree with the separate kernels to
  * FP32 partial-sum rounding. */
