@@ -316,6 +316,114 @@ __device__ __forceinline__ uint32_t half_sweep(const TaskView& t, const Geo& g, 
     return accepted;
 }
 
+/* The same colour half-sweep for L_x = 32, walking along z.  A warp owns a
+ * pair of rows (y0, y0 + 1) for a run of planes: lanes 0-15 hold row y0 and
+ * lanes 16-31 row y0 + 1, lane k of a group updating the colour-c site of
+ * compact index k (x = 2k + parity).  At every plane the lane keeps the trig
+ * of the other colour's site of the same compact index on the planes below,
+ * at and above (the z neighbours; a window that takes one sincos per plane);
+ * the x neighbours are that value of lanes k and k -/+ 1, the y neighbour
+ * inside the pair the other group's, and only the y neighbour outside the
+ * pair is loaded: four sincos per update instead of eight, and no per-site
+ * index division.  Operands, rounding order and randoms are those of
+ * half_sweep, so decisions and new angles are bit-identical.  The lane pair
+ * (2m, 2m + 1) shares one Philox block per plane: the even lane computes the
+ * block of plane z and the odd lane that of plane z + 1, and each passes the
+ * other the two words it needs. */
+template <bool kMeasure>
+__device__ __forceinline__ uint32_t half_sweep_walk32(const TaskView& t, const Geo& g, Smem& s, uint64_t sweep,
+                                                      uint32_t colour, double (&acc)[8]) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t grp = lane >> 4, k = lane & 15u, odd = k & 1u;
+    const uint32_t own = colour * g.stride1, other = (colour ^ 1u) * g.stride1;
+    const uint32_t pairs = g.ly >> 1;
+    /* planes per unit: every warp gets work when there are fewer pairs than warps */
+    const uint32_t nseg = max(1u, min(g.lz / 2, nwarps / max(1u, pairs)));
+    const uint32_t seglen = (g.lz + nseg - 1) / nseg;
+    const uint32_t lk = grp * 16u + ((k + 15u) & 15u), rk = grp * 16u + ((k + 1u) & 15u);
+    uint32_t accepted = 0;
+    for (uint32_t u = warp; u < pairs * nseg; u += nwarps) {
+        const uint32_t m = u / nseg, sgi = u - m * nseg;
+        const uint32_t z_lo = sgi * seglen, z_hi = min(g.lz, z_lo + seglen);
+        if (z_lo >= z_hi) continue;
+        const uint32_t yr = 2u * m + grp;
+        const uint32_t yext = grp ? (yr + 1 == g.ly ? 0u : yr + 1) : (yr == 0 ? g.ly - 1 : yr - 1);
+        auto trig_other = [&](uint32_t y, uint32_t z) {
+            float sn, cn;
+            __sincosf(s.th[other + (y + g.ly * z) * 16u + k], &sn, &cn);
+            return make_float2(cn, sn);
+        };
+        float2 om = trig_other(yr, z_lo == 0 ? g.lz - 1 : z_lo - 1);
+        float2 o0 = trig_other(yr, z_lo);
+        slsf_u32x4 blk = {0, 0, 0, 0};
+        uint32_t w0 = 0, w1 = 0;
+        for (uint32_t z = z_lo; z < z_hi; ++z) {
+            const uint32_t zi = z - z_lo;
+            if ((zi & 1u) == 0) {
+                /* the pair's blocks for planes z and z + 1 */
+                const uint32_t unit = ((yr + g.ly * (z + odd)) * 16u + k) >> 1;
+                blk = slsf_stream(t.seed, sweep, SLSF_PURPOSE_METRO, colour, unit);
+                w0 = __shfl_xor_sync(0xffffffffu, odd ? blk.x : blk.z, 1);
+                w1 = __shfl_xor_sync(0xffffffffu, odd ? blk.y : blk.w, 1);
+            }
+            /* plane z: the even lane's own block (x, y), the odd lane the even
+             * lane's (z, w); plane z + 1: the even lane the odd lane's (x, y),
+             * the odd lane its own (z, w) */
+            const bool first = (zi & 1u) == 0;
+            const uint32_t wp = first ? (odd ? w0 : blk.x) : (odd ? blk.z : w0);
+            const uint32_t wa = first ? (odd ? w1 : blk.y) : (odd ? blk.w : w1);
+            const float u_prop = slsf_u24f(wp), u_acc = slsf_u24f(wa);
+            const float2 op = trig_other(yr, z + 1 == g.lz ? 0u : z + 1);
+            const float2 oy = trig_other(yext, z);
+            /* neighbours: x from this group's window, y inside the pair from the other group */
+            const float lc = __shfl_sync(0xffffffffu, o0.x, lk), ls = __shfl_sync(0xffffffffu, o0.y, lk);
+            const float rc = __shfl_sync(0xffffffffu, o0.x, rk), rs = __shfl_sync(0xffffffffu, o0.y, rk);
+            const float pc = __shfl_xor_sync(0xffffffffu, o0.x, 16), ps = __shfl_xor_sync(0xffffffffu, o0.y, 16);
+            const uint32_t parity = (colour + yr + z) & 1u;
+            /* parity 0: +x is this lane's other-colour site, -x lane k - 1's; parity 1: -x own, +x lane k + 1's */
+            const float cxp = parity ? rc : o0.x, sxp = parity ? rs : o0.y;
+            const float cxm = parity ? o0.x : lc, sxm = parity ? o0.y : ls;
+            const float cyp = grp ? oy.x : pc, syp = grp ? oy.y : ps;
+            const float cym = grp ? pc : oy.x, sym = grp ? ps : oy.y;
+            const uint32_t q = (yr + g.ly * z) * 16u + k;
+            const float jx = s.jxy[z], jzp = s.jz[z], jzm = s.jz[z == 0 ? g.lz - 1 : z - 1];
+            const float th = s.th[own + q];
+            float si, ci;
+            __sincosf(th, &si, &ci);
+            if (kMeasure) {
+                acc[0] += (double)ci + (double)cxp;
+                acc[1] += (double)si + (double)sxp;
+                acc[2] += (double)bond_cos(jx, ci, si, cxp, sxp) + (double)bond_cos(jx, cxm, sxm, ci, si);
+                acc[5] += (double)bond_sin(jx, ci, si, cxp, sxp) + (double)bond_sin(jx, cxm, sxm, ci, si);
+                acc[3] += (double)bond_cos(jx, ci, si, cyp, syp) + (double)bond_cos(jx, cym, sym, ci, si);
+                acc[6] += (double)bond_sin(jx, ci, si, cyp, syp) + (double)bond_sin(jx, cym, sym, ci, si);
+                acc[4] += (double)bond_cos(jzp, ci, si, op.x, op.y) + (double)bond_cos(jzm, om.x, om.y, ci, si);
+                acc[7] += (double)bond_sin(jzp, ci, si, op.x, op.y) + (double)bond_sin(jzm, om.x, om.y, ci, si);
+            }
+            const float hx01 = __fadd_rn(cxp, cxm), hy01 = __fadd_rn(sxp, sxm);
+            const float hx23 = __fadd_rn(cyp, cym), hy23 = __fadd_rn(syp, sym);
+            const float hx = field_from_pairs(jx, jzp, jzm, hx01, hx23, op.x, om.x);
+            const float hy = field_from_pairs(jx, jzp, jzm, hy01, hy23, op.y, om.y);
+            float tn, sn, cn;
+            if (metro_decide(th, ci, si, hx, hy, t.beta, t.width, u_prop, u_acc, &tn, &sn, &cn)) {
+                s.th[own + q] = tn;
+                ++accepted;
+            }
+            om = o0;
+            o0 = op;
+        }
+    }
+    return accepted;
+}
+
+/* One colour half-sweep: the z walk for L_x = 32, the general form otherwise. */
+template <bool kMeasure>
+__device__ __forceinline__ uint32_t sweep_colour(const TaskView& t, const Geo& g, Smem& s, uint64_t sweep,
+                                                 uint32_t colour, double (&acc)[8]) {
+    if (g.lx == 32) return half_sweep_walk32<kMeasure>(t, g, s, sweep, colour, acc);
+    return half_sweep<kMeasure>(t, g, s, sweep, colour, acc);
+}
+
 __device__ __forceinline__ float site_theta(const Geo& g, const Smem& s, uint32_t idx, const Coords& c) {
     return s.th[slot(g, idx, (c.x + c.y + c.z) & 1u)];
 }
@@ -842,18 +950,18 @@ __global__ void __launch_bounds__(kBThreads, 1)
             const uint64_t sweep = t.metro_sweeps + sw;
             double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             if (measuring && sw > 0 && sweep > t.thermalization) {
-                accepted += half_sweep<true>(t, g, s, sweep, 0, acc);
+                accepted += sweep_colour<true>(t, g, s, sweep, 0, acc);
                 double tot[8];
 #pragma unroll
                 for (int k = 0; k < 8; ++k) tot[k] = acc[k];
                 block_sum<8>(tot, red);
                 if (threadIdx.x == 0) bin_measurement(t, g.volume, sweep, tot, bin_acc, bin_cur);
             } else {
-                accepted += half_sweep<false>(t, g, s, sweep, 0, acc);
+                accepted += sweep_colour<false>(t, g, s, sweep, 0, acc);
             }
             __syncthreads();
             SLSF_PHASE(0);
-            accepted += half_sweep<false>(t, g, s, sweep, 1, acc);
+            accepted += sweep_colour<false>(t, g, s, sweep, 1, acc);
             __syncthreads();
             SLSF_PHASE(1);
             for (uint32_t k = 0; k < t.wolff_steps; ++k)
