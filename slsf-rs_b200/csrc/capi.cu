@@ -1296,8 +1296,10 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
         size_t hi = lo;
         const uint32_t parts = c.kind == slsf::kKernelCluster ? c.cluster : 1;
         uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0, max_lx = 0, max_cd = 0;
+        bool cube32 = false;
         while (hi < n && rank(order[hi]) == key) {
             const slsf_task* t = tasks[order[hi]];
+            cube32 |= t->lx == 32 && t->ly == 32 && t->lz == 32;
             max_cd = std::max(max_cd, rcorr_doubles(t));
             max_vs = std::max(max_vs, t->volume / parts);
             max_rows = std::max(max_rows, t->ly * (t->lz / parts));
@@ -1311,7 +1313,7 @@ static int batch_run_impl(slsf_ctx* ctx, slsf_task* const* all_tasks, size_t n_a
         } else if (c.kind == slsf::kKernelResident) {
             SLSF_CUDA(slsf::launch_resident(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
                                             ctx->device, st, max_vs, max_rows, max_lz, c.threads, nullptr,
-                                            max_cd ? ctx->d_rcorr + lo : nullptr, max_cd));
+                                            max_cd ? ctx->d_rcorr + lo : nullptr, max_cd, cube32));
             ctx->launches += 1;
         } else {
             SLSF_CUDA(slsf::launch_batched(ctx->d_views + lo, (uint32_t)(hi - lo), n_sweeps, ctx->d_queue + q,
@@ -1472,8 +1474,10 @@ int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n
         size_t hi = lo;
         const uint32_t parts = c.kind == slsf::kKernelCluster ? c.cluster : 1;
         uint32_t max_vs = 0, max_rows = 0, max_lz = 0, max_plane = 0, max_lx = 0, max_cd = 0;
+        bool cube32 = false;
         while (hi < n && rank(order[hi]) == key) {
             const slsf_task* t = tasks[order[hi]];
+            cube32 |= t->lx == 32 && t->ly == 32 && t->lz == 32;
             max_cd = std::max(max_cd, rcorr_doubles(t));
             max_vs = std::max(max_vs, t->volume / parts);
             max_rows = std::max(max_rows, t->ly * (t->lz / parts));
@@ -1486,7 +1490,7 @@ int slsf_batch_open(slsf_ctx* ctx, slsf_task* const* tasks, size_t n, uint32_t n
             if (c.kind == slsf::kKernelResident)
                 e = slsf::launch_resident(b->d_views + lo, (uint32_t)(hi - lo), n_sweeps, b->d_queue + q, ctx->device,
                                           st, max_vs, max_rows, max_lz, c.threads, b->d_counters + 2 * lo,
-                                          max_cd ? b->d_rcorr + lo : nullptr, max_cd);
+                                          max_cd ? b->d_rcorr + lo : nullptr, max_cd, cube32);
             else
                 e = slsf::launch_batched(b->d_views + lo, (uint32_t)(hi - lo), n_sweeps, b->d_queue + q, ctx->device,
                                          st, c.cluster, c.threads, max_vs, max_rows, max_lz, max_plane, max_lx,

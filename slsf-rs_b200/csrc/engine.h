@@ -143,11 +143,12 @@ bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);
  * `queue` is a zeroed device counter.  With `counters` (2 per view, may be
  * NULL) the Metropolis and Wolff counters come from there instead of the
  * views and are advanced in place, so a replayed launch continues.  max_* are the largest volume, row
- * count (Ly Lz) and Lz over the views. */
+ * count (Ly Lz) and Lz over the views; cube32: some view is a 32^3 lattice (its Wolff growth then runs
+ * the warp-scan closure of bitgrow.cuh in 17 KB of extra shared memory). */
 cudaError_t launch_resident(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                             int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
                             uint32_t threads, unsigned long long* counters, const ResidentCorr* corr_dev = nullptr,
-                            uint32_t corr_doubles = 0);
+                            uint32_t corr_doubles = 0, bool cube32 = false);
 /* Shared doubles the fused correlation measurement of one task needs (0 without). */
 uint32_t resident_corr_doubles(uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
 

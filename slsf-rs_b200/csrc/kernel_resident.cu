@@ -33,6 +33,7 @@
 #include <algorithm>
 
 #include "bins.cuh"
+#include "bitgrow.cuh"
 #include "engine.h"
 #include "fastdiv.h"
 #include "xy_device.cuh"
@@ -165,10 +166,15 @@ struct Smem {
     uint32_t* cl;
     float* jxy;
     float* jz;
-    double* corr; /* fused correlation scratch (resident_corr_doubles) */
+    uint32_t* blk; /* 32^3 replicas: cluster and bond words as [z][y] blocks of pitch 33 (cube32), else NULL */
+    double* corr;  /* fused correlation scratch (resident_corr_doubles) */
 };
 
-__device__ __forceinline__ Smem carve(unsigned char* base, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz) {
+/* Words of the padded blocks of a 32^3 replica's Wolff growth (C, BY, BZ, BX). */
+constexpr uint32_t kBlockWords = 4 * kGrowEdge * (kGrowEdge + 1);
+
+__device__ __forceinline__ Smem carve(unsigned char* base, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
+                                      uint32_t cube32) {
     Smem s;
     s.th = reinterpret_cast<float*>(base);
     uint32_t* w = reinterpret_cast<uint32_t*>(base + 4ull * (max_volume + 2 * kPad));
@@ -178,8 +184,11 @@ __device__ __forceinline__ Smem carve(unsigned char* base, uint32_t max_volume, 
     s.cl = w + 3 * max_rows;
     s.jxy = reinterpret_cast<float*>(w + 4 * max_rows);
     s.jz = s.jxy + max_lz;
+    uint32_t* after = reinterpret_cast<uint32_t*>(s.jz + max_lz);
+    s.blk = cube32 ? after : nullptr;
+    if (cube32) after += kBlockWords;
     /* 8-byte aligned: the volume is even, the other arrays are whole words */
-    s.corr = reinterpret_cast<double*>(s.jz + max_lz);
+    s.corr = reinterpret_cast<double*>(after);
     return s;
 }
 
@@ -671,7 +680,26 @@ __device__ __forceinline__ void wolff_update(const TaskView& t, const Geo& g, Sm
     const uint32_t bound = t.loop_limit ? min(t.loop_limit, g.volume) : g.volume;
     uint32_t pass = 0;
     bool converged = false;
-    if (g.rows <= blockDim.x) {
+    if (s.blk && g.lx == 32 && g.ly == 32 && g.lz == 32 && blockDim.x == 1024) {
+        /* a 32^3 replica is one block of the shared bit-parallel closure: warp
+         * scans along y and z, a few passes instead of one row step per pass */
+        typedef uint32_t Row[kGrowEdge + 1];
+        Row* C = reinterpret_cast<Row*>(s.blk);
+        Row* BY = C + kGrowEdge;
+        Row* BZ = BY + kGrowEdge;
+        Row* BX = BZ + kGrowEdge;
+        const uint32_t z = threadIdx.x >> 5, y = threadIdx.x & 31u, r = y + 32u * z;
+        C[z][y] = s.cl[r];
+        BY[z][y] = s.by[r];
+        BZ[z][y] = s.bz[r];
+        BX[z][y] = s.bx[r];
+        __syncthreads();
+        const uint32_t used = close_block(C, BY, BZ, BX, true, true, true, bound + 1);
+        converged = used != 0;
+        pass = used ? used - 1 : bound;
+        s.cl[r] = C[z][y];
+        __syncthreads();
+    } else if (g.rows <= blockDim.x) {
         /* one row per thread: its neighbour rows and bond masks stay fixed
          * during the growth, so they are read once */
         const uint32_t r = threadIdx.x;
@@ -910,7 +938,7 @@ template <bool kCorr>
 __global__ void __launch_bounds__(kBThreads, 1)
     k_resident(const TaskView* __restrict__ views, uint32_t n, uint32_t n_sweeps, unsigned int* __restrict__ queue,
                uint32_t max_volume, uint32_t max_rows, uint32_t max_lz, unsigned long long* __restrict__ counters,
-               const ResidentCorr* __restrict__ corr) {
+               const ResidentCorr* __restrict__ corr, uint32_t cube32) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[8 * 32];
     __shared__ double bin_acc[kBinCols];
@@ -929,7 +957,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
             t.wolff_done = counters[2 * item + 1];
         }
         const Geo g = make_geo(t);
-        Smem s = carve(smem_raw, max_volume, max_rows, max_lz);
+        Smem s = carve(smem_raw, max_volume, max_rows, max_lz, cube32);
         if (threadIdx.x == 0) {
             s_cluster = 0;
             s_accepted = 0;
@@ -1005,16 +1033,18 @@ __global__ void __launch_bounds__(kBThreads, 1)
     }
 }
 
-size_t smem_bytes(uint32_t max_volume, uint32_t max_rows, uint32_t max_lz, uint32_t corr_doubles = 0) {
-    return 4ull * (max_volume + 2 * kPad) + 16ull * max_rows + 8ull * max_lz + 8ull * corr_doubles;
+size_t smem_bytes(uint32_t max_volume, uint32_t max_rows, uint32_t max_lz, uint32_t corr_doubles = 0,
+                  bool cube32 = false) {
+    return 4ull * (max_volume + 2 * kPad) + 16ull * max_rows + 8ull * max_lz + (cube32 ? 4ull * kBlockWords : 0ull) +
+           8ull * corr_doubles;
 }
 
 template <bool kCorr>
 cudaError_t launch_resident_t(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                               int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
                               uint32_t threads, unsigned long long* counters, const ResidentCorr* corr,
-                              uint32_t corr_doubles) {
-    const size_t smem = smem_bytes(max_volume, max_rows, max_lz, corr_doubles);
+                              uint32_t corr_doubles, bool cube32) {
+    const size_t smem = smem_bytes(max_volume, max_rows, max_lz, corr_doubles, cube32);
     cudaError_t e = cudaFuncSetAttribute(k_resident<kCorr>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int sms = 0, per_sm = 0;
@@ -1025,7 +1055,7 @@ cudaError_t launch_resident_t(const TaskView* views_dev, uint32_t n, uint32_t n_
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const uint32_t grid = std::min<uint32_t>(n, (uint32_t)(sms * per_sm));
     k_resident<kCorr><<<grid, threads, smem, s>>>(views_dev, n, n_sweeps, queue, max_volume, max_rows, max_lz,
-                                                  counters, corr);
+                                                  counters, corr, cube32 ? 1u : 0u);
     return cudaGetLastError();
 }
 
@@ -1053,15 +1083,18 @@ uint32_t resident_corr_doubles(uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t 
 cudaError_t launch_resident(const TaskView* views_dev, uint32_t n, uint32_t n_sweeps, unsigned int* queue,
                             int device, cudaStream_t s, uint32_t max_volume, uint32_t max_rows, uint32_t max_lz,
                             uint32_t threads, unsigned long long* counters, const ResidentCorr* corr_dev,
-                            uint32_t corr_doubles) {
+                            uint32_t corr_doubles, bool cube32) {
     if (threads < 32 || threads > (uint32_t)kBThreads || threads % 32) return cudaErrorInvalidConfiguration;
+    /* the padded growth blocks of 32^3 replicas, when they fit beside the largest replica */
+    if (cube32 && smem_bytes(max_volume, max_rows, max_lz, corr_doubles, true) > (size_t)max_dynamic_smem(device))
+        cube32 = false;
     /* the fused correlation measurement is compiled into its own instance, so
      * groups without it run the kernel unchanged */
     if (corr_dev && corr_doubles)
         return launch_resident_t<true>(views_dev, n, n_sweeps, queue, device, s, max_volume, max_rows, max_lz,
-                                       threads, counters, corr_dev, corr_doubles);
+                                       threads, counters, corr_dev, corr_doubles, cube32);
     return launch_resident_t<false>(views_dev, n, n_sweeps, queue, device, s, max_volume, max_rows, max_lz,
-                                    threads, counters, nullptr, 0);
+                                    threads, counters, nullptr, 0, cube32);
 }
 
 }  // namespace slsf

@@ -38,6 +38,7 @@
  */
 #include <algorithm>
 
+#include "bitgrow.cuh"
 #include "engine.h"
 #include "xy_device.cuh"
 
@@ -45,7 +46,7 @@ namespace slsf {
 
 namespace {
 
-constexpr uint32_t kRegion = 32; /* region edge in sites along y and z; one word along x */
+constexpr uint32_t kRegion = kGrowEdge; /* region edge in sites along y and z; one word along x */
 constexpr uint32_t kGrowThreads = kRegion * kRegion;
 constexpr int kBondThreads = 256;
 constexpr int kFlipThreads = 256;
@@ -79,76 +80,6 @@ struct WolffBits {
 };
 
 __host__ __device__ inline uint64_t round256(uint64_t b) { return (b + 255) & ~255ull; }
-
-/* Periodic rotations of a 32-bit row word (L_x == 32: the row is one word). */
-__device__ __forceinline__ uint32_t rotl32(uint32_t w, uint32_t s) { return __funnelshift_l(w, w, s); }
-__device__ __forceinline__ uint32_t rotr32(uint32_t w, uint32_t s) { return __funnelshift_r(w, w, s); }
-
-/* Closure of the cluster bits c of one word along x through its bonds b
- * (bit j: bond j -- j+1), by doubling in both directions.  periodic: the
- * word is a whole row (L_x == 32) and bit 31 bonds to bit 0; otherwise the
- * word is open at both ends (bits crossing words enter between passes). */
-__device__ __forceinline__ uint32_t close_word(uint32_t c, uint32_t b, bool periodic) {
-    if (periodic) {
-        uint32_t gr = c, pr = b, gl = c, pl = rotl32(b, 1);
-#pragma unroll
-        for (uint32_t s = 1; s < 32; s <<= 1) {
-            gr |= rotl32(gr & pr, s);
-            pr &= rotr32(pr, s);
-            gl |= rotr32(gl & pl, s);
-            pl &= rotl32(pl, s);
-        }
-        return gr | gl;
-    }
-    /* open word: bond bit 31 leads out of the word and is not used here */
-    const uint32_t bi = b & 0x7fffffffu;
-    uint32_t gr = c, pr = bi, gl = c, pl = bi << 1;
-#pragma unroll
-    for (uint32_t s = 1; s < 32; s <<= 1) {
-        gr |= (gr & pr) << s;
-        pr &= pr >> s;
-        gl |= (gl & pl) >> s;
-        pl &= pl << s;
-    }
-    return gr | gl;
-}
-
-/* Closure along a line of 32 words held one per lane (lane = position):
- * bit x of lane i passes to lane i+1 when bit x of p (the lane's bond to the
- * next position) is set.  Doubling in both directions; periodic lines wrap
- * from lane 31 to lane 0. */
-__device__ __forceinline__ uint32_t close_line(uint32_t c, uint32_t p, bool periodic) {
-    const uint32_t lane = threadIdx.x & 31u;
-    /* upward: G(i) |= P(i) & G(i - s), P(i) = bonds i-1 -> i over the span */
-    uint32_t g = c;
-    uint32_t q = __shfl_sync(0xffffffffu, p, (lane + 31u) & 31u);
-    if (!periodic && lane == 0) q = 0;
-#pragma unroll
-    for (uint32_t s = 1; s < 32; s <<= 1) {
-        const uint32_t src = (lane - s) & 31u;
-        const uint32_t gs = __shfl_sync(0xffffffffu, g, src);
-        const uint32_t qs = __shfl_sync(0xffffffffu, q, src);
-        if (periodic || lane >= s) {
-            g |= q & gs;
-            q &= qs;
-        }
-    }
-    /* downward: H(i) |= R(i) & H(i + s), R(i) = bonds i -> i+1 over the span */
-    uint32_t h = c;
-    uint32_t r = p;
-    if (!periodic && lane == 31) r = 0;
-#pragma unroll
-    for (uint32_t s = 1; s < 32; s <<= 1) {
-        const uint32_t src = (lane + s) & 31u;
-        const uint32_t hs = __shfl_sync(0xffffffffu, h, src);
-        const uint32_t rs = __shfl_sync(0xffffffffu, r, src);
-        if (periodic || lane + s < 32) {
-            h |= r & hs;
-            r &= rs;
-        }
-    }
-    return g | h;
-}
 
 __device__ __forceinline__ float proj_at(const float* __restrict__ theta, uint32_t i, float cphi, float sphi) {
     float sn, cn;
@@ -299,51 +230,9 @@ __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, u
     BY[warp][lane] = byw;
     BZ[warp][lane] = bzw;
     __syncthreads();
-    /* passes: even ones scan y (lane = y, warp = z), odd ones scan z (lane =
-     * z, warp = y); each also takes one step along the other axis and closes
-     * x.  A pass that changes nothing means the region is closed. */
-    bool ok = false;
-    /* every pass that changes something sets a bit: at most 32^3 of them */
-    for (uint32_t pass = 0; pass <= kRegion * kGrowThreads; ++pass) {
-        int changed = 0;
-        if ((pass & 1u) == 0) {
-            const uint32_t z = warp, y = lane;
-            const uint32_t old = C[z][y];
-            const uint32_t by_ = BY[z][y];
-            /* a warp scans only if some bit of it sits on a bond along the line */
-            const uint32_t by_in = __shfl_sync(0xffffffffu, by_, (lane + 31u) & 31u);
-            uint32_t v = __any_sync(0xffffffffu, (old & (by_ | by_in)) != 0u) ? close_line(old, by_, g.py) : old;
-            if (z > 0) v |= C[z - 1][y] & BZ[z - 1][y];
-            else if (g.pz) v |= C[kRegion - 1][y] & BZ[kRegion - 1][y];
-            if (z + 1 < kRegion) v |= C[z + 1][y] & BZ[z][y];
-            else if (g.pz) v |= C[0][y] & BZ[z][y];
-            if (__any_sync(0xffffffffu, v != old)) v = close_word(v, BX[z][y], g.px);
-            if (v != old) {
-                C[z][y] = v;
-                changed = 1;
-            }
-        } else {
-            const uint32_t z = lane, y = warp;
-            const uint32_t old = C[z][y];
-            const uint32_t bz_ = BZ[z][y];
-            const uint32_t bz_in = __shfl_sync(0xffffffffu, bz_, (lane + 31u) & 31u);
-            uint32_t v = __any_sync(0xffffffffu, (old & (bz_ | bz_in)) != 0u) ? close_line(old, bz_, g.pz) : old;
-            if (y > 0) v |= C[z][y - 1] & BY[z][y - 1];
-            else if (g.py) v |= C[z][kRegion - 1] & BY[z][kRegion - 1];
-            if (y + 1 < kRegion) v |= C[z][y + 1] & BY[z][y];
-            else if (g.py) v |= C[z][0] & BY[z][y];
-            if (__any_sync(0xffffffffu, v != old)) v = close_word(v, BX[z][y], g.px);
-            if (v != old) {
-                C[z][y] = v;
-                changed = 1;
-            }
-        }
-        if (!__syncthreads_or(changed)) {
-            ok = true;
-            SLSF_WB_COUNT(1, pass + 1);
-            break;
-        }
-    }
+    const uint32_t passes = close_block(C, BY, BZ, BX, g.px, g.py, g.pz);
+    SLSF_WB_COUNT(1, passes);
+    const bool ok = passes != 0;
     c = C[warp][lane];
     if (c != c0) atomicOr(&wb.cl[w], c);
     __threadfence();
