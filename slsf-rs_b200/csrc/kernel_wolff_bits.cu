@@ -56,7 +56,18 @@ constexpr uint32_t kNoRegion = 0xffffffffu;
 /* Optional counters (build with -DSLSF_WB_STATS): regions processed, growth
  * passes, grow launches, and region loads that changed nothing. */
 #ifdef SLSF_WB_STATS
-__device__ unsigned long long g_wb_stats[4];
+/* [0] regions processed, [1] passes, [2] grow launches, [3] loads without new
+ * bits, [4..7] cycles of thread 0 in: waiting for work, loading, closing,
+ * writing back and queueing neighbours */
+__device__ unsigned long long g_wb_stats[8];
+#define SLSF_WB_CLOCK(k, t0)                                                                     \
+    do {                                                                                         \
+        if (threadIdx.x == 0) {                                                                  \
+            const long long t1_ = clock64();                                                     \
+            atomicAdd(&g_wb_stats[k], (unsigned long long)(t1_ - (t0)));                         \
+            (t0) = t1_;                                                                          \
+        }                                                                                        \
+    } while (0)
 #define SLSF_WB_COUNT(k, n)                                                          \
     do {                                                                             \
         if (threadIdx.x == 0) atomicAdd(&g_wb_stats[k], (unsigned long long)(n));    \
@@ -64,6 +75,9 @@ __device__ unsigned long long g_wb_stats[4];
 #else
 #define SLSF_WB_COUNT(k, n) \
     do {                    \
+    } while (0)
+#define SLSF_WB_CLOCK(k, t0) \
+    do {                     \
     } while (0)
 #endif
 
@@ -185,12 +199,15 @@ __device__ __forceinline__ uint32_t region_of(const GrowGeo& g, uint32_t k, uint
  * false if a pass bound was hit. */
 __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, uint32_t seed_site,
                             uint32_t (*C)[kRegion + 1], uint32_t (*BY)[kRegion + 1], uint32_t (*BZ)[kRegion + 1],
-                            uint32_t (*BX)[kRegion + 1], uint32_t* keep) {
+                            uint32_t (*BX)[kRegion + 1], uint32_t* keep, uint32_t* s_want) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t k = r % g.words, rest = r / g.words, ry = rest % g.ry_n, rz = rest / g.ry_n;
     const uint32_t rowlen = g.words; /* words per row */
     const uint32_t gy = ry * kRegion + lane, gz = rz * kRegion + warp;
     auto word = [&](uint32_t kk, uint32_t yy, uint32_t zz) { return kk + rowlen * (yy + g.ly * zz); };
+#ifdef SLSF_WB_STATS
+    long long tclk = clock64();
+#endif
     const uint32_t w = word(k, gy, gz);
     const uint32_t c0 = __ldcg(&wb.cl[w]);
     const uint32_t bxw = wb.bx[w], byw = wb.by[w], bzw = wb.bz[w];
@@ -199,29 +216,48 @@ __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, u
     const uint32_t kl = k == 0 ? g.words - 1 : k - 1, kr = k + 1 == g.words ? 0 : k + 1;
     const uint32_t ym = gy == 0 ? g.ly - 1 : gy - 1, yp = gy + 1 == g.ly ? 0 : gy + 1;
     const uint32_t zm = gz == 0 ? g.lz - 1 : gz - 1, zp = gz + 1 == g.lz ? 0 : gz + 1;
+    /* the faces' neighbour words as loaded here also decide, at the end,
+     * which neighbours to queue: a neighbour word only ever gains bits, so a
+     * stale copy can queue a region that needs nothing, never miss one */
+    uint32_t cl_l = ~0u, bx_l = 0, cl_r = ~0u, cl_ym = ~0u, by_ym = 0, cl_yp = ~0u, cl_zm = ~0u, bz_zm = 0, cl_zp = ~0u;
     if (!g.px) {
         const uint32_t wl = word(kl, gy, gz), wr = word(kr, gy, gz);
-        c |= (__ldcg(&wb.cl[wl]) >> 31) & (wb.bx[wl] >> 31);
-        c |= ((__ldcg(&wb.cl[wr]) & 1u) & (bxw >> 31)) << 31;
+        cl_l = __ldcg(&wb.cl[wl]);
+        bx_l = wb.bx[wl];
+        cl_r = __ldcg(&wb.cl[wr]);
+        c |= (cl_l >> 31) & (bx_l >> 31);
+        c |= ((cl_r & 1u) & (bxw >> 31)) << 31;
     }
     if (!g.py) {
         if (lane == 0) {
             const uint32_t wm = word(k, ym, gz);
-            c |= __ldcg(&wb.cl[wm]) & wb.by[wm];
+            cl_ym = __ldcg(&wb.cl[wm]);
+            by_ym = wb.by[wm];
+            c |= cl_ym & by_ym;
         }
-        if (lane == kRegion - 1) c |= __ldcg(&wb.cl[word(k, yp, gz)]) & byw;
+        if (lane == kRegion - 1) {
+            cl_yp = __ldcg(&wb.cl[word(k, yp, gz)]);
+            c |= cl_yp & byw;
+        }
     }
     if (!g.pz) {
         if (warp == 0) {
             const uint32_t wm = word(k, gy, zm);
-            c |= __ldcg(&wb.cl[wm]) & wb.bz[wm];
+            cl_zm = __ldcg(&wb.cl[wm]);
+            bz_zm = wb.bz[wm];
+            c |= cl_zm & bz_zm;
         }
-        if (warp == kRegion - 1) c |= __ldcg(&wb.cl[word(k, gy, zp)]) & bzw;
+        if (warp == kRegion - 1) {
+            cl_zp = __ldcg(&wb.cl[word(k, gy, zp)]);
+            c |= cl_zp & bzw;
+        }
     }
     if (w == seed_site >> 5) c |= 1u << (seed_site & 31u);
     c = close_word(c, bxw, g.px);
     /* the stored region is closed already: without new bits nothing changes */
-    if (!__syncthreads_or(c != c0)) {
+    const int any_new = __syncthreads_or(c != c0);
+    SLSF_WB_CLOCK(5, tclk);
+    if (!any_new) {
         SLSF_WB_COUNT(3, 1);
         return true;
     }
@@ -232,31 +268,41 @@ __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, u
     __syncthreads();
     const uint32_t passes = close_block(C, BY, BZ, BX, g.px, g.py, g.pz);
     SLSF_WB_COUNT(1, passes);
+    SLSF_WB_CLOCK(6, tclk);
     const bool ok = passes != 0;
     c = C[warp][lane];
     if (c != c0) atomicOr(&wb.cl[w], c);
-    __threadfence();
-    /* neighbours that the region's bits can enter */
+    /* neighbours that the region's bits can enter: bit 0/1 -x/+x, 2/3 -y/+y, 4/5 -z/+z */
+    uint32_t want = 0;
     if (!g.px) {
-        const uint32_t wl = word(kl, gy, gz), wr = word(kr, gy, gz);
-        if ((c & 1u) && (wb.bx[wl] >> 31) && !(__ldcg(&wb.cl[wl]) >> 31)) push_region(wb, region_of(g, kl, ry, rz), keep);
-        if ((c >> 31) && (bxw >> 31) && !(__ldcg(&wb.cl[wr]) & 1u)) push_region(wb, region_of(g, kr, ry, rz), keep);
+        if ((c & 1u) && (bx_l >> 31) && !(cl_l >> 31)) want |= 1u;
+        if ((c >> 31) && (bxw >> 31) && !(cl_r & 1u)) want |= 2u;
     }
     if (!g.py) {
-        if (lane == 0) {
-            const uint32_t wm = word(k, ym, gz);
-            if (c & wb.by[wm] & ~__ldcg(&wb.cl[wm])) push_region(wb, region_of(g, k, ry == 0 ? g.ry_n - 1 : ry - 1, rz), keep);
-        }
-        if (lane == kRegion - 1 && (c & byw & ~__ldcg(&wb.cl[word(k, yp, gz)])))
-            push_region(wb, region_of(g, k, ry + 1 == g.ry_n ? 0 : ry + 1, rz), keep);
+        if (lane == 0 && (c & by_ym & ~cl_ym)) want |= 4u;
+        if (lane == kRegion - 1 && (c & byw & ~cl_yp)) want |= 8u;
     }
     if (!g.pz) {
-        if (warp == 0) {
-            const uint32_t wm = word(k, gy, zm);
-            if (c & wb.bz[wm] & ~__ldcg(&wb.cl[wm])) push_region(wb, region_of(g, k, ry, rz == 0 ? g.rz_n - 1 : rz - 1), keep);
+        if (warp == 0 && (c & bz_zm & ~cl_zm)) want |= 16u;
+        if (warp == kRegion - 1 && (c & bzw & ~cl_zp)) want |= 32u;
+    }
+    want = __reduce_or_sync(0xffffffffu, want);
+    if (lane == 0 && want) atomicOr(s_want, want);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t m = *s_want;
+        *s_want = 0;
+        if (m) {
+            /* the block's cluster words are written (barrier above); one fence
+             * orders them before the neighbours can be taken */
+            __threadfence();
+            if (m & 1u) push_region(wb, region_of(g, k == 0 ? g.words - 1 : k - 1, ry, rz), keep);
+            if (m & 2u) push_region(wb, region_of(g, k + 1 == g.words ? 0 : k + 1, ry, rz), keep);
+            if (m & 4u) push_region(wb, region_of(g, k, ry == 0 ? g.ry_n - 1 : ry - 1, rz), keep);
+            if (m & 8u) push_region(wb, region_of(g, k, ry + 1 == g.ry_n ? 0 : ry + 1, rz), keep);
+            if (m & 16u) push_region(wb, region_of(g, k, ry, rz == 0 ? g.rz_n - 1 : rz - 1), keep);
+            if (m & 32u) push_region(wb, region_of(g, k, ry, rz + 1 == g.rz_n ? 0 : rz + 1), keep);
         }
-        if (warp == kRegion - 1 && (c & bzw & ~__ldcg(&wb.cl[word(k, gy, zp)])))
-            push_region(wb, region_of(g, k, ry, rz + 1 == g.rz_n ? 0 : rz + 1), keep);
     }
     return ok;
 }
@@ -269,6 +315,7 @@ __global__ void __launch_bounds__(kGrowThreads, 1)
     __shared__ uint32_t BX[kRegion][kRegion + 1];
     __shared__ uint32_t s_item;
     __shared__ uint32_t s_keep;
+    __shared__ uint32_t s_want;
     /* Each CTA takes regions until nothing is queued or in flight: the
      * neighbour it claimed while processing the last one (no queue round
      * trip), else the queue entry of its ticket (one atomic; the producer
@@ -277,10 +324,19 @@ __global__ void __launch_bounds__(kGrowThreads, 1)
     constexpr uint32_t kSpin = 1u << 24;
     const uint32_t seed_site = __ldcg(&wb.ctl[4]) - 1;
     bool ok = true;
-    if (threadIdx.x == 0) s_keep = kNoRegion;
+    if (threadIdx.x == 0) {
+        s_keep = kNoRegion;
+        s_want = 0;
+    }
     __syncthreads();
+#ifdef SLSF_WB_STATS
+    long long tq = clock64();
+#endif
     for (uint32_t item = 0; item < max_items; ++item) {
         if (threadIdx.x == 0) {
+#ifdef SLSF_WB_STATS
+            tq = clock64();
+#endif
             uint32_t got = s_keep;
             if (got == kNoRegion) {
                 got = 0xfffffffeu; /* gave up, unless set below */
@@ -307,19 +363,21 @@ __global__ void __launch_bounds__(kGrowThreads, 1)
             s_item = got;
         }
         __syncthreads();
+        SLSF_WB_CLOCK(4, tq);
         const uint32_t r = s_item;
         if (r == 0xffffffffu) break;
         if (r >= wb.regions) {
             ok = false;
             break;
         }
-        ok &= grow_region(wb, g, r, seed_site, C, BY, BZ, BX, &s_keep);
+        ok &= grow_region(wb, g, r, seed_site, C, BY, BZ, BX, &s_keep, &s_want);
         SLSF_WB_COUNT(0, 1);
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();
             atomicSub(&wb.ctl[2], 1u);
         }
+        SLSF_WB_CLOCK(7, tq);
         if (item + 1 == max_items) ok = false;
     }
     if (!ok && threadIdx.x == 0) {
@@ -449,10 +507,10 @@ int launch_wolff_bits(const TaskView& t, uint64_t counter, void* scratch, uint8_
 }  // namespace slsf
 
 #ifdef SLSF_WB_STATS
-extern "C" int slsf_debug_wb_stats(unsigned long long out[4], int reset) {
-    cudaError_t e = cudaMemcpyFromSymbol(out, slsf::g_wb_stats, sizeof(unsigned long long) * 4);
+extern "C" int slsf_debug_wb_stats(unsigned long long out[8], int reset) {
+    cudaError_t e = cudaMemcpyFromSymbol(out, slsf::g_wb_stats, sizeof(unsigned long long) * 8);
     if (e == cudaSuccess && reset) {
-        const unsigned long long zero[4] = {0, 0, 0, 0};
+        const unsigned long long zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         e = cudaMemcpyToSymbol(slsf::g_wb_stats, zero, sizeof(zero));
     }
     return e == cudaSuccess ? 0 : 1;
