@@ -35,7 +35,8 @@ def run(slsf, ctx, dims, choice, sweeps=4):
     return theta, bins
 
 
-@pytest.mark.parametrize("dims", [(8, 8, 8), (16, 16, 16), (32, 32, 32), (48, 48, 48), (64, 64, 64), (24, 16, 32)])
+@pytest.mark.parametrize("dims", [(8, 8, 8), (16, 16, 16), (32, 32, 32), (48, 48, 48), (64, 64, 64), (24, 16, 32),
+                                  (8, 80, 8), (8, 8, 64), (40, 34, 8)])
 def test_every_choice_gives_the_same_trajectory(slsf, ctx, dims):
     ref = None
     tried = 0
