@@ -124,26 +124,26 @@ __global__ void __launch_bounds__(kBondThreads)
     const float jx = jxy[z], jzz = jz[z];
     const uint32_t y0 = sg * seg;
     float ri = proj_at(theta, zbase + y0 * lx + x, cphi, sphi);
+    /* lane j < seg (seg <= 32): the projection of the first site of the next
+     * word in row y0 + j, the +x partner of lane 31 in that row */
+    const float r_next_word = proj_at(theta, zbase + (y0 + (lane < seg ? lane : 0u)) * lx + xn, cphi, sphi);
     /* the angles of the next row's loads, one row ahead */
     auto yrow = [&](uint32_t y) { return (y + 1 == ly) ? 0u : y + 1; };
     float t_yp = theta[zbase + yrow(y0) * lx + x], t_zp = theta[zp_base + y0 * lx + x];
-    float t_xn = theta[zbase + y0 * lx + xn];
     for (uint32_t y = y0; y < y0 + seg; ++y) {
         const uint32_t row = zbase + y * lx;
         const uint32_t i = row + x;
-        const float a_yp = t_yp, a_zp = t_zp, a_xn = t_xn;
+        const float a_yp = t_yp, a_zp = t_zp;
         if (y + 1 < y0 + seg) {
             t_yp = theta[zbase + yrow(y + 1) * lx + x];
             t_zp = theta[zp_base + (y + 1) * lx + x];
-            t_xn = theta[row + lx + xn];
         }
         float sn, cn;
         __sincosf(a_yp, &sn, &cn);
         const float ryp = wolff_projection(cn, sn, cphi, sphi);
         __sincosf(a_zp, &sn, &cn);
         const float rzp = wolff_projection(cn, sn, cphi, sphi);
-        __sincosf(a_xn, &sn, &cn);
-        const float rnext = wolff_projection(cn, sn, cphi, sphi);
+        const float rnext = __shfl_sync(0xffffffffu, r_next_word, y - y0);
         float rxp = __shfl_sync(0xffffffffu, ri, (lane + 1u) & 31u);
         if (lane == 31) rxp = rnext;
         const slsf_u32x4 b = slsf_stream(seed, counter, SLSF_PURPOSE_WOLFF_BOND, 0, i);
