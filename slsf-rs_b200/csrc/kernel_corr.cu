@@ -134,7 +134,7 @@ __device__ void fft_tables(FftTables& T, uint32_t n) {
  * ordered-phase lines, against the 2e-6 agreement held with the FP64
  * oracle. */
 template <uint32_t N1>
-__device__ void corr_z_spectral(const float2* __restrict__ tile, const FftTables& T, double* P, uint32_t cols,
+__device__ void corr_z_spectral(const float2* tile, const FftTables& T, double* P, uint32_t cols,
                                 double* __restrict__ out) {
     constexpr uint32_t n = 32 * N1;
     constexpr uint32_t bits = N1 == 1 ? 0 : (N1 == 2 ? 1 : (N1 == 4 ? 2 : 3));
@@ -183,16 +183,19 @@ __device__ void corr_z_spectral(const float2* __restrict__ tile, const FftTables
             pw[j] += re * re + im * im;
         }
     }
-    /* the item's spectrum: warps add theirs in order; slot j of lane t is
-     * frequency bitrev(j) + N1 bitrev5(t) */
+    /* the item's spectrum: each warp's sums go to its own row of the tile
+     * (read by no warp any more), then the rows are added in warp order;
+     * slot j of lane t is frequency bitrev(j) + N1 bitrev5(t) */
     const uint32_t s = __brev(lane) >> 27;
-    for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) P[q] = 0.0;
-    for (uint32_t w = 0; w < nwarps; ++w) {
-        __syncthreads();
-        if (warp == w) {
+    double* rows = reinterpret_cast<double*>(const_cast<float2*>(tile)); /* [nwarps][n] */
+    __syncthreads();
 #pragma unroll
-            for (uint32_t j = 0; j < N1; ++j) P[bitrev_bits(j, bits) + N1 * s] += pw[j];
-        }
+    for (uint32_t j = 0; j < N1; ++j) rows[warp * n + bitrev_bits(j, bits) + N1 * s] = pw[j];
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) {
+        double a = 0.0;
+        for (uint32_t w = 0; w < nwarps; ++w) a += rows[w * n + q];
+        P[q] = a;
     }
     __syncthreads();
     /* the folded spectrum F(0) = P(0), F(q) = P(q) + P(n - q), F(n/2) = P(n/2):
@@ -462,6 +465,10 @@ __global__ void __launch_bounds__(kFinThreads) k_corr_finalize(const CorrTask* _
         for (uint32_t q = 0; q < kZParts; ++q) sz += zpart[q * zc + r];
         zcol[r] = sz;
     }
+    /* cos(2 pi m / n) for the n residues m of q * lag, evaluated once each */
+    __shared__ double ctab[kFftMax];
+    if (sh.spectral)
+        for (uint32_t m = threadIdx.x; m < lz; m += blockDim.x) ctab[m] = cospi(2.0 * (double)m / (double)lz);
     __syncthreads();
     for (uint32_t r = threadIdx.x; r < Rz; r += blockDim.x) {
         double sz = zcol[r];
@@ -469,7 +476,7 @@ __global__ void __launch_bounds__(kFinThreads) k_corr_finalize(const CorrTask* _
             /* lag r + 1 from the summed folded spectrum, in frequency order */
             const uint32_t n = lz, lag = r + 1;
             sz = 0.0;
-            for (uint32_t q = 0; q <= n / 2; ++q) sz += zcol[q] * cospi(2.0 * (double)((q * lag) % n) / (double)n);
+            for (uint32_t q = 0; q <= n / 2; ++q) sz += zcol[q] * ctab[(q * lag) % n];
             sz /= (double)n;
         }
         emit(3 * R + lz * R + r, sz / volume);
@@ -516,7 +523,6 @@ bool corr_supports(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t
 
 cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t n_tasks, uint32_t n_items,
                         uint32_t max_len, uint32_t max_r, uint32_t max_nz, int sm_count, cudaStream_t s) {
-    (void)sm_count; /* one block per item: the hardware spreads them */
     /* a warp takes 8 lags per pass: blocks of one or two warps for small
      * radii, so that short lines do not hold idle warps */
     const int line_threads = max_r <= 16 ? 64 : (max_r <= 32 ? 128 : kCorrThreads);
@@ -540,7 +546,10 @@ cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t
             const size_t zsmem = (size_t)kFftMax * kCorrPitch * sizeof(float2);
             e = cudaFuncSetAttribute(k_corr_zfft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem);
             if (e != cudaSuccess) return e;
-            k_corr_zfft<<<grid, kCorrThreads, zsmem, s>>>(one ? nullptr : tasks_dev, by_value, n_tasks, n_items);
+            /* blocks loop over the items, so each computes its twiddle tables
+             * once: three per SM (the kernel's occupancy) */
+            const uint32_t zgrid = sm_count > 0 ? std::min<uint32_t>(grid, 3u * (uint32_t)sm_count) : grid;
+            k_corr_zfft<<<zgrid, kCorrThreads, zsmem, s>>>(one ? nullptr : tasks_dev, by_value, n_tasks, n_items);
             e = cudaGetLastError();
             if (e != cudaSuccess) return e;
         }
