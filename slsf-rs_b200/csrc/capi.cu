@@ -165,7 +165,7 @@ struct slsf_ctx {
      * repeated batch reuses it without an upload */
     std::vector<const slsf_task*> corr_last;
     std::vector<uint64_t> corr_last_gen;
-    uint32_t corr_last_items = 0, corr_last_len = 0, corr_last_r = 0, corr_last_nz = 0;
+    uint32_t corr_last_items = 0, corr_last_zunits = 0, corr_last_len = 0, corr_last_r = 0, corr_last_nz = 0;
     uint64_t corr_gen = 0; /* slsf_task_corr_setup calls so far */
 };
 
@@ -756,9 +756,9 @@ int slsf_task_correlations(slsf_task* t, uint32_t rmax_xy, uint32_t rmax_z, doub
                          reinterpret_cast<double*>(d), reinterpret_cast<double*>(d + off_values), nullptr, nullptr};
     std::vector<double> h(nv);
     const uint32_t items = slsf::corr_items(t->lx, t->ly, t->lz, rmax_xy, rmax_z);
-    e = slsf::launch_corr(nullptr, &ct, 1, items, slsf::corr_len(t->lx, t->ly, t->lz, rmax_xy, rmax_z),
-                          std::max(rmax_xy, rmax_z), slsf::corr_z_items(t->lx, t->ly, t->lz, rmax_xy, rmax_z),
-                          ctx->sm_count, ctx->stream);
+    e = slsf::launch_corr(nullptr, &ct, 1, items, slsf::corr_z_units(t->lx, t->ly, t->lz, rmax_xy, rmax_z),
+                          slsf::corr_len(t->lx, t->ly, t->lz, rmax_xy, rmax_z), std::max(rmax_xy, rmax_z),
+                          slsf::corr_z_items(t->lx, t->ly, t->lz, rmax_xy, rmax_z), ctx->sm_count, ctx->stream);
     ctx->launches += corr_launch_count(items, slsf::corr_z_items(t->lx, t->ly, t->lz, rmax_xy, rmax_z));
     if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), ct.values, 8ull * nv, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -900,13 +900,14 @@ int slsf_batch_correlations(slsf_ctx* ctx, slsf_task* const* tasks, size_t n) {
             SLSF_CUDA(cudaHostAlloc(&ctx->h_corr, sizeof(slsf::CorrTask) * n, cudaHostAllocDefault));
             ctx->corr_cap = n;
         }
-        uint32_t items = 0, max_len = 0, max_r = 0, max_nz = 0;
+        uint32_t items = 0, zunits = 0, max_len = 0, max_r = 0, max_nz = 0;
         for (size_t i = 0; i < n; ++i) {
             slsf_task* t = tasks[i];
             ctx->h_corr[i] = slsf::CorrTask{t->theta, t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz, items,
                                             t->corr_binsize, t->corr_n_bins, t->corr_partial, nullptr, t->corr_bins,
-                                            t->corr_count_dev};
+                                            t->corr_count_dev, zunits};
             items += slsf::corr_items(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz);
+            zunits += slsf::corr_z_units(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz);
             max_len = std::max(max_len, slsf::corr_len(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz));
             max_r = std::max(max_r, std::max(t->corr_rxy, t->corr_rz));
             max_nz = std::max(max_nz, slsf::corr_z_items(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz));
@@ -917,11 +918,13 @@ int slsf_batch_correlations(slsf_ctx* ctx, slsf_task* const* tasks, size_t n) {
         ctx->corr_last.assign(tasks, tasks + n);
         for (size_t i = 0; i < n; ++i) ctx->corr_last_gen.push_back(tasks[i]->corr_gen);
         ctx->corr_last_items = items;
+        ctx->corr_last_zunits = zunits;
         ctx->corr_last_len = max_len;
         ctx->corr_last_r = max_r;
         ctx->corr_last_nz = max_nz;
     }
-    SLSF_CUDA(slsf::launch_corr(ctx->d_corr, nullptr, (uint32_t)n, ctx->corr_last_items, ctx->corr_last_len,
+    SLSF_CUDA(slsf::launch_corr(ctx->d_corr, nullptr, (uint32_t)n, ctx->corr_last_items, ctx->corr_last_zunits,
+                                ctx->corr_last_len,
                                 ctx->corr_last_r, ctx->corr_last_nz, ctx->sm_count, ctx->stream));
     ctx->launches += corr_launch_count(ctx->corr_last_items, ctx->corr_last_nz);
     for (size_t i = 0; i < n; ++i) tasks[i]->corr_count += 1;
@@ -1113,7 +1116,8 @@ static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v, 
                                        t->corr_n_bins,   t->corr_partial, nullptr,      t->corr_bins,
                                        t->corr_count_dev};
             const uint32_t items = slsf::corr_items(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz);
-            slsf::launch_corr(nullptr, &ct, 1, items, slsf::corr_len(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz),
+            slsf::launch_corr(nullptr, &ct, 1, items, slsf::corr_z_units(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz),
+                              slsf::corr_len(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz),
                               std::max(t->corr_rxy, t->corr_rz),
                               slsf::corr_z_items(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz), ctx->sm_count, st);
             ctx->launches +=

@@ -119,6 +119,7 @@ struct CorrTask {
     double* values;     /* or NULL */
     double* bins;       /* [n_bins][values] sums, or NULL */
     unsigned long long* count; /* or NULL */
+    uint32_t zunit0;    /* the task's first spectral z unit in the launch */
 };
 uint32_t corr_items(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
 size_t corr_partial_doubles(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
@@ -128,14 +129,19 @@ uint32_t corr_values(uint32_t lz, uint32_t rxy, uint32_t rz);
 uint32_t corr_len(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
 uint32_t corr_ext(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
 bool corr_supports(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
-/* tasks_dev: n_tasks entries in item order (item0 ascending, n_items in
- * all) in device memory; or, for one task, `one` on the host (passed to the
- * kernels by value, no copy).  max_len, max_r, max_nz: the largest corr_len,
- * radius and corr_z_items of them (they size the launches). */
+/* tasks_dev: n_tasks entries in item order (item0 and zunit0 ascending,
+ * n_items and n_zunits in all) in device memory; or, for one task, `one` on
+ * the host (passed to the kernels by value, no copy).  max_len, max_r,
+ * max_nz: the largest corr_len, radius and corr_z_items of them (they size
+ * the launches). */
 cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t n_tasks, uint32_t n_items,
-                        uint32_t max_len, uint32_t max_r, uint32_t max_nz, int sm_count, cudaStream_t s);
+                        uint32_t n_zunits, uint32_t max_len, uint32_t max_r, uint32_t max_nz, int sm_count,
+                        cudaStream_t s);
 /* z-line work items of a task (0 without C_z). */
 uint32_t corr_z_items(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
+/* Spectral z units of a task: groups of consecutive z items whose power
+ * spectra one block sums (0 off the spectral route). */
+uint32_t corr_z_units(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz);
 
 /* ---- batched persistent engine, one CTA per replica (kernel_resident.cu) ---- */
 bool resident_supports(uint32_t lx, uint32_t ly, uint32_t lz, int device);

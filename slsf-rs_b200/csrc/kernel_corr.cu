@@ -90,6 +90,16 @@ __host__ __device__ inline CorrShape corr_shape(uint32_t lx, uint32_t ly, uint32
 
 
 
+/* Spectral route: one block sums the power spectra of kZGroup consecutive z
+ * items of a task (a unit) and writes one folded spectrum per unit, which
+ * cuts the rows the finalize adds by kZGroup; the units are fixed by the
+ * task's own item numbering, so the sums do not depend on the launch. */
+constexpr uint32_t kZGroup = 4;
+
+__host__ __device__ inline uint32_t corr_zunits_of(const CorrShape& sh) {
+    return sh.spectral ? (sh.nz + kZGroup - 1) / kZGroup : 0;
+}
+
 /* Twiddles of the spectral route (FP32), laid out so that a warp reads 32
  * consecutive entries: stage[k][t] = w_(2h)^(t mod h) for the lane stage of
  * half-size h = 16 >> k, slot[j][t] = w_n^(t bitrev(j)) for register slot j,
@@ -127,84 +137,6 @@ __device__ void fft_tables(FftTables& T, uint32_t n) {
     }
 }
 
-/* The spectral route for one item of z lines: tile [n][kCorrPitch] holds
- * (cos, sin) of `cols` lines (zero past them); P[n] receives the item's
- * summed power spectrum (FP64), out[0 .. n/2] its folded form.  The
- * transforms run in FP32: their rounding moves C_z by about 1e-8 on
- * ordered-phase lines, against the 2e-6 agreement held with the FP64
- * oracle. */
-template <uint32_t N1>
-__device__ void corr_z_spectral(const float2* tile, const FftTables& T, double* P, uint32_t cols,
-                                double* __restrict__ out) {
-    constexpr uint32_t n = 32 * N1;
-    constexpr uint32_t bits = N1 == 1 ? 0 : (N1 == 2 ? 1 : (N1 == 4 ? 2 : 3));
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    double pw[N1];
-#pragma unroll
-    for (uint32_t m = 0; m < N1; ++m) pw[m] = 0.0;
-    for (uint32_t c = warp; c < cols; c += nwarps) {
-        float2 X[N1];
-#pragma unroll
-        for (uint32_t j = 0; j < N1; ++j) X[j] = tile[(lane + 32 * j) * kCorrPitch + c];
-        /* radix-2 decimation in frequency over j in registers (N1-point DFT of
-         * the elements lane + 32 j); slot j ends with frequency bitrev(j) */
-#pragma unroll
-        for (uint32_t h = N1 / 2; h > 0; h >>= 1) {
-#pragma unroll
-            for (uint32_t j = 0; j < N1; ++j) {
-                if (j & h) continue;
-                const float2 a = X[j], b = X[j + h];
-                const float2 w = T.reg[(j & (h - 1)) * (n / (2 * h))]; /* same entry across the warp */
-                X[j] = make_float2(a.x + b.x, a.y + b.y);
-                X[j + h] = cmulf(make_float2(a.x - b.x, a.y - b.y), w);
-            }
-        }
-#pragma unroll
-        for (uint32_t j = 1; j < N1; ++j) X[j] = cmulf(X[j], T.slot[j][lane]);
-        /* 32-point decimation-in-frequency FFT across the lanes; lane t ends
-         * with frequency index bitrev5(t) */
-#pragma unroll
-        for (uint32_t k = 0; k < 5; ++k) {
-            const uint32_t h = 16u >> k;
-            const bool upper = lane & h;
-            const float2 w = T.stage[k][lane];
-#pragma unroll
-            for (uint32_t j = 0; j < N1; ++j) {
-                const float yx = __shfl_xor_sync(0xffffffffu, X[j].x, h);
-                const float yy = __shfl_xor_sync(0xffffffffu, X[j].y, h);
-                const float2 sum = make_float2(X[j].x + yx, X[j].y + yy);
-                const float2 dif = cmulf(make_float2(yx - X[j].x, yy - X[j].y), w);
-                X[j] = upper ? dif : sum;
-            }
-        }
-#pragma unroll
-        for (uint32_t j = 0; j < N1; ++j) {
-            const double re = (double)X[j].x, im = (double)X[j].y;
-            pw[j] += re * re + im * im;
-        }
-    }
-    /* the item's spectrum: each warp's sums go to its own row of the tile
-     * (read by no warp any more), then the rows are added in warp order;
-     * slot j of lane t is frequency bitrev(j) + N1 bitrev5(t) */
-    const uint32_t s = __brev(lane) >> 27;
-    double* rows = reinterpret_cast<double*>(const_cast<float2*>(tile)); /* [nwarps][n] */
-    __syncthreads();
-#pragma unroll
-    for (uint32_t j = 0; j < N1; ++j) rows[warp * n + bitrev_bits(j, bits) + N1 * s] = pw[j];
-    __syncthreads();
-    for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) {
-        double a = 0.0;
-        for (uint32_t w = 0; w < nwarps; ++w) a += rows[w * n + q];
-        P[q] = a;
-    }
-    __syncthreads();
-    /* the folded spectrum F(0) = P(0), F(q) = P(q) + P(n - q), F(n/2) = P(n/2):
-     * the item's lag sums are (1/n) sum_q F(q) cos(2 pi q r / n), formed once
-     * per task by the finalize from the items' summed F */
-    for (uint32_t q = threadIdx.x; q <= n / 2; q += blockDim.x)
-        out[q] = (q == 0 || q == n / 2) ? P[q] : P[q] + P[n - q];
-}
-
 /* Stages n rows of `cols` consecutive angles (row k at base + k * stride) as
  * (cos, sin) pairs into tile[k * pitch + c], zero past `cols`.  Eight loads
  * per thread are issued before their trig, so the block keeps many loads in
@@ -231,47 +163,129 @@ __device__ __forceinline__ void stage_rows(float2* __restrict__ tile, uint32_t p
     }
 }
 
-/* The task of a work item: the last one whose first item is at or before it. */
-__device__ __forceinline__ const CorrTask& item_task(const CorrTask* __restrict__ tasks, const CorrTask& one,
-                                                    uint32_t n_tasks, uint32_t item) {
+/* The spectral route for unit g of task T: for each of its z items (32
+ * lines of one row y), the tile [n][kCorrPitch] receives the lines' (cos,
+ * sin) and each warp transforms its lines, adding their power spectra into
+ * its per-lane sums (FP64); the warps' sums are added in warp order into P[n]
+ * (FP64) and out[0 .. n/2] receives the folded form.  The transforms run in
+ * FP32: their rounding moves C_z by about 1e-8 on ordered-phase lines,
+ * against the 2e-6 agreement held with the FP64 oracle. */
+template <uint32_t N1>
+__device__ void corr_z_unit(const CorrTask& Tk, const CorrShape& sh, uint32_t g, float2* tile, const FftTables& T,
+                            double* P, double* __restrict__ out) {
+    constexpr uint32_t n = 32 * N1;
+    constexpr uint32_t bits = N1 == 1 ? 0 : (N1 == 2 ? 1 : (N1 == 4 ? 2 : 3));
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t plane = Tk.lx * Tk.ly, q1 = min(sh.nz, (g + 1) * kZGroup);
+    double pw[N1];
+#pragma unroll
+    for (uint32_t m = 0; m < N1; ++m) pw[m] = 0.0;
+    for (uint32_t item = g * kZGroup; item < q1; ++item) {
+        const uint32_t y = item / sh.cy, x0 = (item % sh.cy) * kCorrCols;
+        const uint32_t cols = min(kCorrCols, Tk.lx - x0);
+        __syncthreads(); /* the previous item's tile is no longer read */
+        stage_rows(tile, kCorrPitch, Tk.theta, y * Tk.lx + x0, plane, n, cols);
+        __syncthreads();
+        for (uint32_t c = warp; c < cols; c += nwarps) {
+            float2 X[N1];
+#pragma unroll
+            for (uint32_t j = 0; j < N1; ++j) X[j] = tile[(lane + 32 * j) * kCorrPitch + c];
+            /* radix-2 decimation in frequency over j in registers (N1-point DFT
+             * of the elements lane + 32 j); slot j ends with frequency bitrev(j) */
+#pragma unroll
+            for (uint32_t h = N1 / 2; h > 0; h >>= 1) {
+#pragma unroll
+                for (uint32_t j = 0; j < N1; ++j) {
+                    if (j & h) continue;
+                    const float2 a = X[j], b = X[j + h];
+                    const float2 w = T.reg[(j & (h - 1)) * (n / (2 * h))]; /* same entry across the warp */
+                    X[j] = make_float2(a.x + b.x, a.y + b.y);
+                    X[j + h] = cmulf(make_float2(a.x - b.x, a.y - b.y), w);
+                }
+            }
+#pragma unroll
+            for (uint32_t j = 1; j < N1; ++j) X[j] = cmulf(X[j], T.slot[j][lane]);
+            /* 32-point decimation-in-frequency FFT across the lanes; lane t
+             * ends with frequency index bitrev5(t) */
+#pragma unroll
+            for (uint32_t k = 0; k < 5; ++k) {
+                const uint32_t h = 16u >> k;
+                const bool upper = lane & h;
+                const float2 w = T.stage[k][lane];
+#pragma unroll
+                for (uint32_t j = 0; j < N1; ++j) {
+                    const float yx = __shfl_xor_sync(0xffffffffu, X[j].x, h);
+                    const float yy = __shfl_xor_sync(0xffffffffu, X[j].y, h);
+                    const float2 sum = make_float2(X[j].x + yx, X[j].y + yy);
+                    const float2 dif = cmulf(make_float2(yx - X[j].x, yy - X[j].y), w);
+                    X[j] = upper ? dif : sum;
+                }
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < N1; ++j) {
+                const double re = (double)X[j].x, im = (double)X[j].y;
+                pw[j] += re * re + im * im;
+            }
+        }
+    }
+    /* the unit's spectrum: each warp's sums go to its own row of the tile
+     * (read by no warp any more), then the rows are added in warp order;
+     * slot j of lane t is frequency bitrev(j) + N1 bitrev5(t) */
+    const uint32_t s = __brev(lane) >> 27;
+    double* rows = reinterpret_cast<double*>(tile); /* [nwarps][n] */
+    __syncthreads();
+#pragma unroll
+    for (uint32_t j = 0; j < N1; ++j) rows[warp * n + bitrev_bits(j, bits) + N1 * s] = pw[j];
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) {
+        double a = 0.0;
+        for (uint32_t w = 0; w < nwarps; ++w) a += rows[w * n + q];
+        P[q] = a;
+    }
+    __syncthreads();
+    /* the folded spectrum F(0) = P(0), F(q) = P(q) + P(n - q), F(n/2) = P(n/2):
+     * the lag sums are (1/n) sum_q F(q) cos(2 pi q r / n), formed once per
+     * task by the finalize from the units' summed F */
+    for (uint32_t q = threadIdx.x; q <= n / 2; q += blockDim.x)
+        out[q] = (q == 0 || q == n / 2) ? P[q] : P[q] + P[n - q];
+}
+
+/* The task of a spectral unit: the last one whose first unit is at or
+ * before it (tasks without units share the next task's zunit0). */
+__device__ __forceinline__ const CorrTask& unit_task(const CorrTask* __restrict__ tasks, const CorrTask& one,
+                                                    uint32_t n_tasks, uint32_t unit) {
     uint32_t lo = 0, hi = n_tasks;
     while (tasks && hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (tasks[mid].item0 <= item) lo = mid;
+        if (tasks[mid].zunit0 <= unit) lo = mid;
         else hi = mid;
     }
     return tasks ? tasks[lo] : one;
 }
 
-/* The spectral route for z items (one block per item; other items return). */
+/* The spectral route: blocks loop over the units of all tasks. */
 __global__ void __launch_bounds__(kCorrThreads, 3)
-    k_corr_zfft(const CorrTask* __restrict__ tasks, CorrTask one, uint32_t n_tasks, uint32_t n_items) {
+    k_corr_zfft(const CorrTask* __restrict__ tasks, CorrTask one, uint32_t n_tasks, uint32_t n_units) {
     extern __shared__ float2 tile[]; /* [n][kCorrPitch] */
     __shared__ FftTables tabs;
     __shared__ double spec[kFftMax];
     uint32_t tab_n = 0; /* the line length the tables hold */
-    for (uint32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
-        const CorrTask& T = item_task(tasks, one, n_tasks, item);
+    for (uint32_t unit = blockIdx.x; unit < n_units; unit += gridDim.x) {
+        const CorrTask& T = unit_task(tasks, one, n_tasks, unit);
         const CorrShape sh = corr_shape(T.lx, T.ly, T.lz, T.rxy, T.rz);
-        const uint32_t local = item - T.item0;
-        const uint32_t n = T.lz;
-        if (local < sh.nx + sh.ny || !corr_fft_len(n)) continue; /* block-uniform */
-        const uint32_t plane = T.lx * T.ly;
-        const uint32_t q = local - sh.nx - sh.ny, y = q / sh.cy, x0 = (q % sh.cy) * kCorrCols;
-        const uint32_t cols = min(kCorrCols, T.lx - x0), base = y * T.lx + x0;
-        __syncthreads(); /* the previous item's tile and spectrum are no longer read */
-        stage_rows(tile, kCorrPitch, T.theta, base, plane, n, cols);
+        const uint32_t n = T.lz, g = unit - T.zunit0;
+        if (!sh.spectral || g >= corr_zunits_of(sh)) continue; /* block-uniform; not reached for valid launches */
         if (n != tab_n) {
+            __syncthreads(); /* the previous unit's tables are no longer read */
             fft_tables(tabs, n);
             tab_n = n;
         }
-        __syncthreads();
-        double* out = T.partial + (size_t)local * sh.rp;
+        double* out = T.partial + (size_t)(sh.nx + sh.ny + g) * sh.rp;
         switch (n) {
-            case 32: corr_z_spectral<1>(tile, tabs, spec, cols, out); break;
-            case 64: corr_z_spectral<2>(tile, tabs, spec, cols, out); break;
-            case 128: corr_z_spectral<4>(tile, tabs, spec, cols, out); break;
-            default: corr_z_spectral<8>(tile, tabs, spec, cols, out); break;
+            case 32: corr_z_unit<1>(T, sh, g, tile, tabs, spec, out); break;
+            case 64: corr_z_unit<2>(T, sh, g, tile, tabs, spec, out); break;
+            case 128: corr_z_unit<4>(T, sh, g, tile, tabs, spec, out); break;
+            default: corr_z_unit<8>(T, sh, g, tile, tabs, spec, out); break;
         }
     }
 }
@@ -442,20 +456,21 @@ __global__ void __launch_bounds__(kFinThreads) k_corr_finalize(const CorrTask* _
      * every launch of a task gives the same bits */
     __shared__ double zpart[kZParts * kMaxZLags];
     const uint32_t zc = sh.spectral ? lz / 2 + 1 : Rz; /* columns */
+    const uint32_t zrows = sh.spectral ? corr_zunits_of(sh) : sh.nz; /* rows: units, or items */
     for (uint32_t idx = threadIdx.x; idx < zc * kZParts; idx += blockDim.x) {
         const uint32_t r = idx % zc, q = idx / zc;
         const double* col = part + (size_t)(sh.nx + sh.ny) * sh.rp + r;
         /* in item order; 16 loads in flight before their adds */
         double a = 0.0;
         uint32_t p = q;
-        for (; p + 15 * kZParts < sh.nz; p += 16 * kZParts) {
+        for (; p + 15 * kZParts < zrows; p += 16 * kZParts) {
             double v[16];
 #pragma unroll
             for (uint32_t j = 0; j < 16; ++j) v[j] = col[(size_t)(p + j * kZParts) * sh.rp];
 #pragma unroll
             for (uint32_t j = 0; j < 16; ++j) a += v[j];
         }
-        for (; p < sh.nz; p += kZParts) a += col[(size_t)p * sh.rp];
+        for (; p < zrows; p += kZParts) a += col[(size_t)p * sh.rp];
         zpart[idx] = a;
     }
     __syncthreads();
@@ -503,6 +518,10 @@ uint32_t corr_z_items(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint3
     return corr_shape(lx, ly, lz, rxy, rz).nz;
 }
 
+uint32_t corr_z_units(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
+    return corr_zunits_of(corr_shape(lx, ly, lz, rxy, rz));
+}
+
 uint32_t corr_len(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t rz) {
     uint32_t n = 0;
     if (rxy) n = std::max(lx, ly);
@@ -522,7 +541,8 @@ bool corr_supports(uint32_t lx, uint32_t ly, uint32_t lz, uint32_t rxy, uint32_t
 }
 
 cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t n_tasks, uint32_t n_items,
-                        uint32_t max_len, uint32_t max_r, uint32_t max_nz, int sm_count, cudaStream_t s) {
+                        uint32_t n_zunits, uint32_t max_len, uint32_t max_r, uint32_t max_nz, int sm_count,
+                        cudaStream_t s) {
     /* a warp takes 8 lags per pass: blocks of one or two warps for small
      * radii, so that short lines do not hold idle warps */
     const int line_threads = max_r <= 16 ? 64 : (max_r <= 32 ? 128 : kCorrThreads);
@@ -541,15 +561,15 @@ cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t
         k_corr_lines<<<grid, line_threads, smem, s>>>(one ? nullptr : tasks_dev, by_value, n_tasks, n_items);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
-        if (max_nz > 0) {
+        if (n_zunits > 0) {
             /* z items of lines of 32..256 sites: the spectral route */
             const size_t zsmem = (size_t)kFftMax * kCorrPitch * sizeof(float2);
             e = cudaFuncSetAttribute(k_corr_zfft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem);
             if (e != cudaSuccess) return e;
-            /* blocks loop over the items, so each computes its twiddle tables
+            /* blocks loop over the units, so each computes its twiddle tables
              * once: three per SM (the kernel's occupancy) */
-            const uint32_t zgrid = sm_count > 0 ? std::min<uint32_t>(grid, 3u * (uint32_t)sm_count) : grid;
-            k_corr_zfft<<<zgrid, kCorrThreads, zsmem, s>>>(one ? nullptr : tasks_dev, by_value, n_tasks, n_items);
+            const uint32_t zgrid = sm_count > 0 ? std::min<uint32_t>(n_zunits, 3u * (uint32_t)sm_count) : n_zunits;
+            k_corr_zfft<<<zgrid, kCorrThreads, zsmem, s>>>(one ? nullptr : tasks_dev, by_value, n_tasks, n_zunits);
             e = cudaGetLastError();
             if (e != cudaSuccess) return e;
         }
