@@ -1086,11 +1086,18 @@ int slsf_task_reset_bins(slsf_task* t) {
 
 /* `v.sweeps` sweeps of one task through the grid-wide kernels, measuring
  * after every sweep past thermalization into the task's bin sums as the
- * persistent kernels do; counters accumulate into v.stats. */
+ * persistent kernels do: the state after a sweep is measured by the next
+ * sweep's colour-0 kernel, the launch's last state by the measurement
+ * kernel; counters accumulate into v.stats. */
 static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v, cudaStream_t st) {
+    double* pending = nullptr; /* bin row of the state after the previous sweep, not yet measured */
     for (uint32_t sw = 0; sw < v.sweeps; ++sw) {
         const uint64_t sweep = t->metro_sweeps + sw;
-        slsf::launch_metro_colour(v, sweep, 0, nullptr, st);
+        if (pending)
+            slsf::launch_metro_colour0_measure(v, sweep, t->partials, t->done, t->result, pending, st);
+        else
+            slsf::launch_metro_colour(v, sweep, 0, nullptr, st);
+        pending = nullptr;
         slsf::launch_metro_colour(v, sweep, 1, nullptr, st);
         ctx->launches += 2;
         for (uint32_t k = 0; k < t->wolff_steps; ++k) {
@@ -1100,11 +1107,7 @@ static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v, 
         const uint64_t done = sweep + 1;
         if (done > t->thermalization && t->n_bins) {
             const uint64_t b = (done - t->thermalization - 1) / t->binsize;
-            if (b < t->n_bins) {
-                slsf::launch_measure_into_bin(v, t->partials, t->done, t->result, t->bins + b * slsf::kBinCols,
-                                              st);
-                ctx->launches += 1;
-            }
+            if (b < t->n_bins) pending = t->bins + b * slsf::kBinCols;
         }
         /* ThetaModel::measure's correlations of the state after this sweep
          * (slsf_task_corr_fuse), as the one-CTA kernel takes them: measurement
@@ -1123,6 +1126,10 @@ static void run_grid_task(slsf_ctx* ctx, const slsf_task* t, const TaskView& v, 
             ctx->launches +=
                 corr_launch_count(items, slsf::corr_z_items(t->lx, t->ly, t->lz, t->corr_rxy, t->corr_rz));
         }
+    }
+    if (pending) {
+        slsf::launch_measure_into_bin(v, t->partials, t->done, t->result, pending, st);
+        ctx->launches += 1;
     }
 }
 

@@ -75,6 +75,10 @@ int report_error(int code, const std::string& message);
 void launch_init_random(float* theta, uint32_t volume, uint64_t seed, cudaStream_t s);
 void launch_metro_colour(const TaskView& t, uint64_t sweep, uint32_t colour, uint8_t* record,
                          cudaStream_t s);
+/* Colour 0 of a sweep fused with the measurement of the state it starts from
+ * (the observables' sums into `result`, added into `bin_row` if given). */
+void launch_metro_colour0_measure(const TaskView& t, uint64_t sweep, double* partials, unsigned int* done,
+                                  double* result, double* bin_row, cudaStream_t s);
 /* One Wolff update; returns the number of kernels launched.  bonds [V] and
  * parent [V] are the task's scratch; with record_bonds the per-site bond
  * bits (+x, +y, +z in bits 0-2) are left in `bonds`. */

@@ -60,6 +60,56 @@ __device__ __forceinline__ void block_count(uint32_t v, unsigned long long* stat
     if (threadIdx.x == 0 && s_sum) atomicAdd(&stats[slot], (unsigned long long)s_sum);
 }
 
+/* Sums of the measurement (mx, my, J cos and J sin per axis) and where they
+ * go: per-block partials, a block counter, the totals and an optional bin
+ * row -- the last block adds the partials in block order. */
+struct MeasureSink {
+    double* partials;
+    unsigned int* done;
+    double* result;
+    double* bin_row;
+};
+
+/* The last block's reduction of the per-block measurement partials into the
+ * totals and the bin row (ThetaModel::measure's stream, src/model.rs:406-409,
+ * in the batched kernels' column order). */
+__device__ __forceinline__ void finish_measure(double (&acc)[8], double* scratch, const MeasureSink& m,
+                                               uint32_t volume) {
+    __shared__ bool last;
+    block_sum<8>(acc, scratch);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 8; ++k) m.partials[blockIdx.x * 8 + k] = acc[k];
+        __threadfence();
+        last = (atomicAdd(m.done, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+        for (int k = 0; k < 8; ++k) tot[k] += ((volatile double*)m.partials)[b * 8 + k];
+    block_sum<8>(tot, scratch);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 8; ++k) m.result[k] = tot[k];
+        if (m.bin_row) {
+            const double v = (double)volume;
+            const double e = -(tot[2] + tot[3] + tot[4]) / v;
+            const double vals[kBinCols] = {e,      e * e,  (tot[0] * tot[0] + tot[1] * tot[1]) / (v * v),
+                                           tot[2], tot[3], tot[4],
+                                           tot[5], tot[6], tot[7],
+                                           tot[5] * tot[5], tot[6] * tot[6], tot[7] * tot[7]};
+            for (int q = 0; q < kBinCols; ++q) m.bin_row[q] += vals[q];
+        }
+        *m.done = 0;
+    }
+}
+
+/* Colour 0 of a sweep, grid-stride blocks, measuring the state it starts
+ * from as the batched kernels do: every
+ * bond has exactly one colour-0 end, so the three forward and three backward
+ * bonds of the colour-0 sites and the magnetisation of each colour-0 site and
+ * of its +x neighbour cover the lattice once; the FP32 bond terms are the
+ * measurement kernels' (bond_cos / bond_sin), summed in FP64. */
 template <bool kRecord>
 __global__ void __launch_bounds__(kThreads)
     k_metro_colour(float* __restrict__ theta, const float* __restrict__ jxy,
@@ -108,6 +158,69 @@ __global__ void __launch_bounds__(kThreads)
         }
     }
     block_count(accepted, stats, kStatAccepted);
+}
+
+__global__ void __launch_bounds__(kThreads, 3)
+    k_metro_colour0_measure(float* __restrict__ theta, const float* __restrict__ jxy,
+                   const float* __restrict__ jz, uint32_t lx, uint32_t ly, uint32_t lz, float beta,
+                   float width, uint64_t seed, uint64_t sweep, uint32_t colour, slsf_fastdiv div_hx,
+                   slsf_fastdiv div_ly, unsigned long long* __restrict__ stats, MeasureSink sink) {
+    const uint32_t volume = lx * ly * lz;
+    const uint32_t half = volume >> 1;
+    const uint32_t npairs = (half + 1) >> 1;
+    uint32_t accepted = 0;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    auto pair = [&](uint32_t p) {
+        const slsf_u32x4 blk = slsf_stream(seed, sweep, SLSF_PURPOSE_METRO, colour, p);
+#pragma unroll
+        for (uint32_t lane = 0; lane < 2; ++lane) {
+            const uint32_t h = 2 * p + lane;
+            if (h >= half) break;
+            /* the h-th site of this colour: row = h / (L_x / 2) (x + L_x row = site index),
+             * x = 2 (h mod L_x / 2) + (colour + y + z) mod 2; divisions as multiply-shifts */
+            SiteXYZ s;
+            const uint32_t row = slsf_fastdiv_div(h, div_hx), k = h - row * div_hx.d;
+            s.z = slsf_fastdiv_div(row, div_ly);
+            s.y = row - s.z * ly;
+            s.x = 2u * k + ((colour + s.y + s.z) & 1u);
+            s.idx = s.x + lx * row;
+            uint32_t nb[6];
+            neighbour_indices(s, lx, ly, lz, nb);
+            float ns[6], nc[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) __sincosf(theta[nb[k]], &ns[k], &nc[k]);
+            const float jx = jxy[s.z], jzp = jz[s.z], jzm = jz[s.z == 0 ? lz - 1 : s.z - 1];
+            const float hx = field_component(jx, jzp, jzm, nc[0], nc[1], nc[2], nc[3], nc[4], nc[5]);
+            const float hy = field_component(jx, jzp, jzm, ns[0], ns[1], ns[2], ns[3], ns[4], ns[5]);
+            const float th = theta[s.idx];
+            float si, ci;
+            __sincosf(th, &si, &ci);
+            {
+                /* neighbours in the order +x -x +y -y +z -z; a backward bond
+                 * starts at the neighbour (its layer's coupling for z) */
+                acc[0] += (double)ci + (double)nc[0];
+                acc[1] += (double)si + (double)ns[0];
+                acc[2] += (double)bond_cos(jx, ci, si, nc[0], ns[0]) + (double)bond_cos(jx, nc[1], ns[1], ci, si);
+                acc[3] += (double)bond_cos(jx, ci, si, nc[2], ns[2]) + (double)bond_cos(jx, nc[3], ns[3], ci, si);
+                acc[4] += (double)bond_cos(jzp, ci, si, nc[4], ns[4]) + (double)bond_cos(jzm, nc[5], ns[5], ci, si);
+                acc[5] += (double)bond_sin(jx, ci, si, nc[0], ns[0]) + (double)bond_sin(jx, nc[1], ns[1], ci, si);
+                acc[6] += (double)bond_sin(jx, ci, si, nc[2], ns[2]) + (double)bond_sin(jx, nc[3], ns[3], ci, si);
+                acc[7] += (double)bond_sin(jzp, ci, si, nc[4], ns[4]) + (double)bond_sin(jzm, nc[5], ns[5], ci, si);
+            }
+            float u_prop, u_acc;
+            slsf_metro_uniforms(blk, lane, &u_prop, &u_acc);
+            float tn, sn, cn;
+            const bool ok = metro_decide(th, ci, si, hx, hy, beta, width, u_prop, u_acc, &tn, &sn, &cn);
+            if (ok) {
+                theta[s.idx] = tn;
+                ++accepted;
+            }
+        }
+    };
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) pair(p);
+    block_count(accepted, stats, kStatAccepted);
+    __shared__ double scratch[8 * 32];
+    finish_measure(acc, scratch, sink, volume);
 }
 
 /* Smallest lattice whose Wolff update grows the seed's cluster on bit-packed
@@ -579,6 +692,28 @@ void launch_metro_colour(const TaskView& t, uint64_t sweep, uint32_t colour, uin
     else
         k_metro_colour<false><<<grid, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, t.beta, t.width,
                                                         t.seed, sweep, colour, dhx, dly, t.stats, nullptr);
+}
+
+void launch_metro_colour0_measure(const TaskView& t, uint64_t sweep, double* partials, unsigned int* done,
+                                  double* result, double* bin_row, cudaStream_t s) {
+    const uint32_t volume = t.lx * t.ly * t.lz;
+    const uint32_t npairs = ((volume >> 1) + 1) >> 1;
+    /* grid-stride blocks, as many as stay resident (at most kMeasureMaxBlocks,
+     * the partials' rows); a fixed count per device keeps the sums' order */
+    static int per_sm = 0;
+    if (per_sm == 0 &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_metro_colour0_measure, kThreads, 0) !=
+            cudaSuccess)
+        per_sm = 1;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t cap = (uint32_t)std::max(1, std::min(per_sm * sms, kMeasureMaxBlocks));
+    const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(blocks_for(npairs, kThreads), cap));
+    const slsf_fastdiv dhx = slsf_fastdiv_make(t.lx / 2), dly = slsf_fastdiv_make(t.ly);
+    const MeasureSink sink = {partials, done, result, bin_row};
+    k_metro_colour0_measure<<<grid, kThreads, 0, s>>>(t.theta, t.jxy, t.jz, t.lx, t.ly, t.lz, t.beta, t.width,
+                                                      t.seed, sweep, 0, dhx, dly, t.stats, sink);
 }
 
 int launch_wolff(const TaskView& t, uint64_t counter, uint8_t* bonds, uint32_t* parent,

@@ -139,7 +139,8 @@ def test_batched_grid_tasks_in_the_mix(slsf, ctx, orc):
                       o["sin_x"], o["sin_y"], o["sin_z"], o["sin_x"] ** 2, o["sin_y"] ** 2, o["sin_z"] ** 2]
                      for o in series])
     for b in range(n_bins):
-        # same measure kernel on both paths: equal up to the host's FP64 averaging order
+        # the same FP32 bond terms on both paths (the grid path measures most states inside the next
+        # sweep's colour-0 kernel): equal up to the FP64 summation and averaging order
         assert np.allclose(bins[b], rows[b * binsize:(b + 1) * binsize].mean(axis=0), rtol=1e-12, atol=1e-12)
     for spec, t in zip(specs[1:], mix[1:]):
         [alone] = batched_tasks(slsf, ctx, orc, [spec])
