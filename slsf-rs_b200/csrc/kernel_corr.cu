@@ -163,6 +163,28 @@ __device__ __forceinline__ void stage_rows(float2* __restrict__ tile, uint32_t p
     }
 }
 
+/* Stages n rows of `cols` consecutive angles (row k at base + k * stride)
+ * into raw[k * kCorrPitch + c] as they are, zero past `cols`; eight loads
+ * per thread in flight. */
+__device__ __forceinline__ void stage_raw(float* __restrict__ raw, const float* __restrict__ theta, uint32_t base,
+                                          uint32_t stride, uint32_t n, uint32_t cols) {
+    constexpr uint32_t kU = 8;
+    const uint32_t total = n * kCorrCols;
+    for (uint32_t e0 = threadIdx.x; e0 < total; e0 += kU * blockDim.x) {
+        float v[kU];
+#pragma unroll
+        for (uint32_t u = 0; u < kU; ++u) {
+            const uint32_t e = e0 + u * blockDim.x, k = e / kCorrCols, c = e % kCorrCols;
+            v[u] = (e < total && c < cols) ? theta[base + k * stride + c] : 0.0f;
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < kU; ++u) {
+            const uint32_t e = e0 + u * blockDim.x, k = e / kCorrCols, c = e % kCorrCols;
+            if (e < total) raw[k * kCorrPitch + c] = v[u];
+        }
+    }
+}
+
 /* The spectral route for unit g of task T: for each of its z items (32
  * lines of one row y), the tile [n][kCorrPitch] receives the lines' (cos,
  * sin) and each warp transforms its lines, adding their power spectra into
@@ -171,25 +193,30 @@ __device__ __forceinline__ void stage_rows(float2* __restrict__ tile, uint32_t p
  * FP32: their rounding moves C_z by about 1e-8 on ordered-phase lines,
  * against the 2e-6 agreement held with the FP64 oracle. */
 template <uint32_t N1>
-__device__ void corr_z_unit(const CorrTask& Tk, const CorrShape& sh, uint32_t g, float2* tile, const FftTables& T,
-                            double* P, double* __restrict__ out) {
+__device__ void corr_z_unit(const CorrTask& Tk, const CorrShape& sh, uint32_t g, float* raw, double* rows,
+                            const FftTables& T, double* __restrict__ out) {
     constexpr uint32_t n = 32 * N1;
     constexpr uint32_t bits = N1 == 1 ? 0 : (N1 == 2 ? 1 : (N1 == 4 ? 2 : 3));
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const uint32_t plane = Tk.lx * Tk.ly, q1 = min(sh.nz, (g + 1) * kZGroup);
-    double pw[N1];
+    /* the warp's power sums, slot j of lane t at rows[warp][j][t] */
+    double* pw = rows + warp * n;
 #pragma unroll
-    for (uint32_t m = 0; m < N1; ++m) pw[m] = 0.0;
+    for (uint32_t j = 0; j < N1; ++j) pw[j * 32 + lane] = 0.0;
     for (uint32_t item = g * kZGroup; item < q1; ++item) {
         const uint32_t y = item / sh.cy, x0 = (item % sh.cy) * kCorrCols;
         const uint32_t cols = min(kCorrCols, Tk.lx - x0);
-        __syncthreads(); /* the previous item's tile is no longer read */
-        stage_rows(tile, kCorrPitch, Tk.theta, y * Tk.lx + x0, plane, n, cols);
+        __syncthreads(); /* the previous item's angles are no longer read */
+        stage_raw(raw, Tk.theta, y * Tk.lx + x0, plane, n, cols);
         __syncthreads();
         for (uint32_t c = warp; c < cols; c += nwarps) {
             float2 X[N1];
 #pragma unroll
-            for (uint32_t j = 0; j < N1; ++j) X[j] = tile[(lane + 32 * j) * kCorrPitch + c];
+            for (uint32_t j = 0; j < N1; ++j) {
+                float sn, cn;
+                __sincosf(raw[(lane + 32 * j) * kCorrPitch + c], &sn, &cn);
+                X[j] = make_float2(cn, sn);
+            }
             /* radix-2 decimation in frequency over j in registers (N1-point DFT
              * of the elements lane + 32 j); slot j ends with frequency bitrev(j) */
 #pragma unroll
@@ -224,22 +251,19 @@ __device__ void corr_z_unit(const CorrTask& Tk, const CorrShape& sh, uint32_t g,
 #pragma unroll
             for (uint32_t j = 0; j < N1; ++j) {
                 const double re = (double)X[j].x, im = (double)X[j].y;
-                pw[j] += re * re + im * im;
+                pw[j * 32 + lane] += re * re + im * im;
             }
         }
     }
-    /* the unit's spectrum: each warp's sums go to its own row of the tile
-     * (read by no warp any more), then the rows are added in warp order;
-     * slot j of lane t is frequency bitrev(j) + N1 bitrev5(t) */
-    const uint32_t s = __brev(lane) >> 27;
-    double* rows = reinterpret_cast<double*>(tile); /* [nwarps][n] */
-    __syncthreads();
-#pragma unroll
-    for (uint32_t j = 0; j < N1; ++j) rows[warp * n + bitrev_bits(j, bits) + N1 * s] = pw[j];
+    /* the unit's spectrum: the warps' sums added in warp order; slot j of
+     * lane t is frequency bitrev(j) + N1 bitrev5(t); P takes the angle
+     * area, read by no warp any more */
+    double* P = reinterpret_cast<double*>(raw);
     __syncthreads();
     for (uint32_t q = threadIdx.x; q < n; q += blockDim.x) {
+        const uint32_t j = bitrev_bits(q & (N1 - 1), bits), t = __brev(q / N1) >> 27;
         double a = 0.0;
-        for (uint32_t w = 0; w < nwarps; ++w) a += rows[w * n + q];
+        for (uint32_t w = 0; w < nwarps; ++w) a += rows[w * n + j * 32 + t];
         P[q] = a;
     }
     __syncthreads();
@@ -266,9 +290,10 @@ __device__ __forceinline__ const CorrTask& unit_task(const CorrTask* __restrict_
 /* The spectral route: blocks loop over the units of all tasks. */
 __global__ void __launch_bounds__(kCorrThreads, 3)
     k_corr_zfft(const CorrTask* __restrict__ tasks, CorrTask one, uint32_t n_tasks, uint32_t n_units) {
-    extern __shared__ float2 tile[]; /* [n][kCorrPitch] */
+    extern __shared__ double zsm[]; /* power sums [warps][n], then angles [n][kCorrPitch] */
     __shared__ FftTables tabs;
-    __shared__ double spec[kFftMax];
+    double* rows = zsm;
+    float* raw = reinterpret_cast<float*>(zsm + (kCorrThreads / 32) * kFftMax);
     uint32_t tab_n = 0; /* the line length the tables hold */
     for (uint32_t unit = blockIdx.x; unit < n_units; unit += gridDim.x) {
         const CorrTask& T = unit_task(tasks, one, n_tasks, unit);
@@ -282,10 +307,10 @@ __global__ void __launch_bounds__(kCorrThreads, 3)
         }
         double* out = T.partial + (size_t)(sh.nx + sh.ny + g) * sh.rp;
         switch (n) {
-            case 32: corr_z_unit<1>(T, sh, g, tile, tabs, spec, out); break;
-            case 64: corr_z_unit<2>(T, sh, g, tile, tabs, spec, out); break;
-            case 128: corr_z_unit<4>(T, sh, g, tile, tabs, spec, out); break;
-            default: corr_z_unit<8>(T, sh, g, tile, tabs, spec, out); break;
+            case 32: corr_z_unit<1>(T, sh, g, raw, rows, tabs, out); break;
+            case 64: corr_z_unit<2>(T, sh, g, raw, rows, tabs, out); break;
+            case 128: corr_z_unit<4>(T, sh, g, raw, rows, tabs, out); break;
+            default: corr_z_unit<8>(T, sh, g, raw, rows, tabs, out); break;
         }
     }
 }
@@ -563,11 +588,12 @@ cudaError_t launch_corr(const CorrTask* tasks_dev, const CorrTask* one, uint32_t
         if (e != cudaSuccess) return e;
         if (n_zunits > 0) {
             /* z items of lines of 32..256 sites: the spectral route */
-            const size_t zsmem = (size_t)kFftMax * kCorrPitch * sizeof(float2);
+            const size_t zsmem = (size_t)(kCorrThreads / 32) * kFftMax * sizeof(double) +
+                                 (size_t)kFftMax * kCorrPitch * sizeof(float);
             e = cudaFuncSetAttribute(k_corr_zfft, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem);
             if (e != cudaSuccess) return e;
             /* blocks loop over the units, so each computes its twiddle tables
-             * once: three per SM (the kernel's occupancy) */
+             * once: four per SM (the kernel's occupancy) */
             const uint32_t zgrid = sm_count > 0 ? std::min<uint32_t>(n_zunits, 3u * (uint32_t)sm_count) : n_zunits;
             k_corr_zfft<<<zgrid, kCorrThreads, zsmem, s>>>(one ? nullptr : tasks_dev, by_value, n_tasks, n_zunits);
             e = cudaGetLastError();
