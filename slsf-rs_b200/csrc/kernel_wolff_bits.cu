@@ -289,21 +289,26 @@ __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, u
     want = __reduce_or_sync(0xffffffffu, want);
     if (lane == 0 && want) atomicOr(s_want, want);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const uint32_t m = *s_want;
-        *s_want = 0;
-        if (m) {
-            /* the block's cluster words are written (barrier above); one fence
-             * orders them before the neighbours can be taken */
-            __threadfence();
-            if (m & 1u) push_region(wb, region_of(g, k == 0 ? g.words - 1 : k - 1, ry, rz), keep);
-            if (m & 2u) push_region(wb, region_of(g, k + 1 == g.words ? 0 : k + 1, ry, rz), keep);
-            if (m & 4u) push_region(wb, region_of(g, k, ry == 0 ? g.ry_n - 1 : ry - 1, rz), keep);
-            if (m & 8u) push_region(wb, region_of(g, k, ry + 1 == g.ry_n ? 0 : ry + 1, rz), keep);
-            if (m & 16u) push_region(wb, region_of(g, k, ry, rz == 0 ? g.rz_n - 1 : rz - 1), keep);
-            if (m & 32u) push_region(wb, region_of(g, k, ry, rz + 1 == g.rz_n ? 0 : rz + 1), keep);
+    /* thread d queues the neighbour in direction d, so that the six queue
+     * operations (each a few dependent atomics) overlap; the block's cluster
+     * words are written (barrier above) and each pushing thread's fence
+     * orders them before its neighbour can be taken */
+    const uint32_t m = *s_want;
+    if (threadIdx.x < 6 && ((m >> threadIdx.x) & 1u)) {
+        uint32_t nb;
+        switch (threadIdx.x) {
+            case 0: nb = region_of(g, k == 0 ? g.words - 1 : k - 1, ry, rz); break;
+            case 1: nb = region_of(g, k + 1 == g.words ? 0 : k + 1, ry, rz); break;
+            case 2: nb = region_of(g, k, ry == 0 ? g.ry_n - 1 : ry - 1, rz); break;
+            case 3: nb = region_of(g, k, ry + 1 == g.ry_n ? 0 : ry + 1, rz); break;
+            case 4: nb = region_of(g, k, ry, rz == 0 ? g.rz_n - 1 : rz - 1); break;
+            default: nb = region_of(g, k, ry, rz + 1 == g.rz_n ? 0 : rz + 1); break;
         }
+        __threadfence();
+        push_region(wb, nb, keep);
     }
+    __syncthreads(); /* every thread has read the mask before it is cleared */
+    if (threadIdx.x == 0) *s_want = 0;
     return ok;
 }
 
