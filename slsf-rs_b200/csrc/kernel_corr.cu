@@ -32,15 +32,17 @@
  * the circular correlation of a line is the inverse transform of its power
  * spectrum, sum_k s_k . s_{k+r} = Re (1/n) sum_q |A(q)|^2 e^{2 pi i q r / n}
  * with A the discrete Fourier transform of cos + i sin along the line.  A
- * warp transforms one line at a time in FP64 (lane t holds elements t + 32 j:
+ * block takes a unit of four consecutive z items of a task (128 lines); a
+ * warp transforms one line at a time in FP32 (lane t holds elements t + 32 j:
  * a radix-(n/32) DFT in registers, twiddles, then a 32-point decimation-in-
- * frequency FFT across the lanes), the item sums |A|^2 over its lines in a
- * fixed order, and one thread per lag forms the item's per-lag sum from the
- * spectrum.  O(n log n) per line instead of O(n R); the FP32 products of the
- * direct form become FP64 transforms of the same FP32 trig values.
+ * frequency FFT across the lanes) from the raw angles staged in shared
+ * memory, adds |A|^2 into its FP64 sums in shared memory, and the unit's
+ * spectrum (the warps' sums in warp order) is stored folded.  O(n log n) per
+ * line instead of O(n R).
  *
  * k_corr_finalize: one block per task sums the item partials in a fixed
- * order (per layer for x and y, over everything for z), forms the values in
+ * order (per layer for x and y, over everything for z; on the spectral route
+ * the units' spectra, inverted once with tabulated cosines), forms the values in
  * ThetaModel::measure's order (src/model.rs:420-437) -- C_x, C_y, C_xy,
  * C_xy(z, r) z-major, C_z -- and writes them out and/or adds them into row
  * count / binsize of the task's correlation bin sums.  Everything is

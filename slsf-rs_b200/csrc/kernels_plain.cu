@@ -5,6 +5,8 @@
  *   k_metro_colour       one colour of metropolis_sweep_with_scratch
  *                        (src/updates.rs:440-486), one thread per Philox block
  *                        (two same-colour sites)
+ *   k_metro_colour0_measure  colour 0 fused with the measurement of the state
+ *                        it starts from (the batched grid path)
  *   k_wolff_tiles        per-site +x/+y/+z bond activation of
  *   k_wolff_boundary     wolff_cluster_step_with_theta_scratch
  *   k_wolff_compress     (src/updates.rs:551-620): components inside
