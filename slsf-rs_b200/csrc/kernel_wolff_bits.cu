@@ -209,8 +209,17 @@ __device__ bool grow_region(const WolffBits& wb, const GrowGeo& g, uint32_t r, u
     long long tclk = clock64();
 #endif
     const uint32_t w = word(k, gy, gz);
+    /* the region's own words (written only by processings of this region) */
     const uint32_t c0 = __ldcg(&wb.cl[w]);
     const uint32_t bxw = wb.bx[w], byw = wb.by[w], bzw = wb.bz[w];
+    /* claimable again from here on: the reset is visible before the
+     * neighbours' words are read, so a neighbour that adds face bits later
+     * finds the region unqueued and queues it */
+    if (threadIdx.x == 0) {
+        wb.queued[r] = 0u;
+        __threadfence();
+    }
+    __syncthreads();
     uint32_t c = c0;
     /* bits entering through the faces */
     const uint32_t kl = k == 0 ? g.words - 1 : k - 1, kr = k + 1 == g.words ? 0 : k + 1;
@@ -363,8 +372,6 @@ __global__ void __launch_bounds__(kGrowThreads, 1)
                 }
             }
             s_keep = kNoRegion;
-            if (got < wb.regions) wb.queued[got] = 0u; /* claimable again from here on */
-            __threadfence();
             s_item = got;
         }
         __syncthreads();
